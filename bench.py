@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""Benchmark: KIFMM3d evaluate() throughput on one B200 (and N replicas).
+
+Workload (the configuration the metric is quoted on): Laplace single layer,
+N = 1,048,576 points (50% on a sphere of radius 0.49 about the box centre,
+50% in 8 Gaussian clusters, sigma 0.02), sources = targets, densities N(0,1),
+np = 6, ptsMax = 64, seeded synthetic data.  One step = one evaluate() of one
+right-hand side with the tree, lists and operators resident (the reference's
+-do_2nd_eval semantics).  value = targets / s of the device-timed step;
+e2e = the same metric through fmmg_evaluate() with pinned host buffers, the
+H2D copy of the densities and the D2H copy of the values inside the timing.
+
+--gpus N (under torchrun): every rank holds a replica of the tree and
+evaluates its own right-hand side (multi-RHS sharding, weak scaling, no
+collective on the data path); the step time is the max over ranks.
+
+--impl reference: the CPU restatement of the reference evaluate() (oracle/),
+timed on the host cores with all threads, on a bounded sample of the same
+workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(ROOT, "fmm-g_b200"), os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = json.load(open(os.path.join(ROOT, "BASELINE.json")))["metric"] if os.path.exists(
+    os.path.join(ROOT, "BASELINE.json")) else "Laplace 1M-pt points/s"
+UNIT = "points/s"
+WORKLOAD = "laplace_s_1M_sphere_clusters_np6_ptsmax64"
+CPU_SAMPLE = 1 << 17      # single-thread oracle sample (about 10-30 s on one core)
+REF_SAMPLE = 1 << 18      # all-threads oracle sample per reference-arm step
+CHECK_TARGETS = 4096
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=1 << 20)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def oracle_rate(n, nthreads, reps=1):
+    """Oracle (CPU restatement of the reference evaluate) points/s on an n-point sample."""
+    import oracle as O
+    import workloads as W
+    rng = np.random.default_rng(W.SEED + 2)
+    src = W.sphere_clusters(n, rng)
+    den = rng.normal(size=n)
+    o = O.Oracle(111, np_=6, pts_max=64, nthreads=nthreads)
+    o.setup(src, src, src)
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        o.evaluate(den)
+        times.append(time.perf_counter() - t0)
+    return n / float(np.median(times)), times
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    nthreads = os.cpu_count() or 1
+    import oracle as O
+    import workloads as W
+    rng = np.random.default_rng(W.SEED + 2)
+    n = min(args.n, REF_SAMPLE)
+    src = W.sphere_clusters(n, rng)
+    den = rng.normal(size=n)
+    o = O.Oracle(111, np_=6, pts_max=64, nthreads=nthreads)
+    o.setup(src, src, src)
+    for _ in range(args.warmup):
+        o.evaluate(den)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.evaluate(den)
+    dt = (time.perf_counter() - t0) / max(args.steps, 1)
+    v = n / dt
+    sample = "%d-point sample of the workload's distribution per step, tree and operators prebuilt" % n
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "points": args.n, "sample_points": n, "kernel": "laplace_s_u", "np": 6,
+                   "pts_max": 64, "k_rhs": 1},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def measure_fp64_peak(torch):
+    """cuBLAS DGEMM 8192^3 best of 3 (TFLOP/s): the FP64 roof for CUDA-core kernels."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    best = 1e30
+    for _ in range(3):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+
+
+def run_ours(args):
+    import torch
+    import fmmg
+    import workloads as W
+    ws, rank, local = dist_env()
+    dist = ws > 1
+    if dist:
+        import datetime
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    stream = torch.cuda.Stream()  # one stream for the flush, the events and every library kernel
+    torch.cuda.set_stream(stream)
+    cfg = W.config2(args.n)
+    src = cfg["src"]
+    rng = np.random.default_rng(W.SEED + 2 + 1000 * rank)
+    den_h = cfg["den"] if rank == 0 else rng.normal(size=args.n)
+    prec = fmmg.PREC_FP64 if args.precision == "fp64" else fmmg.PREC_MIXED
+    t0 = time.perf_counter()
+    f = fmmg.FMM3d(111, np_=6, pts_max=64, device=dev, stream=stream.cuda_stream)
+    f.setup(src)
+    setup_s = time.perf_counter() - t0
+    info = f.info()
+    n = args.n
+    den = torch.from_numpy(den_h).to("cuda")
+    out = torch.zeros(n, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+    f.set_timing(True)
+    for _ in range(max(args.warmup, 3)):
+        f.evaluate_device(den, out, 1, prec)
+    torch.cuda.synchronize()
+    if dist:
+        tdist.barrier()
+    clocks = ClockSampler(dev if not os.environ.get("CUDA_VISIBLE_DEVICES") else
+                          os.environ["CUDA_VISIBLE_DEVICES"].split(",")[dev])
+    clocks.start()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    kern = {}
+    launches = 0
+    for i in range(args.steps):
+        flush.zero_()
+        ev[i][0].record(stream)
+        f.evaluate_device(den, out, 1, prec)
+        ev[i][1].record(stream)
+        for k, v in f.kernel_times().items():
+            kern[k] = kern.get(k, 0.0) + v
+        launches += f.launch_count()
+    torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    ms = float(np.mean(step_ms))
+    clk = clocks.stop()
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        ms = float(t.item())
+    kern = {k: v / args.steps for k, v in kern.items()}
+    stages = f.stage_times()
+    # error of this step against the FP64 dense sum at sampled targets (check())
+    vals = out.cpu().numpy()
+    idx = np.random.default_rng(W.SEED + 99).choice(n, CHECK_TARGETS, replace=False)
+    rel, mx, _ = f.check(den_h, vals, idx)
+    # end to end through fmmg_evaluate: pinned host in, pinned host out
+    hin = torch.from_numpy(den_h).pin_memory()
+    hout = torch.zeros(n, dtype=torch.float64).pin_memory()
+    f.evaluate_host_ptr(hin.data_ptr(), hout.data_ptr())
+    e2e_ms = []
+    for _ in range(args.steps):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.zero_()
+        s.record(stream)
+        f.evaluate_host_ptr(hin.data_ptr(), hout.data_ptr())
+        e.record(stream)
+        e.synchronize()
+        e2e_ms.append(s.elapsed_time(e))
+    e2e = float(np.mean(e2e_ms))
+    if dist:
+        t = torch.tensor([e2e], device="cuda")
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        e2e = float(t.item())
+        tdist.barrier()
+    if rank == 0:
+        roof = roofline(f, info, kern, torch)
+        cpu = None
+        if not args.no_cpu_baseline and not dist:
+            rate, times = oracle_rate(CPU_SAMPLE, 1)
+            cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
+                   "sample": "%d-point sample of the workload distribution, 1 thread (one MPI rank), "
+                             "tree/operators prebuilt, %.1f s" % (CPU_SAMPLE, times[0])}
+        total_pts = n * ws
+        line = {
+            "metric": METRIC, "value": total_pts / (ms * 1e-3), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if prec == fmmg.PREC_FP64 else "f32+f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "points": n, "kernel": "laplace_s_u", "np": 6, "pts_max": 64,
+                       "k_rhs_per_gpu": 1, "precision": args.precision, "parallelism": "rhs-replicas x%d" % ws,
+                       "l2": "256 MB written between steps; per-step working set > L2",
+                       "nodes": info["nodes"], "leaves": info["leaves"], "max_depth": info["max_depth"]},
+            "e2e": {"value": total_pts / (e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 8 * n,
+                    "d2h_bytes_per_step": 8 * n},
+            "gpu_launches": launches,
+            "rel_err_vs_dense": rel, "max_abs_err_vs_dense": mx, "check_targets": CHECK_TARGETS,
+            "stage_ms": stages, "kernel_ms": kern, "setup_s": setup_s,
+            "roofline": roof, "clocks": clk,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line))
+    f.close()
+    if dist:
+        tdist.destroy_process_group()
+
+
+def roofline(f, info, kern, torch):
+    """Roofline of the dominant kernel class of the step."""
+    peaks = {}
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pp):
+        peaks = json.load(open(pp))
+    top = max((k for k in kern if k not in ("prep", "scatter")), key=lambda k: kern[k])
+    t = kern[top] * 1e-3
+    work = f.algorithmic_work()
+    w = work.get(top)
+    out = {"kernel": top, "avg_ms": kern[top]}
+    if w is None:
+        out.update({"bound": None, "achieved": None, "peak": None, "unit": None, "frac": None, "traffic": None})
+        return out
+    if w["bound"] == "hbm":
+        peak = peaks.get("hbm_gbs", 6650.0)
+        ach = w["bytes"] / t / 1e9
+        out.update({"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                    "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650",
+                    "algorithmic_bytes": w["bytes"]})
+    else:
+        peak = measure_fp64_peak(torch)
+        ach = w["flops"] / t / 1e12
+        out.update({"bound": "fp64", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+                    "peak_source": "measured in bench: cuBLAS DGEMM 8192^3 best of 3",
+                    "algorithmic_flops": w["flops"], "pairs": w.get("pairs")})
+    out["traffic"] = None
+    return out
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,482 @@
+// capi.cpp -- the C ABI of include/fmmg.h over the host plan and the device
+// engine.  Every entry point validates its arguments, catches host
+// exceptions and reports CUDA failures as status codes.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/fmmg.h"
+#include "engine.hpp"
+#include "kernels.hpp"
+#include "plan.hpp"
+
+struct fmmg_handle {
+  fmmg::Options opt;
+  int device = 0;
+  bool hostOnly = false;
+  bool setupDone = false;
+  bool opsDirty = false;
+  bool timing = false;
+  int64_t launches = 0;
+  fmmg::Plan plan;
+  fmmg::DevState dev;
+  double* dDenIO = nullptr;
+  double* dValIO = nullptr;
+  std::vector<double> trgHost;  // caller-order targets for check()
+  std::string err;
+};
+
+static thread_local std::string g_create_err;
+
+static fmmg_status fail(fmmg_handle* h, fmmg_status s, const std::string& msg) {
+  if (h) h->err = msg;
+  else g_create_err = msg;
+  return s;
+}
+
+#define FMMG_GUARD(h)                                                    \
+  catch (const std::bad_alloc&) { return fail(h, FMMG_OOM, "host allocation failed"); } \
+  catch (const std::exception& ex) { return fail(h, FMMG_INVALID_ARG, ex.what()); }
+
+extern "C" {
+
+fmmg_status fmmg_default_options(fmmg_options* opt) {
+  if (!opt) return FMMG_INVALID_ARG;
+  std::memset(opt, 0, sizeof(*opt));
+  opt->kernel_type = FMMG_KNL_LAP_S_U;
+  opt->coefs[0] = 1.0;
+  opt->coefs[1] = 0.25;
+  opt->np = 6;
+  opt->pts_max = 150;
+  opt->max_level = 30;
+  opt->ctr[0] = opt->ctr[1] = opt->ctr[2] = 0.5;
+  opt->root_level = 1;
+  opt->device = 0;
+  opt->stream = nullptr;
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_create(const fmmg_options* o, fmmg_handle** out) {
+  if (!out) return fail(nullptr, FMMG_INVALID_ARG, "out is NULL");
+  *out = nullptr;
+  if (!o) return fail(nullptr, FMMG_INVALID_ARG, "options is NULL");
+  if (fmmg::kernel_mm(o->kernel_type) < 0)
+    return fail(nullptr, FMMG_NOT_SUPPORTED, "kernel type not supported by setup() (fmm3d_setup_mpi.cpp:113-126)");
+  if (o->np < 3 || o->np > 8) return fail(nullptr, FMMG_NOT_SUPPORTED, "np must be in [3, 8]");
+  if (o->pts_max < 1) return fail(nullptr, FMMG_INVALID_ARG, "pts_max must be >= 1");
+  if (o->max_level < 1 || o->max_level > 30) return fail(nullptr, FMMG_INVALID_ARG, "max_level must be in [1, 30]");
+  if (o->root_level < 0 || o->root_level > 30) return fail(nullptr, FMMG_INVALID_ARG, "root_level must be in [0, 30]");
+  for (int d = 0; d < 3; d++)
+    if (!std::isfinite(o->ctr[d])) return fail(nullptr, FMMG_INVALID_ARG, "ctr is not finite");
+  if (!std::isfinite(o->coefs[0]) || !std::isfinite(o->coefs[1]) || o->coefs[0] == 0.0)
+    return fail(nullptr, FMMG_INVALID_ARG, "coefs must be finite with mu != 0");
+  if ((o->kernel_type == FMMG_KNL_NAV_S_U || o->kernel_type == FMMG_KNL_NAV_D_U) && o->coefs[1] == 1.0)
+    return fail(nullptr, FMMG_INVALID_ARG, "Navier kernels need nu != 1");
+  fmmg_handle* h = nullptr;
+  try {
+    h = new fmmg_handle();
+    h->opt.kt = o->kernel_type;
+    h->opt.coefs[0] = o->coefs[0];
+    h->opt.coefs[1] = o->coefs[1];
+    h->opt.np = o->np;
+    h->opt.ptsMax = o->pts_max;
+    h->opt.maxLevel = o->max_level;
+    for (int d = 0; d < 3; d++) h->opt.ctr[d] = o->ctr[d];
+    h->opt.rootLevel = o->root_level;
+    h->device = o->device;
+    h->hostOnly = o->device < 0;
+    h->plan.o = h->opt;
+    std::string e = h->plan.build_operators();
+    if (!e.empty()) {
+      delete h;
+      return fail(nullptr, FMMG_NOT_SUPPORTED, e);
+    }
+    if (!h->hostOnly) {
+      int ndev = 0;
+      cudaError_t ce = cudaGetDeviceCount(&ndev);
+      if (ce != cudaSuccess || o->device >= ndev) {
+        std::string m = std::string("no such CUDA device: ") + (ce != cudaSuccess ? cudaGetErrorString(ce) : "index");
+        delete h;
+        return fail(nullptr, FMMG_CUDA_ERROR, m);
+      }
+      h->dev.device = o->device;
+      ce = cudaSetDevice(o->device);
+      if (ce == cudaSuccess) {
+        if (o->stream) {
+          h->dev.stream = (cudaStream_t)o->stream;
+        } else {
+          ce = cudaStreamCreateWithFlags(&h->dev.stream, cudaStreamNonBlocking);
+          h->dev.ownStream = true;
+        }
+      }
+      if (ce != cudaSuccess) {
+        std::string m = cudaGetErrorString(ce);
+        delete h;
+        return fail(nullptr, FMMG_CUDA_ERROR, m);
+      }
+    }
+  } catch (const std::bad_alloc&) {
+    delete h;
+    return fail(nullptr, FMMG_OOM, "host allocation failed");
+  }
+  *out = h;
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_setup(fmmg_handle* h, int64_t ns, const double* src, const double* nrm, int64_t nt,
+                       const double* trg) {
+  if (!h) return fail(nullptr, FMMG_INVALID_ARG, "handle is NULL");
+  if (ns < 1 || !src) return fail(h, FMMG_INVALID_ARG, "need n_src >= 1 and src_xyz");
+  if (nt < 0 || (nt > 0 && !trg)) return fail(h, FMMG_INVALID_ARG, "need n_trg >= 0 and trg_xyz");
+  if (ns > (int64_t)1 << 31 || nt > (int64_t)1 << 31) return fail(h, FMMG_INVALID_ARG, "too many points");
+  if (fmmg::kernel_has_normal(h->opt.kt) && !nrm)
+    return fail(h, FMMG_INVALID_ARG, "double-layer kernel needs src_nrm");
+  const double R = std::pow(2.0, -h->opt.rootLevel);
+  auto inside = [&](const double* p, int64_t n) {
+    for (int64_t i = 0; i < n; i++)
+      for (int d = 0; d < 3; d++) {
+        double v = p[3 * i + d];
+        if (!std::isfinite(v) || v < h->opt.ctr[d] - R || v > h->opt.ctr[d] + R) return false;
+      }
+    return true;
+  };
+  if (!inside(src, ns)) return fail(h, FMMG_INVALID_ARG, "a source lies outside the root box or is not finite");
+  if (nt > 0 && !inside(trg, nt)) return fail(h, FMMG_INVALID_ARG, "a target lies outside the root box or is not finite");
+  if (nrm)
+    for (int64_t i = 0; i < 3 * ns; i++)
+      if (!std::isfinite(nrm[i])) return fail(h, FMMG_INVALID_ARG, "a normal is not finite");
+  try {
+    if (h->setupDone) {
+      fmmg::dev_free(h->dev);
+      h->dDenIO = h->dValIO = nullptr;
+      fmmg::Plan fresh;
+      fresh.o = h->opt;
+      std::string e = fresh.build_operators();
+      if (!e.empty()) return fail(h, FMMG_NOT_SUPPORTED, e);
+      h->plan = std::move(fresh);
+      h->setupDone = false;
+    }
+    std::string e = h->plan.build(h->opt, ns, src, nrm, nt, nt > 0 ? trg : src);
+    if (!e.empty()) return fail(h, FMMG_INVALID_ARG, e);
+    h->trgHost.assign(trg ? trg : src, (trg ? trg : src) + 3 * nt);
+    if (!h->hostOnly) {
+      e = fmmg::dev_upload(h->plan, h->dev, src, nrm, nt > 0 ? trg : src);
+      if (!e.empty()) {
+        fmmg::dev_free(h->dev);
+        return fail(h, e.find("cudaMalloc") != std::string::npos ? FMMG_OOM : FMMG_CUDA_ERROR, e);
+      }
+      void* p = nullptr;
+      if (cudaMalloc(&p, sizeof(double) * (size_t)ns * h->plan.sd) != cudaSuccess)
+        return fail(h, FMMG_OOM, "cudaMalloc density buffer");
+      h->dev.allocs.push_back(p);
+      h->dDenIO = (double*)p;
+      if (cudaMalloc(&p, sizeof(double) * (size_t)std::max<int64_t>(nt, 1) * h->plan.td) != cudaSuccess)
+        return fail(h, FMMG_OOM, "cudaMalloc value buffer");
+      h->dev.allocs.push_back(p);
+      h->dValIO = (double*)p;
+    }
+    h->opsDirty = false;
+    h->setupDone = true;
+  }
+  FMMG_GUARD(h)
+  return FMMG_OK;
+}
+
+static fmmg_status ready(fmmg_handle* h) {
+  if (!h) return fail(nullptr, FMMG_INVALID_ARG, "handle is NULL");
+  if (!h->setupDone) return fail(h, FMMG_STATE, "evaluate before setup");
+  if (h->hostOnly) return fail(h, FMMG_STATE, "handle was created host-only (device < 0)");
+  if (h->opsDirty) {
+    std::string e = fmmg::dev_upload_operators(h->plan, h->dev);
+    if (!e.empty()) return fail(h, FMMG_CUDA_ERROR, e);
+    h->opsDirty = false;
+  }
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_evaluate_stages(fmmg_handle* h, const double* dDen, double* dVal, int precision, int mask) {
+  fmmg_status s = ready(h);
+  if (s != FMMG_OK) return s;
+  if (!dDen || (!dVal && h->plan.nt > 0)) return fail(h, FMMG_INVALID_ARG, "NULL density or value pointer");
+  if (precision != FMMG_PREC_FP64 && precision != FMMG_PREC_MIXED)
+    return fail(h, FMMG_INVALID_ARG, "unknown precision");
+  if (precision == FMMG_PREC_MIXED) return fail(h, FMMG_NOT_SUPPORTED, "mixed precision is not built yet");
+  try {
+    std::string e = fmmg::dev_evaluate(h->plan, h->dev, dDen, dVal, precision, mask & 63, h->timing, nullptr);
+    if (!e.empty()) return fail(h, FMMG_CUDA_ERROR, e);
+    h->launches = h->dev.lastLaunches;
+  }
+  FMMG_GUARD(h)
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_evaluate_device(fmmg_handle* h, int k, const double* dDen, double* dVal, int precision) {
+  fmmg_status s = ready(h);
+  if (s != FMMG_OK) return s;
+  if (k < 1) return fail(h, FMMG_INVALID_ARG, "k must be >= 1");
+  if (!dDen || (!dVal && h->plan.nt > 0)) return fail(h, FMMG_INVALID_ARG, "NULL density or value pointer");
+  if (precision != FMMG_PREC_FP64 && precision != FMMG_PREC_MIXED)
+    return fail(h, FMMG_INVALID_ARG, "unknown precision");
+  if (precision == FMMG_PREC_MIXED) return fail(h, FMMG_NOT_SUPPORTED, "mixed precision is not built yet");
+  try {
+    const int64_t sdn = h->plan.ns * h->plan.sd, tdn = h->plan.nt * h->plan.td;
+    h->launches = 0;
+    for (int r = 0; r < k; r++) {
+      std::string e = fmmg::dev_evaluate(h->plan, h->dev, dDen + r * sdn, dVal + r * tdn, precision, 63,
+                                         h->timing, nullptr);
+      if (!e.empty()) return fail(h, FMMG_CUDA_ERROR, e);
+      h->launches += h->dev.lastLaunches;
+    }
+  }
+  FMMG_GUARD(h)
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_synchronize(fmmg_handle* h) {
+  if (!h) return fail(nullptr, FMMG_INVALID_ARG, "handle is NULL");
+  if (h->hostOnly || !h->dev.stream) return FMMG_OK;
+  cudaError_t ce = cudaStreamSynchronize(h->dev.stream);
+  if (ce != cudaSuccess) return fail(h, FMMG_CUDA_ERROR, cudaGetErrorString(ce));
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_evaluate(fmmg_handle* h, const double* den, double* val) {
+  fmmg_status s = ready(h);
+  if (s != FMMG_OK) return s;
+  if (!den || (!val && h->plan.nt > 0)) return fail(h, FMMG_INVALID_ARG, "NULL density or value pointer");
+  try {
+    cudaStream_t st = h->dev.stream;
+    const size_t bi = sizeof(double) * (size_t)h->plan.ns * h->plan.sd;
+    const size_t bo = sizeof(double) * (size_t)h->plan.nt * h->plan.td;
+    cudaError_t ce = cudaMemcpyAsync(h->dDenIO, den, bi, cudaMemcpyHostToDevice, st);
+    if (ce != cudaSuccess) return fail(h, FMMG_CUDA_ERROR, cudaGetErrorString(ce));
+    std::string e = fmmg::dev_evaluate(h->plan, h->dev, h->dDenIO, h->dValIO, FMMG_PREC_FP64, 63, true, nullptr);
+    if (!e.empty()) return fail(h, FMMG_CUDA_ERROR, e);
+    h->launches = h->dev.lastLaunches;
+    if (bo) {
+      ce = cudaMemcpyAsync(val, h->dValIO, bo, cudaMemcpyDeviceToHost, st);
+      if (ce != cudaSuccess) return fail(h, FMMG_CUDA_ERROR, cudaGetErrorString(ce));
+    }
+    ce = cudaStreamSynchronize(st);
+    if (ce != cudaSuccess) return fail(h, FMMG_CUDA_ERROR, cudaGetErrorString(ce));
+  }
+  FMMG_GUARD(h)
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_check(fmmg_handle* h, const double* den, const double* val, int64_t nchk, const int64_t* idx,
+                       double* rel, double* maxabs, double* denseOut) {
+  fmmg_status s = ready(h);
+  if (s != FMMG_OK) return s;
+  if (!den || !val || !idx || nchk < 1) return fail(h, FMMG_INVALID_ARG, "bad check arguments");
+  try {
+    const int td = h->plan.td;
+    std::vector<double> pos(3 * (size_t)nchk), dense((size_t)nchk * td);
+    for (int64_t i = 0; i < nchk; i++) {
+      if (idx[i] < 0 || idx[i] >= h->plan.nt) return fail(h, FMMG_INVALID_ARG, "check index out of range");
+      for (int d = 0; d < 3; d++) pos[3 * i + d] = h->trgHost[3 * idx[i] + d];
+    }
+    cudaError_t ce = cudaMemcpyAsync(h->dDenIO, den, sizeof(double) * h->plan.ns * h->plan.sd,
+                                     cudaMemcpyHostToDevice, h->dev.stream);
+    if (ce != cudaSuccess) return fail(h, FMMG_CUDA_ERROR, cudaGetErrorString(ce));
+    std::string e = fmmg::dev_dense(h->plan, h->dev, h->dDenIO, nchk, pos.data(), dense.data());
+    if (!e.empty()) return fail(h, FMMG_CUDA_ERROR, e);
+    double en = 0, dn = 0, mx = 0;
+    for (int64_t i = 0; i < nchk; i++)
+      for (int c = 0; c < td; c++) {
+        double a = val[idx[i] * td + c], b = dense[i * td + c];
+        en += (a - b) * (a - b);
+        dn += b * b;
+        mx = std::max(mx, std::fabs(a - b));
+      }
+    if (rel) *rel = dn > 0 ? std::sqrt(en / dn) : std::sqrt(en);
+    if (maxabs) *maxabs = mx;
+    if (denseOut) std::copy(dense.begin(), dense.end(), denseOut);
+  }
+  FMMG_GUARD(h)
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_info(const fmmg_handle* h, int* sd, int* td, int64_t* nn, int64_t* nl, int* md) {
+  if (!h) return FMMG_INVALID_ARG;
+  if (sd) *sd = fmmg::kernel_src_dof(h->opt.kt);
+  if (td) *td = fmmg::kernel_trg_dof(h->opt.kt);
+  if (nn) *nn = h->setupDone ? h->plan.nn : 0;
+  if (nl) {
+    int64_t c = 0;
+    if (h->setupDone)
+      for (int n = 0; n < h->plan.nn; n++) c += h->plan.chd[n] < 0;
+    *nl = c;
+  }
+  if (md) *md = h->setupDone ? h->plan.maxDepth : 0;
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_stage_times(const fmmg_handle* h, double* ms, int n) {
+  if (!h || !ms || n < 7) return FMMG_INVALID_ARG;
+  for (int i = 0; i < 7; i++) ms[i] = h->dev.stageMs[i];
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_kernel_times(const fmmg_handle* h, double* ms, int n) {
+  if (!h || !ms || n < fmmg::EV_COUNT - 1) return FMMG_INVALID_ARG;
+  for (int i = 0; i < fmmg::EV_COUNT - 1; i++) ms[i] = h->dev.kernMs[i];
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_plan_stats(const fmmg_handle* h, int64_t* st, int n) {
+  if (!h || !st || n < 16) return FMMG_INVALID_ARG;
+  if (!h->setupDone) return FMMG_STATE;
+  const fmmg::Plan& P = h->plan;
+  const int64_t ue = (int64_t)P.nUE * P.sdm, uc = (int64_t)P.nUC * P.tdm;
+  const int64_t de = (int64_t)P.nDE * P.sdm, dc = (int64_t)P.nDC * P.tdm;
+  int64_t nearPairs = 0, s2mPairs = 0, s2lPairs = 0, m2tPairs = 0, l2tPairs = 0, upFlops = 0, dnFlops = 0;
+  for (size_t r = 0; r < P.evtrLeaves.size(); r++) {
+    int g = P.evtrLeaves[r];
+    int64_t s = 0;
+    for (int64_t e = P.nearSrc.ptr[r]; e < P.nearSrc.ptr[r + 1]; e++) s += P.srcCnt[P.nearSrc.idx[e]];
+    nearPairs += P.trgCnt[g] * s;
+    m2tPairs += P.trgCnt[g] * (P.farUE.ptr[r + 1] - P.farUE.ptr[r]) * P.nUE;
+    if (P.depth[g] >= 2) l2tPairs += P.trgCnt[g] * P.nDE;
+  }
+  for (int g : P.s2mLeaves) s2mPairs += P.srcCnt[g] * P.nUC;
+  for (size_t r = 0; r < P.s2lNodes.size(); r++)
+    for (int64_t e = P.s2lSrc.ptr[r]; e < P.s2lSrc.ptr[r + 1]; e++) s2lPairs += P.srcCnt[P.s2lSrc.idx[e]] * P.nDC;
+  for (int d = 0; d <= P.maxDepth; d++) {
+    upFlops += (int64_t)P.upM2M[d].size() * 2 * uc * 8 * ue + (int64_t)P.upC2E[d].size() * 2 * ue * uc;
+    if (d >= 3) dnFlops += (int64_t)P.dnL2L[d - 1].size() * 2 * 8 * dc * de;
+    dnFlops += (int64_t)P.dnC2E[d].size() * 2 * de * dc;
+  }
+  int64_t v[16] = {nearPairs, s2mPairs, s2lPairs, m2tPairs, l2tPairs,
+                   (int64_t)P.vSrcNodes.size(), (int64_t)P.vTrgNodes.size(), (int64_t)P.vParents.size(),
+                   (int64_t)P.vNbr.idx.size(), (int64_t)P.V.idx.size(), upFlops, dnFlops,
+                   (int64_t)P.nEff, (int64_t)P.sdm, (int64_t)P.tdm, (int64_t)P.nn};
+  std::copy(v, v + 16, st);
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_launch_count(const fmmg_handle* h, int64_t* n) {
+  if (!h || !n) return FMMG_INVALID_ARG;
+  *n = h->launches;
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_set_timing(fmmg_handle* h, int on) {
+  if (!h) return FMMG_INVALID_ARG;
+  h->timing = on != 0;
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_tree(const fmmg_handle* h, int32_t* rec, int64_t* ps, int64_t* pt) {
+  if (!h) return FMMG_INVALID_ARG;
+  if (!h->setupDone) return FMMG_STATE;
+  const fmmg::Plan& P = h->plan;
+  if (rec)
+    for (int n = 0; n < P.nn; n++) {
+      int32_t* r = rec + 9 * (size_t)n;
+      r[0] = P.depth[n];
+      r[1] = P.path[3 * (size_t)n];
+      r[2] = P.path[3 * (size_t)n + 1];
+      r[3] = P.path[3 * (size_t)n + 2];
+      r[4] = P.par[n];
+      r[5] = P.chd[n];
+      uint8_t f = P.flags[n];
+      r[6] = ((f & fmmg::NF_CBTR) ? 1 : 0) | ((f & fmmg::NF_USER) ? 2 : 0) | ((f & fmmg::NF_EVTR) ? 4 : 0) |
+             ((f & fmmg::NF_SRCE) ? 24 : 0);
+      r[7] = (int32_t)P.srcCnt[n];
+      r[8] = (int32_t)P.trgCnt[n];
+    }
+  if (ps) std::copy(P.srcPerm.begin(), P.srcPerm.end(), ps);
+  if (pt) std::copy(P.trgPerm.begin(), P.trgPerm.end(), pt);
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_lists(const fmmg_handle* h, int which, int64_t* ptr, int32_t* idx, int64_t* total) {
+  if (!h || which < 0 || which > 3) return FMMG_INVALID_ARG;
+  if (!h->setupDone) return FMMG_STATE;
+  const fmmg::CSR& L = which == 0 ? h->plan.U : which == 1 ? h->plan.V : which == 2 ? h->plan.W : h->plan.X;
+  if (ptr) std::copy(L.ptr.begin(), L.ptr.end(), ptr);
+  if (idx) std::copy(L.idx.begin(), L.idx.end(), idx);
+  if (total) *total = (int64_t)L.idx.size();
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_operator(fmmg_handle* h, int which, int idx, double* get, const double* set, int64_t* count) {
+  if (!h) return FMMG_INVALID_ARG;
+  fmmg::Plan& P = h->plan;
+  const int64_t ue = (int64_t)P.nUE * P.sdm, uc = (int64_t)P.nUC * P.tdm;
+  const int64_t de = (int64_t)P.nDE * P.sdm, dc = (int64_t)P.nDC * P.tdm;
+  int64_t n = 0;
+  switch (which) {
+    case 0:  // reference (ue x uc) column-major
+      n = ue * uc;
+      for (int64_t i = 0; i < ue; i++)
+        for (int64_t j = 0; j < uc; j++) {
+          if (get) get[j * ue + i] = P.uc2ue[i * uc + j];
+          if (set) P.uc2ue[i * uc + j] = set[j * ue + i];
+        }
+      break;
+    case 1:  // octant idx: (uc x ue)
+      if (idx < 0 || idx > 7) return fail(h, FMMG_INVALID_ARG, "octant index");
+      n = uc * ue;
+      for (int64_t r = 0; r < uc; r++)
+        for (int64_t c = 0; c < ue; c++) {
+          if (get) get[c * uc + r] = P.m2m[r * 8 * ue + idx * ue + c];
+          if (set) P.m2m[r * 8 * ue + idx * ue + c] = set[c * uc + r];
+        }
+      break;
+    case 2:
+      n = de * dc;
+      for (int64_t i = 0; i < de; i++)
+        for (int64_t j = 0; j < dc; j++) {
+          if (get) get[j * de + i] = P.dc2de[i * dc + j];
+          if (set) P.dc2de[i * dc + j] = set[j * de + i];
+        }
+      break;
+    case 3:
+      if (idx < 0 || idx > 7) return fail(h, FMMG_INVALID_ARG, "octant index");
+      n = dc * de;
+      for (int64_t r = 0; r < dc; r++)
+        for (int64_t c = 0; c < de; c++) {
+          if (get) get[c * dc + r] = P.l2l[((int64_t)idx * dc + r) * de + c];
+          if (set) P.l2l[((int64_t)idx * dc + r) * de + c] = set[c * dc + r];
+        }
+      break;
+    case 4: {
+      if (idx < 0 || idx > 315) return fail(h, FMMG_INVALID_ARG, "translation index");
+      const int64_t m = (int64_t)P.nEff * P.sdm * P.tdm;
+      n = 2 * m;
+      double* base = (double*)(P.m2lT.data() + (size_t)idx * m);
+      if (get) std::memcpy(get, base, sizeof(double) * n);
+      if (set) std::memcpy(base, set, sizeof(double) * n);
+    } break;
+    default:
+      return fail(h, FMMG_INVALID_ARG, "operator id");
+  }
+  if (count) *count = n;
+  if (set) h->opsDirty = true;
+  return FMMG_OK;
+}
+
+const char* fmmg_last_error(const fmmg_handle* h) {
+  return h ? h->err.c_str() : g_create_err.c_str();
+}
+
+fmmg_status fmmg_destroy(fmmg_handle* h) {
+  if (!h) return FMMG_OK;
+  if (!h->hostOnly) {
+    cudaSetDevice(h->dev.device);
+    if (h->dev.stream) cudaStreamSynchronize(h->dev.stream);
+    fmmg::dev_free(h->dev);
+    if (h->dev.ownStream && h->dev.stream) cudaStreamDestroy(h->dev.stream);
+  }
+  delete h;
+  return FMMG_OK;
+}
+
+}  // extern "C"

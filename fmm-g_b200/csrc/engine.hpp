@@ -1,0 +1,86 @@
+// engine.hpp -- device-resident state of one evaluator handle and the stage
+// launcher.  All kernels live in stages.cu; the C ABI is capi.cpp.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "plan.hpp"
+
+namespace fmmg {
+
+// timing marks recorded on the handle's stream around each kernel class;
+// interval k runs from mark k to mark k+1
+enum {
+  EV_BEGIN = 0, EV_PREP, EV_S2M, EV_UP_GEMM, EV_NEAR, EV_M2L_FWD, EV_M2L_HAD, EV_M2L_INV, EV_M2T, EV_S2L,
+  EV_DN_GEMM, EV_L2T, EV_END, EV_COUNT
+};
+
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+};
+
+struct DevState {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool ownStream = false;
+  // geometry (permuted order)
+  double *src = nullptr, *nrm = nullptr, *trg = nullptr;
+  int64_t *srcPerm = nullptr, *trgPerm = nullptr;
+  double *ctr = nullptr, *rad = nullptr;
+  int64_t *srcBeg = nullptr, *srcCnt = nullptr, *trgBeg = nullptr, *trgCnt = nullptr;
+  int32_t *chd = nullptr, *depth = nullptr;
+  double* sam[4] = {nullptr, nullptr, nullptr, nullptr};
+  int32_t* surfIJK = nullptr;  // np-surface point -> packed (i, j, k)
+  // work lists
+  int32_t *evtrLeaves = nullptr;
+  int64_t *nearPtr = nullptr; int32_t *nearIdx = nullptr;     // merged near list
+  int64_t *nearUPtr = nullptr; int32_t *nearUIdx = nullptr;   // stage-split forms
+  int64_t *nearWPtr = nullptr; int32_t *nearWIdx = nullptr;
+  int64_t *nearXPtr = nullptr; int32_t *nearXIdx = nullptr;
+  int64_t *farPtr = nullptr; int32_t *farIdx = nullptr;
+  int32_t *s2lNodes = nullptr; int64_t *s2lPtr = nullptr; int32_t *s2lIdx = nullptr;
+  int32_t *s2mLeaves = nullptr;
+  int32_t *levelRows = nullptr;  // concatenated per-level row lists
+  std::vector<int64_t> offUpC2E, offUpM2M, offDnL2L, offDnC2E;  // host offsets into levelRows, size maxDepth+2
+  int32_t *vParents = nullptr; int64_t *vPtr = nullptr; int32_t *vIdx = nullptr; int8_t *vOff = nullptr;
+  int32_t *vSrcSlot = nullptr, *vTrgSlot = nullptr, *vSrcNodes = nullptr, *vTrgNodes = nullptr;
+  // operators
+  double *uc2ue = nullptr, *m2m = nullptr, *dc2de = nullptr, *l2l = nullptr;
+  double2* m2lT = nullptr;
+  // per-evaluate work arrays
+  double *den = nullptr, *val = nullptr, *uchk = nullptr, *uden = nullptr, *dchk = nullptr, *dden = nullptr;
+  double2 *effDen = nullptr, *effVal = nullptr;
+  // dense check scratch
+  double *chkPos = nullptr, *chkOut = nullptr;
+  size_t chkCap = 0;
+  // timing
+  cudaEvent_t ev[EV_COUNT] = {};
+  bool evReady = false;
+  float stageMs[7] = {0, 0, 0, 0, 0, 0, 0};
+  float kernMs[EV_COUNT - 1] = {};
+  int lastLaunches = 0;  // kernels launched by the last single-RHS evaluate  // interval k = ev[k] .. ev[k+1]
+  std::vector<void*> allocs;
+};
+
+// counts of the last stage launch list (for reporting)
+struct LaunchStats {
+  int launches = 0;
+};
+
+std::string dev_upload(const Plan& P, DevState& D, const double* src, const double* nrm, const double* trg);
+std::string dev_upload_operators(const Plan& P, DevState& D);
+void dev_free(DevState& D);
+// run one right-hand side; den/val are device arrays in caller order
+std::string dev_evaluate(const Plan& P, DevState& D, const double* dDenCaller, double* dValCaller,
+                         int precision, int stageMask, bool timed, LaunchStats* st);
+// dense FP64 sums at device positions (caller-order source arrays are the
+// permuted copies held on the device plus the permuted density)
+std::string dev_dense(const Plan& P, DevState& D, const double* dDenCaller, int64_t nchk,
+                      const double* hPos, double* hOut);
+
+}  // namespace fmmg

@@ -1,0 +1,155 @@
+// linalg.cpp -- dense linear algebra for the operator builder (setup only).
+//
+// pinv_jacobi: the truncated pseudo-inverse of common/vecmatop.cpp:129-164
+// (common/svdrep.cpp:38-80 keeps the singular values >= eps * s_max), computed
+// from a one-sided Jacobi SVD, which is accurate in the small singular values
+// that the truncation tests.  rfft3_host: the r2c transform with FFTW's rank-3
+// layout used for the M2L translation tables (fmm3d_mpi/matmgnt3d_mpi.cpp:408).
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <vector>
+
+#include "plan.hpp"
+
+namespace fmmg {
+
+// A is m x n column-major with m >= n after an optional transpose.  Columns
+// are orthogonalised pairwise in tournament order (n/2 disjoint pairs per
+// round, so rounds parallelise and the result is thread-count independent).
+static void svd_onesided(int m, int n, std::vector<double>& W /* m x n, becomes U*S */,
+                         std::vector<double>& V /* n x n */) {
+  V.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; i++) V[(size_t)i * n + i] = 1.0;
+  const int nn = n + (n & 1);
+  std::vector<int> top(nn / 2), bot(nn / 2);
+  for (int i = 0; i < nn / 2; i++) { top[i] = 2 * i; bot[i] = 2 * i + 1; }
+  std::vector<double> norms(n);
+  for (int sweep = 0; sweep < 80; sweep++) {
+    int rotated = 0;
+    for (int j = 0; j < n; j++) {
+      double s = 0;
+      const double* w = &W[(size_t)j * m];
+      for (int i = 0; i < m; i++) s += w[i] * w[i];
+      norms[j] = s;
+    }
+    for (int round = 0; round < nn - 1; round++) {
+#pragma omp parallel for schedule(static) reduction(+ : rotated)
+      for (int k = 0; k < nn / 2; k++) {
+        int p = std::min(top[k], bot[k]), q = std::max(top[k], bot[k]);
+        if (q >= n) continue;
+        double* wp = &W[(size_t)p * m];
+        double* wq = &W[(size_t)q * m];
+        double a = 0, b = 0, g = 0;
+        for (int i = 0; i < m; i++) {
+          a += wp[i] * wp[i];
+          b += wq[i] * wq[i];
+          g += wp[i] * wq[i];
+        }
+        if (a == 0.0 || b == 0.0) continue;
+        if (std::fabs(g) <= 1e-15 * std::sqrt(a * b)) continue;
+        rotated++;
+        double zeta = (b - a) / (2.0 * g);
+        double t = std::copysign(1.0, zeta) / (std::fabs(zeta) + std::hypot(1.0, zeta));
+        double c = 1.0 / std::hypot(1.0, t), s = c * t;
+        for (int i = 0; i < m; i++) {
+          double x = wp[i], y = wq[i];
+          wp[i] = c * x - s * y;
+          wq[i] = s * x + c * y;
+        }
+        double* vp = &V[(size_t)p * n];
+        double* vq = &V[(size_t)q * n];
+        for (int i = 0; i < n; i++) {
+          double x = vp[i], y = vq[i];
+          vp[i] = c * x - s * y;
+          vq[i] = s * x + c * y;
+        }
+      }
+      // tournament rotation (player 0 stays)
+      if (nn / 2 > 1) {
+        int tlast = top[nn / 2 - 1], b0 = bot[0];
+        for (int i = nn / 2 - 1; i > 1; i--) top[i] = top[i - 1];
+        top[1] = b0;
+        for (int i = 0; i < nn / 2 - 1; i++) bot[i] = bot[i + 1];
+        bot[nn / 2 - 1] = tlast;
+      }
+    }
+    if (!rotated) break;
+  }
+}
+
+void pinv_jacobi(int m, int n, const double* A, double eps, double* R) {
+  // R (n x m) = V_k S_k^-1 U_k^T with A = U S V^T
+  bool tr = m < n;
+  int M = tr ? n : m, N = tr ? m : n;
+  std::vector<double> W((size_t)M * N), V;
+  if (!tr) std::memcpy(W.data(), A, sizeof(double) * M * N);
+  else
+    for (int i = 0; i < m; i++)
+      for (int j = 0; j < n; j++) W[(size_t)i * n + j] = A[(size_t)j * m + i];
+  svd_onesided(M, N, W, V);
+  std::vector<double> S(N);
+  for (int j = 0; j < N; j++) {
+    double s = 0;
+    for (int i = 0; i < M; i++) s += W[(size_t)j * M + i] * W[(size_t)j * M + i];
+    S[j] = std::sqrt(s);
+  }
+  double smax = *std::max_element(S.begin(), S.end());
+  double cutoff = eps * smax;
+  std::fill(R, R + (size_t)n * m, 0.0);
+  // For A = W V^T with W = U S: pinv(A) = V S^-2 W^T restricted to kept columns.
+  for (int c = 0; c < N; c++) {
+    if (!(S[c] >= cutoff) || S[c] == 0.0) continue;
+    double inv2 = 1.0 / (S[c] * S[c]);
+    const double* w = &W[(size_t)c * M];
+    const double* v = &V[(size_t)c * N];
+    if (!tr) {  // R(i, j) += v_i w_j / s^2, R is n x m
+      for (int j = 0; j < m; j++) {
+        double f = w[j] * inv2;
+        double* r = R + (size_t)j * n;
+        for (int i = 0; i < n; i++) r[i] += v[i] * f;
+      }
+    } else {  // A^T = W V^T  ->  pinv(A) = W S^-2 V^T : R(i, j) += w_i v_j / s^2
+      for (int j = 0; j < m; j++) {
+        double f = v[j] * inv2;
+        double* r = R + (size_t)j * n;
+        for (int i = 0; i < n; i++) r[i] += w[i] * f;
+      }
+    }
+  }
+}
+
+// out[kz][ky][kx][h], kx in [0, n/2]; in[z][y][x][h] (x fastest), e^{-2 pi i}
+void rfft3_host(int n, int howmany, const double* in, std::complex<double>* out) {
+  typedef std::complex<double> C;
+  const int nh = n / 2 + 1;
+  std::vector<C> w(n);
+  for (int j = 0; j < n; j++) w[j] = C(std::cos(2.0 * M_PI * j / n), -std::sin(2.0 * M_PI * j / n));
+  std::vector<C> a((size_t)n * n * nh), b((size_t)n * n * nh);
+  for (int h = 0; h < howmany; h++) {
+    for (int z = 0; z < n; z++)
+      for (int y = 0; y < n; y++)
+        for (int kx = 0; kx < nh; kx++) {
+          C s = 0;
+          for (int x = 0; x < n; x++) s += in[(((size_t)z * n + y) * n + x) * howmany + h] * w[(kx * x) % n];
+          a[((size_t)z * n + y) * nh + kx] = s;
+        }
+    for (int z = 0; z < n; z++)
+      for (int ky = 0; ky < n; ky++)
+        for (int kx = 0; kx < nh; kx++) {
+          C s = 0;
+          for (int y = 0; y < n; y++) s += a[((size_t)z * n + y) * nh + kx] * w[(ky * y) % n];
+          b[((size_t)z * n + ky) * nh + kx] = s;
+        }
+    for (int kz = 0; kz < n; kz++)
+      for (int ky = 0; ky < n; ky++)
+        for (int kx = 0; kx < nh; kx++) {
+          C s = 0;
+          for (int z = 0; z < n; z++) s += b[((size_t)z * n + ky) * nh + kx] * w[(kz * z) % n];
+          out[(((size_t)kz * n + ky) * nh + kx) * howmany + h] = s;
+        }
+  }
+}
+
+}  // namespace fmmg

@@ -1,0 +1,477 @@
+// plan.cpp -- host setup: octree, lists, GPU work lists, operator tables.
+#include "plan.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <queue>
+
+#include "kernels.hpp"
+
+namespace fmmg {
+
+// ------------------------------------------------------------------ geometry
+// Centre of a box: fmm3d_mpi/let3d_mpi.cpp:1808-1818.  The expression order
+// is kept so that the point binning (p >= centre) is reproducible bit for bit.
+void Plan::node_center(int d, const int* p, double* c) const {
+  double R = std::pow(2.0, -o.rootLevel);
+  double ll[3] = {o.ctr[0] - R, o.ctr[1] - R, o.ctr[2] - R};
+  int tmp = 1 << d;
+  for (int k = 0; k < 3; k++) c[k] = ll[k] + (2 * R) * (p[k] + 0.5) / double(tmp);
+}
+
+// Adaptive octree (stands in for DENDRO points2Octree + CreateAncestors,
+// fmm3d_mpi/let3d_mpi.cpp:268-288, 611-726): an octant is split while it
+// holds more than ptsMax sources and is above maxLevel, the root is always
+// split, a split makes all 8 children.  Sources are binned by p >= centre per
+// axis (let3d_mpi.cpp:1255-1267) with a stable partition, which leaves every
+// subtree's sources contiguous in Morton order.
+void Plan::build_tree(const double* src) {
+  depth.assign(1, 0); par.assign(1, -1); chd.assign(1, -1);
+  path.assign(3, 0);
+  srcBeg.assign(1, 0); srcCnt.assign(1, ns);
+  srcPerm.resize(ns);
+  std::iota(srcPerm.begin(), srcPerm.end(), (int64_t)0);
+  std::vector<int64_t> tmp(ns);
+  levelBeg.assign(1, 0);
+  int lvS = 0, lvE = 1, d = 0;
+  while (lvS < lvE) {
+    // child ids in parent order
+    std::vector<int> first(lvE - lvS, -1);
+    int next = lvE;
+    for (int n = lvS; n < lvE; n++) {
+      bool split = (n == 0) || (srcCnt[n] > o.ptsMax && d < o.maxLevel);
+      if (split) { first[n - lvS] = next; next += 8; }
+    }
+    int total = next;
+    depth.resize(total); par.resize(total); chd.resize(total); path.resize(3 * (size_t)total);
+    srcBeg.resize(total); srcCnt.resize(total);
+#pragma omp parallel for schedule(dynamic, 8)
+    for (int n = lvS; n < lvE; n++) {
+      int f = first[n - lvS];
+      if (f < 0) continue;
+      chd[n] = f;
+      double c[3];
+      node_center(d, &path[3 * (size_t)n], c);
+      int64_t b = srcBeg[n], e = b + srcCnt[n];
+      int64_t cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      for (int64_t i = b; i < e; i++) {
+        const double* p = src + 3 * srcPerm[i];
+        int code = (p[0] >= c[0]) * 4 + (p[1] >= c[1]) * 2 + (p[2] >= c[2]);
+        cnt[code]++;
+      }
+      int64_t off[8];
+      off[0] = b;
+      for (int k = 1; k < 8; k++) off[k] = off[k - 1] + cnt[k - 1];
+      for (int k = 0; k < 8; k++) {
+        int ch = f + k;
+        depth[ch] = d + 1; par[ch] = n; chd[ch] = -1;
+        path[3 * (size_t)ch + 0] = 2 * path[3 * (size_t)n + 0] + (k >> 2);
+        path[3 * (size_t)ch + 1] = 2 * path[3 * (size_t)n + 1] + ((k >> 1) & 1);
+        path[3 * (size_t)ch + 2] = 2 * path[3 * (size_t)n + 2] + (k & 1);
+        srcBeg[ch] = off[k]; srcCnt[ch] = cnt[k];
+      }
+      int64_t w[8];
+      std::memcpy(w, off, sizeof(w));
+      for (int64_t i = b; i < e; i++) {
+        const double* p = src + 3 * srcPerm[i];
+        int code = (p[0] >= c[0]) * 4 + (p[1] >= c[1]) * 2 + (p[2] >= c[2]);
+        tmp[w[code]++] = srcPerm[i];
+      }
+      std::memcpy(&srcPerm[b], &tmp[b], sizeof(int64_t) * (e - b));
+    }
+    levelBeg.push_back(lvE);
+    lvS = lvE; lvE = total; d++;
+  }
+  nn = (int)depth.size();
+  maxDepth = 0;
+  for (int n = 0; n < nn; n++) maxDepth = std::max(maxDepth, depth[n]);
+  levelBeg.resize(maxDepth + 2);
+  levelBeg[maxDepth + 1] = nn;
+}
+
+// Targets binned into the source tree (fmm3d_mpi/let3d_mpi.cpp:1470-1538).
+void Plan::bin_targets(const double* trg) {
+  trgBeg.assign(nn, 0); trgCnt.assign(nn, 0);
+  trgPerm.resize(nt);
+  std::iota(trgPerm.begin(), trgPerm.end(), (int64_t)0);
+  std::vector<int64_t> tmp(nt);
+  trgCnt[0] = nt;
+  for (int d = 0; d <= maxDepth; d++) {
+#pragma omp parallel for schedule(dynamic, 8)
+    for (int n = levelBeg[d]; n < levelBeg[d + 1]; n++) {
+      if (chd[n] < 0) continue;
+      double c[3];
+      node_center(d, &path[3 * (size_t)n], c);
+      int64_t b = trgBeg[n], e = b + trgCnt[n];
+      int64_t cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      for (int64_t i = b; i < e; i++) {
+        const double* p = trg + 3 * trgPerm[i];
+        cnt[(p[0] >= c[0]) * 4 + (p[1] >= c[1]) * 2 + (p[2] >= c[2])]++;
+      }
+      int64_t off[8];
+      off[0] = b;
+      for (int k = 1; k < 8; k++) off[k] = off[k - 1] + cnt[k - 1];
+      for (int k = 0; k < 8; k++) { trgBeg[chd[n] + k] = off[k]; trgCnt[chd[n] + k] = cnt[k]; }
+      for (int64_t i = b; i < e; i++) {
+        const double* p = trg + 3 * trgPerm[i];
+        int code = (p[0] >= c[0]) * 4 + (p[1] >= c[1]) * 2 + (p[2] >= c[2]);
+        tmp[off[code]++] = trgPerm[i];
+      }
+      std::memcpy(&trgPerm[b], &tmp[b], sizeof(int64_t) * (e - b));
+    }
+  }
+}
+
+// fmm3d_mpi/let3d_mpi.cpp:1833-1853
+int Plan::find_node(int wntDepth, const int* wp) const {
+  int cur = 0;
+  int p[3] = {wp[0], wp[1], wp[2]};
+  while (depth[cur] < wntDepth && chd[cur] >= 0) {
+    int t = 1 << (wntDepth - depth[cur] - 1);
+    int c0 = p[0] / t, c1 = p[1] / t, c2 = p[2] / t;
+    p[0] -= c0 * t; p[1] -= c1 * t; p[2] -= c2 * t;
+    cur = chd[cur] + c0 * 4 + c1 * 2 + c2;
+  }
+  return cur;
+}
+
+// fmm3d_mpi/let3d_mpi.cpp:1856-1876: boxes touch (face, edge or corner)
+bool Plan::adjacent(int a, int b) const {
+  int md = std::max(depth[a], depth[b]);
+  int ra = 1 << (md - depth[a]), rb = 1 << (md - depth[b]);
+  int rs = ra + rb, linf = 0;
+  bool le = true;
+  for (int k = 0; k < 3; k++) {
+    int dif = std::abs((2 * path[3 * (size_t)a + k] + 1) * ra - (2 * path[3 * (size_t)b + k] + 1) * rb);
+    le = le && dif <= rs;
+    linf = std::max(linf, dif);
+  }
+  return le && linf == rs;
+}
+
+// U/V/W/X lists of every evaluator node (fmm3d_mpi/let3d_mpi.cpp:1637-1768):
+// the candidates are the children of the parent's neighbours at the node's
+// depth, resolved to the deepest existing box; lists hold sorted unique ids.
+void Plan::build_lists() {
+  std::vector<std::vector<int32_t>> Lu(nn), Lv(nn), Lw(nn), Lx(nn);
+#pragma omp parallel for schedule(dynamic, 32)
+  for (int g = 0; g < nn; g++) {
+    if (!(flags[g] & NF_EVTR)) continue;
+    std::vector<int32_t>& Us = Lu[g];
+    std::vector<int32_t>& Vs = Lv[g];
+    std::vector<int32_t>& Ws = Lw[g];
+    std::vector<int32_t>& Xs = Lx[g];
+    const bool term = leaf(g);
+    if (g != 0) {
+      const int P = par[g], dg = depth[g];
+      const int lim = 1 << dg;
+      const int* pp = &path[3 * (size_t)P];
+      const int* pg = &path[3 * (size_t)g];
+      for (int i = -2; i < 4; i++)
+        for (int j = -2; j < 4; j++)
+          for (int k = -2; k < 4; k++) {
+            int tp[3] = {2 * pp[0] + i, 2 * pp[1] + j, 2 * pp[2] + k};
+            if (tp[0] < 0 || tp[1] < 0 || tp[2] < 0 || tp[0] >= lim || tp[1] >= lim || tp[2] >= lim) continue;
+            if (tp[0] == pg[0] && tp[1] == pg[1] && tp[2] == pg[2]) continue;
+            int res = find_node(dg, tp);
+            bool adj = adjacent(res, g);
+            if (depth[res] < dg) {
+              if (adj) { if (term) Us.push_back(res); }
+              else Xs.push_back(res);
+            } else if (!adj) {
+              Vs.push_back(res);
+            } else if (term) {
+              std::queue<int> rest;
+              rest.push(res);
+              while (!rest.empty()) {
+                int f = rest.front();
+                rest.pop();
+                if (!adjacent(f, g)) Ws.push_back(f);
+                else if (leaf(f)) Us.push_back(f);
+                else for (int c = 0; c < 8; c++) rest.push(chd[f] + c);
+              }
+            }
+          }
+    }
+    if (term) Us.push_back(g);
+    auto fin = [&](std::vector<int32_t>& L, uint8_t need) {
+      std::sort(L.begin(), L.end());
+      L.erase(std::unique(L.begin(), L.end()), L.end());
+      L.erase(std::remove_if(L.begin(), L.end(), [&](int32_t s) { return !(flags[s] & need); }), L.end());
+    };
+    fin(Us, NF_LSRC); fin(Vs, NF_SRCE); fin(Ws, NF_SRCE); fin(Xs, NF_LSRC);
+  }
+  auto flat = [&](std::vector<std::vector<int32_t>>& L, CSR& out) {
+    out.ptr.assign(nn + 1, 0);
+    for (int n = 0; n < nn; n++) out.ptr[n + 1] = out.ptr[n] + (int64_t)L[n].size();
+    out.idx.resize(out.ptr[nn]);
+    for (int n = 0; n < nn; n++) std::copy(L[n].begin(), L[n].end(), out.idx.begin() + out.ptr[n]);
+    for (int32_t s : out.idx) flags[s] |= NF_USER;
+  };
+  flat(Lu, U); flat(Lv, V); flat(Lw, W); flat(Lx, X);
+}
+
+// Flattened work for the GPU stages, following the per-node decisions of
+// fmm3d_mpi/fmm3d_eval_mpi.cpp: W sources with fewer than |UE|*srcDOF values
+// and X sources of a leaf with fewer than |DC|*trgDOF values are summed
+// directly (S2T, :1146 and :1249); the others go through the UE surface (M2T)
+// or the DC surface (S2L).
+void Plan::build_worklists() {
+  const int64_t ueSize = (int64_t)nUE * sdm, dcSize = (int64_t)nDC * tdm;
+  evtrLeaves.clear(); nearSrc.clear(); farUE.clear();
+  s2lNodes.clear(); s2lSrc.clear(); s2mLeaves.clear();
+  for (int g = 0; g < nn; g++) {
+    if ((flags[g] & NF_LSRC)) s2mLeaves.push_back(g);
+    if (!(flags[g] & NF_EVTR)) continue;
+    bool xDirect = leaf(g) && trgCnt[g] * td < dcSize;
+    if (leaf(g)) {
+      evtrLeaves.push_back(g);
+      for (int64_t e = U.ptr[g]; e < U.ptr[g + 1]; e++) nearSrc.idx.push_back(U.idx[e]);
+      for (int64_t e = W.ptr[g]; e < W.ptr[g + 1]; e++) {
+        int w = W.idx[e];
+        if ((flags[w] & NF_LSRC) && srcCnt[w] * sd < ueSize) nearSrc.idx.push_back(w);
+        else farUE.idx.push_back(w);
+      }
+      if (xDirect)
+        for (int64_t e = X.ptr[g]; e < X.ptr[g + 1]; e++) nearSrc.idx.push_back(X.idx[e]);
+      nearSrc.ptr.push_back((int64_t)nearSrc.idx.size());
+      farUE.ptr.push_back((int64_t)farUE.idx.size());
+    }
+    if (!xDirect && X.ptr[g + 1] > X.ptr[g]) {
+      s2lNodes.push_back(g);
+      for (int64_t e = X.ptr[g]; e < X.ptr[g + 1]; e++) s2lSrc.idx.push_back(X.idx[e]);
+      s2lSrc.ptr.push_back((int64_t)s2lSrc.idx.size());
+    }
+  }
+  // level lists for the batched equivalent-density GEMMs
+  upC2E.assign(maxDepth + 1, {}); upM2M.assign(maxDepth + 1, {});
+  dnL2L.assign(maxDepth + 1, {}); dnC2E.assign(maxDepth + 1, {});
+  for (int g = 0; g < nn; g++) {
+    int d = depth[g];
+    if (flags[g] & NF_CBTR) {
+      upC2E[d].push_back(g);
+      if (!leaf(g)) upM2M[d].push_back(g);
+    }
+    if ((flags[g] & NF_EVTR) && d >= 2) {
+      dnC2E[d].push_back(g);
+      if (!leaf(g)) dnL2L[d].push_back(g);
+    }
+  }
+  // M2L by parent pairs: V(c) for a child c of P is the set of children of
+  // P's same-depth non-leaf neighbours Q that do not touch c
+  // (let3d_mpi.cpp:1687-1698); grouping by (P, Q) lets the 8 x 8 child pairs
+  // share one pass over Q's spectra.
+  vParents.clear(); vNbr.clear(); vNbrOff.clear();
+  vSrcSlot.assign(nn, -1); vTrgSlot.assign(nn, -1);
+  vSrcNodes.clear(); vTrgNodes.clear();
+  for (int d = 1; d < maxDepth; d++) {
+    for (int P = levelBeg[d]; P < levelBeg[d + 1]; P++) {
+      if (leaf(P)) continue;
+      bool anyE = false;
+      for (int c = 0; c < 8; c++) anyE = anyE || (flags[chd[P] + c] & NF_EVTR);
+      if (!anyE) continue;
+      const int* pp = &path[3 * (size_t)P];
+      const int lim = 1 << d;
+      size_t before = vNbr.idx.size();
+      for (int dx = -1; dx <= 1; dx++)
+        for (int dy = -1; dy <= 1; dy++)
+          for (int dz = -1; dz <= 1; dz++) {
+            if (!dx && !dy && !dz) continue;
+            int q[3] = {pp[0] + dx, pp[1] + dy, pp[2] + dz};
+            if (q[0] < 0 || q[1] < 0 || q[2] < 0 || q[0] >= lim || q[1] >= lim || q[2] >= lim) continue;
+            int Q = find_node(d, q);
+            if (depth[Q] != d || leaf(Q)) continue;
+            vNbr.idx.push_back(Q);
+            vNbrOff.push_back((int8_t)((dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)));
+            for (int c = 0; c < 8; c++) {
+              int v = chd[Q] + c;
+              if ((flags[v] & NF_CBTR) && vSrcSlot[v] < 0) {
+                vSrcSlot[v] = (int32_t)vSrcNodes.size();
+                vSrcNodes.push_back(v);
+              }
+            }
+          }
+      if (vNbr.idx.size() == before) continue;
+      vParents.push_back(P);
+      vNbr.ptr.push_back((int64_t)vNbr.idx.size());
+      for (int c = 0; c < 8; c++) {
+        int t = chd[P] + c;
+        if ((flags[t] & NF_EVTR) && vTrgSlot[t] < 0) {
+          vTrgSlot[t] = (int32_t)vTrgNodes.size();
+          vTrgNodes.push_back(t);
+        }
+      }
+    }
+  }
+}
+
+std::string Plan::build(const Options& opt, int64_t ns_, const double* src, const double* nrmIn, int64_t nt_,
+                        const double* trg) {
+  o = opt;
+  ns = ns_; nt = nt_;
+  build_tree(src);
+  bin_targets(trg);
+  flags.assign(nn, 0);
+  center.resize(3 * (size_t)nn);
+  radius.resize(nn);
+  const double R0 = std::pow(2.0, -o.rootLevel);
+  for (int n = 0; n < nn; n++) {
+    uint8_t f = 0;
+    bool lf = chd[n] < 0;
+    if (lf) f |= NF_LEAF;
+    if (n != 0 && srcCnt[n] > 0) f |= NF_CBTR;
+    if (n != 0 && (!lf || srcCnt[n] > 0)) f |= NF_SRCE;
+    if (lf && srcCnt[n] > 0) f |= NF_LSRC;
+    if (trgCnt[n] > 0) f |= NF_EVTR;
+    flags[n] = f;
+    node_center(depth[n], &path[3 * (size_t)n], &center[3 * (size_t)n]);
+    radius[n] = R0 / double(1 << depth[n]);  // let3d_mpi.cpp:1824-1827
+  }
+  build_lists();
+  build_worklists();
+  (void)nrmIn;
+  return std::string();
+}
+
+// ------------------------------------------------------------------ operators
+static void sam_pos(int np, double R, std::vector<double>& pos) {  // matmgnt3d_mpi.cpp:451-475
+  pos.clear();
+  double step = 2.0 / (np - 1);
+  for (int i = 0; i < np; i++)
+    for (int j = 0; j < np; j++)
+      for (int k = 0; k < np; k++)
+        if (i == 0 || i == np - 1 || j == 0 || j == np - 1 || k == 0 || k == np - 1) {
+          pos.push_back(R * (-1.0 + i * step));
+          pos.push_back(R * (-1.0 + j * step));
+          pos.push_back(R * (-1.0 + k * step));
+        }
+}
+
+// column-major kernel matrix (nt*TD) x (ns*SD) of the equivalent kernel
+template <int KT>
+static void mm_matrix(const double* coefs, int ns, const double* sp, int nt, const double* tp,
+                      std::vector<double>& out) {
+  constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD;
+  const int64_t m = (int64_t)nt * TD;
+  out.assign((size_t)m * ns * SD, 0.0);
+  double K[16];
+  for (int j = 0; j < ns; j++)
+    for (int i = 0; i < nt; i++) {
+      double x = tp[3 * i] - sp[3 * j], y = tp[3 * i + 1] - sp[3 * j + 1], z = tp[3 * i + 2] - sp[3 * j + 2];
+      if (!kblock<KT, double>(x, y, z, sp + 3 * j, K, coefs[0], coefs[1])) continue;
+      for (int t = 0; t < TD; t++)
+        for (int s = 0; s < SD; s++) out[(size_t)(j * SD + s) * m + i * TD + t] = K[t * SD + s];
+    }
+}
+
+static void mm_matrix_rt(int kt, const double* coefs, int ns, const double* sp, int nt, const double* tp,
+                         std::vector<double>& out) {
+  switch (kt) {
+    case LAP_S_U: mm_matrix<LAP_S_U>(coefs, ns, sp, nt, tp, out); break;
+    case STK_F_U: mm_matrix<STK_F_U>(coefs, ns, sp, nt, tp, out); break;
+    case NAV_S_U: mm_matrix<NAV_S_U>(coefs, ns, sp, nt, tp, out); break;
+  }
+}
+
+// The operator set of MatMgnt3d_MPI (fmm3d_mpi/matmgnt3d_mpi.cpp:52-71,
+// 107-274, 373-411) for a homogeneous equivalent kernel: unit-radius tables,
+// level scaling 2^(+-l*deg) applied by the GPU stages.
+std::string Plan::build_operators() {
+  sd = kernel_src_dof(o.kt);
+  td = kernel_trg_dof(o.kt);
+  mm = kernel_mm(o.kt);
+  if (mm < 0 || sd == 0) return "unsupported kernel type";
+  sdm = kernel_src_dof(mm);
+  tdm = kernel_trg_dof(mm);
+  nrm = kernel_has_normal(o.kt);
+  kernel_hom_deg(mm, deg);
+  const int np = o.np;
+  sam_pos(np, 1.0, sam[0]);
+  sam_pos(np + 2, 3.0, sam[1]);
+  sam_pos(np, 3.0, sam[2]);
+  sam_pos(np, 1.0, sam[3]);
+  nUE = (int)sam[0].size() / 3; nUC = (int)sam[1].size() / 3;
+  nDE = (int)sam[2].size() / 3; nDC = (int)sam[3].size() / 3;
+  const int n = 2 * np;
+  nReg = n * n * n;
+  nEff = n * n * (n / 2 + 1);
+  const double eps = std::pow(0.1, np + 1);  // matmgnt3d_mpi.cpp:37-40
+  const int ue = nUE * sdm, uc = nUC * tdm, de = nDE * sdm, dc = nDC * tdm;
+  std::vector<double> A, Rm;
+  // C2E up: pinv of the UE -> UC matrix
+  mm_matrix_rt(mm, o.coefs, nUE, sam[0].data(), nUC, sam[1].data(), A);
+  Rm.assign((size_t)ue * uc, 0.0);
+  pinv_jacobi(uc, ue, A.data(), eps, Rm.data());
+  uc2ue.resize((size_t)ue * uc);
+  for (int r = 0; r < ue; r++)
+    for (int c = 0; c < uc; c++) uc2ue[(size_t)r * uc + c] = Rm[(size_t)c * ue + r];
+  // C2E down
+  mm_matrix_rt(mm, o.coefs, nDE, sam[2].data(), nDC, sam[3].data(), A);
+  Rm.assign((size_t)de * dc, 0.0);
+  pinv_jacobi(dc, de, A.data(), eps, Rm.data());
+  dc2de.resize((size_t)de * dc);
+  for (int r = 0; r < de; r++)
+    for (int c = 0; c < dc; c++) dc2de[(size_t)r * dc + c] = Rm[(size_t)c * de + r];
+  // M2M / L2L octant matrices
+  m2m.assign((size_t)uc * 8 * ue, 0.0);
+  l2l.assign((size_t)8 * dc * de, 0.0);
+  for (int oc = 0; oc < 8; oc++) {
+    int id[3] = {oc >> 2, (oc >> 1) & 1, oc & 1};
+    std::vector<double> chk(3 * (size_t)nUC), den(3 * (size_t)nUE);
+    for (int j = 0; j < nUC; j++)
+      for (int k = 0; k < 3; k++) chk[3 * j + k] = 2.0 * sam[1][3 * j + k];
+    for (int j = 0; j < nUE; j++)
+      for (int k = 0; k < 3; k++) den[3 * j + k] = sam[0][3 * j + k] + (2 * id[k] - 1) * 1.0;
+    mm_matrix_rt(mm, o.coefs, nUE, den.data(), nUC, chk.data(), A);  // uc x ue, col-major
+    for (int r = 0; r < uc; r++)
+      for (int c = 0; c < ue; c++) m2m[(size_t)r * 8 * ue + oc * ue + c] = A[(size_t)c * uc + r];
+    std::vector<double> chk2(3 * (size_t)nDC), den2(sam[2]);
+    for (int j = 0; j < nDC; j++)
+      for (int k = 0; k < 3; k++) chk2[3 * j + k] = 0.5 * sam[3][3 * j + k] + (double(id[k]) - 0.5) * 1.0;
+    mm_matrix_rt(mm, o.coefs, nDE, den2.data(), nDC, chk2.data(), A);  // dc x de
+    for (int r = 0; r < dc; r++)
+      for (int c = 0; c < de; c++) l2l[((size_t)oc * dc + r) * de + c] = A[(size_t)c * dc + r];
+  }
+  // M2L translation spectra: the kernel from a point at 2*idx sampled on the
+  // (2np)^3 regular grid, r2c transformed (matmgnt3d_mpi.cpp:385-411)
+  int cnt = 0;
+  for (int i1 = -3; i1 <= 3; i1++)
+    for (int i2 = -3; i2 <= 3; i2++)
+      for (int i3 = -3; i3 <= 3; i3++)
+        transId[i1 + 3][i2 + 3][i3 + 3] =
+            (std::abs(i1) > 1 || std::abs(i2) > 1 || std::abs(i3) > 1) ? cnt++ : -1;
+  std::vector<double> reg(3 * (size_t)nReg);
+  {
+    double step = 2.0 / (np - 1);
+    size_t c = 0;
+    for (int k = 0; k < n; k++)
+      for (int j = 0; j < n; j++)
+        for (int i = 0; i < n; i++, c++) {
+          reg[3 * c + 0] = (i < np ? i : i - n) * step;
+          reg[3 * c + 1] = (j < np ? j : j - n) * step;
+          reg[3 * c + 2] = (k < np ? k : k - n) * step;
+        }
+  }
+  const int mdof = sdm * tdm;
+  m2lT.assign((size_t)316 * nEff * mdof, std::complex<double>(0, 0));
+#pragma omp parallel for schedule(dynamic, 2)
+  for (int t = 0; t < 343; t++) {
+    int i1 = t / 49 - 3, i2 = (t / 7) % 7 - 3, i3 = t % 7 - 3;
+    int id = transId[i1 + 3][i2 + 3][i3 + 3];
+    if (id < 0) continue;
+    double sp[3] = {i1 * 2.0, i2 * 2.0, i3 * 2.0};
+    std::vector<double> tt;
+    mm_matrix_rt(mm, o.coefs, 1, sp, nReg, reg.data(), tt);  // (nReg*tdm) x sdm
+    std::vector<double> grid((size_t)nReg * mdof);
+    for (int k = 0; k < nReg; k++)
+      for (int i = 0; i < tdm; i++)
+        for (int j = 0; j < sdm; j++)
+          grid[(size_t)k * mdof + j * tdm + i] = tt[(size_t)j * nReg * tdm + i + (size_t)k * tdm];
+    rfft3_host(n, mdof, grid.data(), &m2lT[(size_t)id * nEff * mdof]);
+  }
+  return std::string();
+}
+
+}  // namespace fmmg

@@ -1,0 +1,120 @@
+// plan.hpp -- host-side setup of the evaluator: the adaptive octree, the
+// U/V/W/X interaction lists, their flattened GPU work lists, and the
+// operator tables.  This is the setup() half of the reference FMM3d_MPI
+// (fmm3d_mpi/fmm3d_setup_mpi.cpp, fmm3d_mpi/let3d_mpi.cpp,
+// fmm3d_mpi/matmgnt3d_mpi.cpp) re-laid-out for the GPU:
+//  * nodes are numbered level by level (depth-major) and the 8 children of a
+//    node are consecutive, so per-node arrays of one level are contiguous and
+//    "all children of P" is a single row range;
+//  * sources and targets are permuted so that every leaf (and every subtree)
+//    owns a contiguous range, in Morton order of the leaves;
+//  * each interaction list becomes a CSR array of node ids.
+#pragma once
+
+#include <complex>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace fmmg {
+
+struct Options {
+  int kt = 111;
+  double coefs[2] = {1.0, 0.25};
+  int np = 6;
+  int ptsMax = 150;
+  int maxLevel = 30;
+  double ctr[3] = {0.5, 0.5, 0.5};
+  int rootLevel = 1;
+};
+
+// node flag bits (fmm3d_mpi/let3d_mpi.hpp:28-39 meanings at one rank)
+enum : uint8_t {
+  NF_CBTR = 1,   // has sources, not the root: carries an upward density
+  NF_USER = 2,   // appears in some list
+  NF_EVTR = 4,   // has targets: carries downward data / target values
+  NF_SRCE = 16,  // non-root and (non-leaf or has sources)
+  NF_LEAF = 32,
+  NF_LSRC = 64,  // leaf with sources (glbSrcExaNum > 0 in the reference)
+};
+
+struct CSR {
+  std::vector<int64_t> ptr;  // size rows + 1
+  std::vector<int32_t> idx;
+  void clear() { ptr.assign(1, 0); idx.clear(); }
+};
+
+struct Plan {
+  Options o;
+  int sd = 0, td = 0, mm = 0, sdm = 0, tdm = 0;
+  double deg[4] = {0, 0, 0, 0};
+  bool nrm = false;
+  // surfaces and grid (matmgnt3d_mpi.cpp:451-499)
+  int nUE = 0, nUC = 0, nDE = 0, nDC = 0, nReg = 0, nEff = 0;
+  std::vector<double> sam[4];  // UE, UC, DE, DC templates at unit radius scale, [n][3]
+
+  // ---- tree
+  int64_t ns = 0, nt = 0;
+  int nn = 0, maxDepth = 0;
+  std::vector<int> levelBeg;  // nodes of depth d: [levelBeg[d], levelBeg[d+1])
+  std::vector<int32_t> depth, par, chd;
+  std::vector<int32_t> path;  // [nn][3]
+  std::vector<uint8_t> flags;
+  std::vector<int64_t> srcBeg, srcCnt, trgBeg, trgCnt;  // subtree ranges in permuted order
+  std::vector<double> center;                           // [nn][3]
+  std::vector<double> radius;                           // [nn]
+  std::vector<int64_t> srcPerm, trgPerm;                // permuted position -> caller index
+
+  // ---- lists in the reference form (sorted node ids)
+  CSR U, V, W, X;
+
+  // ---- GPU work lists
+  std::vector<int32_t> evtrLeaves;  // EVTR leaves (rows of near/far-to-target work)
+  CSR nearSrc;                      // per EVTR leaf: source leaves for true-kernel direct sums
+  CSR farUE;                        // per EVTR leaf: W nodes evaluated from their UE surface
+  std::vector<int32_t> s2lNodes;    // EVTR nodes with X entries evaluated on the DC surface
+  CSR s2lSrc;                       // per s2lNodes row: source leaves
+  std::vector<int32_t> s2mLeaves;   // leaves with sources (S2M)
+  // per level d: CBTR nodes (upward C2E), CBTR non-leaf parents at d (M2M
+  // into them), EVTR non-leaves at d (L2L from them), EVTR nodes at d (C2E down)
+  std::vector<std::vector<int32_t>> upC2E, upM2M, dnL2L, dnC2E;
+  // M2L grouped by parent pairs: for each target parent P (non-leaf, depth >=1,
+  // with an EVTR child) the same-depth non-leaf neighbours Q and offset code
+  std::vector<int32_t> vParents;  // rows
+  CSR vNbr;                       // idx = Q node id
+  std::vector<int8_t> vNbrOff;    // parallel to vNbr.idx: (dx+1)*9+(dy+1)*3+(dz+1)
+  std::vector<int32_t> vSrcSlot;  // per node: row in the source-spectrum array or -1
+  std::vector<int32_t> vSrcNodes; // slot -> node
+  std::vector<int32_t> vTrgSlot;  // per node: row in the target-spectrum array or -1
+  std::vector<int32_t> vTrgNodes; // slot -> node
+
+  // ---- operators (homogeneous equivalent kernels: unit-radius tables)
+  // row-major for the GPU GEMMs:
+  std::vector<double> uc2ue;     // [nUE*sdm][nUC*tdm]       C2E up (pinv)
+  std::vector<double> m2m;       // [nUC*tdm][8*nUE*sdm]     8 octant UE->UC matrices side by side
+  std::vector<double> dc2de;     // [nDE*sdm][nDC*tdm]       C2E down (pinv)
+  std::vector<double> l2l;       // [8*nDC*tdm][nDE*sdm]     8 octant DE->DC matrices stacked
+  std::vector<std::complex<double>> m2lT;  // [316][nEff][sdm*tdm] (FFTW r2c layout)
+  int transId[7][7][7];
+
+  std::string build(const Options& opt, int64_t ns, const double* src, const double* nrm, int64_t nt,
+                    const double* trg);
+  std::string build_operators();
+  int child(int n, int o) const { return chd[n] + o; }
+  bool leaf(int n) const { return chd[n] < 0; }
+
+ private:
+  void build_tree(const double* src);
+  void bin_targets(const double* trg);
+  void build_lists();
+  void build_worklists();
+  int find_node(int wntDepth, const int* p) const;
+  bool adjacent(int a, int b) const;
+  void node_center(int depth, const int* path, double* c) const;
+};
+
+// linear algebra used by the operator builder (linalg.cpp)
+void pinv_jacobi(int m, int n, const double* A_colmajor, double eps, double* R_colmajor);
+void rfft3_host(int n, int howmany, const double* in, std::complex<double>* out);
+
+}  // namespace fmmg

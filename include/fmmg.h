@@ -1,0 +1,190 @@
+/* fmmg.h -- C ABI of the B200 (sm_100a) kernel-independent FMM evaluator.
+ *
+ * This is the drop-in boundary for the single-rank, single-GPU evaluate() path
+ * of the reference aashays/fmm-g.  Paths below are relative to the reference
+ * root.  One handle replaces one reference FMM3d_MPI object
+ * (fmm3d_mpi/fmm3d_mpi.hpp:36-249) together with the four GPU entry points
+ * it called per evaluate:
+ *   dense_inter_gpu(point3d_t*)  U-list P2P          fmm3d_mpi/gpu_setup.h:58
+ *   gpu_up(upComp_t*)            S2M                 fmm3d_mpi/gpu_setup.h:60
+ *   gpu_down(dnComp_t*)          L2T                 fmm3d_mpi/gpu_setup.h:62
+ *   cudavlistfunc(...)           V-list Hadamard     fmm3d_mpi/gpu_vlist.h:1
+ * Every stage of evaluate() runs on the GPU behind fmmg_evaluate*; the tree,
+ * the interaction lists and the operators stay resident between calls.
+ *
+ * Conventions
+ *  - Positions and normals are interleaved xyz, FP64, like the reference's
+ *    PETSc Vecs (fmm3d_mpi/knlmat3d_mpi.hpp:50-56).  Densities hold srcDOF
+ *    values per source and values trgDOF per target, interleaved.
+ *  - Inputs and outputs are in the CALLER's point order.  (The reference
+ *    redistributes the caller's Vecs inside setup(); at one rank that order is
+ *    the input order.)  trg_val is overwritten, as in the reference
+ *    (fmm3d_mpi/fmm3d_eval_mpi.cpp:427).
+ *  - Every function returns an fmmg_status and never exits, aborts or traps.
+ *    fmmg_last_error() gives a message for the last failure on a handle.
+ *  - A handle is not thread safe; separate handles may be used concurrently.
+ *    All GPU work of a handle is ordered on its stream.
+ */
+#ifndef FMMG_H_
+#define FMMG_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  FMMG_OK = 0,
+  FMMG_INVALID_ARG = 1,   /* bad option, size, pointer or non-finite input */
+  FMMG_OOM = 2,           /* host or device allocation failed */
+  FMMG_CUDA_ERROR = 3,    /* a CUDA call or kernel launch failed */
+  FMMG_TIMEOUT = 4,       /* reserved: a bounded device wait ran out */
+  FMMG_NOT_SUPPORTED = 5, /* kernel type / np / mode not built */
+  FMMG_STATE = 6          /* call order violated (e.g. evaluate before setup) */
+} fmmg_status;
+
+/* Kernel ids of fmm3d_mpi/kernel3d_mpi.hpp:37-78 that setup() accepts
+ * (fmm3d_mpi/fmm3d_setup_mpi.cpp:113-126). */
+enum {
+  FMMG_KNL_LAP_S_U = 111, FMMG_KNL_LAP_D_U = 121,
+  FMMG_KNL_STK_S_U = 311, FMMG_KNL_STK_S_P = 312,
+  FMMG_KNL_STK_D_U = 321, FMMG_KNL_STK_D_P = 322,
+  FMMG_KNL_NAV_S_U = 511, FMMG_KNL_NAV_D_U = 521
+};
+
+/* Arithmetic of an evaluate. */
+typedef enum {
+  FMMG_PREC_FP64 = 0,  /* plain form: FP64 throughout */
+  FMMG_PREC_MIXED = 1  /* FP32 bulk sums and M2L, FP64 final accumulation */
+} fmmg_precision;
+
+/* Options of FMM3d_MPI and its Let3d_MPI, as plain fields:
+ *   np          -fmm3d_np            (fmm3d_mpi/fmm3d_setup_mpi.cpp:48)
+ *   pts_max     -fmm3d_let3d_ptsMax  (fmm3d_mpi/let3d_mpi.cpp:231)
+ *   max_level   -fmm3d_let3d_maxLevel (fmm3d_mpi/let3d_mpi.cpp:232)
+ *   kernel_type -kt, coefs {mu, nu}  (fmm3d_mpi/tt0.cpp:164-183)
+ *   ctr, root_level                  (FMM3d_MPI::ctr()/rootLevel(), fmm3d_mpi.hpp:177-179)
+ * device < 0 builds the host plan only (tree, lists, operators): evaluate is
+ * then refused with FMMG_STATE.  stream == NULL makes the handle create its own
+ * non-blocking stream. */
+typedef struct {
+  int kernel_type;
+  double coefs[2];
+  int np;
+  int pts_max;
+  int max_level;
+  double ctr[3];
+  int root_level;
+  int device;
+  void* stream; /* cudaStream_t */
+} fmmg_options;
+
+typedef struct fmmg_handle fmmg_handle;
+
+/* Fills *opt with the reference defaults: Laplace single layer, coefs {1, 0.25}
+ * (tt0.cpp:179-183), np 6 (fmm3d_mpi.cpp:33), ptsMax 150 and maxLevel 30
+ * (options_0:47-48), root box [0,1]^3 as ctr 0.5 / rootLevel 1 (tt0.cpp:435-436),
+ * device 0. */
+fmmg_status fmmg_default_options(fmmg_options* opt);
+
+/* new FMM3d_MPI + knl()/np()/ctr()/rootLevel() setters. */
+fmmg_status fmmg_create(const fmmg_options* opt, fmmg_handle** out);
+
+/* FMM3d_MPI::setup() (fmm3d_mpi/fmm3d_setup_mpi.cpp:41-567): builds the
+ * adaptive octree over the sources, bins the targets, builds the U/V/W/X lists
+ * (fmm3d_mpi/let3d_mpi.cpp:1637-1768) and their device CSR forms, the
+ * operators, and uploads everything.  src_nrm may be NULL for single-layer
+ * kernels.  All points must lie in the closed root box; n_src >= 1, n_trg >= 0. */
+fmmg_status fmmg_setup(fmmg_handle* h, int64_t n_src, const double* src_xyz, const double* src_nrm,
+                       int64_t n_trg, const double* trg_xyz);
+
+/* FMM3d_MPI::evaluate(srcDen, trgVal) (fmm3d_mpi/fmm3d_eval_mpi.cpp:396-1515)
+ * on HOST buffers: src_den [n_src*srcDOF], trg_val [n_trg*trgDOF].  Copies in,
+ * runs every stage on the GPU, copies out and synchronises. */
+fmmg_status fmmg_evaluate(fmmg_handle* h, const double* src_den, double* trg_val);
+
+/* k right-hand sides on DEVICE buffers: d_src_den [k][n_src*srcDOF],
+ * d_trg_val [k][n_trg*trgDOF], caller order.  Enqueued on the handle's stream;
+ * returns without synchronising. */
+fmmg_status fmmg_evaluate_device(fmmg_handle* h, int k, const double* d_src_den, double* d_trg_val,
+                                 int precision);
+
+/* Waits for all work enqueued on the handle's stream. */
+fmmg_status fmmg_synchronize(fmmg_handle* h);
+
+/* Like fmmg_evaluate_device with k = 1 but only the stages in stage_mask
+ * (bit 0 upward S2M/M2M/C2E, 1 U-list, 2 V-list, 3 W-list, 4 X-list,
+ * 5 downward L2L/C2E/L2T) -- the reference's per-stage switches exposed for
+ * stage-level checks. */
+fmmg_status fmmg_evaluate_stages(fmmg_handle* h, const double* d_src_den, double* d_trg_val,
+                                 int precision, int stage_mask);
+
+/* FMM3d_MPI::check() (fmm3d_mpi/fmm3d_check_mpi.cpp:34-172): dense FP64 sums
+ * on the GPU at n_chk caller-order target indices, compared with trg_val
+ * (host, caller order).  Returns the relative L2 error and the max abs error;
+ * dense_out (host, [n_chk*trgDOF]) may be NULL. */
+fmmg_status fmmg_check(fmmg_handle* h, const double* src_den, const double* trg_val, int64_t n_chk,
+                       const int64_t* chk_idx, double* rel_l2, double* max_abs, double* dense_out);
+
+/* Sizes: srcDOF, trgDOF, number of tree nodes, leaves, maximum depth. */
+fmmg_status fmmg_info(const fmmg_handle* h, int* src_dof, int* trg_dof, int64_t* n_nodes,
+                      int64_t* n_leaves, int* max_depth);
+
+/* Per-stage device time of the last evaluate, milliseconds, in the order of
+ * the PETSc log events (fmm3d_mpi/manage_petsc_events.cpp:77-140): upward,
+ * U-list, V-list, W-list, X-list, downward (incl. L2T), total.  n >= 7. */
+fmmg_status fmmg_stage_times(const fmmg_handle* h, double* ms, int n);
+
+/* Per-kernel device time of the last timed evaluate, milliseconds, n >= 12:
+ * prep (density gather + clears), S2M, upward GEMMs (M2M + C2E), near-field
+ * P2P (U, direct W and X), M2L forward FFT, M2L Hadamard, M2L inverse FFT,
+ * W-list M2T, X-list S2L, downward GEMMs (L2L + C2E), L2T, value scatter. */
+fmmg_status fmmg_kernel_times(const fmmg_handle* h, double* ms, int n);
+
+/* Algorithmic work of one single-RHS evaluate, from the plan (n >= 16):
+ * kernel-pair counts of the near-field P2P, S2M, S2L, M2T and L2T sums;
+ * M2L source spectra, target spectra, target parents, (parent, neighbour)
+ * pairs and V-list interactions; FLOPs of the upward and downward GEMMs;
+ * spectrum length, equivalent-kernel source and target DOF, node count. */
+fmmg_status fmmg_plan_stats(const fmmg_handle* h, int64_t* stats, int n);
+
+/* Number of this library's kernels launched by the last evaluate call. */
+fmmg_status fmmg_launch_count(const fmmg_handle* h, int64_t* n);
+
+/* on != 0: every later evaluate records per-kernel CUDA events on the
+ * handle's stream and waits for them (fmmg_evaluate always does). */
+fmmg_status fmmg_set_timing(fmmg_handle* h, int on);
+
+/* Host-plan introspection (valid after setup, also with device < 0).
+ * which: 0 U, 1 V, 2 W, 3 X lists in the reference form.  node_rec receives
+ * per node {depth, path x, path y, path z, parent, first child, tag bits,
+ * sources in subtree, targets in subtree}; ptr has n_nodes+1 entries; idx
+ * entries are node ids of this handle's numbering.  NULL buffers only size.
+ * Tag bits follow fmm3d_mpi/let3d_mpi.hpp:28-39 (1 contributor, 2 user,
+ * 4 evaluator, 16 has-sources). */
+fmmg_status fmmg_tree(const fmmg_handle* h, int32_t* node_rec, int64_t* perm_src, int64_t* perm_trg);
+fmmg_status fmmg_lists(const fmmg_handle* h, int which, int64_t* ptr, int32_t* idx, int64_t* total);
+
+/* Operator tables built by this handle.  which: 0 UC->UE pseudo-inverse,
+ * 1 UE->UC (octant idx 0..7), 2 DC->DE pseudo-inverse, 3 DE->DC (octant 0..7),
+ * 4 UE->DC translation spectrum (idx 0..315, complex as pairs).  Matrices are
+ * column-major as the reference NumMat (common/nummat.hpp:96-105); spectra use
+ * the FFTW r2c layout.  *count receives the number of doubles.  With set != NULL
+ * the table is replaced (before the next evaluate) -- used to run the GPU path
+ * on an externally supplied operator set. */
+fmmg_status fmmg_operator(fmmg_handle* h, int which, int idx, double* get, const double* set,
+                          int64_t* count);
+
+/* Message of the last failure on h (or of the last failed fmmg_create when
+ * h == NULL).  Never NULL. */
+const char* fmmg_last_error(const fmmg_handle* h);
+
+fmmg_status fmmg_destroy(fmmg_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FMMG_H_ */
