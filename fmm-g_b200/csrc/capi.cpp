@@ -23,6 +23,7 @@ struct fmmg_handle {
   bool opsDirty = false;
   bool timing = false;
   int64_t launches = 0;
+  int hostPrecision = FMMG_PREC_FP64;
   fmmg::Plan plan;
   fmmg::DevState dev;
   double* dDenIO = nullptr;
@@ -205,7 +206,6 @@ fmmg_status fmmg_evaluate_stages(fmmg_handle* h, const double* dDen, double* dVa
   if (!dDen || (!dVal && h->plan.nt > 0)) return fail(h, FMMG_INVALID_ARG, "NULL density or value pointer");
   if (precision != FMMG_PREC_FP64 && precision != FMMG_PREC_MIXED)
     return fail(h, FMMG_INVALID_ARG, "unknown precision");
-  if (precision == FMMG_PREC_MIXED) return fail(h, FMMG_NOT_SUPPORTED, "mixed precision is not built yet");
   try {
     std::string e = fmmg::dev_evaluate(h->plan, h->dev, dDen, dVal, precision, mask & 63, h->timing, nullptr);
     if (!e.empty()) return fail(h, FMMG_CUDA_ERROR, e);
@@ -222,10 +222,15 @@ fmmg_status fmmg_evaluate_device(fmmg_handle* h, int k, const double* dDen, doub
   if (!dDen || (!dVal && h->plan.nt > 0)) return fail(h, FMMG_INVALID_ARG, "NULL density or value pointer");
   if (precision != FMMG_PREC_FP64 && precision != FMMG_PREC_MIXED)
     return fail(h, FMMG_INVALID_ARG, "unknown precision");
-  if (precision == FMMG_PREC_MIXED) return fail(h, FMMG_NOT_SUPPORTED, "mixed precision is not built yet");
   try {
     const int64_t sdn = h->plan.ns * h->plan.sd, tdn = h->plan.nt * h->plan.td;
     h->launches = 0;
+    if (precision == FMMG_PREC_MIXED) {
+      std::string e = fmmg::dev_evaluate_mixed(h->plan, h->dev, dDen, dVal, k, 63, h->timing, nullptr);
+      if (!e.empty()) return fail(h, e.find("cudaMalloc") != std::string::npos ? FMMG_OOM : FMMG_CUDA_ERROR, e);
+      h->launches = h->dev.lastLaunches;
+      return FMMG_OK;
+    }
     for (int r = 0; r < k; r++) {
       std::string e = fmmg::dev_evaluate(h->plan, h->dev, dDen + r * sdn, dVal + r * tdn, precision, 63,
                                          h->timing, nullptr);
@@ -255,7 +260,7 @@ fmmg_status fmmg_evaluate(fmmg_handle* h, const double* den, double* val) {
     const size_t bo = sizeof(double) * (size_t)h->plan.nt * h->plan.td;
     cudaError_t ce = cudaMemcpyAsync(h->dDenIO, den, bi, cudaMemcpyHostToDevice, st);
     if (ce != cudaSuccess) return fail(h, FMMG_CUDA_ERROR, cudaGetErrorString(ce));
-    std::string e = fmmg::dev_evaluate(h->plan, h->dev, h->dDenIO, h->dValIO, FMMG_PREC_FP64, 63, true, nullptr);
+    std::string e = fmmg::dev_evaluate(h->plan, h->dev, h->dDenIO, h->dValIO, h->hostPrecision, 63, true, nullptr);
     if (!e.empty()) return fail(h, FMMG_CUDA_ERROR, e);
     h->launches = h->dev.lastLaunches;
     if (bo) {
@@ -363,6 +368,13 @@ fmmg_status fmmg_plan_stats(const fmmg_handle* h, int64_t* st, int n) {
 fmmg_status fmmg_launch_count(const fmmg_handle* h, int64_t* n) {
   if (!h || !n) return FMMG_INVALID_ARG;
   *n = h->launches;
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_set_precision(fmmg_handle* h, int precision) {
+  if (!h) return fail(nullptr, FMMG_INVALID_ARG, "handle is NULL");
+  if (precision != FMMG_PREC_FP64 && precision != FMMG_PREC_MIXED) return fail(h, FMMG_INVALID_ARG, "precision");
+  h->hostPrecision = precision;
   return FMMG_OK;
 }
 

@@ -55,6 +55,15 @@ struct DevState {
   // per-evaluate work arrays
   double *den = nullptr, *val = nullptr, *uchk = nullptr, *uden = nullptr, *dchk = nullptr, *dden = nullptr;
   double2 *effDen = nullptr, *effVal = nullptr;
+  // mixed-precision work arrays and FP32 operator copies (allocated on first use)
+  float *uchk32 = nullptr, *uden32 = nullptr, *dchk32 = nullptr, *dden32 = nullptr;
+  float2 *effDen32 = nullptr, *effVal32 = nullptr;
+  float *uc2ue32 = nullptr, *m2m32 = nullptr, *dc2de32 = nullptr, *l2l32 = nullptr;
+  float2* m2lT32 = nullptr;
+  double *denK = nullptr, *valK = nullptr;  // permuted densities / values of a RHS chunk
+  bool mixedReady = false, mixedOpsStale = true;
+  int mixedK = 0;                           // right-hand sides the mixed arrays hold
+  double mixedBudgetBytes = 48e9;           // device bytes for per-density work arrays
   // dense check scratch
   double *chkPos = nullptr, *chkOut = nullptr;
   size_t chkCap = 0;
@@ -78,6 +87,10 @@ void dev_free(DevState& D);
 // run one right-hand side; den/val are device arrays in caller order
 std::string dev_evaluate(const Plan& P, DevState& D, const double* dDenCaller, double* dValCaller,
                          int precision, int stageMask, bool timed, LaunchStats* st);
+// k right-hand sides in caller order ([k][n*DOF]); with timed, the kernel
+// times are those of the last chunk of right-hand sides
+std::string dev_evaluate_mixed(const Plan& P, DevState& D, const double* dDenCaller, double* dValCaller, int k,
+                               int stageMask, bool timed, LaunchStats* st);
 // dense FP64 sums at device positions (caller-order source arrays are the
 // permuted copies held on the device plus the permuted density)
 std::string dev_dense(const Plan& P, DevState& D, const double* dDenCaller, int64_t nchk,

@@ -169,6 +169,24 @@ FMMG_UNROLL
   }
 }
 
+// KB right-hand sides at once: acc[r*TD + t] += sum_s K[t][s] den[r*SD + s];
+// the kernel block is evaluated once and applied to every density.
+template <int KT, int KB, typename R, typename A>
+FMMG_HD void kaccum_multi(R x, R y, R z, const R* n, const R* den, A* acc, R mu, R ve) {
+  constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD;
+  R K[SD * TD];
+  if (!kblock<KT, R>(x, y, z, n, K, mu, ve)) return;
+FMMG_UNROLL
+  for (int r = 0; r < KB; r++)
+FMMG_UNROLL
+    for (int t = 0; t < TD; t++) {
+      R s = R(0);
+FMMG_UNROLL
+      for (int c = 0; c < SD; c++) s += K[t * SD + c] * den[r * SD + c];
+      acc[r * TD + t] += s;
+    }
+}
+
 // Run-time dispatch to a functor templated on the kernel id.
 #define FMMG_DISPATCH_KT(kt, KTV, ...)                                  \
   switch (kt) {                                                         \

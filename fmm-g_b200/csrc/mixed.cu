@@ -1,0 +1,918 @@
+// mixed.cu -- the mixed-precision, multi-right-hand-side evaluate
+// (FMMG_PREC_MIXED).
+//
+// Same stage sequence and work lists as the FP64 form (stages.cu); the bulk
+// arithmetic is FP32 and every kernel handles a block of KB right-hand sides
+// per launch (grid.y or the row index runs over the blocks), so geometry,
+// kernel evaluations, operator tiles and M2L translation spectra are loaded
+// once per block instead of once per density:
+//  * direct sums (near-field P2P, S2M, S2L, M2T, L2T) evaluate the kernel in
+//    FP32 on coordinates taken relative to the centre of the target box (the
+//    subtraction happens in FP64 before rounding), add each shared-memory tile
+//    of at most 128 sources in FP32 and carry the tile sums in FP64; target
+//    values are accumulated in FP64;
+//  * the equivalent-density GEMMs and the spectral M2L (FFTs and Hadamard
+//    products) run in FP32 with FP32 operator tables.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "cuda_common.cuh"
+#include "engine.hpp"
+#include "kernels.hpp"
+
+namespace fmmg {
+
+__constant__ int8_t c_transId32[343];
+
+constexpr int MX_THREADS = 128;
+constexpr int MX_TILE = 128;
+constexpr int MX_MAXE = 256;
+
+// fill eBeg/ePre for entries [ec, ec+ne) and return the total source count
+__device__ __forceinline__ int load_entries(const int32_t* __restrict__ idx, int64_t ec, int ne, int self,
+                                            const int64_t* __restrict__ srcBeg, const int64_t* __restrict__ srcCnt,
+                                            int64_t* eBeg, int32_t* ePre) {
+  __syncthreads();
+  for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+    int s = idx ? idx[ec + e] : self;
+    eBeg[e] = srcBeg[s];
+    ePre[e + 1] = (int32_t)srcCnt[s];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ePre[0] = 0;
+    for (int e = 0; e < ne; e++) ePre[e + 1] += ePre[e];
+  }
+  __syncthreads();
+  return ePre[ne];
+}
+
+__device__ __forceinline__ int64_t entry_source(int j, int ne, const int64_t* eBeg, const int32_t* ePre) {
+  int lo = 0, hi = ne;
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (ePre[mid] <= j) lo = mid; else hi = mid;
+  }
+  return eBeg[lo] + (j - ePre[lo]);
+}
+
+// Shared epilogue of the target-side kernels: reduce the S source splits of
+// each target and add the KB x TD values into val (FP64).
+template <int TD, int KB>
+__device__ __forceinline__ void reduce_store(double* sRed, const double* acc, int tid, int tl, int sp, int TG, int S,
+                                             bool act, double* __restrict__ val, int64_t trgIdx, int rhs0, int nrhs,
+                                             int64_t valStride) {
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < TD * KB; c++) sRed[tid * TD * KB + c] = acc[c];
+  __syncthreads();
+  if (sp == 0 && act) {
+#pragma unroll
+    for (int r = 0; r < KB; r++) {
+      if (rhs0 + r >= nrhs) break;
+#pragma unroll
+      for (int c = 0; c < TD; c++) {
+        double s = 0;
+        for (int k = 0; k < S; k++) s += sRed[(tl + k * TG) * TD * KB + r * TD + c];
+        val[(int64_t)(rhs0 + r) * valStride + trgIdx * TD + c] += s;
+      }
+    }
+  }
+}
+
+// near field: U-list, direct W and X entries; grid (evaluator leaves, RHS blocks)
+template <int KT, int KB>
+__global__ void __launch_bounds__(MX_THREADS)
+    k_p2p_near32(const int32_t* __restrict__ rows, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                 const int64_t* __restrict__ srcBeg, const int64_t* __restrict__ srcCnt,
+                 const int64_t* __restrict__ trgBeg, const int64_t* __restrict__ trgCnt,
+                 const double* __restrict__ src, const double* __restrict__ nrm, const double* __restrict__ den,
+                 int64_t denStride, const double* __restrict__ trg, const double* __restrict__ ctr,
+                 double* __restrict__ val, int64_t valStride, int nrhs, float mu, float ve) {
+  constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD, NRM = KTraits<KT>::NRM;
+  __shared__ float sPos[MX_TILE * 3];
+  __shared__ float sNrm[NRM ? MX_TILE * 3 : 1];
+  __shared__ float sDen[MX_TILE * SD * KB];
+  __shared__ int64_t eBeg[MX_MAXE];
+  __shared__ int32_t ePre[MX_MAXE + 1];
+  __shared__ double sRed[MX_THREADS * TD * KB];
+  const int row = blockIdx.x;
+  const int rhs0 = blockIdx.y * KB;
+  const int g = rows[row];
+  const int64_t tb = trgBeg[g], tn = trgCnt[g];
+  const int64_t e0 = ptr[row], e1 = ptr[row + 1];
+  const double cx = ctr[3 * g], cy = ctr[3 * g + 1], cz = ctr[3 * g + 2];
+  const int tid = threadIdx.x;
+  const int TG = tn <= 32 ? 32 : (tn <= 64 ? 64 : 128);
+  const int S = MX_THREADS / TG;
+  const int tl = tid % TG, sp = tid / TG;
+  for (int64_t t0 = 0; t0 < tn; t0 += TG) {
+    const int64_t t = t0 + tl;
+    const bool act = t < tn;
+    float tx = 0, ty = 0, tz = 0;
+    if (act) {
+      tx = (float)(trg[3 * (tb + t)] - cx);
+      ty = (float)(trg[3 * (tb + t) + 1] - cy);
+      tz = (float)(trg[3 * (tb + t) + 2] - cz);
+    }
+    double acc[TD * KB];
+#pragma unroll
+    for (int c = 0; c < TD * KB; c++) acc[c] = 0.0;
+    for (int64_t ec = e0; ec < e1; ec += MX_MAXE) {
+      const int ne = (int)min((int64_t)MX_MAXE, e1 - ec);
+      const int total = load_entries(idx, ec, ne, 0, srcBeg, srcCnt, eBeg, ePre);
+      for (int base = 0; base < total; base += MX_TILE) {
+        const int cnt = min(MX_TILE, total - base);
+        __syncthreads();
+        for (int i = tid; i < cnt; i += MX_THREADS) {
+          const int64_t s = entry_source(base + i, ne, eBeg, ePre);
+          sPos[3 * i] = (float)(src[3 * s] - cx);
+          sPos[3 * i + 1] = (float)(src[3 * s + 1] - cy);
+          sPos[3 * i + 2] = (float)(src[3 * s + 2] - cz);
+          if (NRM) {
+            sNrm[3 * i] = (float)nrm[3 * s];
+            sNrm[3 * i + 1] = (float)nrm[3 * s + 1];
+            sNrm[3 * i + 2] = (float)nrm[3 * s + 2];
+          }
+#pragma unroll
+          for (int r = 0; r < KB; r++)
+#pragma unroll
+            for (int c = 0; c < SD; c++)
+              sDen[(i * KB + r) * SD + c] =
+                  rhs0 + r < nrhs ? (float)den[(int64_t)(rhs0 + r) * denStride + s * SD + c] : 0.f;
+        }
+        __syncthreads();
+        if (act) {
+          float part[TD * KB];
+#pragma unroll
+          for (int c = 0; c < TD * KB; c++) part[c] = 0.f;
+          for (int i = sp; i < cnt; i += S)
+            kaccum_multi<KT, KB, float, float>(tx - sPos[3 * i], ty - sPos[3 * i + 1], tz - sPos[3 * i + 2],
+                                               NRM ? &sNrm[3 * i] : nullptr, &sDen[i * KB * SD], part, mu, ve);
+#pragma unroll
+          for (int c = 0; c < TD * KB; c++) acc[c] += (double)part[c];
+        }
+      }
+    }
+    reduce_store<TD, KB>(sRed, acc, tid, tl, sp, TG, S, act, val, tb + t, rhs0, nrhs, valStride);
+  }
+}
+
+// equivalent surfaces -> targets: L2T (own DE surface, downward density) and
+// M2T (UE surfaces of the W nodes, upward densities), equivalent kernel
+template <int KM, int KB>
+__global__ void __launch_bounds__(MX_THREADS)
+    k_e2t32(const int32_t* __restrict__ rows, const int64_t* __restrict__ farPtr, const int32_t* __restrict__ farIdx,
+            int useOwn, int useFar, const int32_t* __restrict__ depth, const double* __restrict__ ctr,
+            const double* __restrict__ rad, const double* __restrict__ samUE, int nUE,
+            const double* __restrict__ samDE, int nDE, const float* __restrict__ uden,
+            const float* __restrict__ dden, int64_t rhsStrideU, int64_t rhsStrideD,
+            const int64_t* __restrict__ trgBeg, const int64_t* __restrict__ trgCnt, const double* __restrict__ trg,
+            double* __restrict__ val, int64_t valStride, int nrhs, float mu, float ve) {
+  constexpr int SD = KTraits<KM>::SD, TD = KTraits<KM>::TD;
+  __shared__ float sPos[MX_TILE * 3];
+  __shared__ float sDen[MX_TILE * SD * KB];
+  __shared__ double sRed[MX_THREADS * TD * KB];
+  const int row = blockIdx.x;
+  const int rhs0 = blockIdx.y * KB;
+  const int g = rows[row];
+  const int64_t tb = trgBeg[g], tn = trgCnt[g];
+  const double gx = ctr[3 * g], gy = ctr[3 * g + 1], gz = ctr[3 * g + 2];
+  const int tid = threadIdx.x;
+  const int TG = tn <= 32 ? 32 : (tn <= 64 ? 64 : 128);
+  const int S = MX_THREADS / TG;
+  const int tl = tid % TG, sp = tid / TG;
+  const int own = (useOwn && depth[g] >= 2) ? 1 : 0;
+  const int64_t f0 = farPtr[row], nf = useFar ? farPtr[row + 1] - f0 : 0;
+  for (int64_t t0 = 0; t0 < tn; t0 += TG) {
+    const int64_t t = t0 + tl;
+    const bool act = t < tn;
+    float tx = 0, ty = 0, tz = 0;
+    if (act) {
+      tx = (float)(trg[3 * (tb + t)] - gx);
+      ty = (float)(trg[3 * (tb + t) + 1] - gy);
+      tz = (float)(trg[3 * (tb + t) + 2] - gz);
+    }
+    double acc[TD * KB];
+#pragma unroll
+    for (int c = 0; c < TD * KB; c++) acc[c] = 0.0;
+    for (int64_t e = 0; e < own + nf; e++) {
+      const bool isOwn = e < own;
+      const int node = isOwn ? g : farIdx[f0 + e - own];
+      const double* sam = isOwn ? samDE : samUE;
+      const int ns = isOwn ? nDE : nUE;
+      const float* dsrc = isOwn ? dden + (int64_t)node * ns * SD : uden + (int64_t)node * ns * SD;
+      const int64_t rstr = isOwn ? rhsStrideD : rhsStrideU;
+      const double ox = ctr[3 * node] - gx, oy = ctr[3 * node + 1] - gy, oz = ctr[3 * node + 2] - gz;
+      const double r = rad[node];
+      for (int base = 0; base < ns; base += MX_TILE) {
+        const int cnt = min(MX_TILE, ns - base);
+        __syncthreads();
+        for (int i = tid; i < cnt; i += MX_THREADS) {
+          const int j = base + i;
+          sPos[3 * i] = (float)(ox + r * sam[3 * j]);
+          sPos[3 * i + 1] = (float)(oy + r * sam[3 * j + 1]);
+          sPos[3 * i + 2] = (float)(oz + r * sam[3 * j + 2]);
+#pragma unroll
+          for (int q = 0; q < KB; q++)
+#pragma unroll
+            for (int c = 0; c < SD; c++)
+              sDen[(i * KB + q) * SD + c] = rhs0 + q < nrhs ? dsrc[(rhs0 + q) * rstr + (int64_t)j * SD + c] : 0.f;
+        }
+        __syncthreads();
+        if (act) {
+          float part[TD * KB];
+#pragma unroll
+          for (int c = 0; c < TD * KB; c++) part[c] = 0.f;
+          for (int i = sp; i < cnt; i += S)
+            kaccum_multi<KM, KB, float, float>(tx - sPos[3 * i], ty - sPos[3 * i + 1], tz - sPos[3 * i + 2], nullptr,
+                                               &sDen[i * KB * SD], part, mu, ve);
+#pragma unroll
+          for (int c = 0; c < TD * KB; c++) acc[c] += (double)part[c];
+        }
+      }
+    }
+    reduce_store<TD, KB>(sRed, acc, tid, tl, sp, TG, S, act, val, tb + t, rhs0, nrhs, valStride);
+  }
+}
+
+// point sources -> check surface of a box (S2M onto UC, S2L onto DC), FP32
+// out.  One thread per surface point (a CTA of MX_SURF threads, up to 512
+// points: np <= 8).
+constexpr int MX_SURF = 512;
+template <int KT, int KB>
+__global__ void __launch_bounds__(MX_SURF)
+    k_src2surf32(const int32_t* __restrict__ rows, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                 const int64_t* __restrict__ srcBeg, const int64_t* __restrict__ srcCnt,
+                 const double* __restrict__ src, const double* __restrict__ nrm, const double* __restrict__ den,
+                 int64_t denStride, const double* __restrict__ ctr, const double* __restrict__ rad,
+                 const double* __restrict__ sam, int nSurf, float* __restrict__ out, int64_t ldo,
+                 int64_t outRhsStride, int nrhs, float mu, float ve) {
+  constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD, NRM = KTraits<KT>::NRM;
+  __shared__ float sPos[MX_TILE * 3];
+  __shared__ float sNrm[NRM ? MX_TILE * 3 : 1];
+  __shared__ float sDen[MX_TILE * SD * KB];
+  __shared__ int64_t eBeg[MX_MAXE];
+  __shared__ int32_t ePre[MX_MAXE + 1];
+  const int row = blockIdx.x;
+  const int rhs0 = blockIdx.y * KB;
+  const int g = rows[row];
+  const int tid = threadIdx.x;
+  const double cx = ctr[3 * g], cy = ctr[3 * g + 1], cz = ctr[3 * g + 2], r = rad[g];
+  const bool act = tid < nSurf;
+  const float px = act ? (float)(r * sam[3 * tid]) : 0.f;
+  const float py = act ? (float)(r * sam[3 * tid + 1]) : 0.f;
+  const float pz = act ? (float)(r * sam[3 * tid + 2]) : 0.f;
+  double acc[TD * KB];
+#pragma unroll
+  for (int c = 0; c < TD * KB; c++) acc[c] = 0.0;
+  const int64_t e0 = ptr ? ptr[row] : 0, e1 = ptr ? ptr[row + 1] : 1;
+  for (int64_t ec = e0; ec < e1; ec += MX_MAXE) {
+    const int ne = (int)min((int64_t)MX_MAXE, e1 - ec);
+    const int total = load_entries(ptr ? idx : nullptr, ec, ne, g, srcBeg, srcCnt, eBeg, ePre);
+    for (int base = 0; base < total; base += MX_TILE) {
+      const int cnt = min(MX_TILE, total - base);
+      __syncthreads();
+      for (int i = tid; i < cnt; i += blockDim.x) {
+        const int64_t s = entry_source(base + i, ne, eBeg, ePre);
+        sPos[3 * i] = (float)(src[3 * s] - cx);
+        sPos[3 * i + 1] = (float)(src[3 * s + 1] - cy);
+        sPos[3 * i + 2] = (float)(src[3 * s + 2] - cz);
+        if (NRM) {
+          sNrm[3 * i] = (float)nrm[3 * s];
+          sNrm[3 * i + 1] = (float)nrm[3 * s + 1];
+          sNrm[3 * i + 2] = (float)nrm[3 * s + 2];
+        }
+#pragma unroll
+        for (int q = 0; q < KB; q++)
+#pragma unroll
+          for (int c = 0; c < SD; c++)
+            sDen[(i * KB + q) * SD + c] =
+                rhs0 + q < nrhs ? (float)den[(int64_t)(rhs0 + q) * denStride + s * SD + c] : 0.f;
+      }
+      __syncthreads();
+      if (act) {
+        float part[TD * KB];
+#pragma unroll
+        for (int c = 0; c < TD * KB; c++) part[c] = 0.f;
+        for (int i = 0; i < cnt; i++)
+          kaccum_multi<KT, KB, float, float>(px - sPos[3 * i], py - sPos[3 * i + 1], pz - sPos[3 * i + 2],
+                                             NRM ? &sNrm[3 * i] : nullptr, &sDen[i * KB * SD], part, mu, ve);
+#pragma unroll
+        for (int c = 0; c < TD * KB; c++) acc[c] += (double)part[c];
+      }
+    }
+  }
+  if (act)
+#pragma unroll
+    for (int q = 0; q < KB; q++) {
+      if (rhs0 + q >= nrhs) break;
+#pragma unroll
+      for (int c = 0; c < TD; c++)
+        out[(rhs0 + q) * outRhsStride + (int64_t)g * ldo + (int64_t)tid * TD + c] += (float)acc[q * TD + c];
+    }
+}
+
+// ------------------------------------------------------------------ FP32 row GEMM
+// Y[row] = beta*Y[row] + ys .* (W X[row]) as k_gemm_rows, FP32 operands and
+// accumulation.  Rows run over (right-hand side, node): row r uses node
+// rows[r % nrows] of density r / nrows, so one W tile serves every density.
+constexpr int G32_BM = 64, G32_BN = 64, G32_BK = 32;
+struct Scale4f {
+  float v[4];
+  int mod;
+};
+
+__global__ void __launch_bounds__(256)
+    k_gemm_rows32(int nrows, int nrhs, const int32_t* __restrict__ rows, const int32_t* __restrict__ chd,
+                  int xChild, int yChild, const float* __restrict__ X, int64_t ldx, int64_t xRhs,
+                  const float* __restrict__ W, float* __restrict__ Y, int64_t ldy, int64_t yRhs, int K, int N,
+                  Scale4f xs, Scale4f ys, float beta) {
+  __shared__ float As[G32_BK][G32_BM + 4];
+  __shared__ float Bs[G32_BK][G32_BN + 4];
+  __shared__ const float* xrow[G32_BM];
+  __shared__ float* yrow[G32_BM];
+  const int tid = threadIdx.x;
+  const int r0 = blockIdx.x * G32_BM, n0 = blockIdx.y * G32_BN;
+  if (tid < G32_BM) {
+    int r = r0 + tid;
+    if (r < nrows * nrhs) {
+      int q = r / nrows;
+      int node = rows[r - q * nrows];
+      xrow[tid] = X + q * xRhs + (int64_t)(xChild ? chd[node] : node) * ldx;
+      yrow[tid] = Y + q * yRhs + (int64_t)(yChild ? chd[node] : node) * ldy;
+    } else {
+      xrow[tid] = nullptr;
+      yrow[tid] = nullptr;
+    }
+  }
+  __syncthreads();
+  const int tr = tid / 16, tc = tid % 16;
+  float acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
+  for (int k0 = 0; k0 < K; k0 += G32_BK) {
+#pragma unroll
+    for (int l = 0; l < 8; l++) {
+      int e = tid + l * 256;
+      int r = e / G32_BK, k = e % G32_BK;
+      const float* xr = xrow[r];
+      float v = 0.f;
+      if (xr && k0 + k < K) v = xr[k0 + k] * xs.v[(k0 + k) % xs.mod];
+      As[k][r] = v;
+    }
+#pragma unroll
+    for (int l = 0; l < 8; l++) {
+      int e = tid + l * 256;
+      int n = e / G32_BK, k = e % G32_BK;
+      float v = 0.f;
+      if (n0 + n < N && k0 + k < K) v = W[(int64_t)(n0 + n) * K + k0 + k];
+      Bs[k][n] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < G32_BK; k++) {
+      float a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) a[i] = As[k][tr + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; j++) b[j] = Bs[k][tc + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    float* yr = yrow[tr + 16 * i];
+    if (!yr) continue;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      int n = n0 + tc + 16 * j;
+      if (n < N) {
+        float v = acc[i][j] * ys.v[n % ys.mod];
+        yr[n] = beta == 0.f ? v : beta * yr[n] + v;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ FP32 M2L
+// grid (source slots, right-hand sides)
+template <int NP>
+__global__ void __launch_bounds__(128)
+    k_m2l_fwd32(const int32_t* __restrict__ nodes, const int32_t* __restrict__ depth, int rootLevel, Scale4 deg,
+                int sdm, const float* __restrict__ uden, int64_t udenRhs, const int32_t* __restrict__ ijk, int nUE,
+                float2* __restrict__ effDen, int64_t effRhs, int nEff) {
+  using F = FftDims<NP>;
+  constexpr int N = F::N, NH = F::NH, H = F::H;
+  __shared__ float cube[NP * NP * NP];
+  __shared__ float2 X1[NP * NP * NH];
+  __shared__ float2 X2[NP * N * NH];
+  __shared__ float2 tw[N];
+  const int slot = blockIdx.x;
+  const int v = nodes[slot];
+  const int tid = threadIdx.x;
+  if (tid < N) {
+    double s, c;
+    sincospi(2.0 * tid / N, &s, &c);
+    tw[tid] = make_float2((float)c, (float)-s);
+  }
+  const int l = depth[v] + rootLevel;
+  const float* ud = uden + blockIdx.y * udenRhs + (int64_t)v * nUE * sdm;
+  float2* out = effDen + blockIdx.y * effRhs + (int64_t)slot * nEff * sdm;
+  for (int m = 0; m < sdm; m++) {
+    const float scl = (float)exp2(l * deg.v[m]);
+    for (int i = tid; i < NP * NP * NP; i += blockDim.x) cube[i] = 0.f;
+    __syncthreads();
+    for (int i = tid; i < nUE; i += blockDim.x) {
+      int p = ijk[i];
+      cube[((p >> 16) * NP + ((p >> 8) & 255)) * NP + (p & 255)] = ud[(int64_t)i * sdm + m] * scl;
+    }
+    __syncthreads();
+    for (int e = tid; e < NP * NP * NH; e += blockDim.x) {
+      int kx = e % NH, yb = (e / NH) % NP, zb = e / (NH * NP);
+      float2 s = make_float2(0.f, 0.f);
+      const float* row = &cube[(zb * NP + yb) * NP];
+#pragma unroll
+      for (int xb = 0; xb < NP; xb++) {
+        float2 w = tw[(kx * (xb + H)) % N];
+        s.x += row[xb] * w.x;
+        s.y += row[xb] * w.y;
+      }
+      X1[e] = s;
+    }
+    __syncthreads();
+    for (int e = tid; e < NP * N * NH; e += blockDim.x) {
+      int kx = e % NH, ky = (e / NH) % N, zb = e / (NH * N);
+      float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int yb = 0; yb < NP; yb++) {
+        float2 t = cmul(X1[(zb * NP + yb) * NH + kx], tw[(ky * (yb + H)) % N]);
+        s.x += t.x;
+        s.y += t.y;
+      }
+      X2[e] = s;
+    }
+    __syncthreads();
+    for (int e = tid; e < N * N * NH; e += blockDim.x) {
+      int kx = e % NH, ky = (e / NH) % N, kz = e / (NH * N);
+      float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int zb = 0; zb < NP; zb++) {
+        float2 t = cmul(X2[(zb * N + ky) * NH + kx], tw[(kz * (zb + H)) % N]);
+        s.x += t.x;
+        s.y += t.y;
+      }
+      out[(int64_t)e * sdm + m] = s;
+    }
+    __syncthreads();
+  }
+}
+
+// grid (target parents, 32-frequency chunks, RHS blocks); warp c owns child c;
+// each translation spectrum value is loaded once and applied to KB densities
+template <int SDM, int TDM, int KB>
+__global__ void __launch_bounds__(256)
+    k_m2l_had32(const int32_t* __restrict__ parents, const int64_t* __restrict__ vPtr,
+                const int32_t* __restrict__ vIdx, const int8_t* __restrict__ vOff, const int32_t* __restrict__ chd,
+                const int32_t* __restrict__ srcSlot, const int32_t* __restrict__ trgSlot,
+                const float2* __restrict__ effDen, int64_t denRhs, const float2* __restrict__ T,
+                float2* __restrict__ effVal, int64_t valRhs, int nEff, int nrhs, float nrmfc) {
+  const int b = blockIdx.x;
+  const int P = parents[b];
+  const int c = threadIdx.x >> 5;
+  const int f = blockIdx.y * 32 + (threadIdx.x & 31);
+  const int rhs0 = blockIdx.z * KB;
+  const int t = chd[P] + c;
+  const int ts = trgSlot[t];
+  if (ts < 0) return;
+  const int cx = c >> 2, cy = (c >> 1) & 1, cz = c & 1;
+  float2 acc[KB][TDM];
+#pragma unroll
+  for (int q = 0; q < KB; q++)
+#pragma unroll
+    for (int i = 0; i < TDM; i++) acc[q][i] = make_float2(0.f, 0.f);
+  const bool fin = f < nEff;
+  for (int64_t e = vPtr[b]; e < vPtr[b + 1]; e++) {
+    const int Q = vIdx[e];
+    const int off = vOff[e];
+    const int dx = off / 9 - 1, dy = (off / 3) % 3 - 1, dz = off % 3 - 1;
+    const int q0 = chd[Q];
+#pragma unroll 1
+    for (int c2 = 0; c2 < 8; c2++) {
+      const int s = srcSlot[q0 + c2];
+      if (s < 0) continue;
+      const int rx = 2 * dx + (c2 >> 2) - cx, ry = 2 * dy + ((c2 >> 1) & 1) - cy, rz = 2 * dz + (c2 & 1) - cz;
+      if (max(abs(rx), max(abs(ry), abs(rz))) <= 1) continue;
+      const int id = c_transId32[(rx + 3) * 49 + (ry + 3) * 7 + (rz + 3)];
+      if (!fin) continue;
+      const float2* Tf = T + ((int64_t)id * nEff + f) * (SDM * TDM);
+      float2 tv[SDM * TDM];
+#pragma unroll
+      for (int j = 0; j < SDM * TDM; j++) tv[j] = Tf[j];
+#pragma unroll
+      for (int q = 0; q < KB; q++) {
+        if (rhs0 + q >= nrhs) break;
+        const float2* dp = effDen + (rhs0 + q) * denRhs + ((int64_t)s * nEff + f) * SDM;
+#pragma unroll
+        for (int j = 0; j < SDM; j++) {
+          const float2 d = dp[j];
+#pragma unroll
+          for (int i = 0; i < TDM; i++) {
+            const float2 w = tv[j * TDM + i];
+            acc[q][i].x += w.x * d.x - w.y * d.y;
+            acc[q][i].y += w.x * d.y + w.y * d.x;
+          }
+        }
+      }
+    }
+  }
+  if (fin) {
+#pragma unroll
+    for (int q = 0; q < KB; q++) {
+      if (rhs0 + q >= nrhs) break;
+#pragma unroll
+      for (int i = 0; i < TDM; i++)
+        effVal[(rhs0 + q) * valRhs + ((int64_t)ts * nEff + f) * TDM + i] =
+            make_float2(acc[q][i].x * nrmfc, acc[q][i].y * nrmfc);
+    }
+  }
+}
+
+// grid (target slots, right-hand sides)
+template <int NP>
+__global__ void __launch_bounds__(128)
+    k_m2l_inv32(const int32_t* __restrict__ nodes, const float2* __restrict__ effVal, int64_t valRhs, int nEff,
+                int tdm, const int32_t* __restrict__ ijk, int nDC, float* __restrict__ dchk, int64_t dchkRhs) {
+  using F = FftDims<NP>;
+  constexpr int N = F::N, NH = F::NH, H = F::H;
+  __shared__ float2 Y2[NP * N * NH];
+  __shared__ float2 Y1[NP * NP * NH];
+  __shared__ float2 tw[N];
+  const int slot = blockIdx.x;
+  const int node = nodes[slot];
+  const int tid = threadIdx.x;
+  if (tid < N) {
+    double s, c;
+    sincospi(2.0 * tid / N, &s, &c);
+    tw[tid] = make_float2((float)c, (float)-s);
+  }
+  __syncthreads();
+  const float2* in = effVal + blockIdx.y * valRhs + (int64_t)slot * nEff * tdm;
+  float* dc = dchk + blockIdx.y * dchkRhs + (int64_t)node * nDC * tdm;
+  for (int m = 0; m < tdm; m++) {
+    for (int e = tid; e < NP * N * NH; e += blockDim.x) {
+      int kx = e % NH, ky = (e / NH) % N, zb = e / (NH * N);
+      float2 s = make_float2(0.f, 0.f);
+#pragma unroll 4
+      for (int kz = 0; kz < N; kz++) {
+        float2 t = cmulc(in[((int64_t)(kz * N + ky) * NH + kx) * tdm + m], tw[(kz * (zb + H)) % N]);
+        s.x += t.x;
+        s.y += t.y;
+      }
+      Y2[e] = s;
+    }
+    __syncthreads();
+    for (int e = tid; e < NP * NP * NH; e += blockDim.x) {
+      int kx = e % NH, yb = (e / NH) % NP, zb = e / (NH * NP);
+      float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int ky = 0; ky < N; ky++) {
+        float2 t = cmulc(Y2[(zb * N + ky) * NH + kx], tw[(ky * (yb + H)) % N]);
+        s.x += t.x;
+        s.y += t.y;
+      }
+      Y1[e] = s;
+    }
+    __syncthreads();
+    for (int i = tid; i < nDC; i += blockDim.x) {
+      int p = ijk[i];
+      int a = p & 255, b = (p >> 8) & 255, cc = p >> 16;
+      const float2* y1 = &Y1[(cc * NP + b) * NH];
+      const int x = a + H;
+      float s = 0.f;
+#pragma unroll
+      for (int kx = 0; kx < NH; kx++) {
+        float2 t = cmulc(y1[kx], tw[(kx * x) % N]);
+        s += (kx == 0 || kx == N / 2) ? t.x : 2.f * t.x;
+      }
+      dc[(int64_t)i * tdm + m] += s;
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ launcher
+template <typename T>
+static std::string dalloc(DevState& D, T*& p, size_t n) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
+  if (e != cudaSuccess) return std::string("cudaMalloc: ") + cudaGetErrorString(e);
+  D.allocs.push_back(q);
+  p = (T*)q;
+  return std::string();
+}
+
+// Work arrays for a chunk of kc right-hand sides, and the FP32 operator copies.
+static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
+  const size_t ue = (size_t)P.nUE * P.sdm, uc = (size_t)P.nUC * P.tdm;
+  const size_t de = (size_t)P.nDE * P.sdm, dc = (size_t)P.nDC * P.tdm;
+  if (!D.mixedReady || kc > D.mixedK) {
+    // grow: the old buffers stay in D.allocs until the handle is freed
+    FMMG_TRY(dalloc(D, D.uchk32, (size_t)kc * P.nn * uc));
+    FMMG_TRY(dalloc(D, D.uden32, (size_t)kc * P.nn * ue));
+    FMMG_TRY(dalloc(D, D.dchk32, (size_t)kc * P.nn * dc));
+    FMMG_TRY(dalloc(D, D.dden32, (size_t)kc * P.nn * de));
+    FMMG_TRY(dalloc(D, D.effDen32, (size_t)kc * P.vSrcNodes.size() * P.nEff * P.sdm));
+    FMMG_TRY(dalloc(D, D.effVal32, (size_t)kc * P.vTrgNodes.size() * P.nEff * P.tdm));
+    FMMG_TRY(dalloc(D, D.denK, (size_t)kc * P.ns * P.sd));
+    FMMG_TRY(dalloc(D, D.valK, (size_t)kc * std::max<int64_t>(P.nt, 1) * P.td));
+    if (!D.uc2ue32) {
+      FMMG_TRY(dalloc(D, D.uc2ue32, P.uc2ue.size()));
+      FMMG_TRY(dalloc(D, D.m2m32, P.m2m.size()));
+      FMMG_TRY(dalloc(D, D.dc2de32, P.dc2de.size()));
+      FMMG_TRY(dalloc(D, D.l2l32, P.l2l.size()));
+      FMMG_TRY(dalloc(D, D.m2lT32, P.m2lT.size()));
+    }
+    D.mixedReady = true;
+    D.mixedK = kc;
+  }
+  if (D.mixedOpsStale) {
+    auto put = [&](float* dst, const std::vector<double>& v) -> std::string {
+      std::vector<float> f(v.begin(), v.end());
+      FMMG_CK(cudaMemcpy(dst, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice));
+      return std::string();
+    };
+    FMMG_TRY(put(D.uc2ue32, P.uc2ue));
+    FMMG_TRY(put(D.m2m32, P.m2m));
+    FMMG_TRY(put(D.dc2de32, P.dc2de));
+    FMMG_TRY(put(D.l2l32, P.l2l));
+    std::vector<float2> t(P.m2lT.size());
+    for (size_t i = 0; i < t.size(); i++) t[i] = make_float2((float)P.m2lT[i].real(), (float)P.m2lT[i].imag());
+    FMMG_CK(cudaMemcpy(D.m2lT32, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    int8_t tid[343];
+    for (int i = 0; i < 343; i++) tid[i] = (int8_t)P.transId[i / 49][(i / 7) % 7][i % 7];
+    FMMG_CK(cudaMemcpyToSymbol(c_transId32, tid, sizeof(tid)));
+    D.mixedOpsStale = false;
+  }
+  return std::string();
+}
+
+static Scale4f to_f(const Scale4& s) {
+  Scale4f r;
+  r.mod = s.mod;
+  for (int k = 0; k < 4; k++) r.v[k] = (float)s.v[k];
+  return r;
+}
+
+// one pass over a chunk of kc right-hand sides, KB of them per launch block
+template <int KT, int KB>
+static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats* ls) {
+  if constexpr (KTraits<KT>::TD != 1 && KB > 4) {
+    run_mixed<KT, 4>(P, D, kc, mask, ls);  // pick_kb never asks for this
+    return;
+  }
+  cudaStream_t st = D.stream;
+  const int64_t ue = (int64_t)P.nUE * P.sdm, uc = (int64_t)P.nUC * P.tdm;
+  const int64_t de = (int64_t)P.nDE * P.sdm, dc = (int64_t)P.nDC * P.tdm;
+  const int64_t nn = P.nn;
+  const int rl = P.o.rootLevel;
+  const float mu = (float)P.o.coefs[0], ve = (float)P.o.coefs[1];
+  const int nl = (int)P.evtrLeaves.size();
+  const int kb = (kc + KB - 1) / KB;
+  const int64_t denStride = P.ns * P.sd, valStride = std::max<int64_t>(P.nt, 1) * P.td;
+  auto gemm = [&](int nrows, const int32_t* rows, int xChild, int yChild, const float* X, int64_t ldx, int64_t xR,
+                  const float* W, float* Y, int64_t ldy, int64_t yR, int K, int N, Scale4 xs, Scale4 ys, float beta) {
+    if (nrows <= 0) return;
+    dim3 grid((nrows * kc + G32_BM - 1) / G32_BM, (N + G32_BN - 1) / G32_BN);
+    k_gemm_rows32<<<grid, 256, 0, st>>>(nrows, kc, rows, D.chd, xChild, yChild, X, ldx, xR, W, Y, ldy, yR, K, N,
+                                        to_f(xs), to_f(ys), beta);
+    ls->launches++;
+  };
+  if ((mask & 1) && !P.s2mLeaves.empty()) {
+    k_src2surf32<KT, KB><<<dim3((unsigned)P.s2mLeaves.size(), kb), MX_SURF, 0, st>>>(
+        D.s2mLeaves, nullptr, nullptr, D.srcBeg, D.srcCnt, D.src, D.nrm, D.denK, denStride, D.ctr, D.rad, D.sam[1],
+        P.nUC, D.uchk32, uc, nn * uc, kc, mu, ve);
+    ls->launches++;
+  }
+  cudaEventRecord(D.ev[EV_S2M], st);
+  if (mask & 1) {
+    for (int d = P.maxDepth; d >= 1; d--) {
+      int64_t a = D.offUpM2M[d], b = D.offUpM2M[d + 1];
+      gemm((int)(b - a), D.levelRows + a, 1, 0, D.uden32, ue, nn * ue, D.m2m32, D.uchk32, uc, nn * uc, 8 * ue, uc,
+           level_scale(P, d + 1 + rl, +1.0), unit_scale(), 0.f);
+      a = D.offUpC2E[d];
+      b = D.offUpC2E[d + 1];
+      gemm((int)(b - a), D.levelRows + a, 0, 0, D.uchk32, uc, nn * uc, D.uc2ue32, D.uden32, ue, nn * ue, uc, ue,
+           unit_scale(), level_scale(P, d + rl, -1.0), 0.f);
+    }
+  }
+  cudaEventRecord(D.ev[EV_UP_GEMM], st);
+  auto near = [&](const int64_t* ptr, const int32_t* idx) {
+    if (nl == 0) return;
+    k_p2p_near32<KT, KB><<<dim3(nl, kb), MX_THREADS, 0, st>>>(D.evtrLeaves, ptr, idx, D.srcBeg, D.srcCnt, D.trgBeg,
+                                                             D.trgCnt, D.src, D.nrm, D.denK, denStride, D.trg, D.ctr,
+                                                             D.valK, valStride, kc, mu, ve);
+    ls->launches++;
+  };
+  if ((mask & 2) && (mask & 8) && (mask & 16)) {
+    near(D.nearPtr, D.nearIdx);
+  } else {
+    if (mask & 2) near(D.nearUPtr, D.nearUIdx);
+    if (mask & 8) near(D.nearWPtr, D.nearWIdx);
+    if (mask & 16) near(D.nearXPtr, D.nearXIdx);
+  }
+  cudaEventRecord(D.ev[EV_NEAR], st);
+  const int nsrc = (int)P.vSrcNodes.size(), ntrg = (int)P.vTrgNodes.size(), npar = (int)P.vParents.size();
+  const int64_t effDR = (int64_t)nsrc * P.nEff * P.sdm, effVR = (int64_t)ntrg * P.nEff * P.tdm;
+  if ((mask & 4) && nsrc > 0) {
+    Scale4 deg;
+    deg.mod = P.sdm;
+    for (int k = 0; k < 4; k++) deg.v[k] = P.deg[k];
+#define FMMG_FWD32(NP_)                                                                                         \
+  k_m2l_fwd32<NP_><<<dim3(nsrc, kc), 128, 0, st>>>(D.vSrcNodes, D.depth, rl, deg, P.sdm, D.uden32, nn * ue,    \
+                                                    D.surfIJK, P.nUE, D.effDen32, effDR, P.nEff)
+    switch (P.o.np) {
+      case 3: FMMG_FWD32(3); break;
+      case 4: FMMG_FWD32(4); break;
+      case 5: FMMG_FWD32(5); break;
+      case 6: FMMG_FWD32(6); break;
+      case 7: FMMG_FWD32(7); break;
+      case 8: FMMG_FWD32(8); break;
+    }
+#undef FMMG_FWD32
+    ls->launches++;
+  }
+  cudaEventRecord(D.ev[EV_M2L_FWD], st);
+  if ((mask & 4) && npar > 0 && ntrg > 0) {
+    dim3 grid(npar, (P.nEff + 31) / 32, kb);
+    const float nrmfc = 1.0f / float(P.nReg);
+#define FMMG_HAD32(SD_, TD_)                                                                                   \
+  k_m2l_had32<SD_, TD_, KB><<<grid, 256, 0, st>>>(D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot,      \
+                                                   D.vTrgSlot, D.effDen32, effDR, D.m2lT32, D.effVal32, effVR, \
+                                                   P.nEff, kc, nrmfc)
+    if (P.sdm == 1 && P.tdm == 1) FMMG_HAD32(1, 1);
+    else if (P.sdm == 4 && P.tdm == 3) FMMG_HAD32(4, 3);
+    else FMMG_HAD32(3, 3);
+#undef FMMG_HAD32
+    ls->launches++;
+  }
+  cudaEventRecord(D.ev[EV_M2L_HAD], st);
+  if ((mask & 4) && npar > 0 && ntrg > 0) {
+#define FMMG_INV32(NP_)                                                                                   \
+  k_m2l_inv32<NP_><<<dim3(ntrg, kc), 128, 0, st>>>(D.vTrgNodes, D.effVal32, effVR, P.nEff, P.tdm, D.surfIJK, \
+                                                    P.nDC, D.dchk32, nn * dc)
+    switch (P.o.np) {
+      case 3: FMMG_INV32(3); break;
+      case 4: FMMG_INV32(4); break;
+      case 5: FMMG_INV32(5); break;
+      case 6: FMMG_INV32(6); break;
+      case 7: FMMG_INV32(7); break;
+      case 8: FMMG_INV32(8); break;
+    }
+#undef FMMG_INV32
+    ls->launches++;
+  }
+  cudaEventRecord(D.ev[EV_M2L_INV], st);
+  auto e2t = [&](int own, int far) {
+    if (nl == 0) return;
+    switch (P.mm) {
+#define FMMG_E2T32(KM)                                                                                           \
+  case KM:                                                                                                       \
+    k_e2t32<KM, KB><<<dim3(nl, kb), MX_THREADS, 0, st>>>(D.evtrLeaves, D.farPtr, D.farIdx, own, far, D.depth,    \
+                                                         D.ctr, D.rad, D.sam[0], P.nUE, D.sam[2], P.nDE, D.uden32, \
+                                                         D.dden32, nn * ue, nn * de, D.trgBeg, D.trgCnt, D.trg,    \
+                                                         D.valK, valStride, kc, mu, ve);                           \
+    break;
+      FMMG_E2T32(LAP_S_U)
+      FMMG_E2T32(STK_F_U)
+      FMMG_E2T32(NAV_S_U)
+#undef FMMG_E2T32
+    }
+    ls->launches++;
+  };
+  if (mask & 8) e2t(0, 1);
+  cudaEventRecord(D.ev[EV_M2T], st);
+  if ((mask & 16) && !P.s2lNodes.empty()) {
+    k_src2surf32<KT, KB><<<dim3((unsigned)P.s2lNodes.size(), kb), MX_SURF, 0, st>>>(
+        D.s2lNodes, D.s2lPtr, D.s2lIdx, D.srcBeg, D.srcCnt, D.src, D.nrm, D.denK, denStride, D.ctr, D.rad, D.sam[3],
+        P.nDC, D.dchk32, dc, nn * dc, kc, mu, ve);
+    ls->launches++;
+  }
+  cudaEventRecord(D.ev[EV_S2L], st);
+  if (mask & 32) {
+    for (int d = 2; d <= P.maxDepth; d++) {
+      if (d >= 3) {
+        int64_t a = D.offDnL2L[d - 1], b = D.offDnL2L[d];
+        gemm((int)(b - a), D.levelRows + a, 0, 1, D.dden32, de, nn * de, D.l2l32, D.dchk32, dc, nn * dc, de, 8 * dc,
+             level_scale(P, d - 1 + rl, +1.0), unit_scale(), 1.f);
+      }
+      int64_t a = D.offDnC2E[d], b = D.offDnC2E[d + 1];
+      gemm((int)(b - a), D.levelRows + a, 0, 0, D.dchk32, dc, nn * dc, D.dc2de32, D.dden32, de, nn * de, dc, de,
+           unit_scale(), level_scale(P, d + rl, -1.0), 0.f);
+    }
+  }
+  cudaEventRecord(D.ev[EV_DN_GEMM], st);
+  if (mask & 32) e2t(1, 0);
+  cudaEventRecord(D.ev[EV_L2T], st);
+}
+
+__global__ void k_gather_den_k(int64_t n, int sd, int kc, int64_t stride, const int64_t* __restrict__ perm,
+                               const double* __restrict__ in, double* __restrict__ out) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int64_t s = perm[i];
+  for (int q = 0; q < kc; q++)
+    for (int c = 0; c < sd; c++) out[q * stride + i * sd + c] = in[q * stride + s * sd + c];
+}
+__global__ void k_scatter_val_k(int64_t n, int td, int kc, int64_t stride, const int64_t* __restrict__ perm,
+                                const double* __restrict__ in, double* __restrict__ out) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int64_t t = perm[i];
+  for (int q = 0; q < kc; q++)
+    for (int c = 0; c < td; c++) out[q * stride + t * td + c] = in[q * stride + i * td + c];
+}
+
+// right-hand sides per launch block: up to 8 for scalar targets, 4 otherwise
+static int pick_kb(int kc, int td) {
+  int cap = td == 1 ? 8 : 4;
+  int kb = 1;
+  while (kb * 2 <= std::min(kc, cap)) kb *= 2;
+  return kb;
+}
+
+std::string dev_evaluate_mixed(const Plan& P, DevState& D, const double* dDen, double* dVal, int k, int mask,
+                               bool timed, LaunchStats* lsIn) {
+  LaunchStats local;
+  LaunchStats* ls = lsIn ? lsIn : &local;
+  FMMG_CK(cudaSetDevice(D.device));
+  cudaStream_t st = D.stream;
+  const int64_t ns = P.ns, nt = P.nt;
+  const int64_t ue = (int64_t)P.nUE * P.sdm, uc = (int64_t)P.nUC * P.tdm;
+  const int64_t de = (int64_t)P.nDE * P.sdm, dc = (int64_t)P.nDC * P.tdm;
+  // right-hand sides per pass, bounded by a device-memory budget for the
+  // per-density work arrays (node rows and M2L spectra)
+  const double perRhs = 4.0 * P.nn * (ue + uc + de + dc) +
+                        8.0 * P.nEff * (P.vSrcNodes.size() * P.sdm + P.vTrgNodes.size() * P.tdm) +
+                        8.0 * (ns * P.sd + nt * P.td);
+  const double budget = D.mixedBudgetBytes;
+  int kmax = (int)std::max(1.0, std::floor(budget / std::max(perRhs, 1.0)));
+  int kc = std::min(k, std::min(kmax, 32));
+  FMMG_TRY(dev_prepare_mixed(P, D, kc));
+  const int64_t denStride = ns * P.sd, valStride = std::max<int64_t>(nt, 1) * P.td;
+  int passes = 0;
+  for (int r0 = 0; r0 < k; r0 += kc, passes++) {
+    const int kk = std::min(kc, k - r0);
+    cudaEventRecord(D.ev[EV_BEGIN], st);
+    k_gather_den_k<<<(unsigned)((ns + 255) / 256), 256, 0, st>>>(ns, P.sd, kk, denStride, D.srcPerm,
+                                                                  dDen + r0 * denStride, D.denK);
+    ls->launches++;
+    FMMG_CK(cudaMemsetAsync(D.valK, 0, sizeof(double) * kk * valStride, st));
+    FMMG_CK(cudaMemsetAsync(D.uchk32, 0, sizeof(float) * kk * P.nn * uc, st));
+    FMMG_CK(cudaMemsetAsync(D.uden32, 0, sizeof(float) * kk * P.nn * ue, st));
+    FMMG_CK(cudaMemsetAsync(D.dchk32, 0, sizeof(float) * kk * P.nn * dc, st));
+    FMMG_CK(cudaMemsetAsync(D.dden32, 0, sizeof(float) * kk * P.nn * de, st));
+    cudaEventRecord(D.ev[EV_PREP], st);
+    const int KBv = pick_kb(kk, P.td);
+#define FMMG_RUN_KB(KBC) FMMG_DISPATCH_KT(P.o.kt, KT, run_mixed<KT, KBC>(P, D, kk, mask, ls))
+    if (KBv == 8) { FMMG_RUN_KB(8); }
+    else if (KBv == 4) { FMMG_RUN_KB(4); }
+    else if (KBv == 2) { FMMG_RUN_KB(2); }
+    else { FMMG_RUN_KB(1); }
+#undef FMMG_RUN_KB
+    if (nt > 0) {
+      k_scatter_val_k<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(nt, P.td, kk, valStride, D.trgPerm, D.valK,
+                                                                     dVal + r0 * valStride);
+      ls->launches++;
+    }
+    cudaEventRecord(D.ev[EV_END], st);
+  }
+  D.lastLaunches = ls->launches;
+  FMMG_CK(cudaGetLastError());
+  if (timed) {
+    FMMG_CK(cudaEventSynchronize(D.ev[EV_END]));
+    for (int q = 0; q < EV_COUNT - 1; q++) cudaEventElapsedTime(&D.kernMs[q], D.ev[q], D.ev[q + 1]);
+    const float* m = D.kernMs;
+    D.stageMs[0] = m[EV_S2M - 1] + m[EV_UP_GEMM - 1];
+    D.stageMs[1] = m[EV_NEAR - 1];
+    D.stageMs[2] = m[EV_M2L_FWD - 1] + m[EV_M2L_HAD - 1] + m[EV_M2L_INV - 1];
+    D.stageMs[3] = m[EV_M2T - 1];
+    D.stageMs[4] = m[EV_S2L - 1];
+    D.stageMs[5] = m[EV_DN_GEMM - 1] + m[EV_L2T - 1];
+    cudaEventElapsedTime(&D.stageMs[6], D.ev[EV_BEGIN], D.ev[EV_END]);
+  }
+  (void)passes;
+  return std::string();
+}
+
+}  // namespace fmmg

@@ -22,16 +22,12 @@
 #include <functional>
 #include <string>
 
+#include "cuda_common.cuh"
 #include "engine.hpp"
 #include "kernels.hpp"
 
 namespace fmmg {
 
-#define FMMG_CK(x)                                                               \
-  do {                                                                           \
-    cudaError_t e_ = (x);                                                        \
-    if (e_ != cudaSuccess) return std::string(#x) + ": " + cudaGetErrorString(e_); \
-  } while (0)
 
 __constant__ int8_t c_transId[343];  // (rx+3)*49+(ry+3)*7+(rz+3) -> 0..315 or -1
 
@@ -336,10 +332,6 @@ __global__ void __launch_bounds__(SURF_THREADS)
 // parent form one contiguous row of length 8 * ld.  Used for C2E
 // (pinv GEMV, matmgnt3d_mpi.cpp:107-149, :196-229), M2M (:151-193) and L2L
 // (:231-274) over all nodes of a level at once.
-struct Scale4 {
-  double v[4];
-  int mod;
-};
 constexpr int GM_BM = 64, GM_BN = 64, GM_BK = 16;
 
 __global__ void __launch_bounds__(256)
@@ -429,17 +421,7 @@ __global__ void __launch_bounds__(256)
 // rank-3 layout with the x axis halved.  Because only the np^3 band of each
 // axis is non-zero on input (and needed on output), the three 1-D passes are
 // evaluated as small dense DFTs restricted to that band.
-template <int NP>
-struct FftDims {
-  static constexpr int N = 2 * NP, NH = NP + 1, H = NP / 2;
-};
 
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // a * conj(b)
-  return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
-}
 
 template <int NP>
 __global__ void __launch_bounds__(128)
@@ -693,11 +675,6 @@ static std::string dput(DevState& D, T*& dst, const std::vector<T>& v) {
   return dput(D, dst, v.data(), v.size());
 }
 
-#define FMMG_TRY(x)             \
-  do {                          \
-    std::string e_ = (x);       \
-    if (!e_.empty()) return e_; \
-  } while (0)
 
 void dev_free(DevState& D) {
   for (void* p : D.allocs) cudaFree(p);
@@ -709,6 +686,14 @@ void dev_free(DevState& D) {
   D.m2lT = nullptr;
   D.chkPos = D.chkOut = nullptr;
   D.chkCap = 0;
+  D.uchk32 = D.uden32 = D.dchk32 = D.dden32 = nullptr;
+  D.effDen32 = D.effVal32 = nullptr;
+  D.uc2ue32 = D.m2m32 = D.dc2de32 = D.l2l32 = nullptr;
+  D.m2lT32 = nullptr;
+  D.denK = D.valK = nullptr;
+  D.mixedReady = false;
+  D.mixedOpsStale = true;
+  D.mixedK = 0;
 }
 
 std::string dev_upload_operators(const Plan& P, DevState& D) {
@@ -730,6 +715,7 @@ std::string dev_upload_operators(const Plan& P, DevState& D) {
   int8_t tid[343];
   for (int i = 0; i < 343; i++) tid[i] = (int8_t)P.transId[i / 49][(i / 7) % 7][i % 7];
   FMMG_CK(cudaMemcpyToSymbol(c_transId, tid, sizeof(tid)));
+  D.mixedOpsStale = true;
   return std::string();
 }
 
@@ -852,19 +838,6 @@ std::string dev_upload(const Plan& P, DevState& D, const double* src, const doub
 }
 
 // ------------------------------------------------------------------ launcher
-static Scale4 level_scale(const Plan& P, int level, double sign) {
-  Scale4 s;
-  s.mod = P.sdm;
-  for (int k = 0; k < 4; k++) s.v[k] = k < P.sdm ? std::exp2(sign * level * P.deg[k]) : 1.0;
-  return s;
-}
-static Scale4 unit_scale() {
-  Scale4 s;
-  s.mod = 1;
-  s.v[0] = s.v[1] = s.v[2] = s.v[3] = 1.0;
-  return s;
-}
-
 static void gemm_rows(cudaStream_t st, int nrows, const int32_t* rows, const int32_t* chd, int xChild, int yChild,
                       const double* X, int64_t ldx, const double* W, double* Y, int64_t ldy, int K, int N,
                       Scale4 xs, Scale4 ys, double beta, LaunchStats* ls) {
@@ -1013,7 +986,7 @@ static void run_stages(const Plan& P, DevState& D, int mask, LaunchStats* ls) {
 
 std::string dev_evaluate(const Plan& P, DevState& D, const double* dDen, double* dVal, int precision, int mask,
                          bool timed, LaunchStats* lsIn) {
-  (void)precision;
+  if (precision == 1) return dev_evaluate_mixed(P, D, dDen, dVal, 1, mask, timed, lsIn);
   LaunchStats local;
   LaunchStats* ls = lsIn ? lsIn : &local;
   FMMG_CK(cudaSetDevice(D.device));

@@ -73,6 +73,7 @@ SIGNATURES = {
     "fmmg_kernel_times": ([ctypes.c_void_p, _dp, ctypes.c_int], ctypes.c_int),
     "fmmg_plan_stats": ([ctypes.c_void_p, _i64p, ctypes.c_int], ctypes.c_int),
     "fmmg_launch_count": ([ctypes.c_void_p, _i64p], ctypes.c_int),
+    "fmmg_set_precision": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "fmmg_set_timing": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "fmmg_tree": ([ctypes.c_void_p, _i32p, _i64p, _i64p], ctypes.c_int),
     "fmmg_lists": ([ctypes.c_void_p, ctypes.c_int, _i64p, _i32p, _i64p], ctypes.c_int),
@@ -252,6 +253,10 @@ class FMM3d:
         n = ctypes.c_int64()
         self._chk(lib().fmmg_launch_count(self.h, ctypes.byref(n)))
         return n.value
+
+    def set_precision(self, precision):
+        """Arithmetic of evaluate()/evaluate_host_ptr (host-buffer calls)."""
+        self._chk(lib().fmmg_set_precision(self.h, precision))
 
     def set_timing(self, on=True):
         self._chk(lib().fmmg_set_timing(self.h, 1 if on else 0))

@@ -153,6 +153,9 @@ fmmg_status fmmg_plan_stats(const fmmg_handle* h, int64_t* stats, int n);
 /* Number of this library's kernels launched by the last evaluate call. */
 fmmg_status fmmg_launch_count(const fmmg_handle* h, int64_t* n);
 
+/* Arithmetic used by fmmg_evaluate (host buffers); FMMG_PREC_FP64 by default. */
+fmmg_status fmmg_set_precision(fmmg_handle* h, int precision);
+
 /* on != 0: every later evaluate records per-kernel CUDA events on the
  * handle's stream and waits for them (fmmg_evaluate always does). */
 fmmg_status fmmg_set_timing(fmmg_handle* h, int on);
