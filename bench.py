@@ -49,7 +49,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=1 << 20)
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="all", choices=["fp64", "all"])
+    ap.add_argument("--k", type=int, default=8, help="right-hand sides of the multi-RHS mixed form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -162,10 +163,13 @@ def run_reference(args):
     }))
 
 
-def measure_fp64_peak(torch):
-    """cuBLAS DGEMM 8192^3 best of 3 (TFLOP/s): the FP64 roof for CUDA-core kernels."""
-    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
-    b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+def measure_peak(torch, kind):
+    """cuBLAS GEMM 8192^3 best of 3 (TFLOP/s) in FP64 or FP32 (TF32 off): the
+    roof for the CUDA-core kernels, which MEASURED_PEAKS.json does not hold."""
+    torch.backends.cuda.matmul.allow_tf32 = False
+    dt = torch.float64 if kind == "fp64" else torch.float32
+    a = torch.randn(8192, 8192, dtype=dt, device="cuda")
+    b = torch.randn(8192, 8192, dtype=dt, device="cuda")
     best = 1e30
     for _ in range(3):
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -176,6 +180,26 @@ def measure_fp64_peak(torch):
         best = min(best, s.elapsed_time(e))
     del a, b
     return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+
+
+def time_form(f, torch, stream, den_dev, out_dev, n, k, prec, steps, warmup, flush):
+    """Device time per step of one evaluate form; per-kernel means; launches."""
+    for _ in range(max(warmup, 3)):
+        f.evaluate_device(den_dev, out_dev, k, prec)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    kern, launches = {}, 0
+    for i in range(steps):
+        flush.zero_()
+        ev[i][0].record(stream)
+        f.evaluate_device(den_dev, out_dev, k, prec)
+        ev[i][1].record(stream)
+        for name, v in f.kernel_times().items():
+            kern[name] = kern.get(name, 0.0) + v
+        launches += f.launch_count()
+    torch.cuda.synchronize()
+    ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    return ms, {name: v / steps for name, v in kern.items()}, launches
 
 
 def run_ours(args):
@@ -196,66 +220,59 @@ def run_ours(args):
     torch.cuda.set_stream(stream)
     cfg = W.config2(args.n)
     src = cfg["src"]
+    n = args.n
+    K = args.k
     rng = np.random.default_rng(W.SEED + 2 + 1000 * rank)
-    den_h = cfg["den"] if rank == 0 else rng.normal(size=args.n)
-    prec = fmmg.PREC_FP64 if args.precision == "fp64" else fmmg.PREC_MIXED
+    dens = np.stack([cfg["den"] if (rank == 0 and r == 0) else rng.normal(size=n) for r in range(K)])
     t0 = time.perf_counter()
     f = fmmg.FMM3d(111, np_=6, pts_max=64, device=dev, stream=stream.cuda_stream)
     f.setup(src)
     setup_s = time.perf_counter() - t0
     info = f.info()
-    n = args.n
-    den = torch.from_numpy(den_h).to("cuda")
-    out = torch.zeros(n, dtype=torch.float64, device="cuda")
+    den = torch.from_numpy(dens).to("cuda")
+    out = torch.zeros(K, n, dtype=torch.float64, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
     f.set_timing(True)
-    for _ in range(max(args.warmup, 3)):
-        f.evaluate_device(den, out, 1, prec)
-    torch.cuda.synchronize()
+    idx = np.random.default_rng(W.SEED + 99).choice(n, CHECK_TARGETS, replace=False)
+    forms = [("fp64", fmmg.PREC_FP64, 1), ("mixed", fmmg.PREC_MIXED, 1), ("mixed", fmmg.PREC_MIXED, K)]
+    if args.precision == "fp64":
+        forms = forms[:1]
+    results = []
     if dist:
         tdist.barrier()
     clocks = ClockSampler(dev if not os.environ.get("CUDA_VISIBLE_DEVICES") else
                           os.environ["CUDA_VISIBLE_DEVICES"].split(",")[dev])
     clocks.start()
-    torch.cuda.synchronize()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    kern = {}
-    launches = 0
-    for i in range(args.steps):
-        flush.zero_()
-        ev[i][0].record(stream)
-        f.evaluate_device(den, out, 1, prec)
-        ev[i][1].record(stream)
-        for k, v in f.kernel_times().items():
-            kern[k] = kern.get(k, 0.0) + v
-        launches += f.launch_count()
-    torch.cuda.synchronize()
-    step_ms = [a.elapsed_time(b) for a, b in ev]
-    ms = float(np.mean(step_ms))
+    for name, prec, k in forms:
+        ms, kern, launches = time_form(f, torch, stream, den, out, n, k, prec, args.steps, args.warmup, flush)
+        if dist:
+            t = torch.tensor([ms], device="cuda")
+            tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+            ms = float(t.item())
+        vals = out[0].cpu().numpy()
+        rel, mx, _ = f.check(dens[0], vals, idx)
+        results.append(dict(precision=name, k=k, ms_per_step=ms, points_per_s=n * k * ws / (ms * 1e-3),
+                            rel_err_vs_dense=rel, max_abs_err_vs_dense=mx, kernel_ms=kern,
+                            stage_ms=f.stage_times(), launches=launches))
     clk = clocks.stop()
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        ms = float(t.item())
-    kern = {k: v / args.steps for k, v in kern.items()}
-    stages = f.stage_times()
-    # error of this step against the FP64 dense sum at sampled targets (check())
-    vals = out.cpu().numpy()
-    idx = np.random.default_rng(W.SEED + 99).choice(n, CHECK_TARGETS, replace=False)
-    rel, mx, _ = f.check(den_h, vals, idx)
-    # end to end through fmmg_evaluate: pinned host in, pinned host out
-    hin = torch.from_numpy(den_h).pin_memory()
-    hout = torch.zeros(n, dtype=torch.float64).pin_memory()
-    f.evaluate_host_ptr(hin.data_ptr(), hout.data_ptr())
+    fp64 = results[0]
+    ok = [r for r in results if r["rel_err_vs_dense"] <= 1e-5]
+    head = max(ok, key=lambda r: r["points_per_s"]) if ok else fp64
+    prec_h = fmmg.PREC_FP64 if head["precision"] == "fp64" else fmmg.PREC_MIXED
+    kh = head["k"]
+    # end to end through fmmg_evaluate_host: pinned host densities in, pinned values out
+    hin = torch.from_numpy(dens[:kh].copy()).pin_memory()
+    hout = torch.zeros(kh, n, dtype=torch.float64).pin_memory()
+    f.evaluate_host_k(hin.data_ptr(), hout.data_ptr(), kh, prec_h)
     e2e_ms = []
     for _ in range(args.steps):
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         flush.zero_()
-        s.record(stream)
-        f.evaluate_host_ptr(hin.data_ptr(), hout.data_ptr())
-        e.record(stream)
-        e.synchronize()
-        e2e_ms.append(s.elapsed_time(e))
+        s_.record(stream)
+        f.evaluate_host_k(hin.data_ptr(), hout.data_ptr(), kh, prec_h)
+        e_.record(stream)
+        e_.synchronize()
+        e2e_ms.append(s_.elapsed_time(e_))
     e2e = float(np.mean(e2e_ms))
     if dist:
         t = torch.tensor([e2e], device="cuda")
@@ -263,28 +280,29 @@ def run_ours(args):
         e2e = float(t.item())
         tdist.barrier()
     if rank == 0:
-        roof = roofline(f, info, kern, torch)
+        roof = roofline(f, head["kernel_ms"], torch, kh, head["precision"])
         cpu = None
         if not args.no_cpu_baseline and not dist:
             rate, times = oracle_rate(CPU_SAMPLE, 1)
             cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
                    "sample": "%d-point sample of the workload distribution, 1 thread (one MPI rank), "
                              "tree/operators prebuilt, %.1f s" % (CPU_SAMPLE, times[0])}
-        total_pts = n * ws
         line = {
-            "metric": METRIC, "value": total_pts / (ms * 1e-3), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if prec == fmmg.PREC_FP64 else "f32+f64", "data": "synthetic",
+            "metric": METRIC, "value": head["points_per_s"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if prec_h == fmmg.PREC_FP64 else "f32+f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "points": n, "kernel": "laplace_s_u", "np": 6, "pts_max": 64,
-                       "k_rhs_per_gpu": 1, "precision": args.precision, "parallelism": "rhs-replicas x%d" % ws,
+                       "k_rhs_per_gpu": kh, "precision": head["precision"],
+                       "parallelism": "rhs-replicas x%d" % ws,
                        "l2": "256 MB written between steps; per-step working set > L2",
                        "nodes": info["nodes"], "leaves": info["leaves"], "max_depth": info["max_depth"]},
-            "e2e": {"value": total_pts / (e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 8 * n,
-                    "d2h_bytes_per_step": 8 * n},
-            "gpu_launches": launches,
-            "rel_err_vs_dense": rel, "max_abs_err_vs_dense": mx, "check_targets": CHECK_TARGETS,
-            "stage_ms": stages, "kernel_ms": kern, "setup_s": setup_s,
-            "roofline": roof, "clocks": clk,
+            "e2e": {"value": n * kh * ws / (e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 8 * n * kh,
+                    "d2h_bytes_per_step": 8 * n * kh},
+            "gpu_launches": head["launches"],
+            "rel_err_vs_dense": head["rel_err_vs_dense"], "check_targets": CHECK_TARGETS,
+            "fp64_points_per_s": fp64["points_per_s"],
+            "speedup_vs_fp64": head["points_per_s"] / fp64["points_per_s"],
+            "forms": results, "setup_s": setup_s, "roofline": roof, "clocks": clk,
         }
         if cpu:
             line["cpu_baseline"] = cpu
@@ -294,17 +312,16 @@ def run_ours(args):
         tdist.destroy_process_group()
 
 
-def roofline(f, info, kern, torch):
-    """Roofline of the dominant kernel class of the step."""
+def roofline(f, kern, torch, k, precision):
+    """Roofline of the dominant kernel class of the headline step."""
     peaks = {}
     pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pp):
         peaks = json.load(open(pp))
-    top = max((k for k in kern if k not in ("prep", "scatter")), key=lambda k: kern[k])
+    top = max((name for name in kern if name not in ("prep", "scatter")), key=lambda name: kern[name])
     t = kern[top] * 1e-3
-    work = f.algorithmic_work()
-    w = work.get(top)
-    out = {"kernel": top, "avg_ms": kern[top]}
+    w = f.algorithmic_work(k=k, precision=precision).get(top)
+    out = {"kernel": top, "avg_ms": kern[top], "k_rhs": k}
     if w is None:
         out.update({"bound": None, "achieved": None, "peak": None, "unit": None, "frac": None, "traffic": None})
         return out
@@ -315,10 +332,11 @@ def roofline(f, info, kern, torch):
                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650",
                     "algorithmic_bytes": w["bytes"]})
     else:
-        peak = measure_fp64_peak(torch)
+        fp = w["bound"]
+        peak = measure_peak(torch, fp)
         ach = w["flops"] / t / 1e12
-        out.update({"bound": "fp64", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
-                    "peak_source": "measured in bench: cuBLAS DGEMM 8192^3 best of 3",
+        out.update({"bound": fp, "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+                    "peak_source": "measured in bench: cuBLAS %s GEMM 8192^3 best of 3" % fp,
                     "algorithmic_flops": w["flops"], "pairs": w.get("pairs")})
     out["traffic"] = None
     return out

@@ -28,6 +28,9 @@ struct fmmg_handle {
   fmmg::DevState dev;
   double* dDenIO = nullptr;
   double* dValIO = nullptr;
+  double* dDenK = nullptr;  // k-RHS host-call staging
+  double* dValK = nullptr;
+  int ioK = 0;
   std::vector<double> trgHost;  // caller-order targets for check()
   std::string err;
 };
@@ -155,6 +158,8 @@ fmmg_status fmmg_setup(fmmg_handle* h, int64_t ns, const double* src, const doub
     if (h->setupDone) {
       fmmg::dev_free(h->dev);
       h->dDenIO = h->dValIO = nullptr;
+      h->dDenK = h->dValK = nullptr;
+      h->ioK = 0;
       fmmg::Plan fresh;
       fresh.o = h->opt;
       std::string e = fresh.build_operators();
@@ -265,6 +270,39 @@ fmmg_status fmmg_evaluate(fmmg_handle* h, const double* den, double* val) {
     h->launches = h->dev.lastLaunches;
     if (bo) {
       ce = cudaMemcpyAsync(val, h->dValIO, bo, cudaMemcpyDeviceToHost, st);
+      if (ce != cudaSuccess) return fail(h, FMMG_CUDA_ERROR, cudaGetErrorString(ce));
+    }
+    ce = cudaStreamSynchronize(st);
+    if (ce != cudaSuccess) return fail(h, FMMG_CUDA_ERROR, cudaGetErrorString(ce));
+  }
+  FMMG_GUARD(h)
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_evaluate_host(fmmg_handle* h, int k, const double* den, double* val, int precision) {
+  fmmg_status s = ready(h);
+  if (s != FMMG_OK) return s;
+  if (k < 1 || !den || (!val && h->plan.nt > 0)) return fail(h, FMMG_INVALID_ARG, "bad k or NULL pointer");
+  try {
+    const size_t bi = sizeof(double) * (size_t)h->plan.ns * h->plan.sd;
+    const size_t bo = sizeof(double) * (size_t)h->plan.nt * h->plan.td;
+    if (k > h->ioK) {
+      void* p = nullptr;
+      if (cudaMalloc(&p, bi * k) != cudaSuccess) return fail(h, FMMG_OOM, "cudaMalloc density buffers");
+      h->dev.allocs.push_back(p);
+      h->dDenK = (double*)p;
+      if (cudaMalloc(&p, std::max<size_t>(bo, 8) * k) != cudaSuccess) return fail(h, FMMG_OOM, "cudaMalloc values");
+      h->dev.allocs.push_back(p);
+      h->dValK = (double*)p;
+      h->ioK = k;
+    }
+    cudaStream_t st = h->dev.stream;
+    cudaError_t ce = cudaMemcpyAsync(h->dDenK, den, bi * k, cudaMemcpyHostToDevice, st);
+    if (ce != cudaSuccess) return fail(h, FMMG_CUDA_ERROR, cudaGetErrorString(ce));
+    s = fmmg_evaluate_device(h, k, h->dDenK, h->dValK, precision);
+    if (s != FMMG_OK) return s;
+    if (bo) {
+      ce = cudaMemcpyAsync(val, h->dValK, bo * k, cudaMemcpyDeviceToHost, st);
       if (ce != cudaSuccess) return fail(h, FMMG_CUDA_ERROR, cudaGetErrorString(ce));
     }
     ce = cudaStreamSynchronize(st);

@@ -62,6 +62,7 @@ SIGNATURES = {
     "fmmg_create": ([ctypes.POINTER(_Options), ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "fmmg_setup": ([ctypes.c_void_p, ctypes.c_int64, _dp, _dp, ctypes.c_int64, _dp], ctypes.c_int),
     "fmmg_evaluate": ([ctypes.c_void_p, _dp, _dp], ctypes.c_int),
+    "fmmg_evaluate_host": ([ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_int], ctypes.c_int),
     "fmmg_evaluate_device": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int],
                              ctypes.c_int),
     "fmmg_synchronize": ([ctypes.c_void_p], ctypes.c_int),
@@ -226,28 +227,30 @@ class FMM3d:
         self._chk(lib().fmmg_plan_stats(self.h, st.ctypes.data_as(_i64p), 16))
         return dict(zip(self.PLAN_STATS, st.tolist()))
 
-    def algorithmic_work(self):
+    def algorithmic_work(self, k=1, precision="fp64"):
         """Per kernel class: the roofline that bounds it and its algorithmic work
-        for one single-RHS evaluate (pairs x FLOPs per pair, GEMM FLOPs, or the
-        minimum HBM bytes of the spectral M2L steps)."""
+        for one evaluate of k right-hand sides (pairs x FLOPs per pair x k, GEMM
+        FLOPs x k, or the minimum memory bytes of the spectral M2L steps)."""
         s = self.plan_stats()
         mm = {111: 111, 121: 111, 312: 111, 322: 111, 311: 301, 321: 301, 511: 511, 521: 511}[self.kt]
         fp, fpm = self.PAIR_FLOPS[self.kt], self.PAIR_FLOPS[mm]
         ne, sdm, tdm = s["n_eff"], s["sdm"], s["tdm"]
-        w = {
-            "p2p_near": {"bound": "fp64", "flops": s["near_pairs"] * fp, "pairs": s["near_pairs"]},
-            "s2m": {"bound": "fp64", "flops": s["s2m_pairs"] * fp, "pairs": s["s2m_pairs"]},
-            "s2l": {"bound": "fp64", "flops": s["s2l_pairs"] * fp, "pairs": s["s2l_pairs"]},
-            "m2t": {"bound": "fp64", "flops": s["m2t_pairs"] * fpm, "pairs": s["m2t_pairs"]},
-            "l2t": {"bound": "fp64", "flops": s["l2t_pairs"] * fpm, "pairs": s["l2t_pairs"]},
-            "up_gemm": {"bound": "fp64", "flops": s["up_gemm_flops"]},
-            "dn_gemm": {"bound": "fp64", "flops": s["dn_gemm_flops"]},
-            "m2l_had": {"bound": "hbm", "bytes": 16 * ne * (s["v_src"] * sdm + s["v_trg"] * tdm + 316 * sdm * tdm),
-                        "flops": 8 * ne * sdm * tdm * s["v_interactions"]},
-            "m2l_fwd": {"bound": "hbm", "bytes": 16 * ne * s["v_src"] * sdm},
-            "m2l_inv": {"bound": "hbm", "bytes": 16 * ne * s["v_trg"] * tdm},
+        cb = 16 if precision == "fp64" else 8  # bytes per complex value
+        pipe = "fp64" if precision == "fp64" else "fp32"
+        return {
+            "p2p_near": {"bound": pipe, "flops": k * s["near_pairs"] * fp, "pairs": s["near_pairs"]},
+            "s2m": {"bound": pipe, "flops": k * s["s2m_pairs"] * fp, "pairs": s["s2m_pairs"]},
+            "s2l": {"bound": pipe, "flops": k * s["s2l_pairs"] * fp, "pairs": s["s2l_pairs"]},
+            "m2t": {"bound": pipe, "flops": k * s["m2t_pairs"] * fpm, "pairs": s["m2t_pairs"]},
+            "l2t": {"bound": pipe, "flops": k * s["l2t_pairs"] * fpm, "pairs": s["l2t_pairs"]},
+            "up_gemm": {"bound": pipe, "flops": k * s["up_gemm_flops"]},
+            "dn_gemm": {"bound": pipe, "flops": k * s["dn_gemm_flops"]},
+            "m2l_had": {"bound": "hbm",
+                        "bytes": cb * ne * (k * s["v_src"] * sdm + k * s["v_trg"] * tdm + 316 * sdm * tdm),
+                        "flops": 8 * ne * sdm * tdm * s["v_interactions"] * k},
+            "m2l_fwd": {"bound": "hbm", "bytes": k * cb * ne * s["v_src"] * sdm},
+            "m2l_inv": {"bound": "hbm", "bytes": k * cb * ne * s["v_trg"] * tdm},
         }
-        return w
 
     def launch_count(self):
         n = ctypes.c_int64()
@@ -260,6 +263,11 @@ class FMM3d:
 
     def set_timing(self, on=True):
         self._chk(lib().fmmg_set_timing(self.h, 1 if on else 0))
+
+    def evaluate_host_k(self, den_ptr, val_ptr, k, precision):
+        """fmmg_evaluate_host: k right-hand sides on raw host pointers."""
+        self._chk(lib().fmmg_evaluate_host(self.h, k, ctypes.cast(den_ptr, _dp), ctypes.cast(val_ptr, _dp),
+                                           precision))
 
     def evaluate_host_ptr(self, den_ptr, val_ptr):
         """fmmg_evaluate on raw host pointers (e.g. pinned torch tensors)."""

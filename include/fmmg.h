@@ -105,6 +105,11 @@ fmmg_status fmmg_setup(fmmg_handle* h, int64_t n_src, const double* src_xyz, con
  * runs every stage on the GPU, copies out and synchronises. */
 fmmg_status fmmg_evaluate(fmmg_handle* h, const double* src_den, double* trg_val);
 
+/* k right-hand sides on HOST buffers (pinned memory gives the fastest
+ * copies): src_den [k][n_src*srcDOF], trg_val [k][n_trg*trgDOF].  Copies in,
+ * evaluates with the given precision, copies out and synchronises. */
+fmmg_status fmmg_evaluate_host(fmmg_handle* h, int k, const double* src_den, double* trg_val, int precision);
+
 /* k right-hand sides on DEVICE buffers: d_src_den [k][n_src*srcDOF],
  * d_trg_val [k][n_trg*trgDOF], caller order.  Enqueued on the handle's stream;
  * returns without synchronising. */
