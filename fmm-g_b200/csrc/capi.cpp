@@ -384,9 +384,10 @@ fmmg_status fmmg_plan_stats(const fmmg_handle* h, int64_t* st, int n) {
     int64_t s = 0;
     for (int64_t e = P.nearSrc.ptr[r]; e < P.nearSrc.ptr[r + 1]; e++) s += P.srcCnt[P.nearSrc.idx[e]];
     nearPairs += P.trgCnt[g] * s;
-    m2tPairs += P.trgCnt[g] * (P.farUE.ptr[r + 1] - P.farUE.ptr[r]) * P.nUE;
     if (P.depth[g] >= 2) l2tPairs += P.trgCnt[g] * P.nDE;
   }
+  for (size_t r = 0; r < P.farLeaves.size(); r++)
+    m2tPairs += P.trgCnt[P.farLeaves[r]] * (P.farUE.ptr[r + 1] - P.farUE.ptr[r]) * P.nUE;
   for (int g : P.s2mLeaves) s2mPairs += P.srcCnt[g] * P.nUC;
   for (size_t r = 0; r < P.s2lNodes.size(); r++)
     for (int64_t e = P.s2lSrc.ptr[r]; e < P.s2lSrc.ptr[r + 1]; e++) s2lPairs += P.srcCnt[P.s2lSrc.idx[e]] * P.nDC;

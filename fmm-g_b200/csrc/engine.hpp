@@ -42,7 +42,8 @@ struct DevState {
   int64_t *nearUPtr = nullptr; int32_t *nearUIdx = nullptr;   // stage-split forms
   int64_t *nearWPtr = nullptr; int32_t *nearWIdx = nullptr;
   int64_t *nearXPtr = nullptr; int32_t *nearXIdx = nullptr;
-  int64_t *farPtr = nullptr; int32_t *farIdx = nullptr;
+  int32_t *farLeaves = nullptr; int64_t *farPtr = nullptr; int32_t *farIdx = nullptr;
+  int32_t *l2tLeaves = nullptr;
   int32_t *s2lNodes = nullptr; int64_t *s2lPtr = nullptr; int32_t *s2lIdx = nullptr;
   int32_t *s2mLeaves = nullptr;
   int32_t *levelRows = nullptr;  // concatenated per-level row lists

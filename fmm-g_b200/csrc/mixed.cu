@@ -26,7 +26,7 @@
 
 namespace fmmg {
 
-__constant__ int8_t c_transId32[343];
+__constant__ int16_t c_transId32[343];
 
 constexpr int MX_THREADS = 128;
 constexpr int MX_TILE = 128;
@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(MX_THREADS)
   const int S = MX_THREADS / TG;
   const int tl = tid % TG, sp = tid / TG;
   const int own = (useOwn && depth[g] >= 2) ? 1 : 0;
-  const int64_t f0 = farPtr[row], nf = useFar ? farPtr[row + 1] - f0 : 0;
+  const int64_t f0 = useFar ? farPtr[row] : 0, nf = useFar ? farPtr[row + 1] - f0 : 0;
   for (int64_t t0 = 0; t0 < tn; t0 += TG) {
     const int64_t t = t0 + tl;
     const bool act = t < tn;
@@ -659,8 +659,8 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
     std::vector<float2> t(P.m2lT.size());
     for (size_t i = 0; i < t.size(); i++) t[i] = make_float2((float)P.m2lT[i].real(), (float)P.m2lT[i].imag());
     FMMG_CK(cudaMemcpy(D.m2lT32, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice));
-    int8_t tid[343];
-    for (int i = 0; i < 343; i++) tid[i] = (int8_t)P.transId[i / 49][(i / 7) % 7][i % 7];
+    int16_t tid[343];
+    for (int i = 0; i < 343; i++) tid[i] = (int16_t)P.transId[i / 49][(i / 7) % 7][i % 7];
     FMMG_CK(cudaMemcpyToSymbol(c_transId32, tid, sizeof(tid)));
     D.mixedOpsStale = false;
   }
@@ -784,14 +784,16 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
   }
   cudaEventRecord(D.ev[EV_M2L_INV], st);
   auto e2t = [&](int own, int far) {
-    if (nl == 0) return;
+    const int nr = far ? (int)P.farLeaves.size() : (int)P.l2tLeaves.size();
+    const int32_t* rows = far ? D.farLeaves : D.l2tLeaves;
+    if (nr == 0) return;
     switch (P.mm) {
-#define FMMG_E2T32(KM)                                                                                           \
-  case KM:                                                                                                       \
-    k_e2t32<KM, KB><<<dim3(nl, kb), MX_THREADS, 0, st>>>(D.evtrLeaves, D.farPtr, D.farIdx, own, far, D.depth,    \
-                                                         D.ctr, D.rad, D.sam[0], P.nUE, D.sam[2], P.nDE, D.uden32, \
-                                                         D.dden32, nn * ue, nn * de, D.trgBeg, D.trgCnt, D.trg,    \
-                                                         D.valK, valStride, kc, mu, ve);                           \
+#define FMMG_E2T32(KM)                                                                                          \
+  case KM:                                                                                                      \
+    k_e2t32<KM, KB><<<dim3(nr, kb), MX_THREADS, 0, st>>>(rows, D.farPtr, D.farIdx, own, far, D.depth, D.ctr,    \
+                                                         D.rad, D.sam[0], P.nUE, D.sam[2], P.nDE, D.uden32,     \
+                                                         D.dden32, nn * ue, nn * de, D.trgBeg, D.trgCnt, D.trg, \
+                                                         D.valK, valStride, kc, mu, ve);                        \
     break;
       FMMG_E2T32(LAP_S_U)
       FMMG_E2T32(STK_F_U)

@@ -220,7 +220,7 @@ void Plan::build_lists() {
 // or the DC surface (S2L).
 void Plan::build_worklists() {
   const int64_t ueSize = (int64_t)nUE * sdm, dcSize = (int64_t)nDC * tdm;
-  evtrLeaves.clear(); nearSrc.clear(); farUE.clear();
+  evtrLeaves.clear(); nearSrc.clear(); farUE.clear(); farLeaves.clear(); l2tLeaves.clear();
   s2lNodes.clear(); s2lSrc.clear(); s2mLeaves.clear();
   for (int g = 0; g < nn; g++) {
     if ((flags[g] & NF_LSRC)) s2mLeaves.push_back(g);
@@ -228,6 +228,8 @@ void Plan::build_worklists() {
     bool xDirect = leaf(g) && trgCnt[g] * td < dcSize;
     if (leaf(g)) {
       evtrLeaves.push_back(g);
+      if (depth[g] >= 2) l2tLeaves.push_back(g);
+      size_t farBefore = farUE.idx.size();
       for (int64_t e = U.ptr[g]; e < U.ptr[g + 1]; e++) nearSrc.idx.push_back(U.idx[e]);
       for (int64_t e = W.ptr[g]; e < W.ptr[g + 1]; e++) {
         int w = W.idx[e];
@@ -237,7 +239,10 @@ void Plan::build_worklists() {
       if (xDirect)
         for (int64_t e = X.ptr[g]; e < X.ptr[g + 1]; e++) nearSrc.idx.push_back(X.idx[e]);
       nearSrc.ptr.push_back((int64_t)nearSrc.idx.size());
-      farUE.ptr.push_back((int64_t)farUE.idx.size());
+      if (farUE.idx.size() > farBefore) {
+        farLeaves.push_back(g);
+        farUE.ptr.push_back((int64_t)farUE.idx.size());
+      }
     }
     if (!xDirect && X.ptr[g + 1] > X.ptr[g]) {
       s2lNodes.push_back(g);

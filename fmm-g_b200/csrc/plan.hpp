@@ -71,7 +71,9 @@ struct Plan {
   // ---- GPU work lists
   std::vector<int32_t> evtrLeaves;  // EVTR leaves (rows of near/far-to-target work)
   CSR nearSrc;                      // per EVTR leaf: source leaves for true-kernel direct sums
-  CSR farUE;                        // per EVTR leaf: W nodes evaluated from their UE surface
+  std::vector<int32_t> farLeaves;   // EVTR leaves with W nodes evaluated from their UE surface (M2T)
+  CSR farUE;                        // per farLeaves row: those W nodes
+  std::vector<int32_t> l2tLeaves;   // EVTR leaves at depth >= 2 (L2T)
   std::vector<int32_t> s2lNodes;    // EVTR nodes with X entries evaluated on the DC surface
   CSR s2lSrc;                       // per s2lNodes row: source leaves
   std::vector<int32_t> s2mLeaves;   // leaves with sources (S2M)

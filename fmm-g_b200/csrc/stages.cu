@@ -29,7 +29,7 @@
 namespace fmmg {
 
 
-__constant__ int8_t c_transId[343];  // (rx+3)*49+(ry+3)*7+(rz+3) -> 0..315 or -1
+__constant__ int16_t c_transId[343];  // (rx+3)*49+(ry+3)*7+(rz+3) -> 0..315 or -1
 
 // ------------------------------------------------------------------ helpers
 __global__ void k_gather_den(int64_t n, int sd, const int64_t* __restrict__ perm, const double* __restrict__ in,
@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(P2P_THREADS)
   const int S = P2P_THREADS / TG;
   const int tl = tid % TG, sp = tid / TG;
   const int own = (useOwn && depth[g] >= 2) ? 1 : 0;
-  const int64_t f0 = farPtr[row], nf = useFar ? farPtr[row + 1] - f0 : 0;
+  const int64_t f0 = useFar ? farPtr[row] : 0, nf = useFar ? farPtr[row + 1] - f0 : 0;
   for (int64_t t0 = 0; t0 < tn; t0 += TG) {
     const int64_t t = t0 + tl;
     const bool act = t < tn;
@@ -712,8 +712,8 @@ std::string dev_upload_operators(const Plan& P, DevState& D) {
   } else {
     FMMG_CK(cudaMemcpy(D.m2lT, P.m2lT.data(), P.m2lT.size() * sizeof(double2), cudaMemcpyHostToDevice));
   }
-  int8_t tid[343];
-  for (int i = 0; i < 343; i++) tid[i] = (int8_t)P.transId[i / 49][(i / 7) % 7][i % 7];
+  int16_t tid[343];
+  for (int i = 0; i < 343; i++) tid[i] = (int16_t)P.transId[i / 49][(i / 7) % 7][i % 7];
   FMMG_CK(cudaMemcpyToSymbol(c_transId, tid, sizeof(tid)));
   D.mixedOpsStale = true;
   return std::string();
@@ -788,6 +788,8 @@ std::string dev_upload(const Plan& P, DevState& D, const double* src, const doub
     FMMG_TRY(dput(D, D.nearXPtr, ptr));
     FMMG_TRY(dput(D, D.nearXIdx, idx));
   }
+  FMMG_TRY(dput(D, D.farLeaves, P.farLeaves));
+  FMMG_TRY(dput(D, D.l2tLeaves, P.l2tLeaves));
   FMMG_TRY(dput(D, D.farPtr, P.farUE.ptr));
   FMMG_TRY(dput(D, D.farIdx, P.farUE.idx));
   FMMG_TRY(dput(D, D.s2lNodes, P.s2lNodes));
@@ -868,14 +870,16 @@ static void launch_s2surf(const Plan& P, DevState& D, int nrows, const int32_t* 
 }
 
 static void launch_e2t(const Plan& P, DevState& D, int useOwn, int useFar, LaunchStats* ls) {
-  int n = (int)P.evtrLeaves.size();
+  // L2T runs over the leaves at depth >= 2, M2T over the leaves with W nodes
+  const int n = useFar ? (int)P.farLeaves.size() : (int)P.l2tLeaves.size();
+  const int32_t* rows = useFar ? D.farLeaves : D.l2tLeaves;
   if (n == 0) return;
   switch (P.mm) {
 #define FMMG_E2T(KM)                                                                                          \
   case KM:                                                                                                    \
-    k_e2t<KM><<<n, P2P_THREADS, 0, D.stream>>>(D.evtrLeaves, D.farPtr, D.farIdx, useOwn, useFar, D.depth,     \
-                                               D.ctr, D.rad, D.sam[0], P.nUE, D.sam[2], P.nDE, D.uden, D.dden, \
-                                               D.trgBeg, D.trgCnt, D.trg, D.val, P.o.coefs[0], P.o.coefs[1]); \
+    k_e2t<KM><<<n, P2P_THREADS, 0, D.stream>>>(rows, D.farPtr, D.farIdx, useOwn, useFar, D.depth, D.ctr, D.rad, \
+                                               D.sam[0], P.nUE, D.sam[2], P.nDE, D.uden, D.dden, D.trgBeg,     \
+                                               D.trgCnt, D.trg, D.val, P.o.coefs[0], P.o.coefs[1]);            \
     break;
     FMMG_E2T(LAP_S_U)
     FMMG_E2T(STK_F_U)
