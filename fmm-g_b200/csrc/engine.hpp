@@ -60,6 +60,8 @@ struct DevState {
   float *uchk32 = nullptr, *uden32 = nullptr, *dchk32 = nullptr, *dden32 = nullptr;
   float2 *effDen32 = nullptr, *effVal32 = nullptr;
   float *uc2ue32 = nullptr, *m2m32 = nullptr, *dc2de32 = nullptr, *l2l32 = nullptr;
+  float *upF1 = nullptr, *upF2 = nullptr, *dnF1 = nullptr, *dnF2 = nullptr;  // factored pinvs
+  float *upT32 = nullptr, *dnT32 = nullptr;  // [k][nn][kUp|kDn] intermediate of the factored C2E
   float2* m2lT32 = nullptr;
   double *denK = nullptr, *valK = nullptr;  // permuted densities / values of a RHS chunk
   bool mixedReady = false, mixedOpsStale = true;

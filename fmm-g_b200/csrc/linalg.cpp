@@ -120,6 +120,49 @@ void pinv_jacobi(int m, int n, const double* A, double eps, double* R) {
   }
 }
 
+// The same truncated pseudo-inverse in factored form, pinv(A) = B1^T-free
+// product F2 * F1 with F1 = diag(1/s_k) U_k^T (k x m, row-major) and
+// F2 = V_k (n x k, row-major).  Applying F1 then F2 keeps the rounding error of
+// each factor relative to the size of its own result, which a single product
+// with the large-norm explicit pinv does not (used by the FP32 path).
+int pinv_factors(int m, int n, const double* A, double eps, std::vector<double>& F1, std::vector<double>& F2) {
+  bool tr = m < n;
+  int M = tr ? n : m, N = tr ? m : n;
+  std::vector<double> W((size_t)M * N), V;
+  if (!tr) std::memcpy(W.data(), A, sizeof(double) * M * N);
+  else
+    for (int i = 0; i < m; i++)
+      for (int j = 0; j < n; j++) W[(size_t)i * n + j] = A[(size_t)j * m + i];
+  svd_onesided(M, N, W, V);
+  std::vector<double> S(N);
+  for (int j = 0; j < N; j++) {
+    double s = 0;
+    for (int i = 0; i < M; i++) s += W[(size_t)j * M + i] * W[(size_t)j * M + i];
+    S[j] = std::sqrt(s);
+  }
+  double smax = *std::max_element(S.begin(), S.end());
+  std::vector<int> keep;
+  for (int c = 0; c < N; c++)
+    if (S[c] >= eps * smax && S[c] > 0.0) keep.push_back(c);
+  const int k = (int)keep.size();
+  F1.assign((size_t)k * m, 0.0);
+  F2.assign((size_t)n * k, 0.0);
+  for (int r = 0; r < k; r++) {
+    const int c = keep[r];
+    const double s = S[c];
+    const double* w = &W[(size_t)c * M];  // U_c * s_c (length M)
+    const double* v = &V[(size_t)c * N];  // V_c (length N)
+    if (!tr) {  // A = U S V^T: F1 row = U_c^T / s = w^T / s^2, F2 column = v
+      for (int j = 0; j < m; j++) F1[(size_t)r * m + j] = w[j] / (s * s);
+      for (int i = 0; i < n; i++) F2[(size_t)i * k + r] = v[i];
+    } else {  // A^T = W V^T: A = V S U'^T with U' = W / s: F1 row = v^T / s, F2 column = w / s
+      for (int j = 0; j < m; j++) F1[(size_t)r * m + j] = v[j] / s;
+      for (int i = 0; i < n; i++) F2[(size_t)i * k + r] = w[i] / s;
+    }
+  }
+  return k;
+}
+
 // out[kz][ky][kx][h], kx in [0, n/2]; in[z][y][x][h] (x fastest), e^{-2 pi i}
 void rfft3_host(int n, int howmany, const double* in, std::complex<double>* out) {
   typedef std::complex<double> C;

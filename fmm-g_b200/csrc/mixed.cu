@@ -548,6 +548,70 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Scalar equivalent kernels (SDM = TDM = 1): the CTA stages its 32-frequency
+// slice of all 316 translation spectra in shared memory once (316 x 32 x 8 B =
+// 79 KB) and then walks a block of HAD_PPB target parents, so the spectra are
+// read from L2 once per block instead of once per interaction.  Warp c owns
+// child c of the current parent; lane = frequency.
+constexpr int HAD_PPB = 16;
+template <int KB>
+__global__ void __launch_bounds__(256)
+    k_m2l_had32_s(int nP, const int32_t* __restrict__ parents, const int64_t* __restrict__ vPtr,
+                  const int32_t* __restrict__ vIdx, const int8_t* __restrict__ vOff, const int32_t* __restrict__ chd,
+                  const int32_t* __restrict__ srcSlot, const int32_t* __restrict__ trgSlot,
+                  const float2* __restrict__ effDen, int64_t denRhs, const float2* __restrict__ T,
+                  float2* __restrict__ effVal, int64_t valRhs, int nEff, int nrhs, float nrmfc) {
+  extern __shared__ float2 Ts[];  // [316][32]
+  const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
+  const int f0 = blockIdx.y * 32;
+  const int f = f0 + lane;
+  const int rhs0 = blockIdx.z * KB;
+  for (int i = threadIdx.x; i < 316 * 32; i += blockDim.x) {
+    const int id = i >> 5, ff = f0 + (i & 31);
+    Ts[i] = ff < nEff ? T[(int64_t)id * nEff + ff] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  const bool fin = f < nEff;
+  const int cx = c >> 2, cy = (c >> 1) & 1, cz = c & 1;
+  const int pEnd = min(nP, (int)(blockIdx.x + 1) * HAD_PPB);
+  for (int b = blockIdx.x * HAD_PPB; b < pEnd; b++) {
+    const int P = parents[b];
+    const int ts = trgSlot[chd[P] + c];
+    if (ts < 0) continue;
+    float2 acc[KB];
+#pragma unroll
+    for (int q = 0; q < KB; q++) acc[q] = make_float2(0.f, 0.f);
+    for (int64_t e = vPtr[b]; e < vPtr[b + 1]; e++) {
+      const int Q = vIdx[e];
+      const int off = vOff[e];
+      const int dx = off / 9 - 1, dy = (off / 3) % 3 - 1, dz = off % 3 - 1;
+      const int q0 = chd[Q];
+#pragma unroll 2
+      for (int c2 = 0; c2 < 8; c2++) {
+        const int s = srcSlot[q0 + c2];
+        const int rx = 2 * dx + (c2 >> 2) - cx, ry = 2 * dy + ((c2 >> 1) & 1) - cy, rz = 2 * dz + (c2 & 1) - cz;
+        if (s < 0 || max(abs(rx), max(abs(ry), abs(rz))) <= 1 || !fin) continue;
+        const float2 w = Ts[c_transId32[(rx + 3) * 49 + (ry + 3) * 7 + (rz + 3)] * 32 + lane];
+        const float2* dp = effDen + (int64_t)s * nEff + f;
+#pragma unroll
+        for (int q = 0; q < KB; q++) {
+          if (rhs0 + q < nrhs) {
+            const float2 d = dp[(rhs0 + q) * denRhs];
+            acc[q].x += w.x * d.x - w.y * d.y;
+            acc[q].y += w.x * d.y + w.y * d.x;
+          }
+        }
+      }
+    }
+    if (fin) {
+#pragma unroll
+      for (int q = 0; q < KB; q++)
+        if (rhs0 + q < nrhs)
+          effVal[(rhs0 + q) * valRhs + (int64_t)ts * nEff + f] = make_float2(acc[q].x * nrmfc, acc[q].y * nrmfc);
+    }
+  }
+}
+
 // grid (target slots, right-hand sides)
 template <int NP>
 __global__ void __launch_bounds__(128)
@@ -634,6 +698,8 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
     FMMG_TRY(dalloc(D, D.dden32, (size_t)kc * P.nn * de));
     FMMG_TRY(dalloc(D, D.effDen32, (size_t)kc * P.vSrcNodes.size() * P.nEff * P.sdm));
     FMMG_TRY(dalloc(D, D.effVal32, (size_t)kc * P.vTrgNodes.size() * P.nEff * P.tdm));
+    FMMG_TRY(dalloc(D, D.upT32, (size_t)kc * P.nn * std::max(P.kUp, 1)));
+    FMMG_TRY(dalloc(D, D.dnT32, (size_t)kc * P.nn * std::max(P.kDn, 1)));
     FMMG_TRY(dalloc(D, D.denK, (size_t)kc * P.ns * P.sd));
     FMMG_TRY(dalloc(D, D.valK, (size_t)kc * std::max<int64_t>(P.nt, 1) * P.td));
     if (!D.uc2ue32) {
@@ -642,6 +708,10 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
       FMMG_TRY(dalloc(D, D.dc2de32, P.dc2de.size()));
       FMMG_TRY(dalloc(D, D.l2l32, P.l2l.size()));
       FMMG_TRY(dalloc(D, D.m2lT32, P.m2lT.size()));
+      FMMG_TRY(dalloc(D, D.upF1, P.uc2ueF1.size()));
+      FMMG_TRY(dalloc(D, D.upF2, P.uc2ueF2.size()));
+      FMMG_TRY(dalloc(D, D.dnF1, P.dc2deF1.size()));
+      FMMG_TRY(dalloc(D, D.dnF2, P.dc2deF2.size()));
     }
     D.mixedReady = true;
     D.mixedK = kc;
@@ -656,6 +726,10 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
     FMMG_TRY(put(D.m2m32, P.m2m));
     FMMG_TRY(put(D.dc2de32, P.dc2de));
     FMMG_TRY(put(D.l2l32, P.l2l));
+    FMMG_TRY(put(D.upF1, P.uc2ueF1));
+    FMMG_TRY(put(D.upF2, P.uc2ueF2));
+    FMMG_TRY(put(D.dnF1, P.dc2deF1));
+    FMMG_TRY(put(D.dnF2, P.dc2deF2));
     std::vector<float2> t(P.m2lT.size());
     for (size_t i = 0; i < t.size(); i++) t[i] = make_float2((float)P.m2lT[i].real(), (float)P.m2lT[i].imag());
     FMMG_CK(cudaMemcpy(D.m2lT32, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice));
@@ -712,8 +786,11 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
            level_scale(P, d + 1 + rl, +1.0), unit_scale(), 0.f);
       a = D.offUpC2E[d];
       b = D.offUpC2E[d + 1];
-      gemm((int)(b - a), D.levelRows + a, 0, 0, D.uchk32, uc, nn * uc, D.uc2ue32, D.uden32, ue, nn * ue, uc, ue,
-           unit_scale(), level_scale(P, d + rl, -1.0), 0.f);
+      // C2E as F2 (F1 uchk): the large-norm pinv never multiplies in FP32
+      gemm((int)(b - a), D.levelRows + a, 0, 0, D.uchk32, uc, nn * uc, D.upF1, D.upT32, P.kUp, nn * P.kUp, uc,
+           P.kUp, unit_scale(), unit_scale(), 0.f);
+      gemm((int)(b - a), D.levelRows + a, 0, 0, D.upT32, P.kUp, nn * P.kUp, D.upF2, D.uden32, ue, nn * ue, P.kUp,
+           ue, unit_scale(), level_scale(P, d + rl, -1.0), 0.f);
     }
   }
   cudaEventRecord(D.ev[EV_UP_GEMM], st);
@@ -760,8 +837,14 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
   k_m2l_had32<SD_, TD_, KB><<<grid, 256, 0, st>>>(D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot,      \
                                                    D.vTrgSlot, D.effDen32, effDR, D.m2lT32, D.effVal32, effVR, \
                                                    P.nEff, kc, nrmfc)
-    if (P.sdm == 1 && P.tdm == 1) FMMG_HAD32(1, 1);
-    else if (P.sdm == 4 && P.tdm == 3) FMMG_HAD32(4, 3);
+    if (P.sdm == 1 && P.tdm == 1) {
+      const size_t smem = 316 * 32 * sizeof(float2);
+      cudaFuncSetAttribute(k_m2l_had32_s<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      dim3 g2((npar + HAD_PPB - 1) / HAD_PPB, (P.nEff + 31) / 32, kb);
+      k_m2l_had32_s<KB><<<g2, 256, smem, st>>>(npar, D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot,
+                                                D.vTrgSlot, D.effDen32, effDR, D.m2lT32, D.effVal32, effVR, P.nEff,
+                                                kc, nrmfc);
+    } else if (P.sdm == 4 && P.tdm == 3) FMMG_HAD32(4, 3);
     else FMMG_HAD32(3, 3);
 #undef FMMG_HAD32
     ls->launches++;
@@ -819,8 +902,10 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
              level_scale(P, d - 1 + rl, +1.0), unit_scale(), 1.f);
       }
       int64_t a = D.offDnC2E[d], b = D.offDnC2E[d + 1];
-      gemm((int)(b - a), D.levelRows + a, 0, 0, D.dchk32, dc, nn * dc, D.dc2de32, D.dden32, de, nn * de, dc, de,
-           unit_scale(), level_scale(P, d + rl, -1.0), 0.f);
+      gemm((int)(b - a), D.levelRows + a, 0, 0, D.dchk32, dc, nn * dc, D.dnF1, D.dnT32, P.kDn, nn * P.kDn, dc,
+           P.kDn, unit_scale(), unit_scale(), 0.f);
+      gemm((int)(b - a), D.levelRows + a, 0, 0, D.dnT32, P.kDn, nn * P.kDn, D.dnF2, D.dden32, de, nn * de, P.kDn,
+           de, unit_scale(), level_scale(P, d + rl, -1.0), 0.f);
     }
   }
   cudaEventRecord(D.ev[EV_DN_GEMM], st);
@@ -864,7 +949,7 @@ std::string dev_evaluate_mixed(const Plan& P, DevState& D, const double* dDen, d
   const int64_t de = (int64_t)P.nDE * P.sdm, dc = (int64_t)P.nDC * P.tdm;
   // right-hand sides per pass, bounded by a device-memory budget for the
   // per-density work arrays (node rows and M2L spectra)
-  const double perRhs = 4.0 * P.nn * (ue + uc + de + dc) +
+  const double perRhs = 4.0 * P.nn * (ue + uc + de + dc + P.kUp + P.kDn) +
                         8.0 * P.nEff * (P.vSrcNodes.size() * P.sdm + P.vTrgNodes.size() * P.tdm) +
                         8.0 * (ns * P.sd + nt * P.td);
   const double budget = D.mixedBudgetBytes;

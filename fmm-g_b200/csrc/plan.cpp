@@ -412,6 +412,7 @@ std::string Plan::build_operators() {
   uc2ue.resize((size_t)ue * uc);
   for (int r = 0; r < ue; r++)
     for (int c = 0; c < uc; c++) uc2ue[(size_t)r * uc + c] = Rm[(size_t)c * ue + r];
+  kUp = pinv_factors(uc, ue, A.data(), eps, uc2ueF1, uc2ueF2);
   // C2E down
   mm_matrix_rt(mm, o.coefs, nDE, sam[2].data(), nDC, sam[3].data(), A);
   Rm.assign((size_t)de * dc, 0.0);
@@ -419,6 +420,7 @@ std::string Plan::build_operators() {
   dc2de.resize((size_t)de * dc);
   for (int r = 0; r < de; r++)
     for (int c = 0; c < dc; c++) dc2de[(size_t)r * dc + c] = Rm[(size_t)c * de + r];
+  kDn = pinv_factors(dc, de, A.data(), eps, dc2deF1, dc2deF2);
   // M2M / L2L octant matrices
   m2m.assign((size_t)uc * 8 * ue, 0.0);
   l2l.assign((size_t)8 * dc * de, 0.0);

@@ -97,6 +97,10 @@ struct Plan {
   std::vector<double> dc2de;     // [nDE*sdm][nDC*tdm]       C2E down (pinv)
   std::vector<double> l2l;       // [8*nDC*tdm][nDE*sdm]     8 octant DE->DC matrices stacked
   std::vector<std::complex<double>> m2lT;  // [316][nEff][sdm*tdm] (FFTW r2c layout)
+  // the two pseudo-inverses in factored form for the FP32 path:
+  // C2E = F2 (F1 x), F1 = diag(1/s) U^T [k][check], F2 = V [equiv][k]
+  int kUp = 0, kDn = 0;
+  std::vector<double> uc2ueF1, uc2ueF2, dc2deF1, dc2deF2;
   int transId[7][7][7];
 
   std::string build(const Options& opt, int64_t ns, const double* src, const double* nrm, int64_t nt,
@@ -117,6 +121,8 @@ struct Plan {
 
 // linear algebra used by the operator builder (linalg.cpp)
 void pinv_jacobi(int m, int n, const double* A_colmajor, double eps, double* R_colmajor);
+int pinv_factors(int m, int n, const double* A_colmajor, double eps, std::vector<double>& F1,
+                 std::vector<double>& F2);
 void rfft3_host(int n, int howmany, const double* in, std::complex<double>* out);
 
 }  // namespace fmmg

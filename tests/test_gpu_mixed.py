@@ -67,7 +67,7 @@ def test_mixed_host_path_and_stage_masks():
     vm = _mixed_eval(lib, den)
     assert rel_l2(vh, vm) <= 1e-12  # same arithmetic through the host-buffer call
     vd = gpu_eval(lib, den)
-    assert rel_l2(vm, vd) <= 1e-4
+    assert rel_l2(vm, vd) <= 1e-5
 
 
 def test_mixed_multi_rhs_matches_single_rhs():
