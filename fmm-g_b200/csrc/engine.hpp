@@ -53,6 +53,7 @@ struct DevState {
   // operators
   double *uc2ue = nullptr, *m2m = nullptr, *dc2de = nullptr, *l2l = nullptr;
   double2* m2lT = nullptr;
+  int16_t* transIdDev = nullptr;  // (rx+3)*49+(ry+3)*7+(rz+3) -> translation 0..315 or -1
   // per-evaluate work arrays
   double *den = nullptr, *val = nullptr, *uchk = nullptr, *uden = nullptr, *dchk = nullptr, *dden = nullptr;
   double2 *effDen = nullptr, *effVal = nullptr;

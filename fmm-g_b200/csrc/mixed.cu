@@ -22,6 +22,7 @@
 
 #include "cuda_common.cuh"
 #include "engine.hpp"
+#include "had_smem.cuh"
 #include "kernels.hpp"
 
 namespace fmmg {
@@ -548,70 +549,6 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Scalar equivalent kernels (SDM = TDM = 1): the CTA stages its 32-frequency
-// slice of all 316 translation spectra in shared memory once (316 x 32 x 8 B =
-// 79 KB) and then walks a block of HAD_PPB target parents, so the spectra are
-// read from L2 once per block instead of once per interaction.  Warp c owns
-// child c of the current parent; lane = frequency.
-constexpr int HAD_PPB = 16;
-template <int KB>
-__global__ void __launch_bounds__(256)
-    k_m2l_had32_s(int nP, const int32_t* __restrict__ parents, const int64_t* __restrict__ vPtr,
-                  const int32_t* __restrict__ vIdx, const int8_t* __restrict__ vOff, const int32_t* __restrict__ chd,
-                  const int32_t* __restrict__ srcSlot, const int32_t* __restrict__ trgSlot,
-                  const float2* __restrict__ effDen, int64_t denRhs, const float2* __restrict__ T,
-                  float2* __restrict__ effVal, int64_t valRhs, int nEff, int nrhs, float nrmfc) {
-  extern __shared__ float2 Ts[];  // [316][32]
-  const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
-  const int f0 = blockIdx.y * 32;
-  const int f = f0 + lane;
-  const int rhs0 = blockIdx.z * KB;
-  for (int i = threadIdx.x; i < 316 * 32; i += blockDim.x) {
-    const int id = i >> 5, ff = f0 + (i & 31);
-    Ts[i] = ff < nEff ? T[(int64_t)id * nEff + ff] : make_float2(0.f, 0.f);
-  }
-  __syncthreads();
-  const bool fin = f < nEff;
-  const int cx = c >> 2, cy = (c >> 1) & 1, cz = c & 1;
-  const int pEnd = min(nP, (int)(blockIdx.x + 1) * HAD_PPB);
-  for (int b = blockIdx.x * HAD_PPB; b < pEnd; b++) {
-    const int P = parents[b];
-    const int ts = trgSlot[chd[P] + c];
-    if (ts < 0) continue;
-    float2 acc[KB];
-#pragma unroll
-    for (int q = 0; q < KB; q++) acc[q] = make_float2(0.f, 0.f);
-    for (int64_t e = vPtr[b]; e < vPtr[b + 1]; e++) {
-      const int Q = vIdx[e];
-      const int off = vOff[e];
-      const int dx = off / 9 - 1, dy = (off / 3) % 3 - 1, dz = off % 3 - 1;
-      const int q0 = chd[Q];
-#pragma unroll 2
-      for (int c2 = 0; c2 < 8; c2++) {
-        const int s = srcSlot[q0 + c2];
-        const int rx = 2 * dx + (c2 >> 2) - cx, ry = 2 * dy + ((c2 >> 1) & 1) - cy, rz = 2 * dz + (c2 & 1) - cz;
-        if (s < 0 || max(abs(rx), max(abs(ry), abs(rz))) <= 1 || !fin) continue;
-        const float2 w = Ts[c_transId32[(rx + 3) * 49 + (ry + 3) * 7 + (rz + 3)] * 32 + lane];
-        const float2* dp = effDen + (int64_t)s * nEff + f;
-#pragma unroll
-        for (int q = 0; q < KB; q++) {
-          if (rhs0 + q < nrhs) {
-            const float2 d = dp[(rhs0 + q) * denRhs];
-            acc[q].x += w.x * d.x - w.y * d.y;
-            acc[q].y += w.x * d.y + w.y * d.x;
-          }
-        }
-      }
-    }
-    if (fin) {
-#pragma unroll
-      for (int q = 0; q < KB; q++)
-        if (rhs0 + q < nrhs)
-          effVal[(rhs0 + q) * valRhs + (int64_t)ts * nEff + f] = make_float2(acc[q].x * nrmfc, acc[q].y * nrmfc);
-    }
-  }
-}
-
 // grid (target slots, right-hand sides)
 template <int NP>
 __global__ void __launch_bounds__(128)
@@ -838,12 +775,13 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
                                                    D.vTrgSlot, D.effDen32, effDR, D.m2lT32, D.effVal32, effVR, \
                                                    P.nEff, kc, nrmfc)
     if (P.sdm == 1 && P.tdm == 1) {
-      const size_t smem = 316 * 32 * sizeof(float2);
-      cudaFuncSetAttribute(k_m2l_had32_s<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      dim3 g2((npar + HAD_PPB - 1) / HAD_PPB, (P.nEff + 31) / 32, kb);
-      k_m2l_had32_s<KB><<<g2, 256, smem, st>>>(npar, D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot,
-                                                D.vTrgSlot, D.effDen32, effDR, D.m2lT32, D.effVal32, effVR, P.nEff,
-                                                kc, nrmfc);
+      const size_t smem = had_smem_bytes<float2>();
+      cudaFuncSetAttribute(k_m2l_had_smem<float2, KB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+      dim3 g2((npar + HS_PPB - 1) / HS_PPB, (P.nEff + 31) / 32, kb);
+      k_m2l_had_smem<float2, KB, false><<<g2, HS_THREADS, smem, st>>>(
+          npar, D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot, D.vTrgSlot, D.transIdDev, D.effDen32,
+          effDR, D.m2lT32, D.effVal32, effVR, P.nEff, kc, nrmfc);
     } else if (P.sdm == 4 && P.tdm == 3) FMMG_HAD32(4, 3);
     else FMMG_HAD32(3, 3);
 #undef FMMG_HAD32

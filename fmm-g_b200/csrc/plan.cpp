@@ -312,6 +312,56 @@ void Plan::build_worklists() {
   }
 }
 
+// Inverse of a CSR (rows -> column ids): for every id that occurs, the rows
+// (given by their own node ids) that list it, in increasing row order.
+static void invert_csr(const std::vector<int32_t>& rows, const CSR& L, int nn, std::vector<int32_t>& outRows,
+                       CSR& out) {
+  std::vector<int64_t> cnt(nn + 1, 0);
+  for (int32_t v : L.idx) cnt[v + 1]++;
+  for (int i = 0; i < nn; i++) cnt[i + 1] += cnt[i];
+  std::vector<int32_t> tmp(L.idx.size());
+  std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
+  for (size_t r = 0; r < rows.size(); r++)
+    for (int64_t e = L.ptr[r]; e < L.ptr[r + 1]; e++) tmp[fill[L.idx[e]]++] = rows[r];
+  outRows.clear();
+  out.clear();
+  for (int v = 0; v < nn; v++) {
+    if (cnt[v + 1] == cnt[v]) continue;
+    outRows.push_back(v);
+    out.idx.insert(out.idx.end(), tmp.begin() + cnt[v], tmp.begin() + cnt[v + 1]);
+    out.ptr.push_back((int64_t)out.idx.size());
+  }
+}
+
+// The transposed FMM runs every forward stage backwards: its direct sums go
+// from the forward targets to the forward sources, so each forward work list
+// is needed grouped by its other end.
+void Plan::build_adjoint_lists() {
+  invert_csr(evtrLeaves, nearSrc, nn, adjNearRows, adjNear);
+  invert_csr(farLeaves, farUE, nn, adjFarRows, adjFar);
+  invert_csr(s2lNodes, s2lSrc, nn, adjS2lRows, adjS2l);
+  // grouped M2L: (P, Q, d) -> (Q, P, -d)
+  std::vector<std::vector<std::pair<int32_t, int8_t>>> byQ(nn);
+  for (size_t r = 0; r < vParents.size(); r++)
+    for (int64_t e = vNbr.ptr[r]; e < vNbr.ptr[r + 1]; e++) {
+      int off = vNbrOff[e];
+      int dx = off / 9 - 1, dy = (off / 3) % 3 - 1, dz = off % 3 - 1;
+      byQ[vNbr.idx[e]].push_back({vParents[r], (int8_t)((-dx + 1) * 9 + (-dy + 1) * 3 + (-dz + 1))});
+    }
+  vParentsT.clear();
+  vNbrT.clear();
+  vNbrOffT.clear();
+  for (int q = 0; q < nn; q++) {
+    if (byQ[q].empty()) continue;
+    vParentsT.push_back(q);
+    for (auto& pr : byQ[q]) {
+      vNbrT.idx.push_back(pr.first);
+      vNbrOffT.push_back(pr.second);
+    }
+    vNbrT.ptr.push_back((int64_t)vNbrT.idx.size());
+  }
+}
+
 std::string Plan::build(const Options& opt, int64_t ns_, const double* src, const double* nrmIn, int64_t nt_,
                         const double* trg) {
   o = opt;
@@ -336,6 +386,7 @@ std::string Plan::build(const Options& opt, int64_t ns_, const double* src, cons
   }
   build_lists();
   build_worklists();
+  build_adjoint_lists();
   (void)nrmIn;
   return std::string();
 }

@@ -90,6 +90,18 @@ struct Plan {
   std::vector<int32_t> vTrgSlot;  // per node: row in the target-spectrum array or -1
   std::vector<int32_t> vTrgNodes; // slot -> node
 
+  // ---- adjoint (transposed FMM) work lists: every forward list inverted
+  std::vector<int32_t> adjNearRows;  // source leaves in some near list
+  CSR adjNear;                       // per row: the evaluator leaves that list it
+  std::vector<int32_t> adjFarRows;   // nodes used through their UE surface (M2T)
+  CSR adjFar;                        // per row: the evaluator leaves that list it
+  std::vector<int32_t> adjS2lRows;   // source leaves used by S2L
+  CSR adjS2l;                        // per row: the nodes whose DC surface they feed
+  std::vector<int32_t> vParentsT;    // source parents Q of the grouped M2L
+  CSR vNbrT;                         // per row: target parents P
+  std::vector<int8_t> vNbrOffT;      // offset code of P - Q
+  void build_adjoint_lists();
+
   // ---- operators (homogeneous equivalent kernels: unit-radius tables)
   // row-major for the GPU GEMMs:
   std::vector<double> uc2ue;     // [nUE*sdm][nUC*tdm]       C2E up (pinv)

@@ -24,6 +24,7 @@
 
 #include "cuda_common.cuh"
 #include "engine.hpp"
+#include "had_smem.cuh"
 #include "kernels.hpp"
 
 namespace fmmg {
@@ -552,53 +553,6 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Scalar equivalent kernels: the CTA stages its 32-frequency slice of all 316
-// translation spectra in shared memory (316 x 32 x 16 B = 158 KB) once and
-// then walks a block of HAD64_PPB target parents; warp c owns child c.
-constexpr int HAD64_PPB = 16;
-__global__ void __launch_bounds__(256)
-    k_m2l_had_s(int nP, const int32_t* __restrict__ parents, const int64_t* __restrict__ vPtr,
-                const int32_t* __restrict__ vIdx, const int8_t* __restrict__ vOff, const int32_t* __restrict__ chd,
-                const int32_t* __restrict__ srcSlot, const int32_t* __restrict__ trgSlot,
-                const double2* __restrict__ effDen, const double2* __restrict__ T, double2* __restrict__ effVal,
-                int nEff, double nrmfc) {
-  extern __shared__ double2 Tsd[];  // [316][32]
-  const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
-  const int f0 = blockIdx.y * 32;
-  const int f = f0 + lane;
-  for (int i = threadIdx.x; i < 316 * 32; i += blockDim.x) {
-    const int id = i >> 5, ff = f0 + (i & 31);
-    Tsd[i] = ff < nEff ? T[(int64_t)id * nEff + ff] : make_double2(0.0, 0.0);
-  }
-  __syncthreads();
-  const bool fin = f < nEff;
-  const int cx = c >> 2, cy = (c >> 1) & 1, cz = c & 1;
-  const int pEnd = min(nP, (int)(blockIdx.x + 1) * HAD64_PPB);
-  for (int b = blockIdx.x * HAD64_PPB; b < pEnd; b++) {
-    const int P = parents[b];
-    const int ts = trgSlot[chd[P] + c];
-    if (ts < 0) continue;
-    double2 acc = make_double2(0.0, 0.0);
-    for (int64_t e = vPtr[b]; e < vPtr[b + 1]; e++) {
-      const int Q = vIdx[e];
-      const int off = vOff[e];
-      const int dx = off / 9 - 1, dy = (off / 3) % 3 - 1, dz = off % 3 - 1;
-      const int q0 = chd[Q];
-#pragma unroll 2
-      for (int c2 = 0; c2 < 8; c2++) {
-        const int s = srcSlot[q0 + c2];
-        const int rx = 2 * dx + (c2 >> 2) - cx, ry = 2 * dy + ((c2 >> 1) & 1) - cy, rz = 2 * dz + (c2 & 1) - cz;
-        if (s < 0 || max(abs(rx), max(abs(ry), abs(rz))) <= 1 || !fin) continue;
-        const double2 w = Tsd[c_transId[(rx + 3) * 49 + (ry + 3) * 7 + (rz + 3)] * 32 + lane];
-        const double2 d = effDen[(int64_t)s * nEff + f];
-        acc.x += w.x * d.x - w.y * d.y;
-        acc.y += w.x * d.y + w.y * d.x;
-      }
-    }
-    if (fin) effVal[(int64_t)ts * nEff + f] = make_double2(acc.x * nrmfc, acc.y * nrmfc);
-  }
-}
-
 // k_m2l_inv: c2r of a target box's accumulated spectrum and gather onto its
 // DC surface, added to the downward check values (effVal2PlnVal,
 // matmgnt3d_mpi.cpp:333-371).  The x pass is FFTW's halved c2r: the kx = 0 and
@@ -737,6 +691,7 @@ void dev_free(DevState& D) {
   D.effDen32 = D.effVal32 = nullptr;
   D.uc2ue32 = D.m2m32 = D.dc2de32 = D.l2l32 = nullptr;
   D.upF1 = D.upF2 = D.dnF1 = D.dnF2 = D.upT32 = D.dnT32 = nullptr;
+  D.transIdDev = nullptr;
   D.m2lT32 = nullptr;
   D.denK = D.valK = nullptr;
   D.mixedReady = false;
@@ -763,6 +718,7 @@ std::string dev_upload_operators(const Plan& P, DevState& D) {
   int16_t tid[343];
   for (int i = 0; i < 343; i++) tid[i] = (int16_t)P.transId[i / 49][(i / 7) % 7][i % 7];
   FMMG_CK(cudaMemcpyToSymbol(c_transId, tid, sizeof(tid)));
+  if (!D.transIdDev) FMMG_TRY(dput(D, D.transIdDev, tid, 343));
   D.mixedOpsStale = true;
   return std::string();
 }
@@ -953,11 +909,13 @@ static void launch_m2l_np(const Plan& P, DevState& D, LaunchStats* ls) {
     dim3 grid(npar, (P.nEff + 31) / 32);
     const double nrmfc = 1.0 / double(P.nReg);
     if (P.sdm == 1 && P.tdm == 1) {
-      const size_t smem = 316 * 32 * sizeof(double2);
-      cudaFuncSetAttribute(k_m2l_had_s, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      dim3 g2((npar + HAD64_PPB - 1) / HAD64_PPB, (P.nEff + 31) / 32);
-      k_m2l_had_s<<<g2, 256, smem, D.stream>>>(npar, D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot,
-                                               D.vTrgSlot, D.effDen, D.m2lT, D.effVal, P.nEff, nrmfc);
+      const size_t smem = had_smem_bytes<double2>();
+      cudaFuncSetAttribute(k_m2l_had_smem<double2, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+      dim3 g2((npar + HS_PPB - 1) / HS_PPB, (P.nEff + 31) / 32, 1);
+      k_m2l_had_smem<double2, 1, false><<<g2, HS_THREADS, smem, D.stream>>>(
+          npar, D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot, D.vTrgSlot, D.transIdDev, D.effDen, 0,
+          D.m2lT, D.effVal, 0, P.nEff, 1, nrmfc);
     }
     else if (P.sdm == 4 && P.tdm == 3)
       k_m2l_had<4, 3><<<grid, 256, 0, D.stream>>>(D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot, D.vTrgSlot,
