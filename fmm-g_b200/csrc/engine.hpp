@@ -50,6 +50,8 @@ struct DevState {
   std::vector<int64_t> offUpC2E, offUpM2M, offDnL2L, offDnC2E;  // host offsets into levelRows, size maxDepth+2
   int32_t *vParents = nullptr; int64_t *vPtr = nullptr; int32_t *vIdx = nullptr; int8_t *vOff = nullptr;
   int32_t *vSrcSlot = nullptr, *vTrgSlot = nullptr, *vSrcNodes = nullptr, *vTrgNodes = nullptr;
+  int64_t *vTrgPtr = nullptr, *vSrcPtr = nullptr;   // expanded V-lists per target / source slot
+  int32_t *vTrgEnt = nullptr, *vSrcEnt = nullptr;   // (slot, translation id) pairs
   // operators
   double *uc2ue = nullptr, *m2m = nullptr, *dc2de = nullptr, *l2l = nullptr;
   double2* m2lT = nullptr;

@@ -4,23 +4,22 @@
 //   effVal(c)[f] = (1/(2np)^3) sum_{v in V(c)} T_{v-c}[f] effDen(v)[f]
 //   (cptwvv, fmm3d_mpi/matmgnt3d_mpi.cpp:414-429)
 //
-// One CTA owns a 32-frequency slice (lane = frequency) and stages the slice
-// of all 316 translation spectra in shared memory once; it then walks a block
-// of HS_PPB target parents, HS_SLOTS of them at a time: warp w handles child
-// w % 8 of parent slot w / 8.  The loop over the 8 children of a neighbour
-// parent is unrolled so their slot, spectrum and translation loads issue
-// together.  With ADJ the same kernel applies the transposed operator on the
-// inverted lists: the translation index is reflected and the spectrum
-// conjugated (circular correlation instead of convolution).
+// One CTA owns a 32-frequency slice (lane = frequency) and stages that slice
+// of all 316 translation spectra in shared memory once.  Each warp then takes
+// one output box at a time and walks its expanded interaction list of
+// (input spectrum slot, translation id) pairs -- a warp-uniform load, one
+// shared-memory load and KB spectrum loads per pair.  Sibling output boxes are
+// adjacent in the slot order, so concurrent warps share most input spectra in
+// L1.  With CONJ the conjugated spectra are used: run on the lists inverted per
+// source box, that is the transposed operator (circular correlation).
 #pragma once
 
 #include <cuda_runtime.h>
 
 namespace fmmg {
 
-constexpr int HS_SLOTS = 4;   // parents in flight per CTA
-constexpr int HS_PPB = 32;    // parents per CTA
-constexpr int HS_THREADS = HS_SLOTS * 256;
+constexpr int HS_THREADS = 1024;
+constexpr int HS_BOXES = 128;  // output boxes per CTA
 
 template <typename C>
 struct CplxOps;
@@ -35,20 +34,15 @@ struct CplxOps<float2> {
   static __device__ __forceinline__ float2 zero() { return make_float2(0.f, 0.f); }
 };
 
-template <typename C, int KB, bool ADJ>
+template <typename C, int KB, bool CONJ>
 __global__ void __launch_bounds__(HS_THREADS)
-    k_m2l_had_smem(int nP, const int32_t* __restrict__ parents, const int64_t* __restrict__ vPtr,
-                   const int32_t* __restrict__ vIdx, const int8_t* __restrict__ vOff, const int32_t* __restrict__ chd,
-                   const int32_t* __restrict__ srcSlot, const int32_t* __restrict__ trgSlot,
-                   const int16_t* __restrict__ transId, const C* __restrict__ effDen, int64_t denRhs,
-                   const C* __restrict__ T, C* __restrict__ effVal, int64_t valRhs, int nEff, int nrhs,
-                   typename CplxOps<C>::R nrmfc) {
+    k_m2l_had_list(int nOut, const int64_t* __restrict__ lptr, const int2* __restrict__ lent,
+                   const C* __restrict__ effIn, int64_t inRhs, const C* __restrict__ T, C* __restrict__ effOut,
+                   int64_t outRhs, int nEff, int nrhs, typename CplxOps<C>::R nrmfc) {
   typedef typename CplxOps<C>::R R;
   extern __shared__ unsigned char hs_smem[];
-  C* Ts = reinterpret_cast<C*>(hs_smem);                            // [316][32]
-  int16_t* ids = reinterpret_cast<int16_t*>(Ts + 316 * 32);          // [343]
+  C* Ts = reinterpret_cast<C*>(hs_smem);  // [316][32]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int slotP = warp >> 3, c = warp & 7;
   const int f0 = blockIdx.y * 32;
   const int f = f0 + lane;
   const int rhs0 = blockIdx.z * KB;
@@ -56,62 +50,43 @@ __global__ void __launch_bounds__(HS_THREADS)
     const int id = i >> 5, ff = f0 + (i & 31);
     Ts[i] = ff < nEff ? T[(int64_t)id * nEff + ff] : CplxOps<C>::zero();
   }
-  for (int i = threadIdx.x; i < 343; i += blockDim.x) ids[i] = transId[i];
   __syncthreads();
-  const bool fin = f < nEff;
-  const int cx = c >> 2, cy = (c >> 1) & 1, cz = c & 1;
-  const int pEnd = min(nP, (int)(blockIdx.x + 1) * HS_PPB);
-  for (int b = blockIdx.x * HS_PPB + slotP; b < pEnd; b += HS_SLOTS) {
-    const int P = parents[b];
-    const int ts = trgSlot[chd[P] + c];
-    if (ts < 0) continue;
+  if (f >= nEff) return;
+  const int tEnd = min(nOut, (int)(blockIdx.x + 1) * HS_BOXES);
+  for (int t = blockIdx.x * HS_BOXES + warp; t < tEnd; t += HS_THREADS / 32) {
     C acc[KB];
 #pragma unroll
     for (int q = 0; q < KB; q++) acc[q] = CplxOps<C>::zero();
-    const int64_t e1 = vPtr[b + 1];
-    for (int64_t e = vPtr[b]; e < e1; e++) {
-      const int Q = vIdx[e];
-      const int off = vOff[e];
-      const int dx = off / 9 - 1, dy = (off / 3) % 3 - 1, dz = off % 3 - 1;
-      const int q0 = chd[Q];
-      int sl[8];
+    const int64_t e1 = lptr[t + 1];
+#pragma unroll 4
+    for (int64_t e = lptr[t]; e < e1; e++) {
+      const int2 en = lent[e];
+      C w = Ts[en.y * 32 + lane];
+      if (CONJ) w.y = -w.y;
+      const C* dp = effIn + (int64_t)en.x * nEff + f;
 #pragma unroll
-      for (int c2 = 0; c2 < 8; c2++) sl[c2] = srcSlot[q0 + c2];
-#pragma unroll
-      for (int c2 = 0; c2 < 8; c2++) {
-        int rx = 2 * dx + (c2 >> 2) - cx, ry = 2 * dy + ((c2 >> 1) & 1) - cy, rz = 2 * dz + (c2 & 1) - cz;
-        const bool use = sl[c2] >= 0 && max(abs(rx), max(abs(ry), abs(rz))) > 1 && fin;
-        if (!use) continue;
-        if (ADJ) { rx = -rx; ry = -ry; rz = -rz; }
-        C w = Ts[ids[(rx + 3) * 49 + (ry + 3) * 7 + (rz + 3)] * 32 + lane];
-        if (ADJ) w.y = -w.y;
-        const C* dp = effDen + (int64_t)sl[c2] * nEff + f;
-#pragma unroll
-        for (int q = 0; q < KB; q++) {
-          if (rhs0 + q < nrhs) {
-            const C d = dp[(rhs0 + q) * denRhs];
-            acc[q].x += w.x * d.x - w.y * d.y;
-            acc[q].y += w.x * d.y + w.y * d.x;
-          }
+      for (int q = 0; q < KB; q++) {
+        if (rhs0 + q < nrhs) {
+          const C d = dp[(rhs0 + q) * inRhs];
+          acc[q].x += w.x * d.x - w.y * d.y;
+          acc[q].y += w.x * d.y + w.y * d.x;
         }
       }
     }
-    if (fin) {
 #pragma unroll
-      for (int q = 0; q < KB; q++)
-        if (rhs0 + q < nrhs) {
-          C o;
-          o.x = acc[q].x * (R)nrmfc;
-          o.y = acc[q].y * (R)nrmfc;
-          effVal[(rhs0 + q) * valRhs + (int64_t)ts * nEff + f] = o;
-        }
-    }
+    for (int q = 0; q < KB; q++)
+      if (rhs0 + q < nrhs) {
+        C o;
+        o.x = acc[q].x * (R)nrmfc;
+        o.y = acc[q].y * (R)nrmfc;
+        effOut[(rhs0 + q) * outRhs + (int64_t)t * nEff + f] = o;
+      }
   }
 }
 
 template <typename C>
 inline size_t had_smem_bytes() {
-  return 316 * 32 * sizeof(C) + 343 * sizeof(int16_t);
+  return 316 * 32 * sizeof(C);
 }
 
 }  // namespace fmmg

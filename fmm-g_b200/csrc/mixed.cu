@@ -776,12 +776,12 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
                                                    P.nEff, kc, nrmfc)
     if (P.sdm == 1 && P.tdm == 1) {
       const size_t smem = had_smem_bytes<float2>();
-      cudaFuncSetAttribute(k_m2l_had_smem<float2, KB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(k_m2l_had_list<float2, KB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
-      dim3 g2((npar + HS_PPB - 1) / HS_PPB, (P.nEff + 31) / 32, kb);
-      k_m2l_had_smem<float2, KB, false><<<g2, HS_THREADS, smem, st>>>(
-          npar, D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot, D.vTrgSlot, D.transIdDev, D.effDen32,
-          effDR, D.m2lT32, D.effVal32, effVR, P.nEff, kc, nrmfc);
+      dim3 g2((ntrg + HS_BOXES - 1) / HS_BOXES, (P.nEff + 31) / 32, kb);
+      k_m2l_had_list<float2, KB, false><<<g2, HS_THREADS, smem, st>>>(
+          ntrg, D.vTrgPtr, (const int2*)D.vTrgEnt, D.effDen32, effDR, D.m2lT32, D.effVal32, effVR, P.nEff, kc,
+          nrmfc);
     } else if (P.sdm == 4 && P.tdm == 3) FMMG_HAD32(4, 3);
     else FMMG_HAD32(3, 3);
 #undef FMMG_HAD32

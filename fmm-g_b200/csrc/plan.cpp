@@ -310,6 +310,44 @@ void Plan::build_worklists() {
       }
     }
   }
+  // expanded per-target lists: v = child c2 of Q, c = child of P, idx = v - c
+  vTrgPtr.assign(vTrgNodes.size() + 1, 0);
+  vTrgEnt.clear();
+  std::vector<std::vector<std::pair<int32_t, int32_t>>> bySrc(vSrcNodes.size());
+  for (size_t r = 0; r < vParents.size(); r++) {
+    const int P = vParents[r];
+    for (int c = 0; c < 8; c++) {
+      const int t = chd[P] + c;
+      const int ts = vTrgSlot[t];
+      if (ts < 0) continue;
+      for (int64_t e = vNbr.ptr[r]; e < vNbr.ptr[r + 1]; e++) {
+        const int Q = vNbr.idx[e], off = vNbrOff[e];
+        const int dx = off / 9 - 1, dy = (off / 3) % 3 - 1, dz = off % 3 - 1;
+        for (int c2 = 0; c2 < 8; c2++) {
+          const int s = vSrcSlot[chd[Q] + c2];
+          if (s < 0) continue;
+          const int rx = 2 * dx + (c2 >> 2) - (c >> 2), ry = 2 * dy + ((c2 >> 1) & 1) - ((c >> 1) & 1),
+                    rz = 2 * dz + (c2 & 1) - (c & 1);
+          if (std::max(std::abs(rx), std::max(std::abs(ry), std::abs(rz))) <= 1) continue;
+          const int id = transId[rx + 3][ry + 3][rz + 3];
+          vTrgEnt.push_back(s);
+          vTrgEnt.push_back(id);
+          bySrc[s].push_back({ts, id});
+        }
+      }
+      vTrgPtr[ts + 1] = (int64_t)vTrgEnt.size() / 2;
+    }
+  }
+  for (size_t t = 1; t < vTrgPtr.size(); t++) vTrgPtr[t] = std::max(vTrgPtr[t], vTrgPtr[t - 1]);
+  vSrcPtr.assign(vSrcNodes.size() + 1, 0);
+  vSrcEnt.clear();
+  for (size_t s2 = 0; s2 < bySrc.size(); s2++) {
+    for (auto& pr : bySrc[s2]) {
+      vSrcEnt.push_back(pr.first);
+      vSrcEnt.push_back(pr.second);
+    }
+    vSrcPtr[s2 + 1] = (int64_t)vSrcEnt.size() / 2;
+  }
 }
 
 // Inverse of a CSR (rows -> column ids): for every id that occurs, the rows

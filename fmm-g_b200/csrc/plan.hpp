@@ -89,6 +89,12 @@ struct Plan {
   std::vector<int32_t> vSrcNodes; // slot -> node
   std::vector<int32_t> vTrgSlot;  // per node: row in the target-spectrum array or -1
   std::vector<int32_t> vTrgNodes; // slot -> node
+  // the same V-lists expanded per target slot: (source slot, translation id),
+  // and inverted per source slot for the transposed operator
+  std::vector<int64_t> vTrgPtr;   // [nTrgSlots + 1]
+  std::vector<int32_t> vTrgEnt;   // pairs (source slot, translation id)
+  std::vector<int64_t> vSrcPtr;   // [nSrcSlots + 1]
+  std::vector<int32_t> vSrcEnt;   // pairs (target slot, translation id)
 
   // ---- adjoint (transposed FMM) work lists: every forward list inverted
   std::vector<int32_t> adjNearRows;  // source leaves in some near list

@@ -824,6 +824,10 @@ std::string dev_upload(const Plan& P, DevState& D, const double* src, const doub
   FMMG_TRY(dput(D, D.vTrgSlot, P.vTrgSlot));
   FMMG_TRY(dput(D, D.vSrcNodes, P.vSrcNodes));
   FMMG_TRY(dput(D, D.vTrgNodes, P.vTrgNodes));
+  FMMG_TRY(dput(D, D.vTrgPtr, P.vTrgPtr));
+  FMMG_TRY(dput(D, D.vTrgEnt, P.vTrgEnt));
+  FMMG_TRY(dput(D, D.vSrcPtr, P.vSrcPtr));
+  FMMG_TRY(dput(D, D.vSrcEnt, P.vSrcEnt));
   FMMG_TRY(dev_upload_operators(P, D));
   // work arrays
   const int64_t ue = (int64_t)P.nUE * P.sdm, uc = (int64_t)P.nUC * P.tdm;
@@ -910,12 +914,11 @@ static void launch_m2l_np(const Plan& P, DevState& D, LaunchStats* ls) {
     const double nrmfc = 1.0 / double(P.nReg);
     if (P.sdm == 1 && P.tdm == 1) {
       const size_t smem = had_smem_bytes<double2>();
-      cudaFuncSetAttribute(k_m2l_had_smem<double2, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(k_m2l_had_list<double2, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
-      dim3 g2((npar + HS_PPB - 1) / HS_PPB, (P.nEff + 31) / 32, 1);
-      k_m2l_had_smem<double2, 1, false><<<g2, HS_THREADS, smem, D.stream>>>(
-          npar, D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot, D.vTrgSlot, D.transIdDev, D.effDen, 0,
-          D.m2lT, D.effVal, 0, P.nEff, 1, nrmfc);
+      dim3 g2((ntrg + HS_BOXES - 1) / HS_BOXES, (P.nEff + 31) / 32, 1);
+      k_m2l_had_list<double2, 1, false><<<g2, HS_THREADS, smem, D.stream>>>(
+          ntrg, D.vTrgPtr, (const int2*)D.vTrgEnt, D.effDen, 0, D.m2lT, D.effVal, 0, P.nEff, 1, nrmfc);
     }
     else if (P.sdm == 4 && P.tdm == 3)
       k_m2l_had<4, 3><<<grid, 256, 0, D.stream>>>(D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot, D.vTrgSlot,
