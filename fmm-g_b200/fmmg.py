@@ -79,6 +79,8 @@ SIGNATURES = {
     "fmmg_tree": ([ctypes.c_void_p, _i32p, _i64p, _i64p], ctypes.c_int),
     "fmmg_lists": ([ctypes.c_void_p, ctypes.c_int, _i64p, _i32p, _i64p], ctypes.c_int),
     "fmmg_operator": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp, _i64p], ctypes.c_int),
+    "fmmg_dense_noalloc": ([ctypes.c_int, _dp, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                            ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "fmmg_last_error": ([ctypes.c_void_p], ctypes.c_char_p),
     "fmmg_destroy": ([ctypes.c_void_p], ctypes.c_int),
 }

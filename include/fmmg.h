@@ -185,6 +185,27 @@ fmmg_status fmmg_lists(const fmmg_handle* h, int which, int64_t* ptr, int32_t* i
 fmmg_status fmmg_operator(fmmg_handle* h, int which, int idx, double* get, const double* set,
                           int64_t* count);
 
+/* Dense FP64 direct sum that allocates no memory.  No counterpart in the
+ * reference.  For callers that cannot call cudaMalloc where they need the
+ * result -- work recorded while a stream is captured into a CUDA graph, code
+ * whose device memory is owned by a pool that forbids driver allocations, or
+ * latency-critical paths.  d_val[i*trgDOF+t] = sum over all sources of the
+ * kernel block times the density, like the reference check()'s dense sum
+ * (fmm3d_mpi/fmm3d_check_mpi.cpp:122-131); all arrays are device pointers in
+ * the caller's layout (xyz interleaved positions/normals, DOF interleaved
+ * densities/values); d_nrm may be NULL for single-layer kernels.  The
+ * accumulation scratch is a fixed array of 2^20 doubles inside the library on
+ * every GPU that loads it (held until the process exits): n_trg * trgDOF above
+ * 1,048,576 is rejected with FMMG_INVALID_ARG.  The first call on a device
+ * resolves the scratch address for that device and should come before any
+ * stream capture.  All calls on a device share the scratch: calls that overlap
+ * on the GPU race.  Work is enqueued on `stream` (a cudaStream_t, NULL = the
+ * default stream) and the call returns without synchronising.  Errors are
+ * reported by the status code only. */
+fmmg_status fmmg_dense_noalloc(int kernel_type, const double* coefs, int64_t n_src, const double* d_src,
+                               const double* d_nrm, const double* d_den, int64_t n_trg, const double* d_trg,
+                               double* d_val, void* stream);
+
 /* Message of the last failure on h (or of the last failed fmmg_create when
  * h == NULL).  Never NULL. */
 const char* fmmg_last_error(const fmmg_handle* h);
