@@ -31,6 +31,7 @@ struct fmmg_handle {
   double* dDenK = nullptr;  // k-RHS host-call staging
   double* dValK = nullptr;
   int ioK = 0;
+  double *dAdjW = nullptr, *dAdjG = nullptr, *dAdjGrad = nullptr;  // host-call staging of the adjoint
   std::vector<double> trgHost;  // caller-order targets for check()
   std::string err;
 };
@@ -159,6 +160,7 @@ fmmg_status fmmg_setup(fmmg_handle* h, int64_t ns, const double* src, const doub
       fmmg::dev_free(h->dev);
       h->dDenIO = h->dValIO = nullptr;
       h->dDenK = h->dValK = nullptr;
+      h->dAdjW = h->dAdjG = h->dAdjGrad = nullptr;
       h->ioK = 0;
       fmmg::Plan fresh;
       fresh.o = h->opt;
@@ -242,6 +244,57 @@ fmmg_status fmmg_evaluate_device(fmmg_handle* h, int k, const double* dDen, doub
       if (!e.empty()) return fail(h, FMMG_CUDA_ERROR, e);
       h->launches += h->dev.lastLaunches;
     }
+  }
+  FMMG_GUARD(h)
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_adjoint_device(fmmg_handle* h, const double* dDen, const double* dW, double* dG, double* dGradT) {
+  fmmg_status s = ready(h);
+  if (s != FMMG_OK) return s;
+  if ((!dW && h->plan.nt > 0) || (dGradT && !dDen)) return fail(h, FMMG_INVALID_ARG, "NULL weight or density pointer");
+  if (dGradT && h->opt.kt != 111 && h->opt.kt != 121)
+    return fail(h, FMMG_NOT_SUPPORTED, "target-position gradient: Laplace kernels 111 and 121 only");
+  try {
+    std::string e = fmmg::dev_adjoint(h->plan, h->dev, dDen, dW, dG, dGradT, h->timing);
+    if (!e.empty()) return fail(h, e.find("cudaMalloc") != std::string::npos ? FMMG_OOM : FMMG_CUDA_ERROR, e);
+    h->launches = h->dev.lastLaunches;
+  }
+  FMMG_GUARD(h)
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_adjoint_host(fmmg_handle* h, const double* den, const double* w, double* g, double* gradT) {
+  fmmg_status s = ready(h);
+  if (s != FMMG_OK) return s;
+  if ((!w && h->plan.nt > 0) || (gradT && !den)) return fail(h, FMMG_INVALID_ARG, "NULL weight or density pointer");
+  try {
+    const size_t bs = sizeof(double) * (size_t)h->plan.ns * h->plan.sd;
+    const size_t bt = sizeof(double) * (size_t)h->plan.nt * h->plan.td;
+    const size_t bg = sizeof(double) * 3 * (size_t)h->plan.nt;
+    auto get = [&](double*& p, size_t n) {
+      if (!p) {
+        void* q = nullptr;
+        if (cudaMalloc(&q, std::max<size_t>(n, 8)) != cudaSuccess) return false;
+        h->dev.allocs.push_back(q);
+        p = (double*)q;
+      }
+      return true;
+    };
+    if (!get(h->dAdjW, bt) || !get(h->dAdjG, bs) || !get(h->dAdjGrad, bg))
+      return fail(h, FMMG_OOM, "cudaMalloc adjoint buffers");
+    cudaStream_t st = h->dev.stream;
+    cudaError_t ce = cudaSuccess;
+    if (bt) ce = cudaMemcpyAsync(h->dAdjW, w, bt, cudaMemcpyHostToDevice, st);
+    if (ce == cudaSuccess && gradT) ce = cudaMemcpyAsync(h->dDenIO, den, bs, cudaMemcpyHostToDevice, st);
+    if (ce != cudaSuccess) return fail(h, FMMG_CUDA_ERROR, cudaGetErrorString(ce));
+    s = fmmg_adjoint_device(h, gradT ? h->dDenIO : nullptr, h->dAdjW, g ? h->dAdjG : nullptr,
+                            gradT ? h->dAdjGrad : nullptr);
+    if (s != FMMG_OK) return s;
+    if (g) ce = cudaMemcpyAsync(g, h->dAdjG, bs, cudaMemcpyDeviceToHost, st);
+    if (ce == cudaSuccess && gradT && bg) ce = cudaMemcpyAsync(gradT, h->dAdjGrad, bg, cudaMemcpyDeviceToHost, st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    if (ce != cudaSuccess) return fail(h, FMMG_CUDA_ERROR, cudaGetErrorString(ce));
   }
   FMMG_GUARD(h)
   return FMMG_OK;

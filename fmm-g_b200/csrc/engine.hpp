@@ -70,6 +70,14 @@ struct DevState {
   bool mixedReady = false, mixedOpsStale = true;
   int mixedK = 0;                           // right-hand sides the mixed arrays hold
   double mixedBudgetBytes = 48e9;           // device bytes for per-density work arrays
+  // transposed FMM: inverted work lists, transposed operator tables, target-gradient buffer
+  int32_t *adjNearRows = nullptr, *adjNearIdx = nullptr; int64_t *adjNearPtr = nullptr;
+  int32_t *adjFarRows = nullptr, *adjFarIdx = nullptr; int64_t *adjFarPtr = nullptr;
+  int32_t *adjS2lRows = nullptr, *adjS2lIdx = nullptr; int64_t *adjS2lPtr = nullptr;
+  double *uc2ueT = nullptr, *m2mT = nullptr, *dc2deT = nullptr, *l2lT = nullptr;
+  double* gradT = nullptr;  // [nt][3] permuted order
+  bool adjListsReady = false, adjOpsStale = true;
+  float adjMs = 0.f;
   // dense check scratch
   double *chkPos = nullptr, *chkOut = nullptr;
   size_t chkCap = 0;
@@ -97,6 +105,29 @@ std::string dev_evaluate(const Plan& P, DevState& D, const double* dDenCaller, d
 // times are those of the last chunk of right-hand sides
 std::string dev_evaluate_mixed(const Plan& P, DevState& D, const double* dDenCaller, double* dValCaller, int k,
                                int stageMask, bool timed, LaunchStats* st);
+// FP64 building blocks shared with the adjoint (stages.cu)
+struct Scale4;
+void gemm_rows(cudaStream_t st, int nrows, const int32_t* rows, const int32_t* chd, int xChild, int yChild,
+               const double* X, int64_t ldx, const double* W, double* Y, int64_t ldy, int K, int N, Scale4 xs,
+               Scale4 ys, double beta, LaunchStats* ls);
+void spectral_fwd(const Plan& P, DevState& D, int n, const int32_t* nodes, Scale4 deg, int dof, const double* x,
+                  double2* spec);
+void spectral_inv(const Plan& P, DevState& D, int n, const int32_t* nodes, int dof, const double2* spec, double* y,
+                  Scale4 outDeg);
+void hadamard_list64(const Plan& P, DevState& D, int nOut, const int64_t* ptr, const int32_t* ent, const double2* in,
+                     double2* out, bool conj);
+// internal stage bit: run upward, V, X (S2L) and downward stages only, leaving
+// the target values untouched (the far field the target gradient needs)
+constexpr int STAGE_NO_TARGETS = 256;
+// permutation helpers: out[i] = in[perm[i]] (gather), out[perm[i]] = in[i] (scatter)
+void gather_rows(cudaStream_t st, int64_t n, int dof, const int64_t* perm, const double* in, double* out);
+void scatter_rows(cudaStream_t st, int64_t n, int dof, const int64_t* perm, const double* in, double* out);
+// forward stages into the handle's work arrays for density dDen (caller order)
+std::string dev_far_field(const Plan& P, DevState& D, const double* dDen);
+// transposed FMM: g = A^T w for one right-hand side (caller order), and with
+// gradT != nullptr the target-position gradient of <w, A sigma> ([nt][3])
+std::string dev_adjoint(const Plan& P, DevState& D, const double* dDen, const double* dW, double* dG,
+                        double* dGradT, bool timed);
 // dense FP64 sums at device positions (caller-order source arrays are the
 // permuted copies held on the device plus the permuted density)
 std::string dev_dense(const Plan& P, DevState& D, const double* dDenCaller, int64_t nchk,

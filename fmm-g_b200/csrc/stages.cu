@@ -561,7 +561,8 @@ __global__ void __launch_bounds__(256)
 template <int NP>
 __global__ void __launch_bounds__(128)
     k_m2l_inv(const int32_t* __restrict__ nodes, const double2* __restrict__ effVal, int nEff, int tdm,
-              const int32_t* __restrict__ ijk, int nDC, double* __restrict__ dchk) {
+              const int32_t* __restrict__ ijk, int nDC, double* __restrict__ dchk, const int32_t* __restrict__ depth,
+              int rootLevel, Scale4 outScale) {
   using F = FftDims<NP>;
   constexpr int N = F::N, NH = F::NH, H = F::H;
   __shared__ double2 Y2[NP * N * NH];
@@ -613,7 +614,8 @@ __global__ void __launch_bounds__(128)
         double2 t = cmulc(y1[kx], tw[(kx * x) % N]);
         s += (kx == 0 || kx == N / 2) ? t.x : 2.0 * t.x;
       }
-      dchk[(int64_t)node * nDC * tdm + (int64_t)i * tdm + m] += s;
+      dchk[(int64_t)node * nDC * tdm + (int64_t)i * tdm + m] +=
+          outScale.mod ? s * exp2((depth[node] + rootLevel) * outScale.v[m]) : s;
     }
     __syncthreads();
   }
@@ -658,6 +660,11 @@ void dev_free(DevState& D) {
   D.transIdDev = nullptr;
   D.m2lT32 = nullptr;
   D.denK = D.valK = nullptr;
+  D.adjNearRows = D.adjNearIdx = D.adjFarRows = D.adjFarIdx = D.adjS2lRows = D.adjS2lIdx = nullptr;
+  D.adjNearPtr = D.adjFarPtr = D.adjS2lPtr = nullptr;
+  D.uc2ueT = D.m2mT = D.dc2deT = D.l2lT = D.gradT = nullptr;
+  D.adjListsReady = false;
+  D.adjOpsStale = true;
   D.mixedReady = false;
   D.mixedOpsStale = true;
   D.mixedK = 0;
@@ -684,6 +691,7 @@ std::string dev_upload_operators(const Plan& P, DevState& D) {
   FMMG_CK(cudaMemcpyToSymbol(c_transId, tid, sizeof(tid)));
   if (!D.transIdDev) FMMG_TRY(dput(D, D.transIdDev, tid, 343));
   D.mixedOpsStale = true;
+  D.adjOpsStale = true;
   return std::string();
 }
 
@@ -812,7 +820,7 @@ std::string dev_upload(const Plan& P, DevState& D, const double* src, const doub
 }
 
 // ------------------------------------------------------------------ launcher
-static void gemm_rows(cudaStream_t st, int nrows, const int32_t* rows, const int32_t* chd, int xChild, int yChild,
+void gemm_rows(cudaStream_t st, int nrows, const int32_t* rows, const int32_t* chd, int xChild, int yChild,
                       const double* X, int64_t ldx, const double* W, double* Y, int64_t ldy, int K, int N,
                       Scale4 xs, Scale4 ys, double beta, LaunchStats* ls) {
   if (nrows <= 0) return;
@@ -891,10 +899,69 @@ static void launch_m2l_np(const Plan& P, DevState& D, LaunchStats* ls) {
       k_m2l_had<3, 3><<<grid, 256, 0, D.stream>>>(D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot, D.vTrgSlot,
                                                   D.effDen, D.m2lT, D.effVal, P.nEff, nrmfc);
     cudaEventRecord(D.ev[EV_M2L_HAD], D.stream);
-    k_m2l_inv<NP><<<ntrg, 128, 0, D.stream>>>(D.vTrgNodes, D.effVal, P.nEff, P.tdm, D.surfIJK, P.nDC, D.dchk);
+    Scale4 none;
+    none.mod = 0;
+    k_m2l_inv<NP><<<ntrg, 128, 0, D.stream>>>(D.vTrgNodes, D.effVal, P.nEff, P.tdm, D.surfIJK, P.nDC, D.dchk,
+                                              D.depth, P.o.rootLevel, none);
     if (ls) ls->launches += 2;
   } else {
     cudaEventRecord(D.ev[EV_M2L_HAD], D.stream);
+  }
+}
+
+// FP64 spectral transforms on arbitrary node lists (used by the adjoint):
+// r2c of 2^(l*deg) .* x[node] on the np-surface, and c2r + gather added into
+// y[node] (times 2^(l*outDeg) when outDeg.mod != 0).
+template <int NP>
+static void fwd_np(const Plan& P, DevState& D, int n, const int32_t* nodes, Scale4 deg, int dof, const double* x,
+                   double2* spec) {
+  k_m2l_fwd<NP><<<n, 128, 0, D.stream>>>(nodes, D.depth, P.o.rootLevel, deg, dof, x, D.surfIJK, P.nUE, spec, P.nEff);
+}
+template <int NP>
+static void inv_np(const Plan& P, DevState& D, int n, const int32_t* nodes, int dof, const double2* spec, double* y,
+                   Scale4 outDeg) {
+  k_m2l_inv<NP><<<n, 128, 0, D.stream>>>(nodes, spec, P.nEff, dof, D.surfIJK, P.nDC, y, D.depth, P.o.rootLevel,
+                                         outDeg);
+}
+void spectral_fwd(const Plan& P, DevState& D, int n, const int32_t* nodes, Scale4 deg, int dof, const double* x,
+                  double2* spec) {
+  if (n <= 0) return;
+  switch (P.o.np) {
+    case 3: fwd_np<3>(P, D, n, nodes, deg, dof, x, spec); break;
+    case 4: fwd_np<4>(P, D, n, nodes, deg, dof, x, spec); break;
+    case 5: fwd_np<5>(P, D, n, nodes, deg, dof, x, spec); break;
+    case 6: fwd_np<6>(P, D, n, nodes, deg, dof, x, spec); break;
+    case 7: fwd_np<7>(P, D, n, nodes, deg, dof, x, spec); break;
+    case 8: fwd_np<8>(P, D, n, nodes, deg, dof, x, spec); break;
+  }
+}
+void spectral_inv(const Plan& P, DevState& D, int n, const int32_t* nodes, int dof, const double2* spec, double* y,
+                  Scale4 outDeg) {
+  if (n <= 0) return;
+  switch (P.o.np) {
+    case 3: inv_np<3>(P, D, n, nodes, dof, spec, y, outDeg); break;
+    case 4: inv_np<4>(P, D, n, nodes, dof, spec, y, outDeg); break;
+    case 5: inv_np<5>(P, D, n, nodes, dof, spec, y, outDeg); break;
+    case 6: inv_np<6>(P, D, n, nodes, dof, spec, y, outDeg); break;
+    case 7: inv_np<7>(P, D, n, nodes, dof, spec, y, outDeg); break;
+    case 8: inv_np<8>(P, D, n, nodes, dof, spec, y, outDeg); break;
+  }
+}
+// the scalar Hadamard step on expanded lists; conj selects the transposed operator
+void hadamard_list64(const Plan& P, DevState& D, int nOut, const int64_t* ptr, const int32_t* ent, const double2* in,
+                     double2* out, bool conj) {
+  if (nOut <= 0) return;
+  const size_t smem = had_smem_bytes<double2>();
+  dim3 g2((nOut + HS_BOXES - 1) / HS_BOXES, (P.nEff + 31) / 32, 1);
+  const double nrmfc = 1.0 / double(P.nReg);
+  if (conj) {
+    cudaFuncSetAttribute(k_m2l_had_list<double2, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_m2l_had_list<double2, 1, true><<<g2, HS_THREADS, smem, D.stream>>>(nOut, ptr, (const int2*)ent, in, 0, D.m2lT,
+                                                                         out, 0, P.nEff, 1, nrmfc);
+  } else {
+    cudaFuncSetAttribute(k_m2l_had_list<double2, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_m2l_had_list<double2, 1, false><<<g2, HS_THREADS, smem, D.stream>>>(nOut, ptr, (const int2*)ent, in, 0,
+                                                                          D.m2lT, out, 0, P.nEff, 1, nrmfc);
   }
 }
 
@@ -914,6 +981,7 @@ static void run_stages(const Plan& P, DevState& D, int mask, LaunchStats* ls) {
   cudaStream_t st = D.stream;
   const int ue = P.nUE * P.sdm, uc = P.nUC * P.tdm, de = P.nDE * P.sdm, dc = P.nDC * P.tdm;
   const int rl = P.o.rootLevel;
+  const bool trgOut = !(mask & STAGE_NO_TARGETS);
   if (mask & 1)  // upward: S2M
     launch_s2surf<KT>(P, D, (int)P.s2mLeaves.size(), D.s2mLeaves, nullptr, nullptr, D.sam[1], P.nUC, D.uchk, uc, ls);
   cudaEventRecord(D.ev[EV_S2M], st);
@@ -928,7 +996,8 @@ static void run_stages(const Plan& P, DevState& D, int mask, LaunchStats* ls) {
     }
   }
   cudaEventRecord(D.ev[EV_UP_GEMM], st);
-  if ((mask & 2) && (mask & 8) && (mask & 16)) {
+  if (!trgOut) {
+  } else if ((mask & 2) && (mask & 8) && (mask & 16)) {
     launch_near<KT>(P, D, D.nearPtr, D.nearIdx, ls);
   } else {
     if (mask & 2) launch_near<KT>(P, D, D.nearUPtr, D.nearUIdx, ls);
@@ -943,7 +1012,7 @@ static void run_stages(const Plan& P, DevState& D, int mask, LaunchStats* ls) {
     cudaEventRecord(D.ev[EV_M2L_HAD], st);
   }
   cudaEventRecord(D.ev[EV_M2L_INV], st);
-  if (mask & 8) launch_e2t(P, D, 0, 1, ls);
+  if ((mask & 8) && trgOut) launch_e2t(P, D, 0, 1, ls);
   cudaEventRecord(D.ev[EV_M2T], st);
   if (mask & 16)
     launch_s2surf<KT>(P, D, (int)P.s2lNodes.size(), D.s2lNodes, D.s2lPtr, D.s2lIdx, D.sam[3], P.nDC, D.dchk, dc, ls);
@@ -961,7 +1030,7 @@ static void run_stages(const Plan& P, DevState& D, int mask, LaunchStats* ls) {
     }
   }
   cudaEventRecord(D.ev[EV_DN_GEMM], st);
-  if (mask & 32) launch_e2t(P, D, 1, 0, ls);  // L2T
+  if ((mask & 32) && trgOut) launch_e2t(P, D, 1, 0, ls);  // L2T
   cudaEventRecord(D.ev[EV_L2T], st);
 }
 
@@ -1004,6 +1073,26 @@ std::string dev_evaluate(const Plan& P, DevState& D, const double* dDen, double*
     D.stageMs[5] = m[EV_DN_GEMM - 1] + m[EV_L2T - 1];
     cudaEventElapsedTime(&D.stageMs[6], D.ev[EV_BEGIN], D.ev[EV_END]);
   }
+  return std::string();
+}
+
+void gather_rows(cudaStream_t st, int64_t n, int dof, const int64_t* perm, const double* in, double* out) {
+  if (n > 0) k_gather_den<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, dof, perm, in, out);
+}
+void scatter_rows(cudaStream_t st, int64_t n, int dof, const int64_t* perm, const double* in, double* out) {
+  if (n > 0) k_scatter_val<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, dof, perm, in, out);
+}
+
+std::string dev_far_field(const Plan& P, DevState& D, const double* dDen) {
+  cudaStream_t st = D.stream;
+  const int ue = P.nUE * P.sdm, uc = P.nUC * P.tdm, de = P.nDE * P.sdm, dc = P.nDC * P.tdm;
+  gather_rows(st, P.ns, P.sd, D.srcPerm, dDen, D.den);
+  FMMG_CK(cudaMemsetAsync(D.uchk, 0, sizeof(double) * (size_t)P.nn * uc, st));
+  FMMG_CK(cudaMemsetAsync(D.uden, 0, sizeof(double) * (size_t)P.nn * ue, st));
+  FMMG_CK(cudaMemsetAsync(D.dchk, 0, sizeof(double) * (size_t)P.nn * dc, st));
+  FMMG_CK(cudaMemsetAsync(D.dden, 0, sizeof(double) * (size_t)P.nn * de, st));
+  FMMG_DISPATCH_KT(P.o.kt, KT, run_stages<KT>(P, D, 63 | STAGE_NO_TARGETS, nullptr));
+  FMMG_CK(cudaGetLastError());
   return std::string();
 }
 
