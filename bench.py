@@ -202,6 +202,32 @@ def time_form(f, torch, stream, den_dev, out_dev, n, k, prec, steps, warmup, flu
     return ms, {name: v / steps for name, v in kern.items()}, launches
 
 
+def time_adjoint(f, torch, stream, den_dev, out_dev, n, steps, warmup, flush):
+    """FP64 transposed FMM (d/d density of <w, A sigma>) and the Laplace
+    target-position gradient, device time per step, with w = the first values."""
+    w = out_dev[0].contiguous()
+    g = torch.empty(n, dtype=torch.float64, device="cuda")
+    gt = torch.empty((n, 3), dtype=torch.float64, device="cuda")
+    res = {}
+    f.set_timing(False)  # no host synchronisation inside the timed calls
+    for key, call in (("ms_per_step", lambda: f.adjoint_device(None, w, g, None)),
+                      ("target_grad_ms_per_step", lambda: f.adjoint_device(den_dev[0], w, None, gt))):
+        for _ in range(max(warmup, 3)):
+            call()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for i in range(steps):
+            flush.zero_()
+            ev[i][0].record(stream)
+            call()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        res[key] = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    res["launches"] = f.launch_count()
+    f.set_timing(True)
+    return res
+
+
 def run_ours(args):
     import torch
     import fmmg
@@ -254,8 +280,14 @@ def run_ours(args):
         results.append(dict(precision=name, k=k, ms_per_step=ms, points_per_s=n * k * ws / (ms * 1e-3),
                             rel_err_vs_dense=rel, max_abs_err_vs_dense=mx, kernel_ms=kern,
                             stage_ms=f.stage_times(), launches=launches))
+    adj = time_adjoint(f, torch, stream, den, out, n, args.steps, args.warmup, flush)
+    if dist:
+        t = torch.tensor([adj["ms_per_step"], adj["target_grad_ms_per_step"]], device="cuda")
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        adj["ms_per_step"], adj["target_grad_ms_per_step"] = float(t[0].item()), float(t[1].item())
     clk = clocks.stop()
     fp64 = results[0]
+    adj["ratio_vs_fp64_forward"] = adj["ms_per_step"] / fp64["ms_per_step"]
     ok = [r for r in results if r["rel_err_vs_dense"] <= 1e-5]
     head = max(ok, key=lambda r: r["points_per_s"]) if ok else fp64
     prec_h = fmmg.PREC_FP64 if head["precision"] == "fp64" else fmmg.PREC_MIXED
@@ -302,7 +334,7 @@ def run_ours(args):
             "rel_err_vs_dense": head["rel_err_vs_dense"], "check_targets": CHECK_TARGETS,
             "fp64_points_per_s": fp64["points_per_s"],
             "speedup_vs_fp64": head["points_per_s"] / fp64["points_per_s"],
-            "forms": results, "setup_s": setup_s, "roofline": roof, "clocks": clk,
+            "forms": results, "adjoint": adj, "setup_s": setup_s, "roofline": roof, "clocks": clk,
         }
         if cpu:
             line["cpu_baseline"] = cpu

@@ -530,6 +530,10 @@ static std::string adj_prepare(const Plan& P, DevState& D) {
     FMMG_TRY(aj_put(D, D.adjS2lPtr, P.adjS2l.ptr.data(), P.adjS2l.ptr.size()));
     FMMG_TRY(aj_put(D, D.adjS2lIdx, P.adjS2l.idx.data(), P.adjS2l.idx.size()));
     FMMG_TRY(aj_put<double>(D, D.gradT, nullptr, 3 * (size_t)std::max<int64_t>(P.nt, 1)));
+    FMMG_TRY(aj_put(D, D.vParentsT, P.vParentsT.data(), P.vParentsT.size()));
+    FMMG_TRY(aj_put(D, D.vNbrTPtr, P.vNbrT.ptr.data(), P.vNbrT.ptr.size()));
+    FMMG_TRY(aj_put(D, D.vNbrTIdx, P.vNbrT.idx.data(), P.vNbrT.idx.size()));
+    FMMG_TRY(aj_put(D, D.vNbrOffT, P.vNbrOffT.data(), P.vNbrOffT.size()));
     D.adjListsReady = true;
   }
   if (D.adjOpsStale) {
@@ -618,7 +622,9 @@ static void run_adjoint(const Plan& P, DevState& D, int& launches) {
     none.mod = 1;
     none.v[0] = none.v[1] = none.v[2] = none.v[3] = 0.0;
     spectral_fwd(P, D, ntrg, D.vTrgNodes, none, P.tdm, D.dchk, D.effVal);
-    if (P.sdm == 1 && P.tdm == 1) {
+    if (P.sdm == 1 && P.tdm == 1 && D.hadPQ) {
+      hadamard_pq64_adj(P, D, D.effVal, D.effDen);
+    } else if (P.sdm == 1 && P.tdm == 1) {
       hadamard_list64(P, D, nsrc, D.vSrcPtr, D.vSrcEnt, D.effVal, D.effDen, true);
     } else {
       dim3 grid((nsrc + 7) / 8, (P.nEff + 31) / 32);

@@ -76,7 +76,9 @@ struct DevState {
   int32_t *adjS2lRows = nullptr, *adjS2lIdx = nullptr; int64_t *adjS2lPtr = nullptr;
   double *uc2ueT = nullptr, *m2mT = nullptr, *dc2deT = nullptr, *l2lT = nullptr;
   double* gradT = nullptr;  // [nt][3] permuted order
+  int32_t *vParentsT = nullptr, *vNbrTIdx = nullptr; int64_t *vNbrTPtr = nullptr; int8_t *vNbrOffT = nullptr;
   bool adjListsReady = false, adjOpsStale = true;
+  bool hadPQ = true;  // scalar Hadamard: parent-pair register-blocked kernel (else expanded lists)
   float adjMs = 0.f;
   // dense check scratch
   double *chkPos = nullptr, *chkOut = nullptr;
@@ -114,6 +116,8 @@ void spectral_fwd(const Plan& P, DevState& D, int n, const int32_t* nodes, Scale
                   double2* spec);
 void spectral_inv(const Plan& P, DevState& D, int n, const int32_t* nodes, int dof, const double2* spec, double* y,
                   Scale4 outDeg);
+// transposed scalar Hadamard on the parent pairs inverted per source parent
+void hadamard_pq64_adj(const Plan& P, DevState& D, const double2* in, double2* out);
 void hadamard_list64(const Plan& P, DevState& D, int nOut, const int64_t* ptr, const int32_t* ent, const double2* in,
                      double2* out, bool conj);
 // internal stage bit: run upward, V, X (S2L) and downward stages only, leaving

@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <string>
@@ -25,6 +26,7 @@
 #include "cuda_common.cuh"
 #include "engine.hpp"
 #include "dense_kernel.cuh"
+#include "had_pq.cuh"
 #include "had_smem.cuh"
 #include "kernels.hpp"
 
@@ -662,6 +664,9 @@ void dev_free(DevState& D) {
   D.denK = D.valK = nullptr;
   D.adjNearRows = D.adjNearIdx = D.adjFarRows = D.adjFarIdx = D.adjS2lRows = D.adjS2lIdx = nullptr;
   D.adjNearPtr = D.adjFarPtr = D.adjS2lPtr = nullptr;
+  D.vParentsT = D.vNbrTIdx = nullptr;
+  D.vNbrTPtr = nullptr;
+  D.vNbrOffT = nullptr;
   D.uc2ueT = D.m2mT = D.dc2deT = D.l2lT = D.gradT = nullptr;
   D.adjListsReady = false;
   D.adjOpsStale = true;
@@ -812,6 +817,10 @@ std::string dev_upload(const Plan& P, DevState& D, const double* src, const doub
   FMMG_TRY(dput<double>(D, D.dden, nullptr, (size_t)P.nn * de));
   FMMG_TRY(dput<double2>(D, D.effDen, nullptr, P.vSrcNodes.size() * (size_t)P.nEff * P.sdm));
   FMMG_TRY(dput<double2>(D, D.effVal, nullptr, P.vTrgNodes.size() * (size_t)P.nEff * P.tdm));
+  {
+    const char* hk = std::getenv("FMMG_HADAMARD");
+    D.hadPQ = !(hk && std::strcmp(hk, "list") == 0);
+  }
   if (!D.evReady) {
     for (auto& e : D.ev) FMMG_CK(cudaEventCreate(&e));
     D.evReady = true;
@@ -884,7 +893,14 @@ static void launch_m2l_np(const Plan& P, DevState& D, LaunchStats* ls) {
   if (npar > 0 && ntrg > 0) {
     dim3 grid(npar, (P.nEff + 31) / 32);
     const double nrmfc = 1.0 / double(P.nReg);
-    if (P.sdm == 1 && P.tdm == 1) {
+    if (P.sdm == 1 && P.tdm == 1 && D.hadPQ) {
+      const size_t smem = had_smem_bytes<double2>();
+      cudaFuncSetAttribute(k_m2l_had_pq<double2, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      dim3 g2((npar + PQ_PARENTS - 1) / PQ_PARENTS, (P.nEff + 31) / 32, 1);
+      k_m2l_had_pq<double2, 1, false><<<g2, PQ_THREADS, smem, D.stream>>>(
+          npar, D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot, D.vTrgSlot, D.effDen, 0, D.m2lT, D.effVal, 0,
+          P.nEff, 1, nrmfc, D.transIdDev);
+    } else if (P.sdm == 1 && P.tdm == 1) {
       const size_t smem = had_smem_bytes<double2>();
       cudaFuncSetAttribute(k_m2l_had_list<double2, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
@@ -948,6 +964,16 @@ void spectral_inv(const Plan& P, DevState& D, int n, const int32_t* nodes, int d
   }
 }
 // the scalar Hadamard step on expanded lists; conj selects the transposed operator
+void hadamard_pq64_adj(const Plan& P, DevState& D, const double2* in, double2* out) {
+  const int nrow = (int)P.vParentsT.size();
+  if (nrow <= 0) return;
+  const size_t smem = had_smem_bytes<double2>();
+  cudaFuncSetAttribute(k_m2l_had_pq<double2, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  dim3 g2((nrow + PQ_PARENTS - 1) / PQ_PARENTS, (P.nEff + 31) / 32, 1);
+  k_m2l_had_pq<double2, 1, true><<<g2, PQ_THREADS, smem, D.stream>>>(
+      nrow, D.vParentsT, D.vNbrTPtr, D.vNbrTIdx, D.vNbrOffT, D.chd, D.vTrgSlot, D.vSrcSlot, in, 0, D.m2lT, out, 0,
+      P.nEff, 1, 1.0 / double(P.nReg), D.transIdDev);
+}
 void hadamard_list64(const Plan& P, DevState& D, int nOut, const int64_t* ptr, const int32_t* ent, const double2* in,
                      double2* out, bool conj) {
   if (nOut <= 0) return;
