@@ -534,6 +534,8 @@ static std::string adj_prepare(const Plan& P, DevState& D) {
     FMMG_TRY(aj_put(D, D.vNbrTPtr, P.vNbrT.ptr.data(), P.vNbrT.ptr.size()));
     FMMG_TRY(aj_put(D, D.vNbrTIdx, P.vNbrT.idx.data(), P.vNbrT.idx.size()));
     FMMG_TRY(aj_put(D, D.vNbrOffT, P.vNbrOffT.data(), P.vNbrOffT.size()));
+    FMMG_TRY(aj_put(D, D.vRowOutT, P.vRowOutT.data(), P.vRowOutT.size()));
+    FMMG_TRY(aj_put(D, D.vNbrInT, P.vNbrInT.data(), P.vNbrInT.size()));
     D.adjListsReady = true;
   }
   if (D.adjOpsStale) {

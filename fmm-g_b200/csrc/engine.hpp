@@ -77,6 +77,7 @@ struct DevState {
   double *uc2ueT = nullptr, *m2mT = nullptr, *dc2deT = nullptr, *l2lT = nullptr;
   double* gradT = nullptr;  // [nt][3] permuted order
   int32_t *vParentsT = nullptr, *vNbrTIdx = nullptr; int64_t *vNbrTPtr = nullptr; int8_t *vNbrOffT = nullptr;
+  int32_t *vRowOut = nullptr, *vNbrIn = nullptr, *vRowOutT = nullptr, *vNbrInT = nullptr;  // [rows|entries][8]
   bool adjListsReady = false, adjOpsStale = true;
   bool hadPQ = true;  // scalar Hadamard: parent-pair register-blocked kernel (else expanded lists)
   float adjMs = 0.f;

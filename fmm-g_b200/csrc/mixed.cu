@@ -776,19 +776,20 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
                                                    D.vTrgSlot, D.effDen32, effDR, D.m2lT32, D.effVal32, effVR, \
                                                    P.nEff, kc, nrmfc)
     if (P.sdm == 1 && P.tdm == 1 && D.hadPQ) {
-      const size_t smem = had_smem_bytes<float2>();
-      dim3 g2((npar + PQ_PARENTS - 1) / PQ_PARENTS, (P.nEff + 31) / 32, 1);
-#define FMMG_PQ32(KP)                                                                                            \
-  do {                                                                                                           \
-    cudaFuncSetAttribute(k_m2l_had_pq<float2, KP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
-    g2.z = (kc + KP - 1) / KP;                                                                                   \
-    k_m2l_had_pq<float2, KP, false><<<g2, PQ_THREADS, smem, st>>>(                                               \
-        npar, D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot, D.vTrgSlot, D.effDen32, effDR, D.m2lT32,    \
-        D.effVal32, effVR, P.nEff, kc, nrmfc, D.transIdDev);                                                     \
-  } while (0)
-      if (kc == 1) FMMG_PQ32(1);
-      else FMMG_PQ32(2);
-#undef FMMG_PQ32
+      if (kc == 1) {
+        const size_t smem = pq_smem_bytes<float2>(32);
+        cudaFuncSetAttribute(k_m2l_had_pqx2<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        dim3 g1((npar + PQX_ROWS - 1) / PQX_ROWS, (P.nEff + 31) / 32, 1);
+        k_m2l_had_pqx2<32, false><<<g1, PQX_THREADS, smem, st>>>(npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn,
+                                                                 D.effDen32, effDR, D.m2lT32, D.effVal32, effVR,
+                                                                 P.nEff, kc, nrmfc, D.transIdDev);
+      } else {
+        const size_t smem = pq_smem_bytes<float2>(4);
+        dim3 g8((npar + PQX_ROWS - 1) / PQX_ROWS, (P.nEff + 3) / 4, (kc + 7) / 8);
+        k_m2l_had_pqx2<4, false><<<g8, PQX_THREADS, smem, st>>>(npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn,
+                                                                D.effDen32, effDR, D.m2lT32, D.effVal32, effVR, P.nEff,
+                                                                kc, nrmfc, D.transIdDev);
+      }
     } else if (P.sdm == 1 && P.tdm == 1) {
       const size_t smem = had_smem_bytes<float2>();
       cudaFuncSetAttribute(k_m2l_had_list<float2, KB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,

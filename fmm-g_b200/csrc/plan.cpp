@@ -398,6 +398,15 @@ void Plan::build_adjoint_lists() {
     }
     vNbrT.ptr.push_back((int64_t)vNbrT.idx.size());
   }
+  auto slots8 = [&](const std::vector<int32_t>& nodes, const std::vector<int32_t>& slot, std::vector<int32_t>& out) {
+    out.resize(8 * nodes.size());
+    for (size_t i = 0; i < nodes.size(); i++)
+      for (int c = 0; c < 8; c++) out[8 * i + c] = slot[chd[nodes[i]] + c];
+  };
+  slots8(vParents, vTrgSlot, vRowOut);
+  slots8(vNbr.idx, vSrcSlot, vNbrIn);
+  slots8(vParentsT, vSrcSlot, vRowOutT);
+  slots8(vNbrT.idx, vTrgSlot, vNbrInT);
 }
 
 std::string Plan::build(const Options& opt, int64_t ns_, const double* src, const double* nrmIn, int64_t nt_,

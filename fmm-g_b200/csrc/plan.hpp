@@ -106,6 +106,10 @@ struct Plan {
   std::vector<int32_t> vParentsT;    // source parents Q of the grouped M2L
   CSR vNbrT;                         // per row: target parents P
   std::vector<int8_t> vNbrOffT;      // offset code of P - Q
+  // the parent-pair lists with child slots resolved: per row its 8 output
+  // child slots, per neighbour entry its 8 input child slots (-1: no spectrum)
+  std::vector<int32_t> vRowOut, vNbrIn;     // forward: target slots of P, source slots of Q
+  std::vector<int32_t> vRowOutT, vNbrInT;   // transposed: source slots of Q, target slots of P
   void build_adjoint_lists();
 
   // ---- operators (homogeneous equivalent kernels: unit-radius tables)

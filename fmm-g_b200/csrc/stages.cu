@@ -665,6 +665,7 @@ void dev_free(DevState& D) {
   D.adjNearRows = D.adjNearIdx = D.adjFarRows = D.adjFarIdx = D.adjS2lRows = D.adjS2lIdx = nullptr;
   D.adjNearPtr = D.adjFarPtr = D.adjS2lPtr = nullptr;
   D.vParentsT = D.vNbrTIdx = nullptr;
+  D.vRowOut = D.vNbrIn = D.vRowOutT = D.vNbrInT = nullptr;
   D.vNbrTPtr = nullptr;
   D.vNbrOffT = nullptr;
   D.uc2ueT = D.m2mT = D.dc2deT = D.l2lT = D.gradT = nullptr;
@@ -805,6 +806,8 @@ std::string dev_upload(const Plan& P, DevState& D, const double* src, const doub
   FMMG_TRY(dput(D, D.vTrgEnt, P.vTrgEnt));
   FMMG_TRY(dput(D, D.vSrcPtr, P.vSrcPtr));
   FMMG_TRY(dput(D, D.vSrcEnt, P.vSrcEnt));
+  FMMG_TRY(dput(D, D.vRowOut, P.vRowOut));
+  FMMG_TRY(dput(D, D.vNbrIn, P.vNbrIn));
   FMMG_TRY(dev_upload_operators(P, D));
   // work arrays
   const int64_t ue = (int64_t)P.nUE * P.sdm, uc = (int64_t)P.nUC * P.tdm;
@@ -894,12 +897,12 @@ static void launch_m2l_np(const Plan& P, DevState& D, LaunchStats* ls) {
     dim3 grid(npar, (P.nEff + 31) / 32);
     const double nrmfc = 1.0 / double(P.nReg);
     if (P.sdm == 1 && P.tdm == 1 && D.hadPQ) {
-      const size_t smem = had_smem_bytes<double2>();
+      const size_t smem = pq_smem_bytes<double2>(32);
       cudaFuncSetAttribute(k_m2l_had_pq<double2, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       dim3 g2((npar + PQ_PARENTS - 1) / PQ_PARENTS, (P.nEff + 31) / 32, 1);
       k_m2l_had_pq<double2, 1, false><<<g2, PQ_THREADS, smem, D.stream>>>(
-          npar, D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot, D.vTrgSlot, D.effDen, 0, D.m2lT, D.effVal, 0,
-          P.nEff, 1, nrmfc, D.transIdDev);
+          npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen, 0, D.m2lT, D.effVal, 0, P.nEff, 1, nrmfc,
+          D.transIdDev);
     } else if (P.sdm == 1 && P.tdm == 1) {
       const size_t smem = had_smem_bytes<double2>();
       cudaFuncSetAttribute(k_m2l_had_list<double2, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -967,12 +970,12 @@ void spectral_inv(const Plan& P, DevState& D, int n, const int32_t* nodes, int d
 void hadamard_pq64_adj(const Plan& P, DevState& D, const double2* in, double2* out) {
   const int nrow = (int)P.vParentsT.size();
   if (nrow <= 0) return;
-  const size_t smem = had_smem_bytes<double2>();
+  const size_t smem = pq_smem_bytes<double2>(32);
   cudaFuncSetAttribute(k_m2l_had_pq<double2, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dim3 g2((nrow + PQ_PARENTS - 1) / PQ_PARENTS, (P.nEff + 31) / 32, 1);
   k_m2l_had_pq<double2, 1, true><<<g2, PQ_THREADS, smem, D.stream>>>(
-      nrow, D.vParentsT, D.vNbrTPtr, D.vNbrTIdx, D.vNbrOffT, D.chd, D.vTrgSlot, D.vSrcSlot, in, 0, D.m2lT, out, 0,
-      P.nEff, 1, 1.0 / double(P.nReg), D.transIdDev);
+      nrow, D.vRowOutT, D.vNbrTPtr, D.vNbrOffT, D.vNbrInT, in, 0, D.m2lT, out, 0, P.nEff, 1, 1.0 / double(P.nReg),
+      D.transIdDev);
 }
 void hadamard_list64(const Plan& P, DevState& D, int nOut, const int64_t* ptr, const int32_t* ent, const double2* in,
                      double2* out, bool conj) {
