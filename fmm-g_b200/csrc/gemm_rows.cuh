@@ -1,0 +1,162 @@
+// gemm_rows.cuh -- batched row GEMM of the translation stages, FP64 and FP32.
+//
+// For every listed node (and every right-hand side),
+//   Y[row] = beta * Y[row] + ys .* (W (xs .* X[row])),
+// W N x K row-major.  The X (Y) row of a node starts at its own id or at its
+// first child's id, so the 8 children of a parent form one contiguous row of
+// length 8 * ld.  Serves C2E (pinv GEMV, matmgnt3d_mpi.cpp:107-149, :196-229),
+// M2M (:151-193) and L2L (:231-274) over all nodes of a level at once, and
+// their transposes in the adjoint.
+//
+// Tiling: 128 (rows x right-hand sides) x 64 (outputs) per CTA, K in steps of
+// BK (16 for FP32, 8 for FP64: 48 KB of shared memory either way), 256
+// threads each owning an 8 x 4 register tile.  The next K step is
+// fetched into registers while the current one is multiplied from shared
+// memory (two buffers, one barrier per step).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace fmmg {
+
+constexpr int GR_BM = 128, GR_BN = 64, GR_BK = 16, GR_THREADS = 256;
+
+template <typename T>
+struct GrScale {
+  T v[4];
+  int mod;
+};
+
+// v[i % mod] without dynamic indexing of the by-value parameter (which
+// would place it in local memory)
+template <typename T>
+__device__ __forceinline__ T gr_sel(const GrScale<T>& s, int i) {
+  const int m = s.mod == 1 ? 0 : i % s.mod;
+  return m == 0 ? s.v[0] : (m == 1 ? s.v[1] : (m == 2 ? s.v[2] : s.v[3]));
+}
+
+template <typename T>
+struct GrVec;
+template <>
+struct GrVec<float> {
+  typedef float4 V;
+};
+template <>
+struct GrVec<double> {
+  typedef double2 V;
+};
+
+template <typename T, int BK>
+__global__ void __launch_bounds__(GR_THREADS)
+    k_gemm_rows_t(int nrows, int nrhs, const int32_t* __restrict__ rows, const int32_t* __restrict__ chd, int xChild,
+                  int yChild, const T* __restrict__ X, int64_t ldx, int64_t xRhs, const T* __restrict__ W,
+                  T* __restrict__ Y, int64_t ldy, int64_t yRhs, int K, int N, GrScale<T> xs, GrScale<T> ys, T beta) {
+  constexpr int AK = BK / 2, BKW = BK / 4;  // per thread: A row ra, k ka..ka+AK-1; B output nb, k kb..kb+BKW-1
+  __shared__ __align__(16) T As[2][BK][GR_BM];
+  __shared__ __align__(16) T Bs[2][BK][GR_BN];
+  __shared__ const T* xrow[GR_BM];
+  __shared__ T* yrow[GR_BM];
+  const int tid = threadIdx.x;
+  const int r0 = blockIdx.x * GR_BM, n0 = blockIdx.y * GR_BN;
+  if (tid < GR_BM) {
+    const int r = r0 + tid;
+    if (r < nrows * nrhs) {
+      const int q = r / nrows;
+      const int node = rows[r - q * nrows];
+      xrow[tid] = X + q * xRhs + (int64_t)(xChild ? chd[node] : node) * ldx;
+      yrow[tid] = Y + q * yRhs + (int64_t)(yChild ? chd[node] : node) * ldy;
+    } else {
+      xrow[tid] = nullptr;
+      yrow[tid] = nullptr;
+    }
+  }
+  __syncthreads();
+  const int ra = tid >> 1, ka = (tid & 1) * AK;
+  const int nb = tid >> 2, kb = (tid & 3) * BKW;
+  const T* xr = xrow[ra];
+  const bool bIn = n0 + nb < N;
+  const T* wr = W + (int64_t)(bIn ? n0 + nb : 0) * K;
+  T fa[AK], fb[BKW];
+#define FMMG_GR_FETCH(K0)                                                  \
+  {                                                                        \
+    _Pragma("unroll") for (int i = 0; i < AK; i++) {                       \
+      const int k = (K0) + ka + i;                                         \
+      fa[i] = (xr && k < K) ? xr[k] * gr_sel(xs, k) : T(0);                \
+    }                                                                      \
+    _Pragma("unroll") for (int i = 0; i < BKW; i++) {                      \
+      const int k = (K0) + kb + i;                                         \
+      fb[i] = (bIn && k < K) ? wr[k] : T(0);                               \
+    }                                                                      \
+  }
+#define FMMG_GR_STASH(B_)                                                  \
+  {                                                                        \
+    _Pragma("unroll") for (int i = 0; i < AK; i++) As[B_][ka + i][ra] = fa[i]; \
+    _Pragma("unroll") for (int i = 0; i < BKW; i++) Bs[B_][kb + i][nb] = fb[i]; \
+  }
+  const int tm = tid >> 4, tn = tid & 15;  // rows tm*8 .. +7, outputs tn*4 .. +3
+  T acc[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j] = T(0);
+  FMMG_GR_FETCH(0)
+  FMMG_GR_STASH(0)
+  __syncthreads();
+  int buf = 0;
+  typedef typename GrVec<T>::V V;
+  constexpr int VW = sizeof(V) / sizeof(T);
+  for (int k0 = 0; k0 < K; k0 += BK) {
+    const bool more = k0 + BK < K;
+    if (more) FMMG_GR_FETCH(k0 + BK)
+#pragma unroll
+    for (int k = 0; k < BK; k++) {
+      T a[8], b[4];
+#pragma unroll
+      for (int i = 0; i < 8; i += VW) {
+        const V v = *reinterpret_cast<const V*>(&As[buf][k][tm * 8 + i]);
+        if constexpr (VW == 4) {
+          a[i] = v.x; a[i + 1] = v.y; a[i + 2] = v.z; a[i + 3] = v.w;
+        } else {
+          a[i] = v.x; a[i + 1] = v.y;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 4; j += VW) {
+        const V v = *reinterpret_cast<const V*>(&Bs[buf][k][tn * 4 + j]);
+        if constexpr (VW == 4) {
+          b[j] = v.x; b[j + 1] = v.y; b[j + 2] = v.z; b[j + 3] = v.w;
+        } else {
+          b[j] = v.x; b[j + 1] = v.y;
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    if (more) {
+      FMMG_GR_STASH(buf ^ 1)
+      __syncthreads();
+      buf ^= 1;
+    }
+  }
+#undef FMMG_GR_FETCH
+#undef FMMG_GR_STASH
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    T* yr = yrow[tm * 8 + i];
+    if (!yr) continue;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int n = n0 + tn * 4 + j;
+      if (n < N) {
+        const T v = acc[i][j] * gr_sel(ys, n);
+        yr[n] = beta == T(0) ? v : beta * yr[n] + v;
+      }
+    }
+  }
+}
+
+}  // namespace fmmg

@@ -207,17 +207,26 @@ __device__ __forceinline__ void pq_delta_x2(unsigned long long (&acc)[8], const 
 // right-hand side, FW = 4 for blocks of 8, where every translation value read
 // from shared memory serves 8 lanes and the CTA stages only 4 frequencies of
 // the 316 translations (10 KB), so residency is set by registers.  Grid (rows
-// / PQX_ROWS, nEff / FW, ceil(nrhs / (32 / FW))); dynamic shared memory
+// / PQX_ROWS, nEff / FW, ceil(nrhs / (32 / FW))); blockIdx.z selects the
+// right-hand-side block of the layout below; dynamic shared memory
 // 317 * FW * sizeof(float2) (row 316 is the zero row of touching pairs).
 constexpr int PQX_THREADS = 256;
 constexpr int PQX_ROWS = 64;
+
+// Spectrum layout: value (right-hand side r, slot s, frequency f) of effIn
+// sits at (r / RW) * in.blk + s * in.slot + f * fStride + (r % RW) * rStride
+// (effOut likewise): planes of one right-hand side (RW = 1, fStride = 1), or
+// blocks of 8 interleaved right-hand sides (RW = 8, fStride = 8, rStride = 1).
+struct PqLayout {
+  int64_t blk, slot;
+};
 
 template <int FW, bool ADJ>
 __global__ void __launch_bounds__(PQX_THREADS, 3)
     k_m2l_had_pqx2(int nRows, const int32_t* __restrict__ rowOut, const int64_t* __restrict__ nPtr,
                    const int8_t* __restrict__ nOff, const int32_t* __restrict__ nIn, const float2* __restrict__ effIn,
-                   int64_t inRhs, const float2* __restrict__ T, float2* __restrict__ effOut, int64_t outRhs, int nEff,
-                   int nrhs, float nrmfc, const int16_t* __restrict__ transId) {
+                   PqLayout inL, const float2* __restrict__ T, float2* __restrict__ effOut, PqLayout outL,
+                   int fStride, int rStride, int nEff, int nrhs, float nrmfc, const int16_t* __restrict__ transId) {
   constexpr int RW = 32 / FW;
   extern __shared__ unsigned char pqx_smem[];
   float2* Ts = reinterpret_cast<float2*>(pqx_smem);  // [316][FW]
@@ -234,7 +243,9 @@ __global__ void __launch_bounds__(PQX_THREADS, 3)
   }
   __syncthreads();
   const bool act = f < nEff && rhs < nrhs;
-  const float2* inF = effIn + (int64_t)(act ? rhs : 0) * inRhs + (act ? f : 0);
+  const int64_t lanePos = act ? (int64_t)f * fStride + (int64_t)rl * rStride : 0;
+  const float2* inF = effIn + (act ? blockIdx.z * inL.blk : 0) + lanePos;
+  float2* outF = effOut + blockIdx.z * outL.blk + lanePos;
   const int bEnd = min(nRows, (int)(blockIdx.x + 1) * PQX_ROWS);
   for (int b = blockIdx.x * PQX_ROWS + warp; b < bEnd; b += PQX_THREADS / 32) {
     unsigned long long acc[8];
@@ -254,7 +265,7 @@ __global__ void __launch_bounds__(PQX_THREADS, 3)
       unsigned long long inD[8], inR[8];
 #pragma unroll
       for (int c2 = 0; c2 < 8; c2++) {
-        const float2 d = (act && sl[c2] >= 0) ? inF[(int64_t)sl[c2] * nEff] : make_float2(0.f, 0.f);
+        const float2 d = (act && sl[c2] >= 0) ? inF[(int64_t)sl[c2] * inL.slot] : make_float2(0.f, 0.f);
         inD[c2] = pq_pk(d.x, d.y);
         inR[c2] = pq_pk(-d.y, d.x);
       }
@@ -272,7 +283,7 @@ __global__ void __launch_bounds__(PQX_THREADS, 3)
       const int t = rowOut[8 * b + c];
       if (t < 0) continue;
       const float2 a = pq_unpk(acc[c]);
-      effOut[(int64_t)rhs * outRhs + (int64_t)t * nEff + f] = make_float2(a.x * nrmfc, a.y * nrmfc);
+      outF[(int64_t)t * outL.slot] = make_float2(a.x * nrmfc, a.y * nrmfc);
     }
   }
 }

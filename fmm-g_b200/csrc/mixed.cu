@@ -22,6 +22,7 @@
 
 #include "cuda_common.cuh"
 #include "engine.hpp"
+#include "gemm_rows.cuh"
 #include "had_pq.cuh"
 #include "had_smem.cuh"
 #include "kernels.hpp"
@@ -319,94 +320,6 @@ __global__ void __launch_bounds__(MX_SURF)
     }
 }
 
-// ------------------------------------------------------------------ FP32 row GEMM
-// Y[row] = beta*Y[row] + ys .* (W X[row]) as k_gemm_rows, FP32 operands and
-// accumulation.  Rows run over (right-hand side, node): row r uses node
-// rows[r % nrows] of density r / nrows, so one W tile serves every density.
-constexpr int G32_BM = 64, G32_BN = 64, G32_BK = 32;
-struct Scale4f {
-  float v[4];
-  int mod;
-};
-
-__global__ void __launch_bounds__(256)
-    k_gemm_rows32(int nrows, int nrhs, const int32_t* __restrict__ rows, const int32_t* __restrict__ chd,
-                  int xChild, int yChild, const float* __restrict__ X, int64_t ldx, int64_t xRhs,
-                  const float* __restrict__ W, float* __restrict__ Y, int64_t ldy, int64_t yRhs, int K, int N,
-                  Scale4f xs, Scale4f ys, float beta) {
-  __shared__ float As[G32_BK][G32_BM + 4];
-  __shared__ float Bs[G32_BK][G32_BN + 4];
-  __shared__ const float* xrow[G32_BM];
-  __shared__ float* yrow[G32_BM];
-  const int tid = threadIdx.x;
-  const int r0 = blockIdx.x * G32_BM, n0 = blockIdx.y * G32_BN;
-  if (tid < G32_BM) {
-    int r = r0 + tid;
-    if (r < nrows * nrhs) {
-      int q = r / nrows;
-      int node = rows[r - q * nrows];
-      xrow[tid] = X + q * xRhs + (int64_t)(xChild ? chd[node] : node) * ldx;
-      yrow[tid] = Y + q * yRhs + (int64_t)(yChild ? chd[node] : node) * ldy;
-    } else {
-      xrow[tid] = nullptr;
-      yrow[tid] = nullptr;
-    }
-  }
-  __syncthreads();
-  const int tr = tid / 16, tc = tid % 16;
-  float acc[4][4];
-#pragma unroll
-  for (int i = 0; i < 4; i++)
-#pragma unroll
-    for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
-  for (int k0 = 0; k0 < K; k0 += G32_BK) {
-#pragma unroll
-    for (int l = 0; l < 8; l++) {
-      int e = tid + l * 256;
-      int r = e / G32_BK, k = e % G32_BK;
-      const float* xr = xrow[r];
-      float v = 0.f;
-      if (xr && k0 + k < K) v = xr[k0 + k] * xs.v[(k0 + k) % xs.mod];
-      As[k][r] = v;
-    }
-#pragma unroll
-    for (int l = 0; l < 8; l++) {
-      int e = tid + l * 256;
-      int n = e / G32_BK, k = e % G32_BK;
-      float v = 0.f;
-      if (n0 + n < N && k0 + k < K) v = W[(int64_t)(n0 + n) * K + k0 + k];
-      Bs[k][n] = v;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < G32_BK; k++) {
-      float a[4], b[4];
-#pragma unroll
-      for (int i = 0; i < 4; i++) a[i] = As[k][tr + 16 * i];
-#pragma unroll
-      for (int j = 0; j < 4; j++) b[j] = Bs[k][tc + 16 * j];
-#pragma unroll
-      for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int i = 0; i < 4; i++) {
-    float* yr = yrow[tr + 16 * i];
-    if (!yr) continue;
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      int n = n0 + tc + 16 * j;
-      if (n < N) {
-        float v = acc[i][j] * ys.v[n % ys.mod];
-        yr[n] = beta == 0.f ? v : beta * yr[n] + v;
-      }
-    }
-  }
-}
-
 // ------------------------------------------------------------------ FP32 M2L
 // grid (source slots, right-hand sides)
 template <int NP>
@@ -613,6 +526,158 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+// Scalar equivalent kernels, blocks of 8 right-hand sides: one CTA per
+// (slot, block) transforms the 8 densities together, the right-hand side
+// being the fastest index of every staging array, so the spectra are written
+// (and read back by k_m2l_inv32r8) as [block][slot][frequency][8] in
+// contiguous runs.  Dynamic shared memory r8_fwd_smem<NP>() / r8_inv_smem<NP>().
+template <int NP>
+constexpr size_t r8_fwd_smem() {
+  return sizeof(float) * NP * NP * NP * 8 + sizeof(float2) * (NP * NP * (NP + 1) * 8 + NP * 2 * NP * (NP + 1) * 8 + 2 * NP);
+}
+template <int NP>
+constexpr size_t r8_inv_smem() {
+  return sizeof(float2) * (NP * 2 * NP * (NP + 1) * 8 + NP * NP * (NP + 1) * 8 + 2 * NP);
+}
+
+template <int NP>
+__global__ void __launch_bounds__(256)
+    k_m2l_fwd32r8(const int32_t* __restrict__ nodes, const int32_t* __restrict__ depth, int rootLevel, float deg,
+                  const float* __restrict__ uden, int64_t udenRhs, const int32_t* __restrict__ ijk, int nUE,
+                  float2* __restrict__ effDen, int64_t blkStride, int nEff, int kc) {
+  using F = FftDims<NP>;
+  constexpr int N = F::N, NH = F::NH, H = F::H;
+  extern __shared__ __align__(16) unsigned char r8_smem[];
+  float2* X1 = reinterpret_cast<float2*>(r8_smem);  // [NP][NP][NH][8]
+  float2* X2 = X1 + NP * NP * NH * 8;                // [NP][N][NH][8]
+  float2* tw = X2 + NP * N * NH * 8;                 // [N]
+  float* cube = reinterpret_cast<float*>(tw + N);    // [NP][NP][NP][8]
+  const int slot = blockIdx.x;
+  const int v = nodes[slot];
+  const int r0 = blockIdx.y * 8;
+  const int tid = threadIdx.x;
+  if (tid < N) {
+    double sn, cs;
+    sincospi(2.0 * tid / N, &sn, &cs);
+    tw[tid] = make_float2((float)cs, (float)-sn);
+  }
+  const float scl = (float)exp2((double)(depth[v] + rootLevel) * deg);
+  for (int i = tid; i < NP * NP * NP * 8; i += blockDim.x) cube[i] = 0.f;
+  __syncthreads();
+  for (int i = tid; i < nUE * 8; i += blockDim.x) {
+    const int j = i >> 3, r = i & 7;
+    if (r0 + r >= kc) continue;
+    const int p = ijk[j];
+    cube[(((p >> 16) * NP + ((p >> 8) & 255)) * NP + (p & 255)) * 8 + r] =
+        uden[(int64_t)(r0 + r) * udenRhs + (int64_t)v * nUE + j] * scl;
+  }
+  __syncthreads();
+  for (int i = tid; i < NP * NP * NH * 8; i += blockDim.x) {  // x pass (real -> half spectrum)
+    const int r = i & 7, e = i >> 3;
+    const int kx = e % NH, yb = (e / NH) % NP, zb = e / (NH * NP);
+    const float* row = &cube[(zb * NP + yb) * NP * 8 + r];
+    float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int xb = 0; xb < NP; xb++) {
+      const float2 w = tw[(kx * (xb + H)) % N];
+      s.x += row[xb * 8] * w.x;
+      s.y += row[xb * 8] * w.y;
+    }
+    X1[i] = s;
+  }
+  __syncthreads();
+  for (int i = tid; i < NP * N * NH * 8; i += blockDim.x) {  // y pass
+    const int r = i & 7, e = i >> 3;
+    const int kx = e % NH, ky = (e / NH) % N, zb = e / (NH * N);
+    float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int yb = 0; yb < NP; yb++) {
+      const float2 t = cmul(X1[((zb * NP + yb) * NH + kx) * 8 + r], tw[(ky * (yb + H)) % N]);
+      s.x += t.x;
+      s.y += t.y;
+    }
+    X2[i] = s;
+  }
+  __syncthreads();
+  float2* out = effDen + blockIdx.y * blkStride + (int64_t)slot * nEff * 8;
+  for (int i = tid; i < N * N * NH * 8; i += blockDim.x) {  // z pass
+    const int r = i & 7, e = i >> 3;
+    const int kx = e % NH, ky = (e / NH) % N, kz = e / (NH * N);
+    float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int zb = 0; zb < NP; zb++) {
+      const float2 t = cmul(X2[((zb * N + ky) * NH + kx) * 8 + r], tw[(kz * (zb + H)) % N]);
+      s.x += t.x;
+      s.y += t.y;
+    }
+    out[i] = s;
+  }
+}
+
+template <int NP>
+__global__ void __launch_bounds__(256)
+    k_m2l_inv32r8(const int32_t* __restrict__ nodes, const float2* __restrict__ effVal, int64_t blkStride, int nEff,
+                  const int32_t* __restrict__ ijk, int nDC, float* __restrict__ dchk, int64_t dchkRhs, int kc) {
+  using F = FftDims<NP>;
+  constexpr int N = F::N, NH = F::NH, H = F::H;
+  extern __shared__ __align__(16) unsigned char r8_smem[];
+  float2* Y2 = reinterpret_cast<float2*>(r8_smem);  // [NP][N][NH][8]
+  float2* Y1 = Y2 + NP * N * NH * 8;                 // [NP][NP][NH][8]
+  float2* tw = Y1 + NP * NP * NH * 8;                // [N]
+  const int slot = blockIdx.x;
+  const int node = nodes[slot];
+  const int r0 = blockIdx.y * 8;
+  const int tid = threadIdx.x;
+  if (tid < N) {
+    double sn, cs;
+    sincospi(2.0 * tid / N, &sn, &cs);
+    tw[tid] = make_float2((float)cs, (float)-sn);
+  }
+  __syncthreads();
+  const float2* in = effVal + blockIdx.y * blkStride + (int64_t)slot * nEff * 8;
+  for (int i = tid; i < NP * N * NH * 8; i += blockDim.x) {  // z pass, band outputs only
+    const int r = i & 7, e = i >> 3;
+    const int kx = e % NH, ky = (e / NH) % N, zb = e / (NH * N);
+    float2 s = make_float2(0.f, 0.f);
+#pragma unroll 4
+    for (int kz = 0; kz < N; kz++) {
+      const float2 t = cmulc(in[((kz * N + ky) * NH + kx) * 8 + r], tw[(kz * (zb + H)) % N]);
+      s.x += t.x;
+      s.y += t.y;
+    }
+    Y2[i] = s;
+  }
+  __syncthreads();
+  for (int i = tid; i < NP * NP * NH * 8; i += blockDim.x) {  // y pass
+    const int r = i & 7, e = i >> 3;
+    const int kx = e % NH, yb = (e / NH) % NP, zb = e / (NH * NP);
+    float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int ky = 0; ky < N; ky++) {
+      const float2 t = cmulc(Y2[((zb * N + ky) * NH + kx) * 8 + r], tw[(ky * (yb + H)) % N]);
+      s.x += t.x;
+      s.y += t.y;
+    }
+    Y1[i] = s;
+  }
+  __syncthreads();
+  for (int i = tid; i < nDC * 8; i += blockDim.x) {  // x pass (c2r) at the surface points
+    const int r = i & 7, j = i >> 3;
+    if (r0 + r >= kc) continue;
+    const int p = ijk[j];
+    const int a = p & 255, b = (p >> 8) & 255, cc = p >> 16;
+    const float2* y1 = &Y1[(cc * NP + b) * NH * 8 + r];
+    const int x = a + H;
+    float s = 0.f;
+#pragma unroll
+    for (int kx = 0; kx < NH; kx++) {
+      const float2 t = cmulc(y1[kx * 8], tw[(kx * x) % N]);
+      s += (kx == 0 || kx == N / 2) ? t.x : 2.f * t.x;
+    }
+    dchk[(int64_t)(r0 + r) * dchkRhs + (int64_t)node * nDC + j] += s;
+  }
+}
+
 // ------------------------------------------------------------------ launcher
 template <typename T>
 static std::string dalloc(DevState& D, T*& p, size_t n) {
@@ -634,8 +699,9 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
     FMMG_TRY(dalloc(D, D.uden32, (size_t)kc * P.nn * ue));
     FMMG_TRY(dalloc(D, D.dchk32, (size_t)kc * P.nn * dc));
     FMMG_TRY(dalloc(D, D.dden32, (size_t)kc * P.nn * de));
-    FMMG_TRY(dalloc(D, D.effDen32, (size_t)kc * P.vSrcNodes.size() * P.nEff * P.sdm));
-    FMMG_TRY(dalloc(D, D.effVal32, (size_t)kc * P.vTrgNodes.size() * P.nEff * P.tdm));
+    const size_t kc8 = (size_t)(kc + 7) / 8 * 8;  // the scalar k >= 2 layout stores blocks of 8
+    FMMG_TRY(dalloc(D, D.effDen32, kc8 * P.vSrcNodes.size() * P.nEff * P.sdm));
+    FMMG_TRY(dalloc(D, D.effVal32, kc8 * P.vTrgNodes.size() * P.nEff * P.tdm));
     FMMG_TRY(dalloc(D, D.upT32, (size_t)kc * P.nn * std::max(P.kUp, 1)));
     FMMG_TRY(dalloc(D, D.dnT32, (size_t)kc * P.nn * std::max(P.kDn, 1)));
     FMMG_TRY(dalloc(D, D.denK, (size_t)kc * P.ns * P.sd));
@@ -679,13 +745,6 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
   return std::string();
 }
 
-static Scale4f to_f(const Scale4& s) {
-  Scale4f r;
-  r.mod = s.mod;
-  for (int k = 0; k < 4; k++) r.v[k] = (float)s.v[k];
-  return r;
-}
-
 // one pass over a chunk of kc right-hand sides, KB of them per launch block
 template <int KT, int KB>
 static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats* ls) {
@@ -705,9 +764,16 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
   auto gemm = [&](int nrows, const int32_t* rows, int xChild, int yChild, const float* X, int64_t ldx, int64_t xR,
                   const float* W, float* Y, int64_t ldy, int64_t yR, int K, int N, Scale4 xs, Scale4 ys, float beta) {
     if (nrows <= 0) return;
-    dim3 grid((nrows * kc + G32_BM - 1) / G32_BM, (N + G32_BN - 1) / G32_BN);
-    k_gemm_rows32<<<grid, 256, 0, st>>>(nrows, kc, rows, D.chd, xChild, yChild, X, ldx, xR, W, Y, ldy, yR, K, N,
-                                        to_f(xs), to_f(ys), beta);
+    GrScale<float> gx, gy;
+    gx.mod = xs.mod;
+    gy.mod = ys.mod;
+    for (int k = 0; k < 4; k++) {
+      gx.v[k] = (float)xs.v[k];
+      gy.v[k] = (float)ys.v[k];
+    }
+    dim3 grid((nrows * kc + GR_BM - 1) / GR_BM, (N + GR_BN - 1) / GR_BN);
+    k_gemm_rows_t<float, 16><<<grid, GR_THREADS, 0, st>>>(nrows, kc, rows, D.chd, xChild, yChild, X, ldx, xR, W, Y, ldy,
+                                                       yR, K, N, gx, gy, beta);
     ls->launches++;
   };
   if ((mask & 1) && !P.s2mLeaves.empty()) {
@@ -749,7 +815,29 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
   cudaEventRecord(D.ev[EV_NEAR], st);
   const int nsrc = (int)P.vSrcNodes.size(), ntrg = (int)P.vTrgNodes.size(), npar = (int)P.vParents.size();
   const int64_t effDR = (int64_t)nsrc * P.nEff * P.sdm, effVR = (int64_t)ntrg * P.nEff * P.tdm;
-  if ((mask & 4) && nsrc > 0) {
+  const bool r8 = P.sdm == 1 && P.tdm == 1 && kc >= 2 && D.hadPQ;  // blocks of 8 interleaved right-hand sides
+  const int nblk = (kc + 7) / 8;
+  const int64_t blkDen = (int64_t)nsrc * P.nEff * 8, blkVal = (int64_t)ntrg * P.nEff * 8;
+  if ((mask & 4) && nsrc > 0 && r8) {
+#define FMMG_FWD32R8(NP_)                                                                                      \
+  do {                                                                                                         \
+    constexpr size_t sm = r8_fwd_smem<NP_>();                                                                  \
+    cudaFuncSetAttribute(k_m2l_fwd32r8<NP_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);            \
+    k_m2l_fwd32r8<NP_><<<dim3(nsrc, nblk), 256, sm, st>>>(D.vSrcNodes, D.depth, rl, (float)P.deg[0], D.uden32, \
+                                                          nn * ue, D.surfIJK, P.nUE, D.effDen32, blkDen,       \
+                                                          P.nEff, kc);                                         \
+  } while (0)
+    switch (P.o.np) {
+      case 3: FMMG_FWD32R8(3); break;
+      case 4: FMMG_FWD32R8(4); break;
+      case 5: FMMG_FWD32R8(5); break;
+      case 6: FMMG_FWD32R8(6); break;
+      case 7: FMMG_FWD32R8(7); break;
+      case 8: FMMG_FWD32R8(8); break;
+    }
+#undef FMMG_FWD32R8
+    ls->launches++;
+  } else if ((mask & 4) && nsrc > 0) {
     Scale4 deg;
     deg.mod = P.sdm;
     for (int k = 0; k < 4; k++) deg.v[k] = P.deg[k];
@@ -776,19 +864,19 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
                                                    D.vTrgSlot, D.effDen32, effDR, D.m2lT32, D.effVal32, effVR, \
                                                    P.nEff, kc, nrmfc)
     if (P.sdm == 1 && P.tdm == 1 && D.hadPQ) {
-      if (kc == 1) {
+      if (!r8) {  // planes of one right-hand side
         const size_t smem = pq_smem_bytes<float2>(32);
         cudaFuncSetAttribute(k_m2l_had_pqx2<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        dim3 g1((npar + PQX_ROWS - 1) / PQX_ROWS, (P.nEff + 31) / 32, 1);
-        k_m2l_had_pqx2<32, false><<<g1, PQX_THREADS, smem, st>>>(npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn,
-                                                                 D.effDen32, effDR, D.m2lT32, D.effVal32, effVR,
-                                                                 P.nEff, kc, nrmfc, D.transIdDev);
+        dim3 g1((npar + PQX_ROWS - 1) / PQX_ROWS, (P.nEff + 31) / 32, kc);
+        k_m2l_had_pqx2<32, false><<<g1, PQX_THREADS, smem, st>>>(
+            npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen32, PqLayout{effDR, P.nEff}, D.m2lT32, D.effVal32,
+            PqLayout{effVR, P.nEff}, 1, 0, P.nEff, kc, nrmfc, D.transIdDev);
       } else {
         const size_t smem = pq_smem_bytes<float2>(4);
-        dim3 g8((npar + PQX_ROWS - 1) / PQX_ROWS, (P.nEff + 3) / 4, (kc + 7) / 8);
-        k_m2l_had_pqx2<4, false><<<g8, PQX_THREADS, smem, st>>>(npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn,
-                                                                D.effDen32, effDR, D.m2lT32, D.effVal32, effVR, P.nEff,
-                                                                kc, nrmfc, D.transIdDev);
+        dim3 g8((npar + PQX_ROWS - 1) / PQX_ROWS, (P.nEff + 3) / 4, nblk);
+        k_m2l_had_pqx2<4, false><<<g8, PQX_THREADS, smem, st>>>(
+            npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen32, PqLayout{blkDen, (int64_t)P.nEff * 8}, D.m2lT32,
+            D.effVal32, PqLayout{blkVal, (int64_t)P.nEff * 8}, 8, 1, P.nEff, kc, nrmfc, D.transIdDev);
       }
     } else if (P.sdm == 1 && P.tdm == 1) {
       const size_t smem = had_smem_bytes<float2>();
@@ -804,7 +892,25 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
     ls->launches++;
   }
   cudaEventRecord(D.ev[EV_M2L_HAD], st);
-  if ((mask & 4) && npar > 0 && ntrg > 0) {
+  if ((mask & 4) && npar > 0 && ntrg > 0 && r8) {
+#define FMMG_INV32R8(NP_)                                                                                      \
+  do {                                                                                                         \
+    constexpr size_t sm = r8_inv_smem<NP_>();                                                                  \
+    cudaFuncSetAttribute(k_m2l_inv32r8<NP_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);            \
+    k_m2l_inv32r8<NP_><<<dim3(ntrg, nblk), 256, sm, st>>>(D.vTrgNodes, D.effVal32, blkVal, P.nEff, D.surfIJK,  \
+                                                          P.nDC, D.dchk32, nn * dc, kc);                       \
+  } while (0)
+    switch (P.o.np) {
+      case 3: FMMG_INV32R8(3); break;
+      case 4: FMMG_INV32R8(4); break;
+      case 5: FMMG_INV32R8(5); break;
+      case 6: FMMG_INV32R8(6); break;
+      case 7: FMMG_INV32R8(7); break;
+      case 8: FMMG_INV32R8(8); break;
+    }
+#undef FMMG_INV32R8
+    ls->launches++;
+  } else if ((mask & 4) && npar > 0 && ntrg > 0) {
 #define FMMG_INV32(NP_)                                                                                   \
   k_m2l_inv32<NP_><<<dim3(ntrg, kc), 128, 0, st>>>(D.vTrgNodes, D.effVal32, effVR, P.nEff, P.tdm, D.surfIJK, \
                                                     P.nDC, D.dchk32, nn * dc)

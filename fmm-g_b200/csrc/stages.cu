@@ -26,6 +26,7 @@
 #include "cuda_common.cuh"
 #include "engine.hpp"
 #include "dense_kernel.cuh"
+#include "gemm_rows.cuh"
 #include "had_pq.cuh"
 #include "had_smem.cuh"
 #include "kernels.hpp"
@@ -326,95 +327,6 @@ __global__ void __launch_bounds__(SURF_THREADS)
     if (i < nSurf)
 #pragma unroll
       for (int c = 0; c < TD; c++) out[(int64_t)g * ldo + (int64_t)i * TD + c] += acc[k][c];
-  }
-}
-
-// ------------------------------------------------------------------ GEMMs
-// k_gemm_rows: for every listed node, Y[row] = beta*Y[row] + ys .* (W X[row]),
-// with X[row] scaled by xs on load.  W is N x K row-major.  The X (Y) row of a
-// node starts at its own id or at its first child's id, so the 8 children of a
-// parent form one contiguous row of length 8 * ld.  Used for C2E
-// (pinv GEMV, matmgnt3d_mpi.cpp:107-149, :196-229), M2M (:151-193) and L2L
-// (:231-274) over all nodes of a level at once.
-constexpr int GM_BM = 64, GM_BN = 64, GM_BK = 16;
-
-__global__ void __launch_bounds__(256)
-    k_gemm_rows(int nrows, const int32_t* __restrict__ rows, const int32_t* __restrict__ chd, int xChild,
-                int yChild, const double* __restrict__ X, int64_t ldx, const double* __restrict__ W,
-                double* __restrict__ Y, int64_t ldy, int K, int N, Scale4 xs, Scale4 ys, double beta) {
-  __shared__ double As[GM_BK][GM_BM + 1];
-  __shared__ double Bs[GM_BK][GM_BN + 1];
-  __shared__ const double* xrow[GM_BM];
-  __shared__ double* yrow[GM_BM];
-  const int tid = threadIdx.x;
-  const int r0 = blockIdx.x * GM_BM, n0 = blockIdx.y * GM_BN;
-  if (tid < GM_BM) {
-    int r = r0 + tid;
-    if (r < nrows) {
-      int node = rows[r];
-      int xn = xChild ? chd[node] : node;
-      int yn = yChild ? chd[node] : node;
-      xrow[tid] = X + (int64_t)xn * ldx;
-      yrow[tid] = Y + (int64_t)yn * ldy;
-    } else {
-      xrow[tid] = nullptr;
-      yrow[tid] = nullptr;
-    }
-  }
-  __syncthreads();
-  const int tr = tid / 16, tc = tid % 16;
-  double acc[4][4];
-#pragma unroll
-  for (int i = 0; i < 4; i++)
-#pragma unroll
-    for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
-  for (int k0 = 0; k0 < K; k0 += GM_BK) {
-    // X tile: 64 rows x 16 k
-#pragma unroll
-    for (int l = 0; l < 4; l++) {
-      int e = tid + l * 256;
-      int r = e / GM_BK, k = e % GM_BK;
-      const double* xr = xrow[r];
-      double v = 0.0;
-      if (xr && k0 + k < K) v = xr[k0 + k] * xs.v[(k0 + k) % xs.mod];
-      As[k][r] = v;
-    }
-    // W tile: 64 n x 16 k
-#pragma unroll
-    for (int l = 0; l < 4; l++) {
-      int e = tid + l * 256;
-      int n = e / GM_BK, k = e % GM_BK;
-      double v = 0.0;
-      if (n0 + n < N && k0 + k < K) v = W[(int64_t)(n0 + n) * K + k0 + k];
-      Bs[k][n] = v;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < GM_BK; k++) {
-      double a[4], b[4];
-#pragma unroll
-      for (int i = 0; i < 4; i++) a[i] = As[k][tr + 16 * i];
-#pragma unroll
-      for (int j = 0; j < 4; j++) b[j] = Bs[k][tc + 16 * j];
-#pragma unroll
-      for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int i = 0; i < 4; i++) {
-    double* yr = yrow[tr + 16 * i];
-    if (!yr) continue;
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      int n = n0 + tc + 16 * j;
-      if (n < N) {
-        double v = acc[i][j] * ys.v[n % ys.mod];
-        yr[n] = beta == 0.0 ? v : beta * yr[n] + v;
-      }
-    }
   }
 }
 
@@ -833,11 +745,19 @@ std::string dev_upload(const Plan& P, DevState& D, const double* src, const doub
 
 // ------------------------------------------------------------------ launcher
 void gemm_rows(cudaStream_t st, int nrows, const int32_t* rows, const int32_t* chd, int xChild, int yChild,
-                      const double* X, int64_t ldx, const double* W, double* Y, int64_t ldy, int K, int N,
-                      Scale4 xs, Scale4 ys, double beta, LaunchStats* ls) {
+               const double* X, int64_t ldx, const double* W, double* Y, int64_t ldy, int K, int N, Scale4 xs,
+               Scale4 ys, double beta, LaunchStats* ls) {
   if (nrows <= 0) return;
-  dim3 grid((nrows + GM_BM - 1) / GM_BM, (N + GM_BN - 1) / GM_BN);
-  k_gemm_rows<<<grid, 256, 0, st>>>(nrows, rows, chd, xChild, yChild, X, ldx, W, Y, ldy, K, N, xs, ys, beta);
+  GrScale<double> gx, gy;
+  gx.mod = xs.mod;
+  gy.mod = ys.mod;
+  for (int k = 0; k < 4; k++) {
+    gx.v[k] = xs.v[k];
+    gy.v[k] = ys.v[k];
+  }
+  dim3 grid((nrows + GR_BM - 1) / GR_BM, (N + GR_BN - 1) / GR_BN);
+  k_gemm_rows_t<double, 8><<<grid, GR_THREADS, 0, st>>>(nrows, 1, rows, chd, xChild, yChild, X, ldx, 0, W, Y, ldy, 0, K,
+                                                      N, gx, gy, beta);
   if (ls) ls->launches++;
 }
 
