@@ -589,14 +589,14 @@ static void run_adjoint(const Plan& P, DevState& D, int& launches) {
     const int32_t* rows;
     int n = rows_at(D.offDnC2E, d, rows);
     if (n > 0) {
-      gemm_rows(st, n, rows, D.chd, 0, 0, D.dden, de, D.dc2deT, D.dchk, dc, de, dc, level_scale(P, d + rl, -1.0),
+      gemm_rows(D, n, rows, D.chd, 0, 0, D.dden, de, D.dc2deT, D.dchk, dc, de, dc, level_scale(P, d + rl, -1.0),
                 unit_scale(), 0.0, nullptr);
       launches++;
     }
     if (d >= 3) {
       n = rows_at(D.offDnL2L, d - 1, rows);
       if (n > 0) {
-        gemm_rows(st, n, rows, D.chd, 1, 0, D.dchk, dc, D.l2lT, D.dden, de, 8 * dc, de, unit_scale(),
+        gemm_rows(D, n, rows, D.chd, 1, 0, D.dchk, dc, D.l2lT, D.dden, de, 8 * dc, de, unit_scale(),
                   level_scale(P, d - 1 + rl, +1.0), 1.0, nullptr);
         launches++;
       }
@@ -653,13 +653,13 @@ static void run_adjoint(const Plan& P, DevState& D, int& launches) {
     const int32_t* rows;
     int n = rows_at(D.offUpC2E, d, rows);
     if (n > 0) {
-      gemm_rows(st, n, rows, D.chd, 0, 0, D.uden, ue, D.uc2ueT, D.uchk, uc, ue, uc, level_scale(P, d + rl, -1.0),
+      gemm_rows(D, n, rows, D.chd, 0, 0, D.uden, ue, D.uc2ueT, D.uchk, uc, ue, uc, level_scale(P, d + rl, -1.0),
                 unit_scale(), 0.0, nullptr);
       launches++;
     }
     n = rows_at(D.offUpM2M, d, rows);
     if (n > 0) {
-      gemm_rows(st, n, rows, D.chd, 0, 1, D.uchk, uc, D.m2mT, D.uden, ue, uc, 8 * ue, unit_scale(),
+      gemm_rows(D, n, rows, D.chd, 0, 1, D.uchk, uc, D.m2mT, D.uden, ue, uc, 8 * ue, unit_scale(),
                 level_scale(P, d + 1 + rl, +1.0), 1.0, nullptr);
       launches++;
     }

@@ -79,7 +79,11 @@ struct DevState {
   int32_t *vParentsT = nullptr, *vNbrTIdx = nullptr; int64_t *vNbrTPtr = nullptr; int8_t *vNbrOffT = nullptr;
   int32_t *vRowOut = nullptr, *vNbrIn = nullptr, *vRowOutT = nullptr, *vNbrInT = nullptr;  // [rows|entries][8]
   bool adjListsReady = false, adjOpsStale = true;
-  bool hadPQ = true;  // scalar Hadamard: parent-pair register-blocked kernel (else expanded lists)
+  bool hadPQ = true;
+  // split-K partial tiles of the FP32 row GEMMs, and the SM count
+  double* gemmScratch = nullptr;
+  size_t gemmScratchBytes = 0;
+  int numSMs = 148;  // scalar Hadamard: parent-pair register-blocked kernel (else expanded lists)
   float adjMs = 0.f;
   // dense check scratch
   double *chkPos = nullptr, *chkOut = nullptr;
@@ -110,7 +114,7 @@ std::string dev_evaluate_mixed(const Plan& P, DevState& D, const double* dDenCal
                                int stageMask, bool timed, LaunchStats* st);
 // FP64 building blocks shared with the adjoint (stages.cu)
 struct Scale4;
-void gemm_rows(cudaStream_t st, int nrows, const int32_t* rows, const int32_t* chd, int xChild, int yChild,
+void gemm_rows(DevState& D, int nrows, const int32_t* rows, const int32_t* chd, int xChild, int yChild,
                const double* X, int64_t ldx, const double* W, double* Y, int64_t ldy, int K, int N, Scale4 xs,
                Scale4 ys, double beta, LaunchStats* ls);
 void spectral_fwd(const Plan& P, DevState& D, int n, const int32_t* nodes, Scale4 deg, int dof, const double* x,

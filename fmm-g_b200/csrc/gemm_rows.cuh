@@ -17,6 +17,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 namespace fmmg {
@@ -49,10 +50,11 @@ struct GrVec<double> {
 };
 
 template <typename T, int BK>
-__global__ void __launch_bounds__(GR_THREADS)
+__global__ void __launch_bounds__(GR_THREADS, 2)
     k_gemm_rows_t(int nrows, int nrhs, const int32_t* __restrict__ rows, const int32_t* __restrict__ chd, int xChild,
                   int yChild, const T* __restrict__ X, int64_t ldx, int64_t xRhs, const T* __restrict__ W,
-                  T* __restrict__ Y, int64_t ldy, int64_t yRhs, int K, int N, GrScale<T> xs, GrScale<T> ys, T beta) {
+                  T* __restrict__ Y, int64_t ldy, int64_t yRhs, int K, int N, GrScale<T> xs, GrScale<T> ys, T beta,
+                  int kChunk, T* __restrict__ part) {
   constexpr int AK = BK / 2, BKW = BK / 4;  // per thread: A row ra, k ka..ka+AK-1; B output nb, k kb..kb+BKW-1
   __shared__ __align__(16) T As[2][BK][GR_BM];
   __shared__ __align__(16) T Bs[2][BK][GR_BN];
@@ -75,6 +77,8 @@ __global__ void __launch_bounds__(GR_THREADS)
   __syncthreads();
   const int ra = tid >> 1, ka = (tid & 1) * AK;
   const int nb = tid >> 2, kb = (tid & 3) * BKW;
+  // K range of this split (blockIdx.z); the whole of K without splitting
+  const int kBeg = blockIdx.z * kChunk, kEnd = min(K, kBeg + kChunk);
   const T* xr = xrow[ra];
   const bool bIn = n0 + nb < N;
   const T* wr = W + (int64_t)(bIn ? n0 + nb : 0) * K;
@@ -83,11 +87,11 @@ __global__ void __launch_bounds__(GR_THREADS)
   {                                                                        \
     _Pragma("unroll") for (int i = 0; i < AK; i++) {                       \
       const int k = (K0) + ka + i;                                         \
-      fa[i] = (xr && k < K) ? xr[k] * gr_sel(xs, k) : T(0);                \
+      fa[i] = (xr && k < kEnd) ? xr[k] * gr_sel(xs, k) : T(0);             \
     }                                                                      \
     _Pragma("unroll") for (int i = 0; i < BKW; i++) {                      \
       const int k = (K0) + kb + i;                                         \
-      fb[i] = (bIn && k < K) ? wr[k] : T(0);                               \
+      fb[i] = (bIn && k < kEnd) ? wr[k] : T(0);                            \
     }                                                                      \
   }
 #define FMMG_GR_STASH(B_)                                                  \
@@ -101,14 +105,14 @@ __global__ void __launch_bounds__(GR_THREADS)
   for (int i = 0; i < 8; i++)
 #pragma unroll
     for (int j = 0; j < 4; j++) acc[i][j] = T(0);
-  FMMG_GR_FETCH(0)
+  FMMG_GR_FETCH(kBeg)
   FMMG_GR_STASH(0)
   __syncthreads();
   int buf = 0;
   typedef typename GrVec<T>::V V;
   constexpr int VW = sizeof(V) / sizeof(T);
-  for (int k0 = 0; k0 < K; k0 += BK) {
-    const bool more = k0 + BK < K;
+  for (int k0 = kBeg; k0 < kEnd; k0 += BK) {
+    const bool more = k0 + BK < kEnd;
     if (more) FMMG_GR_FETCH(k0 + BK)
 #pragma unroll
     for (int k = 0; k < BK; k++) {
@@ -144,6 +148,21 @@ __global__ void __launch_bounds__(GR_THREADS)
   }
 #undef FMMG_GR_FETCH
 #undef FMMG_GR_STASH
+  if (part) {  // split K: raw partial tile, reduced by k_gemm_reduce_t
+    const int64_t M = (int64_t)nrows * nrhs;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int r = r0 + tm * 8 + i;
+      if (r >= M) continue;
+      T* pr = part + ((int64_t)blockIdx.z * M + r) * N;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int n = n0 + tn * 4 + j;
+        if (n < N) pr[n] = acc[i][j];
+      }
+    }
+    return;
+  }
 #pragma unroll
   for (int i = 0; i < 8; i++) {
     T* yr = yrow[tm * 8 + i];
@@ -157,6 +176,58 @@ __global__ void __launch_bounds__(GR_THREADS)
       }
     }
   }
+}
+
+// Y[row] = beta * Y[row] + ys .* sum over splits of part[split][row]
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_gemm_reduce_t(int nrows, int nrhs, const int32_t* __restrict__ rows, const int32_t* __restrict__ chd,
+                    int yChild, T* __restrict__ Y, int64_t ldy, int64_t yRhs, int N, int splits,
+                    const T* __restrict__ part, GrScale<T> ys, T beta) {
+  const int64_t M = (int64_t)nrows * nrhs;
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= M * N) return;
+  const int64_t r = i / N;
+  const int n = (int)(i - r * N);
+  T s = T(0);
+  for (int z = 0; z < splits; z++) s += part[((int64_t)z * M + r) * N + n];
+  const int q = (int)(r / nrows);
+  const int node = rows[r - (int64_t)q * nrows];
+  T* yr = Y + q * yRhs + (int64_t)(yChild ? chd[node] : node) * ldy;
+  const T v = s * gr_sel(ys, n);
+  yr[n] = beta == T(0) ? v : beta * yr[n] + v;
+}
+
+// Launches the row GEMM; when the output tiles alone would leave the GPU
+// underfilled (fewer than two CTAs per SM) and K is long, K is split into up to
+// 8 chunks whose partial tiles go to `scratch` (scratchElems values) and are
+// summed in a fixed order by k_gemm_reduce_t, so results stay deterministic.
+// Returns the number of kernels launched.
+template <typename T, int BK>
+inline int launch_gemm_rows(cudaStream_t st, int numSMs, T* scratch, size_t scratchElems, int nrows, int nrhs,
+                            const int32_t* rows, const int32_t* chd, int xChild, int yChild, const T* X, int64_t ldx,
+                            int64_t xRhs, const T* W, T* Y, int64_t ldy, int64_t yRhs, int K, int N, GrScale<T> xs,
+                            GrScale<T> ys, T beta) {
+  if (nrows <= 0 || nrhs <= 0) return 0;
+  const int64_t M = (int64_t)nrows * nrhs;
+  const int tiles = (int)((M + GR_BM - 1) / GR_BM) * ((N + GR_BN - 1) / GR_BN);
+  int splits = 1;
+  if (scratch && tiles < 2 * numSMs && K >= 8 * BK) {
+    splits = std::min(8, (2 * numSMs + tiles - 1) / tiles);
+    splits = std::min(splits, K / (4 * BK));
+    while (splits > 1 && (size_t)splits * M * N > scratchElems) splits--;
+  }
+  const int kChunk = splits > 1 ? ((K + splits - 1) / splits + BK - 1) / BK * BK : K;
+  if (splits > 1) splits = (K + kChunk - 1) / kChunk;
+  dim3 grid((unsigned)((M + GR_BM - 1) / GR_BM), (N + GR_BN - 1) / GR_BN, splits);
+  k_gemm_rows_t<T, BK><<<grid, GR_THREADS, 0, st>>>(nrows, nrhs, rows, chd, xChild, yChild, X, ldx, xRhs, W, Y, ldy,
+                                                     yRhs, K, N, xs, ys, beta, kChunk,
+                                                     splits > 1 ? scratch : nullptr);
+  if (splits == 1) return 1;
+  const int64_t tot = M * N;
+  k_gemm_reduce_t<T><<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(nrows, nrhs, rows, chd, yChild, Y, ldy, yRhs, N,
+                                                                     splits, scratch, ys, beta);
+  return 2;
 }
 
 }  // namespace fmmg

@@ -771,10 +771,9 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
       gx.v[k] = (float)xs.v[k];
       gy.v[k] = (float)ys.v[k];
     }
-    dim3 grid((nrows * kc + GR_BM - 1) / GR_BM, (N + GR_BN - 1) / GR_BN);
-    k_gemm_rows_t<float, 16><<<grid, GR_THREADS, 0, st>>>(nrows, kc, rows, D.chd, xChild, yChild, X, ldx, xR, W, Y, ldy,
-                                                       yR, K, N, gx, gy, beta);
-    ls->launches++;
+    ls->launches += launch_gemm_rows<float, 16>(st, D.numSMs, reinterpret_cast<float*>(D.gemmScratch),
+                                                D.gemmScratchBytes / sizeof(float), nrows, kc, rows, D.chd, xChild,
+                                                yChild, X, ldx, xR, W, Y, ldy, yR, K, N, gx, gy, beta);
   };
   if ((mask & 1) && !P.s2mLeaves.empty()) {
     k_src2surf32<KT, KB><<<dim3((unsigned)P.s2mLeaves.size(), kb), MX_SURF, 0, st>>>(

@@ -578,6 +578,8 @@ void dev_free(DevState& D) {
   D.adjNearPtr = D.adjFarPtr = D.adjS2lPtr = nullptr;
   D.vParentsT = D.vNbrTIdx = nullptr;
   D.vRowOut = D.vNbrIn = D.vRowOutT = D.vNbrInT = nullptr;
+  D.gemmScratch = nullptr;
+  D.gemmScratchBytes = 0;
   D.vNbrTPtr = nullptr;
   D.vNbrOffT = nullptr;
   D.uc2ueT = D.m2mT = D.dc2deT = D.l2lT = D.gradT = nullptr;
@@ -732,6 +734,9 @@ std::string dev_upload(const Plan& P, DevState& D, const double* src, const doub
   FMMG_TRY(dput<double>(D, D.dden, nullptr, (size_t)P.nn * de));
   FMMG_TRY(dput<double2>(D, D.effDen, nullptr, P.vSrcNodes.size() * (size_t)P.nEff * P.sdm));
   FMMG_TRY(dput<double2>(D, D.effVal, nullptr, P.vTrgNodes.size() * (size_t)P.nEff * P.tdm));
+  D.gemmScratchBytes = (size_t)64 << 20;  // split-K partial tiles of the FP32 row GEMMs
+  FMMG_TRY(dput<double>(D, D.gemmScratch, nullptr, D.gemmScratchBytes / sizeof(double)));
+  FMMG_CK(cudaDeviceGetAttribute(&D.numSMs, cudaDevAttrMultiProcessorCount, D.device));
   {
     const char* hk = std::getenv("FMMG_HADAMARD");
     D.hadPQ = !(hk && std::strcmp(hk, "list") == 0);
@@ -744,7 +749,7 @@ std::string dev_upload(const Plan& P, DevState& D, const double* src, const doub
 }
 
 // ------------------------------------------------------------------ launcher
-void gemm_rows(cudaStream_t st, int nrows, const int32_t* rows, const int32_t* chd, int xChild, int yChild,
+void gemm_rows(DevState& D, int nrows, const int32_t* rows, const int32_t* chd, int xChild, int yChild,
                const double* X, int64_t ldx, const double* W, double* Y, int64_t ldy, int K, int N, Scale4 xs,
                Scale4 ys, double beta, LaunchStats* ls) {
   if (nrows <= 0) return;
@@ -755,10 +760,11 @@ void gemm_rows(cudaStream_t st, int nrows, const int32_t* rows, const int32_t* c
     gx.v[k] = xs.v[k];
     gy.v[k] = ys.v[k];
   }
-  dim3 grid((nrows + GR_BM - 1) / GR_BM, (N + GR_BN - 1) / GR_BN);
-  k_gemm_rows_t<double, 8><<<grid, GR_THREADS, 0, st>>>(nrows, 1, rows, chd, xChild, yChild, X, ldx, 0, W, Y, ldy, 0, K,
-                                                      N, gx, gy, beta);
-  if (ls) ls->launches++;
+  // FP64 keeps each output's K sum in sequential order (no split-K scratch):
+  // the 1e-10 parity with the oracle's sequential sums depends on it at np = 7
+  const int n = launch_gemm_rows<double, 8>(D.stream, D.numSMs, nullptr, 0, nrows, 1, rows, chd, xChild, yChild, X,
+                                            ldx, 0, W, Y, ldy, 0, K, N, gx, gy, beta);
+  if (ls) ls->launches += n;
 }
 
 template <int KT>
@@ -937,10 +943,10 @@ static void run_stages(const Plan& P, DevState& D, int mask, LaunchStats* ls) {
   if (mask & 1) {  // upward: M2M + C2E per level
     for (int d = P.maxDepth; d >= 1; d--) {
       int64_t a = D.offUpM2M[d], b = D.offUpM2M[d + 1];
-      gemm_rows(st, (int)(b - a), D.levelRows + a, D.chd, 1, 0, D.uden, ue, D.m2m, D.uchk, uc, 8 * ue, uc,
+      gemm_rows(D, (int)(b - a), D.levelRows + a, D.chd, 1, 0, D.uden, ue, D.m2m, D.uchk, uc, 8 * ue, uc,
                 level_scale(P, d + 1 + rl, +1.0), unit_scale(), 0.0, ls);
       a = D.offUpC2E[d]; b = D.offUpC2E[d + 1];
-      gemm_rows(st, (int)(b - a), D.levelRows + a, D.chd, 0, 0, D.uchk, uc, D.uc2ue, D.uden, ue, uc, ue, unit_scale(),
+      gemm_rows(D, (int)(b - a), D.levelRows + a, D.chd, 0, 0, D.uchk, uc, D.uc2ue, D.uden, ue, uc, ue, unit_scale(),
                 level_scale(P, d + rl, -1.0), 0.0, ls);
     }
   }
@@ -970,11 +976,11 @@ static void run_stages(const Plan& P, DevState& D, int mask, LaunchStats* ls) {
     for (int d = 2; d <= P.maxDepth; d++) {
       if (d >= 3) {
         int64_t a = D.offDnL2L[d - 1], b = D.offDnL2L[d];
-        gemm_rows(st, (int)(b - a), D.levelRows + a, D.chd, 0, 1, D.dden, de, D.l2l, D.dchk, dc, de, 8 * dc,
+        gemm_rows(D, (int)(b - a), D.levelRows + a, D.chd, 0, 1, D.dden, de, D.l2l, D.dchk, dc, de, 8 * dc,
                   level_scale(P, d - 1 + rl, +1.0), unit_scale(), 1.0, ls);
       }
       int64_t a = D.offDnC2E[d], b = D.offDnC2E[d + 1];
-      gemm_rows(st, (int)(b - a), D.levelRows + a, D.chd, 0, 0, D.dchk, dc, D.dc2de, D.dden, de, dc, de,
+      gemm_rows(D, (int)(b - a), D.levelRows + a, D.chd, 0, 0, D.dchk, dc, D.dc2de, D.dden, de, dc, de,
                 unit_scale(), level_scale(P, d + rl, -1.0), 0.0, ls);
     }
   }

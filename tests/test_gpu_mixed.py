@@ -85,8 +85,11 @@ def test_mixed_multi_rhs_matches_single_rhs():
     lib.evaluate_device(d, out, k, fmmg.PREC_MIXED)
     lib.sync()
     V = out.cpu().numpy()
+    # The batched and single forms may split the K sums of the FP32 row GEMMs
+    # differently (split-K is chosen by problem size), so they agree to FP32
+    # rounding; a right-hand side mixed up with another would differ by O(1).
     for r in (0, 7, 10):
-        assert rel_l2(V[r], _mixed_eval(lib, D[r])) <= 1e-12
+        assert rel_l2(V[r], _mixed_eval(lib, D[r])) <= 1e-6
     nrm = W.unit_normals(rng, n)
     g = fmmg.FMM3d(321, np_=4, pts_max=64)
     g.setup(src, nrm)
@@ -97,4 +100,4 @@ def test_mixed_multi_rhs_matches_single_rhs():
     g.sync()
     V3 = out3.cpu().numpy()
     for r in (0, 4):
-        assert rel_l2(V3[r], _mixed_eval(g, D3[r])) <= 1e-12
+        assert rel_l2(V3[r], _mixed_eval(g, D3[r])) <= 1e-6
