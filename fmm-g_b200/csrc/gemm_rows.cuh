@@ -9,7 +9,7 @@
 // their transposes in the adjoint.
 //
 // Tiling: 128 (rows x right-hand sides) x 64 (outputs) per CTA, K in steps of
-// BK (16 for FP32, 8 for FP64: 48 KB of shared memory either way), 256
+// BK (16 for FP32, 8 for FP64: four 16-byte vectors per tile row), 256
 // threads each owning an 8 x 4 register tile.  The next K step is
 // fetched into registers while the current one is multiplied from shared
 // memory (two buffers, one barrier per step).
@@ -49,15 +49,22 @@ struct GrVec<double> {
   typedef double2 V;
 };
 
-template <typename T, int BK>
+// VEC: X rows and W rows are 16-byte aligned with K a multiple of the vector
+// width, so the tiles are fetched as 16-byte vectors along K (4 vectors per
+// row of a K step, consecutive threads on consecutive vectors); otherwise
+// element by element.  Shared tiles are padded against bank conflicts.
+template <typename T, int BK, bool VEC>
 __global__ void __launch_bounds__(GR_THREADS, 2)
     k_gemm_rows_t(int nrows, int nrhs, const int32_t* __restrict__ rows, const int32_t* __restrict__ chd, int xChild,
                   int yChild, const T* __restrict__ X, int64_t ldx, int64_t xRhs, const T* __restrict__ W,
                   T* __restrict__ Y, int64_t ldy, int64_t yRhs, int K, int N, GrScale<T> xs, GrScale<T> ys, T beta,
                   int kChunk, T* __restrict__ part) {
-  constexpr int AK = BK / 2, BKW = BK / 4;  // per thread: A row ra, k ka..ka+AK-1; B output nb, k kb..kb+BKW-1
-  __shared__ __align__(16) T As[2][BK][GR_BM];
-  __shared__ __align__(16) T Bs[2][BK][GR_BN];
+  typedef typename GrVec<T>::V V;
+  constexpr int VW = sizeof(V) / sizeof(T);  // 4 floats or 2 doubles
+  static_assert(BK / VW == 4, "four vectors per tile row");
+  constexpr int PA = GR_BM + VW, PB = GR_BN + VW;  // padded tile rows
+  __shared__ __align__(16) T As[2][BK][PA];
+  __shared__ __align__(16) T Bs[2][BK][PB];
   __shared__ const T* xrow[GR_BM];
   __shared__ T* yrow[GR_BM];
   const int tid = threadIdx.x;
@@ -75,65 +82,81 @@ __global__ void __launch_bounds__(GR_THREADS, 2)
     }
   }
   __syncthreads();
-  const int ra = tid >> 1, ka = (tid & 1) * AK;
-  const int nb = tid >> 2, kb = (tid & 3) * BKW;
   // K range of this split (blockIdx.z); the whole of K without splitting
   const int kBeg = blockIdx.z * kChunk, kEnd = min(K, kBeg + kChunk);
-  const T* xr = xrow[ra];
-  const bool bIn = n0 + nb < N;
-  const T* wr = W + (int64_t)(bIn ? n0 + nb : 0) * K;
-  T fa[AK], fb[BKW];
-#define FMMG_GR_FETCH(K0)                                                  \
-  {                                                                        \
-    _Pragma("unroll") for (int i = 0; i < AK; i++) {                       \
-      const int k = (K0) + ka + i;                                         \
-      fa[i] = (xr && k < kEnd) ? xr[k] * gr_sel(xs, k) : T(0);             \
-    }                                                                      \
-    _Pragma("unroll") for (int i = 0; i < BKW; i++) {                      \
-      const int k = (K0) + kb + i;                                         \
-      fb[i] = (bIn && k < kEnd) ? wr[k] : T(0);                            \
-    }                                                                      \
-  }
-#define FMMG_GR_STASH(B_)                                                  \
-  {                                                                        \
-    _Pragma("unroll") for (int i = 0; i < AK; i++) As[B_][ka + i][ra] = fa[i]; \
-    _Pragma("unroll") for (int i = 0; i < BKW; i++) Bs[B_][kb + i][nb] = fb[i]; \
-  }
+  // fetch mapping: A vectors (row tid/4 and 64 + tid/4, K quad tid%4), B vector (output tid/4, K quad tid%4)
+  const int fr = tid >> 2, fq = (tid & 3) * VW;
+  const T* xa0 = xrow[fr];
+  const T* xa1 = xrow[fr + 64];
+  const bool bIn = n0 + fr < N;
+  const T* wr = W + (int64_t)(bIn ? n0 + fr : 0) * K;
+  T fa0[VW], fa1[VW], fb[VW];
+  auto fetch = [&](int k0) {
+    const int k = k0 + fq;
+    if (VEC) {
+      const bool kin = k < kEnd;  // VW | K and VW | kChunk: the whole vector is in range
+      V a0 = {}, a1 = {}, bv = {};
+      if (xa0 && kin) a0 = *reinterpret_cast<const V*>(xa0 + k);
+      if (xa1 && kin) a1 = *reinterpret_cast<const V*>(xa1 + k);
+      if (bIn && kin) bv = *reinterpret_cast<const V*>(wr + k);
+      const T* pa0 = reinterpret_cast<const T*>(&a0);
+      const T* pa1 = reinterpret_cast<const T*>(&a1);
+      const T* pb = reinterpret_cast<const T*>(&bv);
+#pragma unroll
+      for (int j = 0; j < VW; j++) {
+        const T sc = gr_sel(xs, k + j);
+        fa0[j] = pa0[j] * sc;
+        fa1[j] = pa1[j] * sc;
+        fb[j] = pb[j];
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < VW; j++) {
+        const bool kin = k + j < kEnd;
+        const T sc = gr_sel(xs, k + j);
+        fa0[j] = (xa0 && kin) ? xa0[k + j] * sc : T(0);
+        fa1[j] = (xa1 && kin) ? xa1[k + j] * sc : T(0);
+        fb[j] = (bIn && kin) ? wr[k + j] : T(0);
+      }
+    }
+  };
+  auto stash = [&](int b) {
+#pragma unroll
+    for (int j = 0; j < VW; j++) {
+      As[b][fq + j][fr] = fa0[j];
+      As[b][fq + j][fr + 64] = fa1[j];
+      Bs[b][fq + j][fr] = fb[j];
+    }
+  };
   const int tm = tid >> 4, tn = tid & 15;  // rows tm*8 .. +7, outputs tn*4 .. +3
   T acc[8][4];
 #pragma unroll
   for (int i = 0; i < 8; i++)
 #pragma unroll
     for (int j = 0; j < 4; j++) acc[i][j] = T(0);
-  FMMG_GR_FETCH(kBeg)
-  FMMG_GR_STASH(0)
+  fetch(kBeg);
+  stash(0);
   __syncthreads();
   int buf = 0;
-  typedef typename GrVec<T>::V V;
-  constexpr int VW = sizeof(V) / sizeof(T);
   for (int k0 = kBeg; k0 < kEnd; k0 += BK) {
     const bool more = k0 + BK < kEnd;
-    if (more) FMMG_GR_FETCH(k0 + BK)
+    if (more) fetch(k0 + BK);
 #pragma unroll
     for (int k = 0; k < BK; k++) {
       T a[8], b[4];
 #pragma unroll
       for (int i = 0; i < 8; i += VW) {
         const V v = *reinterpret_cast<const V*>(&As[buf][k][tm * 8 + i]);
-        if constexpr (VW == 4) {
-          a[i] = v.x; a[i + 1] = v.y; a[i + 2] = v.z; a[i + 3] = v.w;
-        } else {
-          a[i] = v.x; a[i + 1] = v.y;
-        }
+        const T* pv = reinterpret_cast<const T*>(&v);
+#pragma unroll
+        for (int j = 0; j < VW; j++) a[i + j] = pv[j];
       }
 #pragma unroll
-      for (int j = 0; j < 4; j += VW) {
-        const V v = *reinterpret_cast<const V*>(&Bs[buf][k][tn * 4 + j]);
-        if constexpr (VW == 4) {
-          b[j] = v.x; b[j + 1] = v.y; b[j + 2] = v.z; b[j + 3] = v.w;
-        } else {
-          b[j] = v.x; b[j + 1] = v.y;
-        }
+      for (int j0 = 0; j0 < 4; j0 += VW) {
+        const V v = *reinterpret_cast<const V*>(&Bs[buf][k][tn * 4 + j0]);
+        const T* pv = reinterpret_cast<const T*>(&v);
+#pragma unroll
+        for (int j = 0; j < VW; j++) b[j0 + j] = pv[j];
       }
 #pragma unroll
       for (int i = 0; i < 8; i++)
@@ -141,13 +164,11 @@ __global__ void __launch_bounds__(GR_THREADS, 2)
         for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
     }
     if (more) {
-      FMMG_GR_STASH(buf ^ 1)
+      stash(buf ^ 1);
       __syncthreads();
       buf ^= 1;
     }
   }
-#undef FMMG_GR_FETCH
-#undef FMMG_GR_STASH
   if (part) {  // split K: raw partial tile, reduced by k_gemm_reduce_t
     const int64_t M = (int64_t)nrows * nrhs;
 #pragma unroll
@@ -219,10 +240,17 @@ inline int launch_gemm_rows(cudaStream_t st, int numSMs, T* scratch, size_t scra
   }
   const int kChunk = splits > 1 ? ((K + splits - 1) / splits + BK - 1) / BK * BK : K;
   if (splits > 1) splits = (K + kChunk - 1) / kChunk;
+  constexpr int VW = 16 / sizeof(T);
+  const bool vec = ((uintptr_t)X % 16 == 0) && ((uintptr_t)W % 16 == 0) && ldx % VW == 0 && xRhs % VW == 0 &&
+                   K % VW == 0;
   dim3 grid((unsigned)((M + GR_BM - 1) / GR_BM), (N + GR_BN - 1) / GR_BN, splits);
-  k_gemm_rows_t<T, BK><<<grid, GR_THREADS, 0, st>>>(nrows, nrhs, rows, chd, xChild, yChild, X, ldx, xRhs, W, Y, ldy,
-                                                     yRhs, K, N, xs, ys, beta, kChunk,
-                                                     splits > 1 ? scratch : nullptr);
+  T* pt = splits > 1 ? scratch : nullptr;
+  if (vec)
+    k_gemm_rows_t<T, BK, true><<<grid, GR_THREADS, 0, st>>>(nrows, nrhs, rows, chd, xChild, yChild, X, ldx, xRhs, W,
+                                                             Y, ldy, yRhs, K, N, xs, ys, beta, kChunk, pt);
+  else
+    k_gemm_rows_t<T, BK, false><<<grid, GR_THREADS, 0, st>>>(nrows, nrhs, rows, chd, xChild, yChild, X, ldx, xRhs, W,
+                                                              Y, ldy, yRhs, K, N, xs, ys, beta, kChunk, pt);
   if (splits == 1) return 1;
   const int64_t tot = M * N;
   k_gemm_reduce_t<T><<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(nrows, nrhs, rows, chd, yChild, Y, ldy, yRhs, N,

@@ -527,17 +527,47 @@ __global__ void __launch_bounds__(128)
 }
 
 // Scalar equivalent kernels, blocks of 8 right-hand sides: one CTA per
-// (slot, block) transforms the 8 densities together, the right-hand side
-// being the fastest index of every staging array, so the spectra are written
-// (and read back by k_m2l_inv32r8) as [block][slot][frequency][8] in
-// contiguous runs.  Dynamic shared memory r8_fwd_smem<NP>() / r8_inv_smem<NP>().
+// (slot, block) transforms the 8 densities together.  A thread owns one grid
+// point or frequency and all 8 right-hand sides, so each twiddle serves 8
+// complex MACs.  Shared staging arrays are planes [8][...] (a warp's accesses
+// are stride-1, free of bank conflicts); in global memory the spectra are
+// written (and read back by k_m2l_inv32r8) as [block][slot][frequency][8]
+// with 16-byte accesses.  The twiddles of every pass come from one table
+// twb[k][b] = exp(-2 pi i k (b + np/2) / 2np).  Dynamic shared memory
+// r8_fwd_smem<NP>() / r8_inv_smem<NP>().
 template <int NP>
 constexpr size_t r8_fwd_smem() {
-  return sizeof(float) * NP * NP * NP * 8 + sizeof(float2) * (NP * NP * (NP + 1) * 8 + NP * 2 * NP * (NP + 1) * 8 + 2 * NP);
+  return sizeof(float) * NP * NP * NP * 8 + sizeof(float2) * (NP * NP * (NP + 1) * 8 + NP * 2 * NP * (NP + 1) * 8) +
+         sizeof(float2) * 2 * NP * NP;
 }
 template <int NP>
 constexpr size_t r8_inv_smem() {
-  return sizeof(float2) * (NP * 2 * NP * (NP + 1) * 8 + NP * NP * (NP + 1) * 8 + 2 * NP);
+  return sizeof(float2) * (NP * 2 * NP * (NP + 1) * 8 + NP * NP * (NP + 1) * 8) + sizeof(float2) * 2 * NP * NP;
+}
+
+__device__ __forceinline__ void r8_load(const float2* p, float2 (&v)[8]) {
+  const float4* q = reinterpret_cast<const float4*>(p);
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const float4 t = q[i];
+    v[2 * i] = make_float2(t.x, t.y);
+    v[2 * i + 1] = make_float2(t.z, t.w);
+  }
+}
+__device__ __forceinline__ void r8_store(float2* p, const float2 (&v)[8]) {
+  float4* q = reinterpret_cast<float4*>(p);
+#pragma unroll
+  for (int i = 0; i < 4; i++) q[i] = make_float4(v[2 * i].x, v[2 * i].y, v[2 * i + 1].x, v[2 * i + 1].y);
+}
+template <int NP>
+__device__ __forceinline__ void r8_twiddles(float2* twb) {
+  using F = FftDims<NP>;
+  for (int i = threadIdx.x; i < F::N * NP; i += blockDim.x) {
+    const int k = i / NP, b = i % NP;
+    double sn, cs;
+    sincospi(2.0 * ((k * (b + F::H)) % F::N) / F::N, &sn, &cs);
+    twb[i] = make_float2((float)cs, (float)-sn);
+  }
 }
 
 template <int NP>
@@ -546,21 +576,18 @@ __global__ void __launch_bounds__(256)
                   const float* __restrict__ uden, int64_t udenRhs, const int32_t* __restrict__ ijk, int nUE,
                   float2* __restrict__ effDen, int64_t blkStride, int nEff, int kc) {
   using F = FftDims<NP>;
-  constexpr int N = F::N, NH = F::NH, H = F::H;
+  constexpr int N = F::N, NH = F::NH;
   extern __shared__ __align__(16) unsigned char r8_smem[];
-  float2* X1 = reinterpret_cast<float2*>(r8_smem);  // [NP][NP][NH][8]
-  float2* X2 = X1 + NP * NP * NH * 8;                // [NP][N][NH][8]
-  float2* tw = X2 + NP * N * NH * 8;                 // [N]
-  float* cube = reinterpret_cast<float*>(tw + N);    // [NP][NP][NP][8]
+  constexpr int S1 = NP * NP * NH, S2 = NP * N * NH, S3 = NP * NP * NP;  // planes per right-hand side
+  float2* X1 = reinterpret_cast<float2*>(r8_smem);  // [8][NP][NP][NH]
+  float2* X2 = X1 + S1 * 8;                          // [8][NP][N][NH]
+  float2* twb = X2 + S2 * 8;                         // [N][NP]
+  float* cube = reinterpret_cast<float*>(twb + N * NP);  // [8][NP][NP][NP]
   const int slot = blockIdx.x;
   const int v = nodes[slot];
   const int r0 = blockIdx.y * 8;
   const int tid = threadIdx.x;
-  if (tid < N) {
-    double sn, cs;
-    sincospi(2.0 * tid / N, &sn, &cs);
-    tw[tid] = make_float2((float)cs, (float)-sn);
-  }
+  r8_twiddles<NP>(twb);
   const float scl = (float)exp2((double)(depth[v] + rootLevel) * deg);
   for (int i = tid; i < NP * NP * NP * 8; i += blockDim.x) cube[i] = 0.f;
   __syncthreads();
@@ -568,49 +595,68 @@ __global__ void __launch_bounds__(256)
     const int j = i >> 3, r = i & 7;
     if (r0 + r >= kc) continue;
     const int p = ijk[j];
-    cube[(((p >> 16) * NP + ((p >> 8) & 255)) * NP + (p & 255)) * 8 + r] =
+    cube[r * S3 + ((p >> 16) * NP + ((p >> 8) & 255)) * NP + (p & 255)] =
         uden[(int64_t)(r0 + r) * udenRhs + (int64_t)v * nUE + j] * scl;
   }
   __syncthreads();
-  for (int i = tid; i < NP * NP * NH * 8; i += blockDim.x) {  // x pass (real -> half spectrum)
-    const int r = i & 7, e = i >> 3;
+  for (int e = tid; e < NP * NP * NH; e += blockDim.x) {  // x pass (real -> half spectrum)
     const int kx = e % NH, yb = (e / NH) % NP, zb = e / (NH * NP);
-    const float* row = &cube[(zb * NP + yb) * NP * 8 + r];
-    float2 s = make_float2(0.f, 0.f);
+    const float* row = &cube[(zb * NP + yb) * NP];
+    float2 s[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) s[r] = make_float2(0.f, 0.f);
 #pragma unroll
     for (int xb = 0; xb < NP; xb++) {
-      const float2 w = tw[(kx * (xb + H)) % N];
-      s.x += row[xb * 8] * w.x;
-      s.y += row[xb * 8] * w.y;
+      const float2 w = twb[kx * NP + xb];
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        const float c = row[r * S3 + xb];
+        s[r].x += c * w.x;
+        s[r].y += c * w.y;
+      }
     }
-    X1[i] = s;
+#pragma unroll
+    for (int r = 0; r < 8; r++) X1[r * S1 + e] = s[r];
   }
   __syncthreads();
-  for (int i = tid; i < NP * N * NH * 8; i += blockDim.x) {  // y pass
-    const int r = i & 7, e = i >> 3;
+  for (int e = tid; e < NP * N * NH; e += blockDim.x) {  // y pass
     const int kx = e % NH, ky = (e / NH) % N, zb = e / (NH * N);
-    float2 s = make_float2(0.f, 0.f);
+    float2 s[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) s[r] = make_float2(0.f, 0.f);
 #pragma unroll
     for (int yb = 0; yb < NP; yb++) {
-      const float2 t = cmul(X1[((zb * NP + yb) * NH + kx) * 8 + r], tw[(ky * (yb + H)) % N]);
-      s.x += t.x;
-      s.y += t.y;
+      const float2 w = twb[ky * NP + yb];
+      const int src = (zb * NP + yb) * NH + kx;
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        const float2 t = cmul(X1[r * S1 + src], w);
+        s[r].x += t.x;
+        s[r].y += t.y;
+      }
     }
-    X2[i] = s;
+#pragma unroll
+    for (int r = 0; r < 8; r++) X2[r * S2 + e] = s[r];
   }
   __syncthreads();
   float2* out = effDen + blockIdx.y * blkStride + (int64_t)slot * nEff * 8;
-  for (int i = tid; i < N * N * NH * 8; i += blockDim.x) {  // z pass
-    const int r = i & 7, e = i >> 3;
+  for (int e = tid; e < N * N * NH; e += blockDim.x) {  // z pass
     const int kx = e % NH, ky = (e / NH) % N, kz = e / (NH * N);
-    float2 s = make_float2(0.f, 0.f);
+    float2 s[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) s[r] = make_float2(0.f, 0.f);
 #pragma unroll
     for (int zb = 0; zb < NP; zb++) {
-      const float2 t = cmul(X2[((zb * N + ky) * NH + kx) * 8 + r], tw[(kz * (zb + H)) % N]);
-      s.x += t.x;
-      s.y += t.y;
+      const float2 w = twb[kz * NP + zb];
+      const int src = (zb * N + ky) * NH + kx;
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        const float2 t = cmul(X2[r * S2 + src], w);
+        s[r].x += t.x;
+        s[r].y += t.y;
+      }
     }
-    out[i] = s;
+    r8_store(&out[(int64_t)e * 8], s);
   }
 }
 
@@ -621,61 +667,77 @@ __global__ void __launch_bounds__(256)
   using F = FftDims<NP>;
   constexpr int N = F::N, NH = F::NH, H = F::H;
   extern __shared__ __align__(16) unsigned char r8_smem[];
-  float2* Y2 = reinterpret_cast<float2*>(r8_smem);  // [NP][N][NH][8]
-  float2* Y1 = Y2 + NP * N * NH * 8;                 // [NP][NP][NH][8]
-  float2* tw = Y1 + NP * NP * NH * 8;                // [N]
+  constexpr int S1 = NP * NP * NH, S2 = NP * N * NH;  // planes per right-hand side
+  float2* Y2 = reinterpret_cast<float2*>(r8_smem);  // [8][NP][N][NH]
+  float2* Y1 = Y2 + S2 * 8;                          // [8][NP][NP][NH]
+  float2* twb = Y1 + S1 * 8;                         // [N][NP]
   const int slot = blockIdx.x;
   const int node = nodes[slot];
   const int r0 = blockIdx.y * 8;
   const int tid = threadIdx.x;
-  if (tid < N) {
-    double sn, cs;
-    sincospi(2.0 * tid / N, &sn, &cs);
-    tw[tid] = make_float2((float)cs, (float)-sn);
-  }
+  r8_twiddles<NP>(twb);
   __syncthreads();
   const float2* in = effVal + blockIdx.y * blkStride + (int64_t)slot * nEff * 8;
-  for (int i = tid; i < NP * N * NH * 8; i += blockDim.x) {  // z pass, band outputs only
-    const int r = i & 7, e = i >> 3;
+  for (int e = tid; e < NP * N * NH; e += blockDim.x) {  // z pass, band outputs only
     const int kx = e % NH, ky = (e / NH) % N, zb = e / (NH * N);
-    float2 s = make_float2(0.f, 0.f);
+    float2 s[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) s[r] = make_float2(0.f, 0.f);
 #pragma unroll 4
     for (int kz = 0; kz < N; kz++) {
-      const float2 t = cmulc(in[((kz * N + ky) * NH + kx) * 8 + r], tw[(kz * (zb + H)) % N]);
-      s.x += t.x;
-      s.y += t.y;
+      const float2 w = twb[kz * NP + zb];
+      float2 x[8];
+      r8_load(&in[((int64_t)(kz * N + ky) * NH + kx) * 8], x);
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        const float2 t = cmulc(x[r], w);
+        s[r].x += t.x;
+        s[r].y += t.y;
+      }
     }
-    Y2[i] = s;
+#pragma unroll
+    for (int r = 0; r < 8; r++) Y2[r * S2 + e] = s[r];
   }
   __syncthreads();
-  for (int i = tid; i < NP * NP * NH * 8; i += blockDim.x) {  // y pass
-    const int r = i & 7, e = i >> 3;
+  for (int e = tid; e < NP * NP * NH; e += blockDim.x) {  // y pass
     const int kx = e % NH, yb = (e / NH) % NP, zb = e / (NH * NP);
-    float2 s = make_float2(0.f, 0.f);
+    float2 s[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) s[r] = make_float2(0.f, 0.f);
 #pragma unroll
     for (int ky = 0; ky < N; ky++) {
-      const float2 t = cmulc(Y2[((zb * N + ky) * NH + kx) * 8 + r], tw[(ky * (yb + H)) % N]);
-      s.x += t.x;
-      s.y += t.y;
+      const float2 w = twb[ky * NP + yb];
+      const int src = (zb * N + ky) * NH + kx;
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        const float2 t = cmulc(Y2[r * S2 + src], w);
+        s[r].x += t.x;
+        s[r].y += t.y;
+      }
     }
-    Y1[i] = s;
+#pragma unroll
+    for (int r = 0; r < 8; r++) Y1[r * S1 + e] = s[r];
   }
   __syncthreads();
-  for (int i = tid; i < nDC * 8; i += blockDim.x) {  // x pass (c2r) at the surface points
-    const int r = i & 7, j = i >> 3;
-    if (r0 + r >= kc) continue;
-    const int p = ijk[j];
+  for (int i = tid; i < nDC; i += blockDim.x) {  // x pass (c2r) at the surface points
+    const int p = ijk[i];
     const int a = p & 255, b = (p >> 8) & 255, cc = p >> 16;
-    const float2* y1 = &Y1[(cc * NP + b) * NH * 8 + r];
-    const int x = a + H;
-    float s = 0.f;
+    const float2* y1 = &Y1[(cc * NP + b) * NH];
+    float s[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) s[r] = 0.f;
 #pragma unroll
     for (int kx = 0; kx < NH; kx++) {
-      const float2 t = cmulc(y1[kx * 8], tw[(kx * x) % N]);
-      s += (kx == 0 || kx == N / 2) ? t.x : 2.f * t.x;
+      const float2 w = twb[kx * NP + a];
+      const float f = (kx == 0 || kx == N / 2) ? 1.f : 2.f;
+#pragma unroll
+      for (int r = 0; r < 8; r++) s[r] += f * cmulc(y1[r * S1 + kx], w).x;
     }
-    dchk[(int64_t)(r0 + r) * dchkRhs + (int64_t)node * nDC + j] += s;
+#pragma unroll
+    for (int r = 0; r < 8; r++)
+      if (r0 + r < kc) dchk[(int64_t)(r0 + r) * dchkRhs + (int64_t)node * nDC + i] += s[r];
   }
+  (void)H;
 }
 
 // ------------------------------------------------------------------ launcher
