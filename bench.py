@@ -231,6 +231,7 @@ def time_adjoint(f, torch, stream, den_dev, out_dev, n, steps, warmup, flush):
 def run_ours(args):
     import torch
     import fmmg
+    import fmmg_dist as FD
     import workloads as W
     ws, rank, local = dist_env()
     dist = ws > 1
@@ -272,9 +273,7 @@ def run_ours(args):
     for name, prec, k in forms:
         ms, kern, launches = time_form(f, torch, stream, den, out, n, k, prec, args.steps, args.warmup, flush)
         if dist:
-            t = torch.tensor([ms], device="cuda")
-            tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-            ms = float(t.item())
+            ms = FD.max_over_ranks(ms, device="cuda")
         vals = out[0].cpu().numpy()
         rel, mx, _ = f.check(dens[0], vals, idx)
         results.append(dict(precision=name, k=k, ms_per_step=ms, points_per_s=n * k * ws / (ms * 1e-3),
@@ -282,9 +281,8 @@ def run_ours(args):
                             stage_ms=f.stage_times(), launches=launches))
     adj = time_adjoint(f, torch, stream, den, out, n, args.steps, args.warmup, flush)
     if dist:
-        t = torch.tensor([adj["ms_per_step"], adj["target_grad_ms_per_step"]], device="cuda")
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        adj["ms_per_step"], adj["target_grad_ms_per_step"] = float(t[0].item()), float(t[1].item())
+        adj["ms_per_step"] = FD.max_over_ranks(adj["ms_per_step"], device="cuda")
+        adj["target_grad_ms_per_step"] = FD.max_over_ranks(adj["target_grad_ms_per_step"], device="cuda")
     clk = clocks.stop()
     fp64 = results[0]
     adj["ratio_vs_fp64_forward"] = adj["ms_per_step"] / fp64["ms_per_step"]
@@ -307,9 +305,7 @@ def run_ours(args):
         e2e_ms.append(s_.elapsed_time(e_))
     e2e = float(np.mean(e2e_ms))
     if dist:
-        t = torch.tensor([e2e], device="cuda")
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        e2e = float(t.item())
+        e2e = FD.max_over_ranks(e2e, device="cuda")
         tdist.barrier()
     if rank == 0:
         roof = roofline(f, head["kernel_ms"], torch, kh, head["precision"])

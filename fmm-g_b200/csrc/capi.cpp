@@ -31,7 +31,8 @@ struct fmmg_handle {
   double* dDenK = nullptr;  // k-RHS host-call staging
   double* dValK = nullptr;
   int ioK = 0;
-  double *dAdjW = nullptr, *dAdjG = nullptr, *dAdjGrad = nullptr;  // host-call staging of the adjoint
+  double *dAdjW = nullptr, *dAdjG = nullptr, *dAdjGrad = nullptr, *dAdjDen = nullptr;  // host-call adjoint staging
+  int adjK = 0;
   std::vector<double> trgHost;  // caller-order targets for check()
   std::string err;
 };
@@ -160,7 +161,8 @@ fmmg_status fmmg_setup(fmmg_handle* h, int64_t ns, const double* src, const doub
       fmmg::dev_free(h->dev);
       h->dDenIO = h->dValIO = nullptr;
       h->dDenK = h->dValK = nullptr;
-      h->dAdjW = h->dAdjG = h->dAdjGrad = nullptr;
+      h->dAdjW = h->dAdjG = h->dAdjGrad = h->dAdjDen = nullptr;
+      h->adjK = 0;
       h->ioK = 0;
       fmmg::Plan fresh;
       fresh.o = h->opt;
@@ -249,50 +251,59 @@ fmmg_status fmmg_evaluate_device(fmmg_handle* h, int k, const double* dDen, doub
   return FMMG_OK;
 }
 
-fmmg_status fmmg_adjoint_device(fmmg_handle* h, const double* dDen, const double* dW, double* dG, double* dGradT) {
+fmmg_status fmmg_adjoint_device(fmmg_handle* h, int k, const double* dDen, const double* dW, double* dG,
+                                double* dGradT) {
   fmmg_status s = ready(h);
   if (s != FMMG_OK) return s;
+  if (k < 1) return fail(h, FMMG_INVALID_ARG, "k must be >= 1");
   if ((!dW && h->plan.nt > 0) || (dGradT && !dDen)) return fail(h, FMMG_INVALID_ARG, "NULL weight or density pointer");
   if (dGradT && h->opt.kt != 111 && h->opt.kt != 121)
     return fail(h, FMMG_NOT_SUPPORTED, "target-position gradient: Laplace kernels 111 and 121 only");
   try {
-    std::string e = fmmg::dev_adjoint(h->plan, h->dev, dDen, dW, dG, dGradT, h->timing);
-    if (!e.empty()) return fail(h, e.find("cudaMalloc") != std::string::npos ? FMMG_OOM : FMMG_CUDA_ERROR, e);
-    h->launches = h->dev.lastLaunches;
+    const int64_t sdn = h->plan.ns * h->plan.sd, tdn = h->plan.nt * h->plan.td, gtn = 3 * h->plan.nt;
+    h->launches = 0;
+    for (int r = 0; r < k; r++) {
+      std::string e = fmmg::dev_adjoint(h->plan, h->dev, dDen ? dDen + r * sdn : nullptr, dW ? dW + r * tdn : nullptr,
+                                        dG ? dG + r * sdn : nullptr, dGradT ? dGradT + r * gtn : nullptr, h->timing);
+      if (!e.empty()) return fail(h, e.find("cudaMalloc") != std::string::npos ? FMMG_OOM : FMMG_CUDA_ERROR, e);
+      h->launches += h->dev.lastLaunches;
+    }
   }
   FMMG_GUARD(h)
   return FMMG_OK;
 }
 
-fmmg_status fmmg_adjoint_host(fmmg_handle* h, const double* den, const double* w, double* g, double* gradT) {
+fmmg_status fmmg_adjoint_host(fmmg_handle* h, int k, const double* den, const double* w, double* g, double* gradT) {
   fmmg_status s = ready(h);
   if (s != FMMG_OK) return s;
+  if (k < 1) return fail(h, FMMG_INVALID_ARG, "k must be >= 1");
   if ((!w && h->plan.nt > 0) || (gradT && !den)) return fail(h, FMMG_INVALID_ARG, "NULL weight or density pointer");
   try {
     const size_t bs = sizeof(double) * (size_t)h->plan.ns * h->plan.sd;
     const size_t bt = sizeof(double) * (size_t)h->plan.nt * h->plan.td;
     const size_t bg = sizeof(double) * 3 * (size_t)h->plan.nt;
-    auto get = [&](double*& p, size_t n) {
-      if (!p) {
+    if (k > h->adjK) {
+      auto get = [&](double*& p, size_t n) {
         void* q = nullptr;
         if (cudaMalloc(&q, std::max<size_t>(n, 8)) != cudaSuccess) return false;
         h->dev.allocs.push_back(q);
         p = (double*)q;
-      }
-      return true;
-    };
-    if (!get(h->dAdjW, bt) || !get(h->dAdjG, bs) || !get(h->dAdjGrad, bg))
-      return fail(h, FMMG_OOM, "cudaMalloc adjoint buffers");
+        return true;
+      };
+      if (!get(h->dAdjW, bt * k) || !get(h->dAdjG, bs * k) || !get(h->dAdjGrad, bg * k) || !get(h->dAdjDen, bs * k))
+        return fail(h, FMMG_OOM, "cudaMalloc adjoint buffers");
+      h->adjK = k;
+    }
     cudaStream_t st = h->dev.stream;
     cudaError_t ce = cudaSuccess;
-    if (bt) ce = cudaMemcpyAsync(h->dAdjW, w, bt, cudaMemcpyHostToDevice, st);
-    if (ce == cudaSuccess && gradT) ce = cudaMemcpyAsync(h->dDenIO, den, bs, cudaMemcpyHostToDevice, st);
+    if (bt) ce = cudaMemcpyAsync(h->dAdjW, w, bt * k, cudaMemcpyHostToDevice, st);
+    if (ce == cudaSuccess && gradT) ce = cudaMemcpyAsync(h->dAdjDen, den, bs * k, cudaMemcpyHostToDevice, st);
     if (ce != cudaSuccess) return fail(h, FMMG_CUDA_ERROR, cudaGetErrorString(ce));
-    s = fmmg_adjoint_device(h, gradT ? h->dDenIO : nullptr, h->dAdjW, g ? h->dAdjG : nullptr,
+    s = fmmg_adjoint_device(h, k, gradT ? h->dAdjDen : nullptr, h->dAdjW, g ? h->dAdjG : nullptr,
                             gradT ? h->dAdjGrad : nullptr);
     if (s != FMMG_OK) return s;
-    if (g) ce = cudaMemcpyAsync(g, h->dAdjG, bs, cudaMemcpyDeviceToHost, st);
-    if (ce == cudaSuccess && gradT && bg) ce = cudaMemcpyAsync(gradT, h->dAdjGrad, bg, cudaMemcpyDeviceToHost, st);
+    if (g) ce = cudaMemcpyAsync(g, h->dAdjG, bs * k, cudaMemcpyDeviceToHost, st);
+    if (ce == cudaSuccess && gradT && bg) ce = cudaMemcpyAsync(gradT, h->dAdjGrad, bg * k, cudaMemcpyDeviceToHost, st);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
     if (ce != cudaSuccess) return fail(h, FMMG_CUDA_ERROR, cudaGetErrorString(ce));
   }

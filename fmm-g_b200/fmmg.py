@@ -66,9 +66,9 @@ SIGNATURES = {
     "fmmg_evaluate_device": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int],
                              ctypes.c_int),
     "fmmg_synchronize": ([ctypes.c_void_p], ctypes.c_int),
-    "fmmg_adjoint_device": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
-                            ctypes.c_int),
-    "fmmg_adjoint_host": ([ctypes.c_void_p, _dp, _dp, _dp, _dp], ctypes.c_int),
+    "fmmg_adjoint_device": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                             ctypes.c_void_p], ctypes.c_int),
+    "fmmg_adjoint_host": ([ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp, _dp], ctypes.c_int),
     "fmmg_evaluate_stages": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int],
                              ctypes.c_int),
     "fmmg_check": ([ctypes.c_void_p, _dp, _dp, ctypes.c_int64, _i64p, _dp, _dp, _dp], ctypes.c_int),
@@ -192,26 +192,30 @@ class FMM3d:
     def sync(self):
         self._chk(lib().fmmg_synchronize(self.h))
 
-    def adjoint(self, w, src_den=None, target_grad=False):
+    def adjoint(self, w, src_den=None, target_grad=False, k=1):
         """Transposed evaluate on host arrays: returns (g, grad_t) with
-        g = A^T w ([n_src, srcDOF]) and, when target_grad, the gradient of
-        <w, A src_den> with respect to the target positions ([n_trg, 3])."""
+        g = A^T w ([n_src, srcDOF], or [k, n_src, srcDOF]) and, when
+        target_grad, the gradient of <w, A src_den> with respect to the target
+        positions ([n_trg, 3], or [k, n_trg, 3])."""
         w = _c(w).ravel()
-        if w.size != self.nt * self.td:
-            raise FmmgError(FMMG_INVALID_ARG, "w has %d values, expected %d" % (w.size, self.nt * self.td))
-        g = np.zeros(self.ns * self.sd)
-        gt = np.zeros(3 * self.nt) if target_grad else None
+        if w.size != k * self.nt * self.td:
+            raise FmmgError(FMMG_INVALID_ARG, "w has %d values, expected %d" % (w.size, k * self.nt * self.td))
+        g = np.zeros(k * self.ns * self.sd)
+        gt = np.zeros(k * 3 * self.nt) if target_grad else None
         den = None if src_den is None else _c(src_den).ravel()
-        self._chk(lib().fmmg_adjoint_host(self.h, None if den is None else _d(den), _d(w), _d(g),
+        self._chk(lib().fmmg_adjoint_host(self.h, k, None if den is None else _d(den), _d(w), _d(g),
                                           None if gt is None else _d(gt)))
-        return g.reshape(self.ns, self.sd), (None if gt is None else gt.reshape(self.nt, 3))
+        shp = (self.ns, self.sd) if k == 1 else (k, self.ns, self.sd)
+        gshp = (self.nt, 3) if k == 1 else (k, self.nt, 3)
+        return g.reshape(shp), (None if gt is None else gt.reshape(gshp))
 
-    def adjoint_device(self, den, w, g=None, grad_t=None):
-        """fmmg_adjoint_device on CUDA tensors (float64, contiguous); g and
-        grad_t are outputs (None skips them); den is needed for grad_t."""
+    def adjoint_device(self, den, w, g=None, grad_t=None, k=1):
+        """fmmg_adjoint_device on CUDA tensors (float64, contiguous) of k
+        right-hand sides; g and grad_t are outputs (None skips them); den is
+        needed for grad_t."""
         self._order_after_torch()
         p = lambda t: None if t is None else ctypes.c_void_p(t.data_ptr())
-        self._chk(lib().fmmg_adjoint_device(self.h, p(den), p(w), p(g), p(grad_t)))
+        self._chk(lib().fmmg_adjoint_device(self.h, k, p(den), p(w), p(g), p(grad_t)))
 
     def check(self, src_den, trg_val, idx):
         """Dense FP64 GPU sums at target indices idx vs trg_val: (rel_l2, max_abs, dense)."""

@@ -118,24 +118,25 @@ fmmg_status fmmg_evaluate_device(fmmg_handle* h, int k, const double* d_src_den,
 
 /* Transposed evaluator (no counterpart in the reference, which has no adjoint).
  * With phi = A(x_t) sigma the map evaluated by fmmg_evaluate_device for the
- * set-up points, and w a weight per target value, it computes on DEVICE
- * buffers in caller order, FP64:
- *   d_g      [n_src*srcDOF] = A^T w, the gradient of <w, phi> with respect to
- *            the source density (the forward stages transposed and run in
+ * set-up points, and w a weight per target value, it computes for each of k
+ * right-hand sides, on DEVICE buffers in caller order, FP64:
+ *   d_g      [k][n_src*srcDOF] = A^T w, the gradient of <w, phi> with respect
+ *            to the source density (the forward stages transposed and run in
  *            reverse order on the same tree and operators); NULL skips it;
- *   d_grad_t [n_trg][3]     = the gradient of <w, phi> with respect to each
+ *   d_grad_t [k][n_trg][3]     = the gradient of <w, phi> with respect to each
  *            target position (sources fixed), from kernel-gradient forms of
  *            the near-field, M2T and L2T sums after a forward upward, V-, X-
  *            and downward pass on d_src_den; NULL skips it.  Laplace kernels
  *            111 and 121 only (FMMG_NOT_SUPPORTED otherwise); needs d_src_den.
- * d_w is [n_trg*trgDOF].  d_src_den may be NULL when d_grad_t is NULL.  Uses
- * the handle's work arrays (not concurrent with evaluate on the same handle);
- * enqueued on the handle's stream, returns without synchronising. */
-fmmg_status fmmg_adjoint_device(fmmg_handle* h, const double* d_src_den, const double* d_w, double* d_g,
+ * d_w is [k][n_trg*trgDOF], d_src_den [k][n_src*srcDOF] (may be NULL when
+ * d_grad_t is NULL).  Uses the handle's work arrays (not concurrent with
+ * evaluate on the same handle); enqueued on the handle's stream, returns
+ * without synchronising.  Forward state is recomputed, never stored. */
+fmmg_status fmmg_adjoint_device(fmmg_handle* h, int k, const double* d_src_den, const double* d_w, double* d_g,
                                 double* d_grad_t);
 
 /* fmmg_adjoint_device on HOST buffers: copies in, runs, copies out, synchronises. */
-fmmg_status fmmg_adjoint_host(fmmg_handle* h, const double* src_den, const double* w, double* g,
+fmmg_status fmmg_adjoint_host(fmmg_handle* h, int k, const double* src_den, const double* w, double* g,
                               double* grad_t);
 
 /* Waits for all work enqueued on the handle's stream. */

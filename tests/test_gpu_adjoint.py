@@ -200,3 +200,16 @@ def test_adjoint_edge_cases():
     with pytest.raises(fmmg.FmmgError) as e:
         f2.adjoint(np.zeros(1500), np.zeros(1500), target_grad=True)
     assert e.value.status == fmmg.FMMG_NOT_SUPPORTED
+
+
+def test_adjoint_k_right_hand_sides():
+    """k right-hand sides in one call equal k single calls (same arithmetic)."""
+    f, src, nrm, trg, rng = _setup(111, 20000, np_=6, pts=64, seed=12, n_trg=3000)
+    k = 3
+    w = rng.normal(size=(k, f.nt))
+    den = rng.normal(size=(k, f.ns))
+    g, gt = f.adjoint(w, den, target_grad=True, k=k)
+    assert g.shape == (k, f.ns, 1) and gt.shape == (k, f.nt, 3)
+    for r in range(k):
+        g1, gt1 = f.adjoint(w[r], den[r], target_grad=True)
+        assert np.array_equal(g[r], g1) and np.array_equal(gt[r], gt1)
