@@ -183,23 +183,32 @@ def measure_peak(torch, kind):
 
 
 def time_form(f, torch, stream, den_dev, out_dev, n, k, prec, steps, warmup, flush):
-    """Device time per step of one evaluate form; per-kernel means; launches."""
+    """Device time per step of one evaluate form, replayed as a CUDA graph
+    (eager first call, captured second call, replays after); then one eager
+    step with per-kernel events for the breakdown (not part of the timing)."""
+    f.set_timing(False)
+    f.set_graph(True)
     for _ in range(max(warmup, 3)):
         f.evaluate_device(den_dev, out_dev, k, prec)
     torch.cuda.synchronize()
+    graph_active, graph_note = f.graph_state()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
-    kern, launches = {}, 0
     for i in range(steps):
         flush.zero_()
         ev[i][0].record(stream)
         f.evaluate_device(den_dev, out_dev, k, prec)
         ev[i][1].record(stream)
-        for name, v in f.kernel_times().items():
-            kern[name] = kern.get(name, 0.0) + v
-        launches += f.launch_count()
     torch.cuda.synchronize()
+    launches = f.launch_count() * steps
     ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
-    return ms, {name: v / steps for name, v in kern.items()}, launches
+    f.set_graph(False)
+    f.set_timing(True)
+    flush.zero_()
+    f.evaluate_device(den_dev, out_dev, k, prec)
+    kern = f.kernel_times()
+    stage = f.stage_times()
+    f.set_timing(False)
+    return ms, kern, stage, launches, {"graph": graph_active, "note": graph_note}
 
 
 def time_adjoint(f, torch, stream, den_dev, out_dev, n, steps, warmup, flush):
@@ -224,7 +233,6 @@ def time_adjoint(f, torch, stream, den_dev, out_dev, n, steps, warmup, flush):
         torch.cuda.synchronize()
         res[key] = float(np.mean([a.elapsed_time(b) for a, b in ev]))
     res["launches"] = f.launch_count()
-    f.set_timing(True)
     return res
 
 
@@ -259,7 +267,6 @@ def run_ours(args):
     den = torch.from_numpy(dens).to("cuda")
     out = torch.zeros(K, n, dtype=torch.float64, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
-    f.set_timing(True)
     idx = np.random.default_rng(W.SEED + 99).choice(n, CHECK_TARGETS, replace=False)
     forms = [("fp64", fmmg.PREC_FP64, 1), ("mixed", fmmg.PREC_MIXED, 1), ("mixed", fmmg.PREC_MIXED, K)]
     if args.precision == "fp64":
@@ -271,14 +278,15 @@ def run_ours(args):
                           os.environ["CUDA_VISIBLE_DEVICES"].split(",")[dev])
     clocks.start()
     for name, prec, k in forms:
-        ms, kern, launches = time_form(f, torch, stream, den, out, n, k, prec, args.steps, args.warmup, flush)
+        ms, kern, stage, launches, graph = time_form(f, torch, stream, den, out, n, k, prec, args.steps, args.warmup,
+                                                     flush)
         if dist:
             ms = FD.max_over_ranks(ms, device="cuda")
         vals = out[0].cpu().numpy()
         rel, mx, _ = f.check(dens[0], vals, idx)
         results.append(dict(precision=name, k=k, ms_per_step=ms, points_per_s=n * k * ws / (ms * 1e-3),
                             rel_err_vs_dense=rel, max_abs_err_vs_dense=mx, kernel_ms=kern,
-                            stage_ms=f.stage_times(), launches=launches))
+                            stage_ms=stage, launches=launches, cuda_graph=graph))
     adj = time_adjoint(f, torch, stream, den, out, n, args.steps, args.warmup, flush)
     if dist:
         adj["ms_per_step"] = FD.max_over_ranks(adj["ms_per_step"], device="cuda")

@@ -33,11 +33,29 @@ struct fmmg_handle {
   int ioK = 0;
   double *dAdjW = nullptr, *dAdjG = nullptr, *dAdjGrad = nullptr, *dAdjDen = nullptr;  // host-call adjoint staging
   int adjK = 0;
+  // CUDA-graph replay of fmmg_evaluate_device (one cached (k, precision, buffers) key)
+  bool graphOn = false;
+  struct GraphKey {
+    int k = -1, precision = -1;
+    const void* den = nullptr;
+    void* val = nullptr;
+    bool operator==(const GraphKey& o) const { return k == o.k && precision == o.precision && den == o.den && val == o.val; }
+  } graphKey, warmKey;
+  cudaGraphExec_t graphExec = nullptr;
+  int64_t graphLaunches = 0;
+  std::string graphNote;
   std::vector<double> trgHost;  // caller-order targets for check()
   std::string err;
 };
 
 static thread_local std::string g_create_err;
+
+static void drop_graph(fmmg_handle* h) {
+  if (h->graphExec) cudaGraphExecDestroy(h->graphExec);
+  h->graphExec = nullptr;
+  h->graphKey = fmmg_handle::GraphKey();
+  h->warmKey = fmmg_handle::GraphKey();
+}
 
 static fmmg_status fail(fmmg_handle* h, fmmg_status s, const std::string& msg) {
   if (h) h->err = msg;
@@ -158,6 +176,7 @@ fmmg_status fmmg_setup(fmmg_handle* h, int64_t ns, const double* src, const doub
       if (!std::isfinite(nrm[i])) return fail(h, FMMG_INVALID_ARG, "a normal is not finite");
   try {
     if (h->setupDone) {
+      drop_graph(h);
       fmmg::dev_free(h->dev);
       h->dDenIO = h->dValIO = nullptr;
       h->dDenK = h->dValK = nullptr;
@@ -224,9 +243,9 @@ fmmg_status fmmg_evaluate_stages(fmmg_handle* h, const double* dDen, double* dVa
   return FMMG_OK;
 }
 
-fmmg_status fmmg_evaluate_device(fmmg_handle* h, int k, const double* dDen, double* dVal, int precision) {
-  fmmg_status s = ready(h);
-  if (s != FMMG_OK) return s;
+static fmmg_status evaluate_eager(fmmg_handle* h, int k, const double* dDen, double* dVal, int precision, bool timed) {
+  fmmg_status s = FMMG_OK;
+  (void)s;
   if (k < 1) return fail(h, FMMG_INVALID_ARG, "k must be >= 1");
   if (!dDen || (!dVal && h->plan.nt > 0)) return fail(h, FMMG_INVALID_ARG, "NULL density or value pointer");
   if (precision != FMMG_PREC_FP64 && precision != FMMG_PREC_MIXED)
@@ -235,19 +254,93 @@ fmmg_status fmmg_evaluate_device(fmmg_handle* h, int k, const double* dDen, doub
     const int64_t sdn = h->plan.ns * h->plan.sd, tdn = h->plan.nt * h->plan.td;
     h->launches = 0;
     if (precision == FMMG_PREC_MIXED) {
-      std::string e = fmmg::dev_evaluate_mixed(h->plan, h->dev, dDen, dVal, k, 63, h->timing, nullptr);
+      std::string e = fmmg::dev_evaluate_mixed(h->plan, h->dev, dDen, dVal, k, 63, timed, nullptr);
       if (!e.empty()) return fail(h, e.find("cudaMalloc") != std::string::npos ? FMMG_OOM : FMMG_CUDA_ERROR, e);
       h->launches = h->dev.lastLaunches;
       return FMMG_OK;
     }
     for (int r = 0; r < k; r++) {
       std::string e = fmmg::dev_evaluate(h->plan, h->dev, dDen + r * sdn, dVal + r * tdn, precision, 63,
-                                         h->timing, nullptr);
+                                         timed, nullptr);
       if (!e.empty()) return fail(h, FMMG_CUDA_ERROR, e);
       h->launches += h->dev.lastLaunches;
     }
   }
   FMMG_GUARD(h)
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_evaluate_device(fmmg_handle* h, int k, const double* dDen, double* dVal, int precision) {
+  fmmg_status s = ready(h);
+  if (s != FMMG_OK) return s;
+  if (k < 1) return fail(h, FMMG_INVALID_ARG, "k must be >= 1");
+  if (!dDen || (!dVal && h->plan.nt > 0)) return fail(h, FMMG_INVALID_ARG, "NULL density or value pointer");
+  if (precision != FMMG_PREC_FP64 && precision != FMMG_PREC_MIXED)
+    return fail(h, FMMG_INVALID_ARG, "unknown precision");
+  if (!h->graphOn || !h->dev.stream) return evaluate_eager(h, k, dDen, dVal, precision, h->timing);
+  fmmg_handle::GraphKey key;
+  key.k = k;
+  key.precision = precision;
+  key.den = dDen;
+  key.val = dVal;
+  cudaStream_t st = h->dev.stream;
+  if (h->graphExec && h->graphKey == key) {  // replay
+    cudaError_t ce = cudaGraphLaunch(h->graphExec, st);
+    if (ce != cudaSuccess) return fail(h, FMMG_CUDA_ERROR, cudaGetErrorString(ce));
+    h->launches = h->graphLaunches;
+    return FMMG_OK;
+  }
+  if (!(h->warmKey == key)) {  // first call with these buffers: eager (allocates what it needs)
+    s = evaluate_eager(h, k, dDen, dVal, precision, false);
+    if (s == FMMG_OK) h->warmKey = key;
+    return s;
+  }
+  // second call: capture the whole evaluate into a graph, then launch it
+  if (h->graphExec) cudaGraphExecDestroy(h->graphExec);
+  h->graphExec = nullptr;
+  cudaError_t ce = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  if (ce != cudaSuccess) {
+    h->graphNote = std::string("capture not started: ") + cudaGetErrorString(ce);
+    return evaluate_eager(h, k, dDen, dVal, precision, false);
+  }
+  s = evaluate_eager(h, k, dDen, dVal, precision, false);
+  cudaGraph_t g = nullptr;
+  cudaError_t ce2 = cudaStreamEndCapture(st, &g);
+  if (s != FMMG_OK || ce2 != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    h->graphNote = std::string("capture failed: ") + (ce2 != cudaSuccess ? cudaGetErrorString(ce2) : h->err);
+    h->graphOn = false;  // stay eager from now on
+    return evaluate_eager(h, k, dDen, dVal, precision, false);
+  }
+  ce = cudaGraphInstantiate(&h->graphExec, g, 0);
+  cudaGraphDestroy(g);
+  if (ce != cudaSuccess) {
+    h->graphExec = nullptr;
+    h->graphNote = std::string("instantiate failed: ") + cudaGetErrorString(ce);
+    h->graphOn = false;
+    return evaluate_eager(h, k, dDen, dVal, precision, false);
+  }
+  h->graphKey = key;
+  h->graphLaunches = h->launches;
+  ce = cudaGraphLaunch(h->graphExec, st);
+  if (ce != cudaSuccess) return fail(h, FMMG_CUDA_ERROR, cudaGetErrorString(ce));
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_set_graph(fmmg_handle* h, int on) {
+  if (!h) return fail(nullptr, FMMG_INVALID_ARG, "handle is NULL");
+  if (h->hostOnly) return fail(h, FMMG_STATE, "host-only handle");
+  drop_graph(h);
+  h->graphOn = on != 0;
+  h->graphNote.clear();
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_graph_state(const fmmg_handle* h, int* active, const char** note) {
+  if (!h) return FMMG_INVALID_ARG;
+  if (active) *active = h->graphExec ? 1 : 0;
+  if (note) *note = h->graphNote.c_str();
   return FMMG_OK;
 }
 
@@ -523,6 +616,7 @@ fmmg_status fmmg_lists(const fmmg_handle* h, int which, int64_t* ptr, int32_t* i
 
 fmmg_status fmmg_operator(fmmg_handle* h, int which, int idx, double* get, const double* set, int64_t* count) {
   if (!h) return FMMG_INVALID_ARG;
+  if (set) drop_graph(h);  // a captured graph holds the FP32 operator copies of the old tables
   fmmg::Plan& P = h->plan;
   const int64_t ue = (int64_t)P.nUE * P.sdm, uc = (int64_t)P.nUC * P.tdm;
   const int64_t de = (int64_t)P.nDE * P.sdm, dc = (int64_t)P.nDC * P.tdm;
@@ -587,6 +681,7 @@ fmmg_status fmmg_destroy(fmmg_handle* h) {
   if (!h->hostOnly) {
     cudaSetDevice(h->dev.device);
     if (h->dev.stream) cudaStreamSynchronize(h->dev.stream);
+    drop_graph(h);
     fmmg::dev_free(h->dev);
     if (h->dev.ownStream && h->dev.stream) cudaStreamDestroy(h->dev.stream);
   }

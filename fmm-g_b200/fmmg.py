@@ -79,6 +79,8 @@ SIGNATURES = {
     "fmmg_launch_count": ([ctypes.c_void_p, _i64p], ctypes.c_int),
     "fmmg_set_precision": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "fmmg_set_timing": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "fmmg_set_graph": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "fmmg_graph_state": ([ctypes.c_void_p, _ip, ctypes.POINTER(ctypes.c_char_p)], ctypes.c_int),
     "fmmg_tree": ([ctypes.c_void_p, _i32p, _i64p, _i64p], ctypes.c_int),
     "fmmg_lists": ([ctypes.c_void_p, ctypes.c_int, _i64p, _i32p, _i64p], ctypes.c_int),
     "fmmg_operator": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp, _i64p], ctypes.c_int),
@@ -293,6 +295,16 @@ class FMM3d:
 
     def set_timing(self, on=True):
         self._chk(lib().fmmg_set_timing(self.h, 1 if on else 0))
+
+    def set_graph(self, on=True):
+        """Replay evaluate_device as a CUDA graph (captured on the second call
+        with the same k, precision and tensors)."""
+        self._chk(lib().fmmg_set_graph(self.h, 1 if on else 0))
+
+    def graph_state(self):
+        act, note = ctypes.c_int(), ctypes.c_char_p()
+        self._chk(lib().fmmg_graph_state(self.h, ctypes.byref(act), ctypes.byref(note)))
+        return bool(act.value), (note.value or b"").decode()
 
     def evaluate_host_k(self, den_ptr, val_ptr, k, precision):
         """fmmg_evaluate_host: k right-hand sides on raw host pointers."""

@@ -188,6 +188,19 @@ fmmg_status fmmg_set_precision(fmmg_handle* h, int precision);
  * handle's stream and waits for them (fmmg_evaluate always does). */
 fmmg_status fmmg_set_timing(fmmg_handle* h, int on);
 
+/* on != 0: fmmg_evaluate_device replays a CUDA graph of the whole evaluate.
+ * The first call for given (k, precision, d_src_den, d_trg_val) runs eagerly
+ * (and allocates what that form needs); the second captures the evaluate on
+ * the handle's stream into a graph, and later calls with the same key launch
+ * it (one key is cached; another key starts over).  The handle's stream must
+ * not be the legacy default stream.  If capture is refused the handle stays
+ * eager and fmmg_graph_state reports why.  Turning it on or off, a new setup
+ * or a changed operator table drops the graph.  No counterpart in the
+ * reference. */
+fmmg_status fmmg_set_graph(fmmg_handle* h, int on);
+/* active: 1 while a captured graph is cached; note: why capture was refused ("" if not). */
+fmmg_status fmmg_graph_state(const fmmg_handle* h, int* active, const char** note);
+
 /* Host-plan introspection (valid after setup, also with device < 0).
  * which: 0 U, 1 V, 2 W, 3 X lists in the reference form.  node_rec receives
  * per node {depth, path x, path y, path z, parent, first child, tag bits,
