@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--precision", default="all", choices=["fp64", "all"])
     ap.add_argument("--k", type=int, default=8, help="right-hand sides of the multi-RHS mixed form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only", default=None, choices=["fp64", "mixed1", "mixedk"],
+                    help="time one form only (profiling runs); the headline then comes from it")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint timing")
     return ap.parse_args()
 
 
@@ -271,6 +274,8 @@ def run_ours(args):
     forms = [("fp64", fmmg.PREC_FP64, 1), ("mixed", fmmg.PREC_MIXED, 1), ("mixed", fmmg.PREC_MIXED, K)]
     if args.precision == "fp64":
         forms = forms[:1]
+    if args.only:
+        forms = [forms[["fp64", "mixed1", "mixedk"].index(args.only)]]
     results = []
     if dist:
         tdist.barrier()
@@ -287,15 +292,17 @@ def run_ours(args):
         results.append(dict(precision=name, k=k, ms_per_step=ms, points_per_s=n * k * ws / (ms * 1e-3),
                             rel_err_vs_dense=rel, max_abs_err_vs_dense=mx, kernel_ms=kern,
                             stage_ms=stage, launches=launches, cuda_graph=graph))
-    adj = time_adjoint(f, torch, stream, den, out, n, args.steps, args.warmup, flush)
-    if dist:
+    adj = {} if args.no_adjoint else time_adjoint(f, torch, stream, den, out, n, args.steps, args.warmup, flush)
+    if dist and adj:
         adj["ms_per_step"] = FD.max_over_ranks(adj["ms_per_step"], device="cuda")
         adj["target_grad_ms_per_step"] = FD.max_over_ranks(adj["target_grad_ms_per_step"], device="cuda")
     clk = clocks.stop()
-    fp64 = results[0]
-    adj["ratio_vs_fp64_forward"] = adj["ms_per_step"] / fp64["ms_per_step"]
+    fp64 = next((r for r in results if r["precision"] == "fp64"), None)
+    fp64_ms = [r["ms_per_step"] for r in results if r["precision"] == "fp64"]
+    if adj and fp64_ms:
+        adj["ratio_vs_fp64_forward"] = adj["ms_per_step"] / fp64_ms[0]
     ok = [r for r in results if r["rel_err_vs_dense"] <= 1e-5]
-    head = max(ok, key=lambda r: r["points_per_s"]) if ok else fp64
+    head = max(ok, key=lambda r: r["points_per_s"]) if ok else (fp64 or results[0])
     prec_h = fmmg.PREC_FP64 if head["precision"] == "fp64" else fmmg.PREC_MIXED
     kh = head["k"]
     # end to end through fmmg_evaluate_host: pinned host densities in, pinned values out
@@ -336,8 +343,8 @@ def run_ours(args):
                     "d2h_bytes_per_step": 8 * n * kh},
             "gpu_launches": head["launches"],
             "rel_err_vs_dense": head["rel_err_vs_dense"], "check_targets": CHECK_TARGETS,
-            "fp64_points_per_s": fp64["points_per_s"],
-            "speedup_vs_fp64": head["points_per_s"] / fp64["points_per_s"],
+            "fp64_points_per_s": fp64["points_per_s"] if fp64 else None,
+            "speedup_vs_fp64": head["points_per_s"] / fp64["points_per_s"] if fp64 else None,
             "forms": results, "adjoint": adj, "setup_s": setup_s, "roofline": roof, "clocks": clk,
         }
         if cpu:
@@ -348,6 +355,16 @@ def run_ours(args):
         tdist.destroy_process_group()
 
 
+# DRAM traffic of the dominant kernels from one ncu capture each (dram__bytes_read.sum +
+# dram__bytes_write.sum) on the 262,144-point case of this workload, with the
+# algorithmic bytes of that launch; a full launch's traffic is scaled by the
+# algorithmic bytes (the units processed).  Summaries under profiles/.
+TRAFFIC = {
+    ("m2l_had", "mixed", 8): {"dram_bytes": 924.900096e6 + 803.798784e6, "algorithmic_bytes": 1679860224,
+                               "profile": "profiles/k_m2l_had_pqx2_laplace_sphere_clusters_262k_np6_k8.md"},
+}
+
+
 def roofline(f, kern, torch, k, precision):
     """Roofline of the dominant kernel class of the headline step."""
     peaks = {}
@@ -356,25 +373,34 @@ def roofline(f, kern, torch, k, precision):
         peaks = json.load(open(pp))
     top = max((name for name in kern if name not in ("prep", "scatter")), key=lambda name: kern[name])
     t = kern[top] * 1e-3
-    w = f.algorithmic_work(k=k, precision=precision).get(top)
+    w = f.algorithmic_work(k=k, precision="fp64" if precision == "fp64" else "fp32").get(top)
     out = {"kernel": top, "avg_ms": kern[top], "k_rhs": k}
     if w is None:
         out.update({"bound": None, "achieved": None, "peak": None, "unit": None, "frac": None, "traffic": None})
         return out
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
     if w["bound"] == "hbm":
-        peak = peaks.get("hbm_gbs", 6650.0)
         ach = w["bytes"] / t / 1e9
-        out.update({"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                    "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650",
-                    "algorithmic_bytes": w["bytes"]})
+        out.update({"bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s", "frac": ach / hbm_peak,
+                    "peak_source": "of measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks
+                    else "of fallback 6650 GB/s", "algorithmic_bytes": w["bytes"]})
     else:
         fp = w["bound"]
         peak = measure_peak(torch, fp)
         ach = w["flops"] / t / 1e12
         out.update({"bound": fp, "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
-                    "peak_source": "measured in bench: cuBLAS %s GEMM 8192^3 best of 3" % fp,
+                    "peak_source": "of measured in bench.py: cuBLAS %s GEMM 8192^3, best of 3 (CUDA cores; "
+                                   "MEASURED_PEAKS.json holds HBM and BF16 only)" % fp,
                     "algorithmic_flops": w["flops"], "pairs": w.get("pairs")})
-    out["traffic"] = None
+        if "bytes" in w:
+            out["hbm"] = {"algorithmic_bytes": w["bytes"], "achieved_gbs": w["bytes"] / t / 1e9,
+                          "peak_gbs": hbm_peak, "frac": w["bytes"] / t / 1e9 / hbm_peak}
+    tr = TRAFFIC.get((top, "fp64" if precision == "fp64" else "mixed", k))
+    if tr and "bytes" in w:
+        out["traffic"] = tr["dram_bytes"] / tr["algorithmic_bytes"] * w["bytes"]
+        out["traffic_source"] = "ncu on the 262,144-point case, scaled by algorithmic bytes; " + tr["profile"]
+    else:
+        out["traffic"] = None
     return out
 
 

@@ -277,7 +277,7 @@ class FMM3d:
             "l2t": {"bound": pipe, "flops": k * s["l2t_pairs"] * fpm, "pairs": s["l2t_pairs"]},
             "up_gemm": {"bound": pipe, "flops": k * s["up_gemm_flops"]},
             "dn_gemm": {"bound": pipe, "flops": k * s["dn_gemm_flops"]},
-            "m2l_had": {"bound": "hbm",
+            "m2l_had": {"bound": pipe,
                         "bytes": cb * ne * (k * s["v_src"] * sdm + k * s["v_trg"] * tdm + 316 * sdm * tdm),
                         "flops": 8 * ne * sdm * tdm * s["v_interactions"] * k},
             "m2l_fwd": {"bound": "hbm", "bytes": k * cb * ne * s["v_src"] * sdm},
