@@ -337,6 +337,22 @@ fmmg_status fmmg_set_graph(fmmg_handle* h, int on) {
   return FMMG_OK;
 }
 
+fmmg_status fmmg_set_gemm_path(fmmg_handle* h, int tensor_cores) {
+  if (!h) return fail(nullptr, FMMG_INVALID_ARG, "handle is NULL");
+  h->dev.gemmTC = tensor_cores != 0;
+  drop_graph(h);
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_device_error(fmmg_handle* h, int* flag) {
+  if (!h || !flag) return fail(h, FMMG_INVALID_ARG, "NULL argument");
+  *flag = 0;
+  if (h->hostOnly || !h->setupDone) return FMMG_OK;
+  std::string e = fmmg::dev_take_error(h->dev, flag);
+  if (!e.empty()) return fail(h, FMMG_CUDA_ERROR, e);
+  return FMMG_OK;
+}
+
 fmmg_status fmmg_graph_state(const fmmg_handle* h, int* active, const char** note) {
   if (!h) return FMMG_INVALID_ARG;
   if (active) *active = h->graphExec ? 1 : 0;

@@ -83,7 +83,9 @@ struct DevState {
   // split-K partial tiles of the FP32 row GEMMs, and the SM count
   double* gemmScratch = nullptr;
   size_t gemmScratchBytes = 0;
-  int numSMs = 148;  // scalar Hadamard: parent-pair register-blocked kernel (else expanded lists)
+  int numSMs = 148;
+  bool gemmTC = false;     // M2M/L2L FP32 row GEMMs on the tensor cores (3xTF32), opt-in
+  int* devErr = nullptr;   // set by kernels whose bounded waits gave up  // scalar Hadamard: parent-pair register-blocked kernel (else expanded lists)
   float adjMs = 0.f;
   // dense check scratch
   double *chkPos = nullptr, *chkOut = nullptr;
@@ -133,6 +135,8 @@ void gather_rows(cudaStream_t st, int64_t n, int dof, const int64_t* perm, const
 void scatter_rows(cudaStream_t st, int64_t n, int dof, const int64_t* perm, const double* in, double* out);
 // forward stages into the handle's work arrays for density dDen (caller order)
 std::string dev_far_field(const Plan& P, DevState& D, const double* dDen);
+// reads and clears the device error flag (synchronises the handle's stream)
+std::string dev_take_error(DevState& D, int* flag);
 // transposed FMM: g = A^T w for one right-hand side (caller order), and with
 // gradT != nullptr the target-position gradient of <w, A sigma> ([nt][3])
 std::string dev_adjoint(const Plan& P, DevState& D, const double* dDen, const double* dW, double* dG,

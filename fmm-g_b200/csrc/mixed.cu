@@ -23,6 +23,7 @@
 #include "cuda_common.cuh"
 #include "engine.hpp"
 #include "gemm_rows.cuh"
+#include "gemm_tc.cuh"
 #include "had_pq.cuh"
 #include "had_smem.cuh"
 #include "kernels.hpp"
@@ -823,8 +824,13 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
   const int nl = (int)P.evtrLeaves.size();
   const int kb = (kc + KB - 1) / KB;
   const int64_t denStride = P.ns * P.sd, valStride = std::max<int64_t>(P.nt, 1) * P.td;
+  // tc: the product may run on the tensor cores (3xTF32) when that path is
+  // enabled.  The factored C2E products always stay on the CUDA cores: the 1/s
+  // factor of the pseudo-inverse amplifies the tensor core's accumulation
+  // rounding past the 1e-5 budget.
   auto gemm = [&](int nrows, const int32_t* rows, int xChild, int yChild, const float* X, int64_t ldx, int64_t xR,
-                  const float* W, float* Y, int64_t ldy, int64_t yR, int K, int N, Scale4 xs, Scale4 ys, float beta) {
+                  const float* W, float* Y, int64_t ldy, int64_t yR, int K, int N, Scale4 xs, Scale4 ys, float beta,
+                  bool tc) {
     if (nrows <= 0) return;
     GrScale<float> gx, gy;
     gx.mod = xs.mod;
@@ -833,9 +839,9 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
       gx.v[k] = (float)xs.v[k];
       gy.v[k] = (float)ys.v[k];
     }
-    ls->launches += launch_gemm_rows<float, 16>(st, D.numSMs, reinterpret_cast<float*>(D.gemmScratch),
-                                                D.gemmScratchBytes / sizeof(float), nrows, kc, rows, D.chd, xChild,
-                                                yChild, X, ldx, xR, W, Y, ldy, yR, K, N, gx, gy, beta);
+    ls->launches += launch_gemm_rows_f32(st, D.numSMs, reinterpret_cast<float*>(D.gemmScratch),
+                                         D.gemmScratchBytes / sizeof(float), D.gemmTC && tc, D.devErr, nrows, kc, rows,
+                                         D.chd, xChild, yChild, X, ldx, xR, W, Y, ldy, yR, K, N, gx, gy, beta);
   };
   if ((mask & 1) && !P.s2mLeaves.empty()) {
     k_src2surf32<KT, KB><<<dim3((unsigned)P.s2mLeaves.size(), kb), MX_SURF, 0, st>>>(
@@ -848,14 +854,14 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
     for (int d = P.maxDepth; d >= 1; d--) {
       int64_t a = D.offUpM2M[d], b = D.offUpM2M[d + 1];
       gemm((int)(b - a), D.levelRows + a, 1, 0, D.uden32, ue, nn * ue, D.m2m32, D.uchk32, uc, nn * uc, 8 * ue, uc,
-           level_scale(P, d + 1 + rl, +1.0), unit_scale(), 0.f);
+           level_scale(P, d + 1 + rl, +1.0), unit_scale(), 0.f, true);
       a = D.offUpC2E[d];
       b = D.offUpC2E[d + 1];
       // C2E as F2 (F1 uchk): the large-norm pinv never multiplies in FP32
       gemm((int)(b - a), D.levelRows + a, 0, 0, D.uchk32, uc, nn * uc, D.upF1, D.upT32, P.kUp, nn * P.kUp, uc,
-           P.kUp, unit_scale(), unit_scale(), 0.f);
+           P.kUp, unit_scale(), unit_scale(), 0.f, false);
       gemm((int)(b - a), D.levelRows + a, 0, 0, D.upT32, P.kUp, nn * P.kUp, D.upF2, D.uden32, ue, nn * ue, P.kUp,
-           ue, unit_scale(), level_scale(P, d + rl, -1.0), 0.f);
+           ue, unit_scale(), level_scale(P, d + rl, -1.0), 0.f, false);
     }
   }
   cudaEventRecord(D.ev[EV_UP_GEMM], st);
@@ -1020,13 +1026,13 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
       if (d >= 3) {
         int64_t a = D.offDnL2L[d - 1], b = D.offDnL2L[d];
         gemm((int)(b - a), D.levelRows + a, 0, 1, D.dden32, de, nn * de, D.l2l32, D.dchk32, dc, nn * dc, de, 8 * dc,
-             level_scale(P, d - 1 + rl, +1.0), unit_scale(), 1.f);
+             level_scale(P, d - 1 + rl, +1.0), unit_scale(), 1.f, true);
       }
       int64_t a = D.offDnC2E[d], b = D.offDnC2E[d + 1];
       gemm((int)(b - a), D.levelRows + a, 0, 0, D.dchk32, dc, nn * dc, D.dnF1, D.dnT32, P.kDn, nn * P.kDn, dc,
-           P.kDn, unit_scale(), unit_scale(), 0.f);
+           P.kDn, unit_scale(), unit_scale(), 0.f, false);
       gemm((int)(b - a), D.levelRows + a, 0, 0, D.dnT32, P.kDn, nn * P.kDn, D.dnF2, D.dden32, de, nn * de, P.kDn,
-           de, unit_scale(), level_scale(P, d + rl, -1.0), 0.f);
+           de, unit_scale(), level_scale(P, d + rl, -1.0), 0.f, false);
     }
   }
   cudaEventRecord(D.ev[EV_DN_GEMM], st);

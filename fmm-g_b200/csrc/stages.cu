@@ -580,6 +580,7 @@ void dev_free(DevState& D) {
   D.vRowOut = D.vNbrIn = D.vRowOutT = D.vNbrInT = nullptr;
   D.gemmScratch = nullptr;
   D.gemmScratchBytes = 0;
+  D.devErr = nullptr;
   D.vNbrTPtr = nullptr;
   D.vNbrOffT = nullptr;
   D.uc2ueT = D.m2mT = D.dc2deT = D.l2lT = D.gradT = nullptr;
@@ -737,6 +738,8 @@ std::string dev_upload(const Plan& P, DevState& D, const double* src, const doub
   D.gemmScratchBytes = (size_t)64 << 20;  // split-K partial tiles of the FP32 row GEMMs
   FMMG_TRY(dput<double>(D, D.gemmScratch, nullptr, D.gemmScratchBytes / sizeof(double)));
   FMMG_CK(cudaDeviceGetAttribute(&D.numSMs, cudaDevAttrMultiProcessorCount, D.device));
+  FMMG_TRY(dput<int>(D, D.devErr, nullptr, 1));
+  FMMG_CK(cudaMemset(D.devErr, 0, sizeof(int)));
   {
     const char* hk = std::getenv("FMMG_HADAMARD");
     D.hadPQ = !(hk && std::strcmp(hk, "list") == 0);
@@ -1036,6 +1039,16 @@ void gather_rows(cudaStream_t st, int64_t n, int dof, const int64_t* perm, const
 }
 void scatter_rows(cudaStream_t st, int64_t n, int dof, const int64_t* perm, const double* in, double* out) {
   if (n > 0) k_scatter_val<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, dof, perm, in, out);
+}
+
+std::string dev_take_error(DevState& D, int* flag) {
+  *flag = 0;
+  if (!D.devErr) return std::string();
+  FMMG_CK(cudaSetDevice(D.device));
+  FMMG_CK(cudaStreamSynchronize(D.stream));
+  FMMG_CK(cudaMemcpy(flag, D.devErr, sizeof(int), cudaMemcpyDeviceToHost));
+  FMMG_CK(cudaMemset(D.devErr, 0, sizeof(int)));
+  return std::string();
 }
 
 std::string dev_far_field(const Plan& P, DevState& D, const double* dDen) {

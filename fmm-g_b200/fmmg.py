@@ -80,6 +80,8 @@ SIGNATURES = {
     "fmmg_set_precision": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "fmmg_set_timing": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "fmmg_set_graph": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "fmmg_set_gemm_path": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "fmmg_device_error": ([ctypes.c_void_p, _ip], ctypes.c_int),
     "fmmg_graph_state": ([ctypes.c_void_p, _ip, ctypes.POINTER(ctypes.c_char_p)], ctypes.c_int),
     "fmmg_tree": ([ctypes.c_void_p, _i32p, _i64p, _i64p], ctypes.c_int),
     "fmmg_lists": ([ctypes.c_void_p, ctypes.c_int, _i64p, _i32p, _i64p], ctypes.c_int),
@@ -300,6 +302,17 @@ class FMM3d:
         """Replay evaluate_device as a CUDA graph (captured on the second call
         with the same k, precision and tensors)."""
         self._chk(lib().fmmg_set_graph(self.h, 1 if on else 0))
+
+    def set_gemm_path(self, tensor_cores=True):
+        """M2M/L2L FP32 row GEMMs on the tensor cores (3xTF32, opt-in) or all on
+        the CUDA cores (default)."""
+        self._chk(lib().fmmg_set_gemm_path(self.h, 1 if tensor_cores else 0))
+
+    def device_error(self):
+        """1 if a kernel gave up a bounded wait since the last call (clears it)."""
+        v = ctypes.c_int()
+        self._chk(lib().fmmg_device_error(self.h, ctypes.byref(v)))
+        return v.value
 
     def graph_state(self):
         act, note = ctypes.c_int(), ctypes.c_char_p()

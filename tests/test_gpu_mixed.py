@@ -101,3 +101,35 @@ def test_mixed_multi_rhs_matches_single_rhs():
     V3 = out3.cpu().numpy()
     for r in (0, 4):
         assert rel_l2(V3[r], _mixed_eval(g, D3[r])) <= 1e-6
+
+
+@pytest.mark.parametrize("k", [1, 8])
+def test_tensor_core_gemms_match_cuda_core_gemms(k):
+    """The FP32 row GEMMs on the tensor cores (3xTF32, tcgen05) against the
+    CUDA-core FP32 GEMMs.  3xTF32 drops the lo*lo term and the tensor core
+    truncates lo, so its products carry a few FP32 roundings (the two paths
+    differ by ~4e-6 at np = 6); both meet the 1e-5 bound against the dense
+    FP64 sum, which is the accuracy gate of the mixed form."""
+    import torch
+    rng = np.random.default_rng(41 + k)
+    n = 60000
+    src = W.sphere_clusters(n, rng)
+    lib = fmmg.FMM3d(111, np_=6, pts_max=64)
+    lib.setup(src)
+    D = rng.normal(size=(k, n))
+    outs = {}
+    for tc in (True, False):
+        lib.set_gemm_path(tc)
+        out = torch.zeros(k, n, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        lib.evaluate_device(torch.from_numpy(D).cuda(), out, k, fmmg.PREC_MIXED)
+        lib.sync()
+        assert lib.device_error() == 0
+        outs[tc] = out.cpu().numpy()
+    assert rel_l2(outs[True], outs[False]) <= 1e-5
+    idx = rng.choice(n, 2000, replace=False)
+    for r in (0, k - 1):
+        for tc in (True, False):
+            rel, _, _ = lib.check(D[r], outs[tc][r], idx)
+            print("k %d rhs %d tensor-cores %s rel err vs dense %.3e" % (k, r, tc, rel))
+            assert rel <= 1e-5
