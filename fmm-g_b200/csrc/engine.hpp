@@ -66,6 +66,8 @@ struct DevState {
   float *upF1 = nullptr, *upF2 = nullptr, *dnF1 = nullptr, *dnF2 = nullptr;  // factored pinvs
   float *upT32 = nullptr, *dnT32 = nullptr;  // [k][nn][kUp|kDn] intermediate of the factored C2E
   float2* m2lT32 = nullptr;
+  float2* m2lTw32 = nullptr;  // combined translations of the 27-product Hadamard [27][27][nEff] (scalar kernels)
+  bool hadW = true;           // FP32 k >= 2 Hadamard in the 27-product form
   double *denK = nullptr, *valK = nullptr;  // permuted densities / values of a RHS chunk
   bool mixedReady = false, mixedOpsStale = true;
   int mixedK = 0;                           // right-hand sides the mixed arrays hold

@@ -182,14 +182,32 @@ __device__ __forceinline__ void pq_fma2(unsigned long long& acc, unsigned long l
   asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(a), "l"(b));
 }
 
+// The translation of this group as the two packed operands (t.x, t.x) and
+// (t.y, t.y): for FW = 4 the CTA stages each translation pre-duplicated as
+// {t.x, t.x, t.y, t.y} (conjugated for ADJ), so one 16-byte shared load gives
+// both; for FW = 32 it stages plain complex values and packs in registers.
+template <bool ADJ, int FW>
+__device__ __forceinline__ void pq_tpair(const void* __restrict__ Ts, int row, int fl, unsigned long long& tx,
+                                         unsigned long long& ty) {
+  if constexpr (FW == 4) {
+    const ulonglong2 t = reinterpret_cast<const ulonglong2*>(Ts)[row * FW + fl];
+    tx = t.x;
+    ty = t.y;
+  } else {
+    const float2 t = reinterpret_cast<const float2*>(Ts)[row * FW + fl];
+    tx = pq_pk(t.x, t.x);
+    ty = ADJ ? pq_pk(-t.y, -t.y) : pq_pk(t.y, t.y);
+  }
+}
+
 template <bool ADJ, int E, int FW>
 __device__ __forceinline__ void pq_delta_x2(unsigned long long (&acc)[8], const unsigned long long (&inD)[8],
-                                            const unsigned long long (&inR)[8], const float2* __restrict__ Ts,
+                                            const unsigned long long (&inR)[8], const void* __restrict__ Ts,
                                             const int16_t* __restrict__ sIdRow, int fl) {
   if constexpr (E < 27) {
     constexpr int ex = E / 9 - 1, ey = (E / 3) % 3 - 1, ez = E % 3 - 1;
-    const float2 t = Ts[sIdRow[E] * FW + fl];
-    const unsigned long long tx = pq_pk(t.x, t.x), ty = ADJ ? pq_pk(-t.y, -t.y) : pq_pk(t.y, t.y);
+    unsigned long long tx, ty;
+    pq_tpair<ADJ, FW>(Ts, sIdRow[E], fl, tx, ty);
 #pragma unroll
     for (int c = 0; c < 8; c++) {
       const int x2 = (c >> 2) + ex, y2 = ((c >> 1) & 1) + ey, z2 = (c & 1) + ez;
@@ -209,9 +227,13 @@ __device__ __forceinline__ void pq_delta_x2(unsigned long long (&acc)[8], const 
 // the 316 translations (10 KB), so residency is set by registers.  Grid (rows
 // / PQX_ROWS, nEff / FW, ceil(nrhs / (32 / FW))); blockIdx.z selects the
 // right-hand-side block of the layout below; dynamic shared memory
-// 317 * FW * sizeof(float2) (row 316 is the zero row of touching pairs).
+// pqx_smem_bytes<FW>() (row 316 is the zero row of touching pairs).
 constexpr int PQX_THREADS = 256;
 constexpr int PQX_ROWS = 64;
+template <int FW>
+inline size_t pqx_smem_bytes() {
+  return (size_t)317 * FW * (FW == 4 ? 16 : 8);
+}
 
 // Spectrum layout: value (right-hand side r, slot s, frequency f) of effIn
 // sits at (r / RW) * in.blk + s * in.slot + f * fStride + (r % RW) * rStride
@@ -228,8 +250,7 @@ __global__ void __launch_bounds__(PQX_THREADS, 3)
                    PqLayout inL, const float2* __restrict__ T, float2* __restrict__ effOut, PqLayout outL,
                    int fStride, int rStride, int nEff, int nrhs, float nrmfc, const int16_t* __restrict__ transId) {
   constexpr int RW = 32 / FW;
-  extern __shared__ unsigned char pqx_smem[];
-  float2* Ts = reinterpret_cast<float2*>(pqx_smem);  // [316][FW]
+  extern __shared__ __align__(16) unsigned char pqx_smem[];
   __shared__ int16_t sId[27 * 27];
   pq_id_table<ADJ>(sId, transId);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -239,9 +260,16 @@ __global__ void __launch_bounds__(PQX_THREADS, 3)
   const int rhs = blockIdx.z * RW + rl;
   for (int i = threadIdx.x; i < 317 * FW; i += blockDim.x) {
     const int id = i / FW, ff = f0 + i % FW;
-    Ts[i] = (ff < nEff && id < 316) ? T[(int64_t)id * nEff + ff] : make_float2(0.f, 0.f);
+    const float2 t = (ff < nEff && id < 316) ? T[(int64_t)id * nEff + ff] : make_float2(0.f, 0.f);
+    if constexpr (FW == 4) {
+      const float ty = ADJ ? -t.y : t.y;
+      reinterpret_cast<float4*>(pqx_smem)[i] = make_float4(t.x, t.x, ty, ty);
+    } else {
+      reinterpret_cast<float2*>(pqx_smem)[i] = t;
+    }
   }
   __syncthreads();
+  const void* Ts = pqx_smem;
   const bool act = f < nEff && rhs < nrhs;
   const int64_t lanePos = act ? (int64_t)f * fStride + (int64_t)rl * rStride : 0;
   const float2* inF = effIn + (act ? blockIdx.z * inL.blk : 0) + lanePos;
@@ -283,6 +311,165 @@ __global__ void __launch_bounds__(PQX_THREADS, 3)
       const int t = rowOut[8 * b + c];
       if (t < 0) continue;
       const float2 a = pq_unpk(acc[c]);
+      outF[(int64_t)t * outL.slot] = make_float2(a.x * nrmfc, a.y * nrmfc);
+    }
+  }
+}
+
+}  // namespace fmmg
+
+namespace fmmg {
+
+// ---------------------------------------------------------------- 27-product form
+// For a neighbour offset o the 8 x 8 child-pair matrix is block-Toeplitz over
+// the 2 x 2 x 2 child grid (entry (c, c2) depends on c2 - c only; touching
+// pairs are zero for the whole (o, c2 - c) class), so per axis
+//   [y0; y1] = [[t0, t1], [t_-1, t0]] [x0; x1]
+// needs the three products m1 = t0 (x0 + x1), m2 = (t1 - t0) x1,
+// m3 = (t_-1 - t0) x0, with y0 = m1 + m2 and y1 = m1 + m3.  Taken over the
+// three axes this is 27 complex products per parent pair instead of 64:
+// combined translations T'[o][j] (j = (jx, jy, jz), each m1/m2/m3) come from
+// the host, the input combinations are sums of child spectra, and the output
+// combination runs once per parent after all neighbours (it is linear).
+//
+// k_m2l_had_w8: FP32, blocks of 8 right-hand sides in the interleaved layout,
+// a warp owns one parent, 4 frequencies and 8 right-hand sides.  The CTA
+// stages T'[27][27][4 frequencies] as {t.x, t.x, -t.y, t.y}, so with u an
+// input combination and s(u) = (u.y, u.x) a complex MAC is
+//   acc = fma2((t.x, t.x), u, acc);  acc = fma2((-t.y, t.y), s(u), acc).
+// Grid (rows / PQX_ROWS, nEff / 4, ceil(nrhs / 8)); dynamic shared memory
+// 27 * 27 * 4 * 16 bytes.
+constexpr int W8_OFFS = 27;  // offset codes 0..26 (13 unused)
+
+__device__ __forceinline__ unsigned long long w8_add(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long w8_swap(unsigned long long a) {
+  const float2 v = pq_unpk(a);
+  return pq_pk(v.y, v.x);
+}
+
+// Sum over the children (bx, by, bz) selected by the y and z combination
+// codes jy, jz (0: both, 1: b = 1, 2: b = 0) for a fixed bx.
+template <int JY, int JZ>
+__device__ __forceinline__ unsigned long long w8_yz(const unsigned long long (&x)[8], int bx) {
+  unsigned long long s = 0ull;
+  bool first = true;
+#pragma unroll
+  for (int by = 0; by < 2; by++)
+#pragma unroll
+    for (int bz = 0; bz < 2; bz++) {
+      if ((JY == 1 && by == 0) || (JY == 2 && by == 1) || (JZ == 1 && bz == 0) || (JZ == 2 && bz == 1)) continue;
+      const unsigned long long v = x[bx * 4 + by * 2 + bz];
+      s = first ? v : w8_add(s, v);
+      first = false;
+    }
+  return s;
+}
+
+template <int J>
+__device__ __forceinline__ void w8_group(unsigned long long (&acc)[27], const unsigned long long (&x)[8],
+                                         const ulonglong2* __restrict__ Tw, int fl) {
+  if constexpr (J < 9) {
+    constexpr int JY = J / 3, JZ = J % 3;
+    const unsigned long long p0 = w8_yz<JY, JZ>(x, 0), p1 = w8_yz<JY, JZ>(x, 1);
+    const unsigned long long q0 = w8_swap(p0), q1 = w8_swap(p1);
+    // jx = m1 (x0 + x1), m2 (x1), m3 (x0); j = jx * 9 + jy * 3 + jz
+    const ulonglong2 t1 = Tw[(0 * 9 + J) * 4 + fl], t2 = Tw[(1 * 9 + J) * 4 + fl], t3 = Tw[(2 * 9 + J) * 4 + fl];
+    const unsigned long long u1 = w8_add(p0, p1), s1 = w8_add(q0, q1);
+    pq_fma2(acc[0 * 9 + J], t1.x, u1);
+    pq_fma2(acc[0 * 9 + J], t1.y, s1);
+    pq_fma2(acc[1 * 9 + J], t2.x, p1);
+    pq_fma2(acc[1 * 9 + J], t2.y, q1);
+    pq_fma2(acc[2 * 9 + J], t3.x, p0);
+    pq_fma2(acc[2 * 9 + J], t3.y, q0);
+    w8_group<J + 1>(acc, x, Tw, fl);
+  }
+}
+
+static __global__ void __launch_bounds__(PQX_THREADS, 2)
+    k_m2l_had_w8(int nRows, const int32_t* __restrict__ rowOut, const int64_t* __restrict__ nPtr,
+                 const int8_t* __restrict__ nOff, const int32_t* __restrict__ nIn, const float2* __restrict__ effIn,
+                 PqLayout inL, const float2* __restrict__ Tw, float2* __restrict__ effOut, PqLayout outL, int nEff,
+                 int nrhs, float nrmfc) {
+  extern __shared__ __align__(16) unsigned char w8_smem[];
+  ulonglong2* Ts = reinterpret_cast<ulonglong2*>(w8_smem);  // [27 offsets][27 combinations][4]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int fl = lane & 3, rl = lane >> 2;
+  const int f0 = blockIdx.y * 4;
+  const int f = f0 + fl;
+  const int rhs = blockIdx.z * 8 + rl;
+  for (int i = threadIdx.x; i < W8_OFFS * 27 * 4; i += blockDim.x) {
+    const int oj = i >> 2, ff = f0 + (i & 3);
+    const float2 t = ff < nEff ? Tw[(int64_t)oj * nEff + ff] : make_float2(0.f, 0.f);
+    reinterpret_cast<float4*>(w8_smem)[i] = make_float4(t.x, t.x, -t.y, t.y);
+  }
+  __syncthreads();
+  const bool act = f < nEff && rhs < nrhs;
+  const int64_t lanePos = act ? (int64_t)f * 8 + rl : 0;
+  const float2* inF = effIn + (act ? blockIdx.z * inL.blk : 0) + lanePos;
+  float2* outF = effOut + blockIdx.z * outL.blk + lanePos;
+  const int bEnd = min(nRows, (int)(blockIdx.x + 1) * PQX_ROWS);
+  for (int b = blockIdx.x * PQX_ROWS + warp; b < bEnd; b += PQX_THREADS / 32) {
+    unsigned long long acc[27];
+#pragma unroll
+    for (int j = 0; j < 27; j++) acc[j] = 0ull;
+    // software pipeline: the spectra of neighbour e + 1 load while neighbour e
+    // multiplies; the child slots run one neighbour further ahead
+    int64_t e = nPtr[b];
+    const int64_t e1 = nPtr[b + 1];
+    float2 raw[8];
+    int offNext = 13;
+    int4 sa = make_int4(-1, -1, -1, -1), sb = sa;
+    if (e < e1) {
+      const int4 a0 = reinterpret_cast<const int4*>(nIn)[2 * e];
+      const int4 b0 = reinterpret_cast<const int4*>(nIn)[2 * e + 1];
+      const int sl[8] = {a0.x, a0.y, a0.z, a0.w, b0.x, b0.y, b0.z, b0.w};
+#pragma unroll
+      for (int c2 = 0; c2 < 8; c2++)
+        raw[c2] = (act && sl[c2] >= 0) ? inF[(int64_t)sl[c2] * inL.slot] : make_float2(0.f, 0.f);
+      offNext = nOff[e];
+      if (e + 1 < e1) {
+        sa = reinterpret_cast<const int4*>(nIn)[2 * (e + 1)];
+        sb = reinterpret_cast<const int4*>(nIn)[2 * (e + 1) + 1];
+      }
+    }
+    for (; e < e1; e++) {
+      unsigned long long x[8];
+#pragma unroll
+      for (int c2 = 0; c2 < 8; c2++) x[c2] = pq_pk(raw[c2].x, raw[c2].y);
+      const int offCur = offNext;
+      if (e + 1 < e1) {
+        const int sl[8] = {sa.x, sa.y, sa.z, sa.w, sb.x, sb.y, sb.z, sb.w};
+#pragma unroll
+        for (int c2 = 0; c2 < 8; c2++)
+          raw[c2] = (act && sl[c2] >= 0) ? inF[(int64_t)sl[c2] * inL.slot] : make_float2(0.f, 0.f);
+        offNext = nOff[e + 1];
+        if (e + 2 < e1) {
+          sa = reinterpret_cast<const int4*>(nIn)[2 * (e + 2)];
+          sb = reinterpret_cast<const int4*>(nIn)[2 * (e + 2) + 1];
+        }
+      }
+      w8_group<0>(acc, x, Ts + offCur * 27 * 4, fl);
+    }
+    if (!act) continue;
+    // output combination: child (cx, cy, cz) sums the products whose codes are
+    // m1 or (m2 for c = 0, m3 for c = 1) on every axis
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      const int t = rowOut[8 * b + c];
+      if (t < 0) continue;
+      const int cx = c >> 2, cy = (c >> 1) & 1, cz = c & 1;
+      unsigned long long s = 0ull;
+#pragma unroll
+      for (int j = 0; j < 27; j++) {
+        const int jx = j / 9, jy = (j / 3) % 3, jz = j % 3;
+        const bool use = (jx == 0 || jx == 1 + cx) && (jy == 0 || jy == 1 + cy) && (jz == 0 || jz == 1 + cz);
+        if (use) s = w8_add(s, acc[j]);
+      }
+      const float2 a = pq_unpk(s);
       outF[(int64_t)t * outL.slot] = make_float2(a.x * nrmfc, a.y * nrmfc);
     }
   }

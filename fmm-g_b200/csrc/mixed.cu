@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <complex>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -775,6 +776,7 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
       FMMG_TRY(dalloc(D, D.dc2de32, P.dc2de.size()));
       FMMG_TRY(dalloc(D, D.l2l32, P.l2l.size()));
       FMMG_TRY(dalloc(D, D.m2lT32, P.m2lT.size()));
+      if (P.sdm == 1 && P.tdm == 1) FMMG_TRY(dalloc(D, D.m2lTw32, (size_t)27 * 27 * P.nEff));
       FMMG_TRY(dalloc(D, D.upF1, P.uc2ueF1.size()));
       FMMG_TRY(dalloc(D, D.upF2, P.uc2ueF2.size()));
       FMMG_TRY(dalloc(D, D.dnF1, P.dc2deF1.size()));
@@ -800,6 +802,37 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
     std::vector<float2> t(P.m2lT.size());
     for (size_t i = 0; i < t.size(); i++) t[i] = make_float2((float)P.m2lT[i].real(), (float)P.m2lT[i].imag());
     FMMG_CK(cudaMemcpy(D.m2lT32, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    if (D.m2lTw32) {  // combined translations of the 27-product Hadamard (had_pq.cuh), FP64 sums
+      auto w = [](int code, int d) -> double {
+        if (code == 0) return d == 0 ? 1.0 : 0.0;
+        if (code == 1) return d == 1 ? 1.0 : (d == 0 ? -1.0 : 0.0);
+        return d == -1 ? 1.0 : (d == 0 ? -1.0 : 0.0);
+      };
+      const int ne = P.nEff;
+      std::vector<float2> tw((size_t)27 * 27 * ne, make_float2(0.f, 0.f));
+      std::vector<std::complex<double>> acc(ne);
+      for (int o = 0; o < 27; o++) {
+        if (o == 13) continue;
+        const int ox = o / 9 - 1, oy = (o / 3) % 3 - 1, oz = o % 3 - 1;
+        for (int j = 0; j < 27; j++) {
+          const int jx = j / 9, jy = (j / 3) % 3, jz = j % 3;
+          std::fill(acc.begin(), acc.end(), std::complex<double>(0.0, 0.0));
+          for (int dx = -1; dx <= 1; dx++)
+            for (int dy = -1; dy <= 1; dy++)
+              for (int dz = -1; dz <= 1; dz++) {
+                const double wt = w(jx, dx) * w(jy, dy) * w(jz, dz);
+                if (wt == 0.0) continue;
+                const int id = P.transId[2 * ox + dx + 3][2 * oy + dy + 3][2 * oz + dz + 3];
+                if (id < 0) continue;  // touching pair
+                const std::complex<double>* Tt = &P.m2lT[(size_t)id * ne];
+                for (int f = 0; f < ne; f++) acc[f] += wt * Tt[f];
+              }
+          float2* dst = &tw[((size_t)o * 27 + j) * ne];
+          for (int f = 0; f < ne; f++) dst[f] = make_float2((float)acc[f].real(), (float)acc[f].imag());
+        }
+      }
+      FMMG_CK(cudaMemcpy(D.m2lTw32, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    }
     int16_t tid[343];
     for (int i = 0; i < 343; i++) tid[i] = (int16_t)P.transId[i / 49][(i / 7) % 7][i % 7];
     FMMG_CK(cudaMemcpyToSymbol(c_transId32, tid, sizeof(tid)));
@@ -932,14 +965,21 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
                                                    P.nEff, kc, nrmfc)
     if (P.sdm == 1 && P.tdm == 1 && D.hadPQ) {
       if (!r8) {  // planes of one right-hand side
-        const size_t smem = pq_smem_bytes<float2>(32);
+        const size_t smem = pqx_smem_bytes<32>();
         cudaFuncSetAttribute(k_m2l_had_pqx2<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         dim3 g1((npar + PQX_ROWS - 1) / PQX_ROWS, (P.nEff + 31) / 32, kc);
         k_m2l_had_pqx2<32, false><<<g1, PQX_THREADS, smem, st>>>(
             npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen32, PqLayout{effDR, P.nEff}, D.m2lT32, D.effVal32,
             PqLayout{effVR, P.nEff}, 1, 0, P.nEff, kc, nrmfc, D.transIdDev);
+      } else if (D.hadW && D.m2lTw32) {  // 27-product form
+        const size_t smem = (size_t)W8_OFFS * 27 * 4 * sizeof(float4);
+        cudaFuncSetAttribute(k_m2l_had_w8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        dim3 g8((npar + PQX_ROWS - 1) / PQX_ROWS, (P.nEff + 3) / 4, nblk);
+        k_m2l_had_w8<<<g8, PQX_THREADS, smem, st>>>(npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen32,
+                                                     PqLayout{blkDen, (int64_t)P.nEff * 8}, D.m2lTw32, D.effVal32,
+                                                     PqLayout{blkVal, (int64_t)P.nEff * 8}, P.nEff, kc, nrmfc);
       } else {
-        const size_t smem = pq_smem_bytes<float2>(4);
+        const size_t smem = pqx_smem_bytes<4>();
         dim3 g8((npar + PQX_ROWS - 1) / PQX_ROWS, (P.nEff + 3) / 4, nblk);
         k_m2l_had_pqx2<4, false><<<g8, PQX_THREADS, smem, st>>>(
             npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen32, PqLayout{blkDen, (int64_t)P.nEff * 8}, D.m2lT32,

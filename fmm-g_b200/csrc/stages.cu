@@ -573,6 +573,7 @@ void dev_free(DevState& D) {
   D.upF1 = D.upF2 = D.dnF1 = D.dnF2 = D.upT32 = D.dnT32 = nullptr;
   D.transIdDev = nullptr;
   D.m2lT32 = nullptr;
+  D.m2lTw32 = nullptr;
   D.denK = D.valK = nullptr;
   D.adjNearRows = D.adjNearIdx = D.adjFarRows = D.adjFarIdx = D.adjS2lRows = D.adjS2lIdx = nullptr;
   D.adjNearPtr = D.adjFarPtr = D.adjS2lPtr = nullptr;
