@@ -334,11 +334,13 @@ namespace fmmg {
 //
 // k_m2l_had_w8: FP32, blocks of 8 right-hand sides in the interleaved layout,
 // a warp owns one parent, 4 frequencies and 8 right-hand sides.  The CTA
-// stages T'[27][27][4 frequencies] as {t.x, t.x, -t.y, t.y}, so with u an
-// input combination and s(u) = (u.y, u.x) a complex MAC is
+// stages T'[27][27][4 frequencies]; with u an input combination and
+// s(u) = (u.y, u.x) a complex MAC is
 //   acc = fma2((t.x, t.x), u, acc);  acc = fma2((-t.y, t.y), s(u), acc).
+// The translations are read as 8-byte values (the kernel is bound by shared-
+// memory wavefronts: 16-byte reads cost 4 per warp, 8-byte ones 2).
 // Grid (rows / PQX_ROWS, nEff / 4, ceil(nrhs / 8)); dynamic shared memory
-// 27 * 27 * 4 * 16 bytes.
+// 27 * 27 * 4 * 8 bytes.
 constexpr int W8_OFFS = 27;  // offset codes 0..26 (13 unused)
 
 __device__ __forceinline__ unsigned long long w8_add(unsigned long long a, unsigned long long b) {
@@ -369,15 +371,23 @@ __device__ __forceinline__ unsigned long long w8_yz(const unsigned long long (&x
   return s;
 }
 
+// one combined translation as the packed operands (t.x, t.x) and (-t.y, t.y),
+// from an 8-byte shared load (served per half-warp: 2 wavefronts)
+__device__ __forceinline__ ulonglong2 w8_t(const float2* __restrict__ Tw, int i) {
+  const float2 t = Tw[i];
+  return make_ulonglong2(pq_pk(t.x, t.x), pq_pk(-t.y, t.y));
+}
+
 template <int J>
 __device__ __forceinline__ void w8_group(unsigned long long (&acc)[27], const unsigned long long (&x)[8],
-                                         const ulonglong2* __restrict__ Tw, int fl) {
+                                         const float2* __restrict__ Tw, int fl) {
   if constexpr (J < 9) {
     constexpr int JY = J / 3, JZ = J % 3;
     const unsigned long long p0 = w8_yz<JY, JZ>(x, 0), p1 = w8_yz<JY, JZ>(x, 1);
     const unsigned long long q0 = w8_swap(p0), q1 = w8_swap(p1);
     // jx = m1 (x0 + x1), m2 (x1), m3 (x0); j = jx * 9 + jy * 3 + jz
-    const ulonglong2 t1 = Tw[(0 * 9 + J) * 4 + fl], t2 = Tw[(1 * 9 + J) * 4 + fl], t3 = Tw[(2 * 9 + J) * 4 + fl];
+    const ulonglong2 t1 = w8_t(Tw, (0 * 9 + J) * 4 + fl), t2 = w8_t(Tw, (1 * 9 + J) * 4 + fl),
+                     t3 = w8_t(Tw, (2 * 9 + J) * 4 + fl);
     const unsigned long long u1 = w8_add(p0, p1), s1 = w8_add(q0, q1);
     pq_fma2(acc[0 * 9 + J], t1.x, u1);
     pq_fma2(acc[0 * 9 + J], t1.y, s1);
@@ -395,7 +405,7 @@ static __global__ void __launch_bounds__(PQX_THREADS, 2)
                  PqLayout inL, const float2* __restrict__ Tw, float2* __restrict__ effOut, PqLayout outL, int nEff,
                  int nrhs, float nrmfc) {
   extern __shared__ __align__(16) unsigned char w8_smem[];
-  ulonglong2* Ts = reinterpret_cast<ulonglong2*>(w8_smem);  // [27 offsets][27 combinations][4]
+  float2* Ts = reinterpret_cast<float2*>(w8_smem);  // [27 offsets][27 combinations][4 frequencies]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int fl = lane & 3, rl = lane >> 2;
   const int f0 = blockIdx.y * 4;
@@ -403,8 +413,7 @@ static __global__ void __launch_bounds__(PQX_THREADS, 2)
   const int rhs = blockIdx.z * 8 + rl;
   for (int i = threadIdx.x; i < W8_OFFS * 27 * 4; i += blockDim.x) {
     const int oj = i >> 2, ff = f0 + (i & 3);
-    const float2 t = ff < nEff ? Tw[(int64_t)oj * nEff + ff] : make_float2(0.f, 0.f);
-    reinterpret_cast<float4*>(w8_smem)[i] = make_float4(t.x, t.x, -t.y, t.y);
+    Ts[i] = ff < nEff ? Tw[(int64_t)oj * nEff + ff] : make_float2(0.f, 0.f);
   }
   __syncthreads();
   const bool act = f < nEff && rhs < nrhs;

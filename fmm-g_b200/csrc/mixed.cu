@@ -972,7 +972,7 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
             npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen32, PqLayout{effDR, P.nEff}, D.m2lT32, D.effVal32,
             PqLayout{effVR, P.nEff}, 1, 0, P.nEff, kc, nrmfc, D.transIdDev);
       } else if (D.hadW && D.m2lTw32) {  // 27-product form
-        const size_t smem = (size_t)W8_OFFS * 27 * 4 * sizeof(float4);
+        const size_t smem = (size_t)W8_OFFS * 27 * 4 * sizeof(float2);
         cudaFuncSetAttribute(k_m2l_had_w8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         dim3 g8((npar + PQX_ROWS - 1) / PQX_ROWS, (P.nEff + 3) / 4, nblk);
         k_m2l_had_w8<<<g8, PQX_THREADS, smem, st>>>(npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen32,
