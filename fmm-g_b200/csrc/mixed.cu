@@ -753,6 +753,21 @@ static std::string dalloc(DevState& D, T*& p, size_t n) {
   return std::string();
 }
 
+static int pad4(int k) { return (k + 3) & ~3; }
+// F1 is k x n row-major: append zero rows up to pad4(k)
+static std::vector<double> pad_rows(const std::vector<double>& F, int k, int n) {
+  std::vector<double> r((size_t)pad4(k) * n, 0.0);
+  std::copy(F.begin(), F.begin() + (size_t)k * n, r.begin());
+  return r;
+}
+// F2 is m x k row-major: widen each row to pad4(k) with zeros
+static std::vector<double> pad_cols(const std::vector<double>& F, int m, int k) {
+  const int kp = pad4(k);
+  std::vector<double> r((size_t)m * kp, 0.0);
+  for (int i = 0; i < m; i++) std::copy(F.begin() + (size_t)i * k, F.begin() + (size_t)(i + 1) * k, r.begin() + (size_t)i * kp);
+  return r;
+}
+
 // Work arrays for a chunk of kc right-hand sides, and the FP32 operator copies.
 static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
   const size_t ue = (size_t)P.nUE * P.sdm, uc = (size_t)P.nUC * P.tdm;
@@ -766,8 +781,8 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
     const size_t kc8 = (size_t)(kc + 7) / 8 * 8;  // the scalar k >= 2 layout stores blocks of 8
     FMMG_TRY(dalloc(D, D.effDen32, kc8 * P.vSrcNodes.size() * P.nEff * P.sdm));
     FMMG_TRY(dalloc(D, D.effVal32, kc8 * P.vTrgNodes.size() * P.nEff * P.tdm));
-    FMMG_TRY(dalloc(D, D.upT32, (size_t)kc * P.nn * std::max(P.kUp, 1)));
-    FMMG_TRY(dalloc(D, D.dnT32, (size_t)kc * P.nn * std::max(P.kDn, 1)));
+    FMMG_TRY(dalloc(D, D.upT32, (size_t)kc * P.nn * std::max(pad4(P.kUp), 4)));
+    FMMG_TRY(dalloc(D, D.dnT32, (size_t)kc * P.nn * std::max(pad4(P.kDn), 4)));
     FMMG_TRY(dalloc(D, D.denK, (size_t)kc * P.ns * P.sd));
     FMMG_TRY(dalloc(D, D.valK, (size_t)kc * std::max<int64_t>(P.nt, 1) * P.td));
     if (!D.uc2ue32) {
@@ -777,10 +792,10 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
       FMMG_TRY(dalloc(D, D.l2l32, P.l2l.size()));
       FMMG_TRY(dalloc(D, D.m2lT32, P.m2lT.size()));
       if (P.sdm == 1 && P.tdm == 1) FMMG_TRY(dalloc(D, D.m2lTw32, (size_t)27 * 27 * P.nEff));
-      FMMG_TRY(dalloc(D, D.upF1, P.uc2ueF1.size()));
-      FMMG_TRY(dalloc(D, D.upF2, P.uc2ueF2.size()));
-      FMMG_TRY(dalloc(D, D.dnF1, P.dc2deF1.size()));
-      FMMG_TRY(dalloc(D, D.dnF2, P.dc2deF2.size()));
+      FMMG_TRY(dalloc(D, D.upF1, (size_t)pad4(P.kUp) * uc));
+      FMMG_TRY(dalloc(D, D.upF2, ue * pad4(P.kUp)));
+      FMMG_TRY(dalloc(D, D.dnF1, (size_t)pad4(P.kDn) * dc));
+      FMMG_TRY(dalloc(D, D.dnF2, de * pad4(P.kDn)));
     }
     D.mixedReady = true;
     D.mixedK = kc;
@@ -795,10 +810,12 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
     FMMG_TRY(put(D.m2m32, P.m2m));
     FMMG_TRY(put(D.dc2de32, P.dc2de));
     FMMG_TRY(put(D.l2l32, P.l2l));
-    FMMG_TRY(put(D.upF1, P.uc2ueF1));
-    FMMG_TRY(put(D.upF2, P.uc2ueF2));
-    FMMG_TRY(put(D.dnF1, P.dc2deF1));
-    FMMG_TRY(put(D.dnF2, P.dc2deF2));
+    // the factors padded to a rank that is a multiple of 4 (zero rows of F1,
+    // zero columns of F2), so the intermediate rows allow 16-byte tile fetches
+    FMMG_TRY(put(D.upF1, pad_rows(P.uc2ueF1, P.kUp, (int)uc)));
+    FMMG_TRY(put(D.upF2, pad_cols(P.uc2ueF2, (int)ue, P.kUp)));
+    FMMG_TRY(put(D.dnF1, pad_rows(P.dc2deF1, P.kDn, (int)dc)));
+    FMMG_TRY(put(D.dnF2, pad_cols(P.dc2deF2, (int)de, P.kDn)));
     std::vector<float2> t(P.m2lT.size());
     for (size_t i = 0; i < t.size(); i++) t[i] = make_float2((float)P.m2lT[i].real(), (float)P.m2lT[i].imag());
     FMMG_CK(cudaMemcpy(D.m2lT32, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice));
@@ -852,6 +869,7 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
   const int64_t ue = (int64_t)P.nUE * P.sdm, uc = (int64_t)P.nUC * P.tdm;
   const int64_t de = (int64_t)P.nDE * P.sdm, dc = (int64_t)P.nDC * P.tdm;
   const int64_t nn = P.nn;
+  const int kUp4 = pad4(P.kUp), kDn4 = pad4(P.kDn);
   const int rl = P.o.rootLevel;
   const float mu = (float)P.o.coefs[0], ve = (float)P.o.coefs[1];
   const int nl = (int)P.evtrLeaves.size();
@@ -891,9 +909,9 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
       a = D.offUpC2E[d];
       b = D.offUpC2E[d + 1];
       // C2E as F2 (F1 uchk): the large-norm pinv never multiplies in FP32
-      gemm((int)(b - a), D.levelRows + a, 0, 0, D.uchk32, uc, nn * uc, D.upF1, D.upT32, P.kUp, nn * P.kUp, uc,
-           P.kUp, unit_scale(), unit_scale(), 0.f, false);
-      gemm((int)(b - a), D.levelRows + a, 0, 0, D.upT32, P.kUp, nn * P.kUp, D.upF2, D.uden32, ue, nn * ue, P.kUp,
+      gemm((int)(b - a), D.levelRows + a, 0, 0, D.uchk32, uc, nn * uc, D.upF1, D.upT32, kUp4, nn * kUp4, uc,
+           kUp4, unit_scale(), unit_scale(), 0.f, false);
+      gemm((int)(b - a), D.levelRows + a, 0, 0, D.upT32, kUp4, nn * kUp4, D.upF2, D.uden32, ue, nn * ue, kUp4,
            ue, unit_scale(), level_scale(P, d + rl, -1.0), 0.f, false);
     }
   }
@@ -1069,9 +1087,9 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
              level_scale(P, d - 1 + rl, +1.0), unit_scale(), 1.f, true);
       }
       int64_t a = D.offDnC2E[d], b = D.offDnC2E[d + 1];
-      gemm((int)(b - a), D.levelRows + a, 0, 0, D.dchk32, dc, nn * dc, D.dnF1, D.dnT32, P.kDn, nn * P.kDn, dc,
-           P.kDn, unit_scale(), unit_scale(), 0.f, false);
-      gemm((int)(b - a), D.levelRows + a, 0, 0, D.dnT32, P.kDn, nn * P.kDn, D.dnF2, D.dden32, de, nn * de, P.kDn,
+      gemm((int)(b - a), D.levelRows + a, 0, 0, D.dchk32, dc, nn * dc, D.dnF1, D.dnT32, kDn4, nn * kDn4, dc,
+           kDn4, unit_scale(), unit_scale(), 0.f, false);
+      gemm((int)(b - a), D.levelRows + a, 0, 0, D.dnT32, kDn4, nn * kDn4, D.dnF2, D.dden32, de, nn * de, kDn4,
            de, unit_scale(), level_scale(P, d + rl, -1.0), 0.f, false);
     }
   }
@@ -1116,7 +1134,7 @@ std::string dev_evaluate_mixed(const Plan& P, DevState& D, const double* dDen, d
   const int64_t de = (int64_t)P.nDE * P.sdm, dc = (int64_t)P.nDC * P.tdm;
   // right-hand sides per pass, bounded by a device-memory budget for the
   // per-density work arrays (node rows and M2L spectra)
-  const double perRhs = 4.0 * P.nn * (ue + uc + de + dc + P.kUp + P.kDn) +
+  const double perRhs = 4.0 * P.nn * (ue + uc + de + dc + pad4(P.kUp) + pad4(P.kDn)) +
                         8.0 * P.nEff * (P.vSrcNodes.size() * P.sdm + P.vTrgNodes.size() * P.tdm) +
                         8.0 * (ns * P.sd + nt * P.td);
   const double budget = D.mixedBudgetBytes;
