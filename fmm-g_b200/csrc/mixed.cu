@@ -543,10 +543,9 @@ constexpr size_t r8_fwd_smem() {
          sizeof(float2) * 2 * NP * NP;
 }
 template <int NP>
-constexpr size_t r8_inv_smem() {
-  return sizeof(float2) * (NP * 2 * NP * (NP + 1) * 8 + NP * NP * (NP + 1) * 8) + sizeof(float2) * 2 * NP * NP;
+constexpr size_t r8_inv_smem() {  // staged input (later reused for Y1) + Y2 + twiddles
+  return sizeof(float2) * (2 * NP * 2 * NP * (NP + 1) * 8 + NP * 2 * NP * (NP + 1) * 8) + sizeof(float2) * 2 * NP * NP;
 }
-
 __device__ __forceinline__ void r8_load(const float2* p, float2 (&v)[8]) {
   const float4* q = reinterpret_cast<const float4*>(p);
 #pragma unroll
@@ -667,20 +666,27 @@ __global__ void __launch_bounds__(256)
     k_m2l_inv32r8(const int32_t* __restrict__ nodes, const float2* __restrict__ effVal, int64_t blkStride, int nEff,
                   const int32_t* __restrict__ ijk, int nDC, float* __restrict__ dchk, int64_t dchkRhs, int kc) {
   using F = FftDims<NP>;
-  constexpr int N = F::N, NH = F::NH, H = F::H;
+  constexpr int N = F::N, NH = F::NH;
+  constexpr int S0 = N * N * NH, S1 = NP * NP * NH, S2 = NP * N * NH;  // planes per right-hand side
   extern __shared__ __align__(16) unsigned char r8_smem[];
-  constexpr int S1 = NP * NP * NH, S2 = NP * N * NH;  // planes per right-hand side
-  float2* Y2 = reinterpret_cast<float2*>(r8_smem);  // [8][NP][N][NH]
-  float2* Y1 = Y2 + S2 * 8;                          // [8][NP][NP][NH]
-  float2* twb = Y1 + S1 * 8;                         // [N][NP]
+  float2* X0 = reinterpret_cast<float2*>(r8_smem);  // [8][N][N][NH]: the node's spectra, staged once
+  float2* Y2 = X0 + S0 * 8;                          // [8][NP][N][NH]
+  float2* twb = Y2 + S2 * 8;                         // [N][NP]
+  float2* Y1 = X0;                                   // [8][NP][NP][NH], reuses the staging space
   const int slot = blockIdx.x;
   const int node = nodes[slot];
   const int r0 = blockIdx.y * 8;
   const int tid = threadIdx.x;
   r8_twiddles<NP>(twb);
+  const float4* in4 = reinterpret_cast<const float4*>(effVal + blockIdx.y * blkStride + (int64_t)slot * nEff * 8);
+  for (int i = tid; i < S0 * 4; i += blockDim.x) {  // coalesced 16-byte reads: 2 right-hand sides of one frequency
+    const float4 v = in4[i];
+    const int f = i >> 2, r = (i & 3) * 2;
+    X0[r * S0 + f] = make_float2(v.x, v.y);
+    X0[(r + 1) * S0 + f] = make_float2(v.z, v.w);
+  }
   __syncthreads();
-  const float2* in = effVal + blockIdx.y * blkStride + (int64_t)slot * nEff * 8;
-  for (int e = tid; e < NP * N * NH; e += blockDim.x) {  // z pass, band outputs only
+  for (int e = tid; e < S2; e += blockDim.x) {  // z pass, band outputs only
     const int kx = e % NH, ky = (e / NH) % N, zb = e / (NH * N);
     float2 s[8];
 #pragma unroll
@@ -688,11 +694,10 @@ __global__ void __launch_bounds__(256)
 #pragma unroll 4
     for (int kz = 0; kz < N; kz++) {
       const float2 w = twb[kz * NP + zb];
-      float2 x[8];
-      r8_load(&in[((int64_t)(kz * N + ky) * NH + kx) * 8], x);
+      const int src = (kz * N + ky) * NH + kx;
 #pragma unroll
       for (int r = 0; r < 8; r++) {
-        const float2 t = cmulc(x[r], w);
+        const float2 t = cmulc(X0[r * S0 + src], w);
         s[r].x += t.x;
         s[r].y += t.y;
       }
@@ -701,7 +706,7 @@ __global__ void __launch_bounds__(256)
     for (int r = 0; r < 8; r++) Y2[r * S2 + e] = s[r];
   }
   __syncthreads();
-  for (int e = tid; e < NP * NP * NH; e += blockDim.x) {  // y pass
+  for (int e = tid; e < S1; e += blockDim.x) {  // y pass
     const int kx = e % NH, yb = (e / NH) % NP, zb = e / (NH * NP);
     float2 s[8];
 #pragma unroll
@@ -739,7 +744,6 @@ __global__ void __launch_bounds__(256)
     for (int r = 0; r < 8; r++)
       if (r0 + r < kc) dchk[(int64_t)(r0 + r) * dchkRhs + (int64_t)node * nDC + i] += s[r];
   }
-  (void)H;
 }
 
 // ------------------------------------------------------------------ launcher

@@ -133,3 +133,25 @@ def test_tensor_core_gemms_match_cuda_core_gemms(k):
             rel, _, _ = lib.check(D[r], outs[tc][r], idx)
             print("k %d rhs %d tensor-cores %s rel err vs dense %.3e" % (k, r, tc, rel))
             assert rel <= 1e-5
+
+
+@pytest.mark.parametrize("np_", [3, 4, 5, 8])
+def test_mixed_rhs_blocks_at_other_np(np_):
+    """The 8-right-hand-side transforms and Hadamard at every grid size they
+    are instantiated for: a block of 3 equals 3 single evaluations to FP32
+    rounding (split-K may sum the GEMMs in another order)."""
+    import torch
+    rng = np.random.default_rng(50 + np_)
+    n = 30000
+    src = W.sphere_clusters(n, rng)
+    lib = fmmg.FMM3d(111, np_=np_, pts_max=64)
+    lib.setup(src)
+    k = 3
+    D = rng.normal(size=(k, n))
+    out = torch.zeros(k, n, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    lib.evaluate_device(torch.from_numpy(D).cuda(), out, k, fmmg.PREC_MIXED)
+    lib.sync()
+    V = out.cpu().numpy()
+    for r in range(k):
+        assert rel_l2(V[r], _mixed_eval(lib, D[r])) <= 1e-6
