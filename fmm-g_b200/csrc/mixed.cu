@@ -529,23 +529,29 @@ __global__ void __launch_bounds__(128)
 }
 
 // Scalar equivalent kernels, blocks of 8 right-hand sides: one CTA per
-// (slot, block) transforms the 8 densities together.  A thread owns one grid
-// point or frequency and all 8 right-hand sides, so each twiddle serves 8
-// complex MACs.  Shared staging arrays are planes [8][...] (a warp's accesses
-// are stride-1, free of bank conflicts); in global memory the spectra are
-// written (and read back by k_m2l_inv32r8) as [block][slot][frequency][8]
-// with 16-byte accesses.  The twiddles of every pass come from one table
+// (slot, block) transforms the 8 densities together.  Each pass is a set of
+// 1-D DFTs along one axis: a thread owns one line of one right-hand side,
+// reads its np (or 2np) inputs from shared memory once and produces all the
+// line's outputs, so shared-memory traffic is one read per input (the kernels
+// are bound by it otherwise).  Shared staging arrays are planes [8][...]
+// padded against bank conflicts; in global memory the spectra are written
+// (and read back by k_m2l_inv32r8) as [block][slot][frequency][8], the
+// forward's last pass ordered right-hand side fastest for contiguous writes.  The twiddles of every pass come from one table
 // twb[k][b] = exp(-2 pi i k (b + np/2) / 2np).  Dynamic shared memory
 // r8_fwd_smem<NP>() / r8_inv_smem<NP>().
+// plane length rounded so that consecutive planes start 8 words apart modulo
+// the 32 shared-memory banks (2-way conflicts at most across right-hand sides)
+constexpr int r8_pad(int s) { return s + ((4 - s % 16) + 16) % 16; }
 template <int NP>
-constexpr size_t r8_fwd_smem() {
-  return sizeof(float) * NP * NP * NP * 8 + sizeof(float2) * (NP * NP * (NP + 1) * 8 + NP * 2 * NP * (NP + 1) * 8) +
-         sizeof(float2) * 2 * NP * NP;
+constexpr size_t r8_fwd_smem() {  // cube + X1 + X2 (padded planes) + twiddles
+  return sizeof(float) * NP * NP * NP * 8 +
+         sizeof(float2) * (8 * r8_pad(NP * NP * (NP + 1)) + 8 * r8_pad(NP * 2 * NP * (NP + 1)) + 2 * NP * NP);
 }
 template <int NP>
 constexpr size_t r8_inv_smem() {  // staged input (later reused for Y1) + Y2 + twiddles
-  return sizeof(float2) * (2 * NP * 2 * NP * (NP + 1) * 8 + NP * 2 * NP * (NP + 1) * 8) + sizeof(float2) * 2 * NP * NP;
+  return sizeof(float2) * (8 * r8_pad(2 * NP * 2 * NP * (NP + 1)) + 8 * r8_pad(NP * 2 * NP * (NP + 1)) + 2 * NP * NP);
 }
+
 __device__ __forceinline__ void r8_load(const float2* p, float2 (&v)[8]) {
   const float4* q = reinterpret_cast<const float4*>(p);
 #pragma unroll
@@ -578,11 +584,11 @@ __global__ void __launch_bounds__(256)
                   float2* __restrict__ effDen, int64_t blkStride, int nEff, int kc) {
   using F = FftDims<NP>;
   constexpr int N = F::N, NH = F::NH;
+  constexpr int S1 = r8_pad(NP * NP * NH), S2 = r8_pad(NP * N * NH), S3 = NP * NP * NP;
   extern __shared__ __align__(16) unsigned char r8_smem[];
-  constexpr int S1 = NP * NP * NH, S2 = NP * N * NH, S3 = NP * NP * NP;  // planes per right-hand side
-  float2* X1 = reinterpret_cast<float2*>(r8_smem);  // [8][NP][NP][NH]
-  float2* X2 = X1 + S1 * 8;                          // [8][NP][N][NH]
-  float2* twb = X2 + S2 * 8;                         // [N][NP]
+  float2* X1 = reinterpret_cast<float2*>(r8_smem);      // [8][NP][NP][NH]
+  float2* X2 = X1 + S1 * 8;                              // [8][NP][N][NH]
+  float2* twb = X2 + S2 * 8;                             // [N][NP]
   float* cube = reinterpret_cast<float*>(twb + N * NP);  // [8][NP][NP][NP]
   const int slot = blockIdx.x;
   const int v = nodes[slot];
@@ -590,7 +596,7 @@ __global__ void __launch_bounds__(256)
   const int tid = threadIdx.x;
   r8_twiddles<NP>(twb);
   const float scl = (float)exp2((double)(depth[v] + rootLevel) * deg);
-  for (int i = tid; i < NP * NP * NP * 8; i += blockDim.x) cube[i] = 0.f;
+  for (int i = tid; i < S3 * 8; i += blockDim.x) cube[i] = 0.f;
   __syncthreads();
   for (int i = tid; i < nUE * 8; i += blockDim.x) {
     const int j = i >> 3, r = i & 7;
@@ -600,64 +606,63 @@ __global__ void __launch_bounds__(256)
         uden[(int64_t)(r0 + r) * udenRhs + (int64_t)v * nUE + j] * scl;
   }
   __syncthreads();
-  for (int e = tid; e < NP * NP * NH; e += blockDim.x) {  // x pass (real -> half spectrum)
-    const int kx = e % NH, yb = (e / NH) % NP, zb = e / (NH * NP);
-    const float* row = &cube[(zb * NP + yb) * NP];
-    float2 s[8];
+  // x pass (real -> half spectrum): a thread owns one x line of one right-hand side
+  for (int i = tid; i < NP * NP * 8; i += blockDim.x) {
+    const int row = i % (NP * NP), r = i / (NP * NP);  // row = zb * NP + yb
+    float c[NP];
 #pragma unroll
-    for (int r = 0; r < 8; r++) s[r] = make_float2(0.f, 0.f);
+    for (int xb = 0; xb < NP; xb++) c[xb] = cube[r * S3 + row * NP + xb];
+#pragma unroll 1
+    for (int kx = 0; kx < NH; kx++) {  // rolled: twiddles stay in shared memory (warp-wide broadcast)
+      float2 s = make_float2(0.f, 0.f);
 #pragma unroll
-    for (int xb = 0; xb < NP; xb++) {
-      const float2 w = twb[kx * NP + xb];
-#pragma unroll
-      for (int r = 0; r < 8; r++) {
-        const float c = row[r * S3 + xb];
-        s[r].x += c * w.x;
-        s[r].y += c * w.y;
+      for (int xb = 0; xb < NP; xb++) {
+        const float2 w = twb[kx * NP + xb];
+        s.x += c[xb] * w.x;
+        s.y += c[xb] * w.y;
       }
+      X1[r * S1 + row * NH + kx] = s;
     }
-#pragma unroll
-    for (int r = 0; r < 8; r++) X1[r * S1 + e] = s[r];
   }
   __syncthreads();
-  for (int e = tid; e < NP * N * NH; e += blockDim.x) {  // y pass
-    const int kx = e % NH, ky = (e / NH) % N, zb = e / (NH * N);
-    float2 s[8];
+  // y pass: a thread owns one y line (kx, zb) of one right-hand side and all N ky outputs
+  for (int i = tid; i < NH * NP * 8; i += blockDim.x) {
+    const int kx = i % NH, zb = (i / NH) % NP, r = i / (NH * NP);
+    float2 c[NP];
 #pragma unroll
-    for (int r = 0; r < 8; r++) s[r] = make_float2(0.f, 0.f);
+    for (int yb = 0; yb < NP; yb++) c[yb] = X1[r * S1 + (zb * NP + yb) * NH + kx];
+#pragma unroll 1
+    for (int ky = 0; ky < N; ky++) {
+      float2 s = make_float2(0.f, 0.f);
 #pragma unroll
-    for (int yb = 0; yb < NP; yb++) {
-      const float2 w = twb[ky * NP + yb];
-      const int src = (zb * NP + yb) * NH + kx;
-#pragma unroll
-      for (int r = 0; r < 8; r++) {
-        const float2 t = cmul(X1[r * S1 + src], w);
-        s[r].x += t.x;
-        s[r].y += t.y;
+      for (int yb = 0; yb < NP; yb++) {
+        const float2 t = cmul(c[yb], twb[ky * NP + yb]);
+        s.x += t.x;
+        s.y += t.y;
       }
+      X2[r * S2 + (zb * N + ky) * NH + kx] = s;
     }
-#pragma unroll
-    for (int r = 0; r < 8; r++) X2[r * S2 + e] = s[r];
   }
   __syncthreads();
+  // z pass: a thread owns one z line (kx, ky) of one right-hand side and all N kz
+  // outputs; right-hand side fastest so the global writes are contiguous
   float2* out = effDen + blockIdx.y * blkStride + (int64_t)slot * nEff * 8;
-  for (int e = tid; e < N * N * NH; e += blockDim.x) {  // z pass
-    const int kx = e % NH, ky = (e / NH) % N, kz = e / (NH * N);
-    float2 s[8];
+  for (int i = tid; i < NH * N * 8; i += blockDim.x) {
+    const int r = i & 7, kx = (i >> 3) % NH, ky = (i >> 3) / NH;
+    float2 c[NP];
 #pragma unroll
-    for (int r = 0; r < 8; r++) s[r] = make_float2(0.f, 0.f);
+    for (int zb = 0; zb < NP; zb++) c[zb] = X2[r * S2 + (zb * N + ky) * NH + kx];
+#pragma unroll 1
+    for (int kz = 0; kz < N; kz++) {
+      float2 s = make_float2(0.f, 0.f);
 #pragma unroll
-    for (int zb = 0; zb < NP; zb++) {
-      const float2 w = twb[kz * NP + zb];
-      const int src = (zb * N + ky) * NH + kx;
-#pragma unroll
-      for (int r = 0; r < 8; r++) {
-        const float2 t = cmul(X2[r * S2 + src], w);
-        s[r].x += t.x;
-        s[r].y += t.y;
+      for (int zb = 0; zb < NP; zb++) {
+        const float2 t = cmul(c[zb], twb[kz * NP + zb]);
+        s.x += t.x;
+        s.y += t.y;
       }
+      out[((int64_t)(kz * N + ky) * NH + kx) * 8 + r] = s;
     }
-    r8_store(&out[(int64_t)e * 8], s);
   }
 }
 
@@ -667,7 +672,7 @@ __global__ void __launch_bounds__(256)
                   const int32_t* __restrict__ ijk, int nDC, float* __restrict__ dchk, int64_t dchkRhs, int kc) {
   using F = FftDims<NP>;
   constexpr int N = F::N, NH = F::NH;
-  constexpr int S0 = N * N * NH, S1 = NP * NP * NH, S2 = NP * N * NH;  // planes per right-hand side
+  constexpr int S0 = r8_pad(N * N * NH), S1 = r8_pad(NP * NP * NH), S2 = r8_pad(NP * N * NH);
   extern __shared__ __align__(16) unsigned char r8_smem[];
   float2* X0 = reinterpret_cast<float2*>(r8_smem);  // [8][N][N][NH]: the node's spectra, staged once
   float2* Y2 = X0 + S0 * 8;                          // [8][NP][N][NH]
@@ -679,70 +684,66 @@ __global__ void __launch_bounds__(256)
   const int tid = threadIdx.x;
   r8_twiddles<NP>(twb);
   const float4* in4 = reinterpret_cast<const float4*>(effVal + blockIdx.y * blkStride + (int64_t)slot * nEff * 8);
-  for (int i = tid; i < S0 * 4; i += blockDim.x) {  // coalesced 16-byte reads: 2 right-hand sides of one frequency
+  for (int i = tid; i < N * N * NH * 4; i += blockDim.x) {  // coalesced 16-byte reads: 2 right-hand sides
     const float4 v = in4[i];
     const int f = i >> 2, r = (i & 3) * 2;
     X0[r * S0 + f] = make_float2(v.x, v.y);
     X0[(r + 1) * S0 + f] = make_float2(v.z, v.w);
   }
   __syncthreads();
-  for (int e = tid; e < S2; e += blockDim.x) {  // z pass, band outputs only
-    const int kx = e % NH, ky = (e / NH) % N, zb = e / (NH * N);
-    float2 s[8];
+  // z pass, band outputs only: a thread owns one z line (kx, ky) of one right-hand side
+  for (int i = tid; i < NH * N * 8; i += blockDim.x) {
+    const int kx = i % NH, ky = (i / NH) % N, r = i / (NH * N);
+    float2 s[NP];
 #pragma unroll
-    for (int r = 0; r < 8; r++) s[r] = make_float2(0.f, 0.f);
-#pragma unroll 4
+    for (int zb = 0; zb < NP; zb++) s[zb] = make_float2(0.f, 0.f);
+#pragma unroll 1
     for (int kz = 0; kz < N; kz++) {
-      const float2 w = twb[kz * NP + zb];
-      const int src = (kz * N + ky) * NH + kx;
+      const float2 c = X0[r * S0 + (kz * N + ky) * NH + kx];
 #pragma unroll
-      for (int r = 0; r < 8; r++) {
-        const float2 t = cmulc(X0[r * S0 + src], w);
-        s[r].x += t.x;
-        s[r].y += t.y;
+      for (int zb = 0; zb < NP; zb++) {
+        const float2 t = cmulc(c, twb[kz * NP + zb]);
+        s[zb].x += t.x;
+        s[zb].y += t.y;
       }
     }
 #pragma unroll
-    for (int r = 0; r < 8; r++) Y2[r * S2 + e] = s[r];
+    for (int zb = 0; zb < NP; zb++) Y2[r * S2 + (zb * N + ky) * NH + kx] = s[zb];
   }
   __syncthreads();
-  for (int e = tid; e < S1; e += blockDim.x) {  // y pass
-    const int kx = e % NH, yb = (e / NH) % NP, zb = e / (NH * NP);
-    float2 s[8];
+  // y pass: a thread owns one y line (kx, zb) of one right-hand side
+  for (int i = tid; i < NH * NP * 8; i += blockDim.x) {
+    const int kx = i % NH, zb = (i / NH) % NP, r = i / (NH * NP);
+    float2 s[NP];
 #pragma unroll
-    for (int r = 0; r < 8; r++) s[r] = make_float2(0.f, 0.f);
-#pragma unroll
+    for (int yb = 0; yb < NP; yb++) s[yb] = make_float2(0.f, 0.f);
+#pragma unroll 1
     for (int ky = 0; ky < N; ky++) {
-      const float2 w = twb[ky * NP + yb];
-      const int src = (zb * N + ky) * NH + kx;
+      const float2 c = Y2[r * S2 + (zb * N + ky) * NH + kx];
 #pragma unroll
-      for (int r = 0; r < 8; r++) {
-        const float2 t = cmulc(Y2[r * S2 + src], w);
-        s[r].x += t.x;
-        s[r].y += t.y;
+      for (int yb = 0; yb < NP; yb++) {
+        const float2 t = cmulc(c, twb[ky * NP + yb]);
+        s[yb].x += t.x;
+        s[yb].y += t.y;
       }
     }
 #pragma unroll
-    for (int r = 0; r < 8; r++) Y1[r * S1 + e] = s[r];
+    for (int yb = 0; yb < NP; yb++) Y1[r * S1 + (zb * NP + yb) * NH + kx] = s[yb];
   }
   __syncthreads();
-  for (int i = tid; i < nDC; i += blockDim.x) {  // x pass (c2r) at the surface points
-    const int p = ijk[i];
+  for (int i = tid; i < nDC * 8; i += blockDim.x) {  // x pass (c2r) at the surface points
+    const int j = i % nDC, r = i / nDC;
+    if (r0 + r >= kc) continue;
+    const int p = ijk[j];
     const int a = p & 255, b = (p >> 8) & 255, cc = p >> 16;
-    const float2* y1 = &Y1[(cc * NP + b) * NH];
-    float s[8];
-#pragma unroll
-    for (int r = 0; r < 8; r++) s[r] = 0.f;
+    const float2* y1 = &Y1[r * S1 + (cc * NP + b) * NH];
+    float s = 0.f;
 #pragma unroll
     for (int kx = 0; kx < NH; kx++) {
       const float2 w = twb[kx * NP + a];
-      const float f = (kx == 0 || kx == N / 2) ? 1.f : 2.f;
-#pragma unroll
-      for (int r = 0; r < 8; r++) s[r] += f * cmulc(y1[r * S1 + kx], w).x;
+      s += ((kx == 0 || kx == N / 2) ? 1.f : 2.f) * cmulc(y1[kx], w).x;
     }
-#pragma unroll
-    for (int r = 0; r < 8; r++)
-      if (r0 + r < kc) dchk[(int64_t)(r0 + r) * dchkRhs + (int64_t)node * nDC + i] += s[r];
+    dchk[(int64_t)(r0 + r) * dchkRhs + (int64_t)node * nDC + j] += s;
   }
 }
 
