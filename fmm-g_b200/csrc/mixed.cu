@@ -549,7 +549,7 @@ constexpr size_t r8_fwd_smem() {  // cube + X1 + X2 (padded planes) + twiddles
 }
 template <int NP>
 constexpr size_t r8_inv_smem() {  // staged input (later reused for Y1) + Y2 + twiddles
-  return sizeof(float2) * (8 * r8_pad(2 * NP * 2 * NP * (NP + 1)) + 8 * r8_pad(NP * 2 * NP * (NP + 1)) + 2 * NP * NP);
+  return sizeof(float2) * (8 * (2 * NP * 2 * NP * (NP + 1)) + 8 * r8_pad(NP * 2 * NP * (NP + 1)) + 2 * NP * NP);
 }
 
 __device__ __forceinline__ void r8_load(const float2* p, float2 (&v)[8]) {
@@ -666,40 +666,80 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// The node's spectra block (contiguous in global memory: [frequency][8]) is
+// brought into shared memory by the bulk-copy (TMA) engine in one
+// cp.async.bulk completed on an mbarrier; the wait is bounded and, if it gives
+// up, sets *errFlag and still waits (bounded) before the CTA exits.
+constexpr long long R8_WAIT_LIMIT = 1ll << 24;
+
+__device__ __forceinline__ bool r8_bar_wait(uint32_t bar, uint32_t parity) {
+  for (long long i = 0; i < R8_WAIT_LIMIT; i++) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 template <int NP>
 __global__ void __launch_bounds__(256)
     k_m2l_inv32r8(const int32_t* __restrict__ nodes, const float2* __restrict__ effVal, int64_t blkStride, int nEff,
-                  const int32_t* __restrict__ ijk, int nDC, float* __restrict__ dchk, int64_t dchkRhs, int kc) {
+                  const int32_t* __restrict__ ijk, int nDC, float* __restrict__ dchk, int64_t dchkRhs, int kc,
+                  int* __restrict__ errFlag) {
   using F = FftDims<NP>;
   constexpr int N = F::N, NH = F::NH;
-  constexpr int S0 = r8_pad(N * N * NH), S1 = r8_pad(NP * NP * NH), S2 = r8_pad(NP * N * NH);
+  constexpr int NF = N * N * NH;  // frequencies
+  constexpr int S1 = r8_pad(NP * NP * NH), S2 = r8_pad(NP * N * NH);
   extern __shared__ __align__(16) unsigned char r8_smem[];
-  float2* X0 = reinterpret_cast<float2*>(r8_smem);  // [8][N][N][NH]: the node's spectra, staged once
-  float2* Y2 = X0 + S0 * 8;                          // [8][NP][N][NH]
+  float2* X0 = reinterpret_cast<float2*>(r8_smem);  // [N][N][NH][8]: the node's spectra, interleaved as in HBM
+  float2* Y2 = X0 + NF * 8;                          // [8][NP][N][NH]
   float2* twb = Y2 + S2 * 8;                         // [N][NP]
   float2* Y1 = X0;                                   // [8][NP][NP][NH], reuses the staging space
+  __shared__ __align__(8) uint64_t bar;
   const int slot = blockIdx.x;
   const int node = nodes[slot];
   const int r0 = blockIdx.y * 8;
   const int tid = threadIdx.x;
-  r8_twiddles<NP>(twb);
-  const float4* in4 = reinterpret_cast<const float4*>(effVal + blockIdx.y * blkStride + (int64_t)slot * nEff * 8);
-  for (int i = tid; i < N * N * NH * 4; i += blockDim.x) {  // coalesced 16-byte reads: 2 right-hand sides
-    const float4 v = in4[i];
-    const int f = i >> 2, r = (i & 3) * 2;
-    X0[r * S0 + f] = make_float2(v.x, v.y);
-    X0[(r + 1) * S0 + f] = make_float2(v.z, v.w);
+  const uint32_t barA = (uint32_t)__cvta_generic_to_shared(&bar);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(barA), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  // z pass, band outputs only: a thread owns one z line (kx, ky) of one right-hand side
+  if (tid == 0) {
+    const uint32_t bytes = (uint32_t)(NF * 8 * sizeof(float2));
+    const float2* src = effVal + blockIdx.y * blkStride + (int64_t)slot * nEff * 8;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(barA), "r"(bytes) : "memory");
+    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(X0);
+    for (uint32_t off = 0; off < bytes; off += 32768u) {  // pieces of at most 32 KB, multiples of 16 bytes
+      const uint32_t piece = bytes - off < 32768u ? bytes - off : 32768u;
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst + off),
+          "l"(reinterpret_cast<const char*>(src) + off), "r"(piece), "r"(barA)
+          : "memory");
+    }
+  }
+  r8_twiddles<NP>(twb);
+  if (!r8_bar_wait(barA, 0)) {
+    if (tid == 0) atomicExch(errFlag, 1);
+    r8_bar_wait(barA, 0);
+  }
+  __syncthreads();
+  // z pass, band outputs only: a thread owns one z line (kx, ky) of one
+  // right-hand side; right-hand side fastest, matching the staged layout
   for (int i = tid; i < NH * N * 8; i += blockDim.x) {
-    const int kx = i % NH, ky = (i / NH) % N, r = i / (NH * N);
+    const int r = i & 7, kx = (i >> 3) % NH, ky = (i >> 3) / NH;
     float2 s[NP];
 #pragma unroll
     for (int zb = 0; zb < NP; zb++) s[zb] = make_float2(0.f, 0.f);
 #pragma unroll 1
     for (int kz = 0; kz < N; kz++) {
-      const float2 c = X0[r * S0 + (kz * N + ky) * NH + kx];
+      const float2 c = X0[((kz * N + ky) * NH + kx) * 8 + r];
 #pragma unroll
       for (int zb = 0; zb < NP; zb++) {
         const float2 t = cmulc(c, twb[kz * NP + zb]);
@@ -1028,7 +1068,7 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
     constexpr size_t sm = r8_inv_smem<NP_>();                                                                  \
     cudaFuncSetAttribute(k_m2l_inv32r8<NP_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);            \
     k_m2l_inv32r8<NP_><<<dim3(ntrg, nblk), 256, sm, st>>>(D.vTrgNodes, D.effVal32, blkVal, P.nEff, D.surfIJK,  \
-                                                          P.nDC, D.dchk32, nn * dc, kc);                       \
+                                                          P.nDC, D.dchk32, nn * dc, kc, D.devErr);             \
   } while (0)
     switch (P.o.np) {
       case 3: FMMG_INV32R8(3); break;
