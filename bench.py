@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--only", default=None, choices=["fp64", "mixed1", "mixedk"],
                     help="time one form only (profiling runs); the headline then comes from it")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint timing")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     return ap.parse_args()
 
 
@@ -283,6 +284,9 @@ def run_ours(args):
                           os.environ["CUDA_VISIBLE_DEVICES"].split(",")[dev])
     clocks.start()
     for name, prec, k in forms:
+        tuned = None
+        if not args.no_autotune:  # launch shapes for this (kernel, np, k, precision), timed on this GPU
+            _, tuned = f.autotune(den, out, k, prec, reps=2)
         ms, kern, stage, launches, graph = time_form(f, torch, stream, den, out, n, k, prec, args.steps, args.warmup,
                                                      flush)
         if dist:
@@ -291,7 +295,7 @@ def run_ours(args):
         rel, mx, _ = f.check(dens[0], vals, idx)
         results.append(dict(precision=name, k=k, ms_per_step=ms, points_per_s=n * k * ws / (ms * 1e-3),
                             rel_err_vs_dense=rel, max_abs_err_vs_dense=mx, kernel_ms=kern,
-                            stage_ms=stage, launches=launches, cuda_graph=graph))
+                            stage_ms=stage, launches=launches, cuda_graph=graph, tuning=tuned))
     adj = {} if args.no_adjoint else time_adjoint(f, torch, stream, den, out, n, args.steps, args.warmup, flush)
     if dist and adj:
         adj["ms_per_step"] = FD.max_over_ranks(adj["ms_per_step"], device="cuda")

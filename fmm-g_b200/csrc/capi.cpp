@@ -353,6 +353,95 @@ fmmg_status fmmg_device_error(fmmg_handle* h, int* flag) {
   return FMMG_OK;
 }
 
+// Autotuner: times real evaluates of (k, precision) on the caller's buffers
+// with CUDA events for each candidate launch shape and keeps the fastest.
+// Coordinate search: Hadamard rows per CTA first, then the split-K threshold
+// of the FP32 GEMMs (mixed form) -- 8 candidates, reps evaluates each.
+fmmg_status fmmg_autotune(fmmg_handle* h, int k, int precision, const double* dDen, double* dVal, int reps,
+                          double* bestMs) {
+  fmmg_status s = ready(h);
+  if (s != FMMG_OK) return s;
+  if (k < 1 || reps < 1 || !dDen || (!dVal && h->plan.nt > 0)) return fail(h, FMMG_INVALID_ARG, "bad autotune arguments");
+  if (precision != FMMG_PREC_FP64 && precision != FMMG_PREC_MIXED) return fail(h, FMMG_INVALID_ARG, "precision");
+  try {
+    cudaStream_t st = h->dev.stream;
+    const bool wasGraph = h->graphOn;
+    h->graphOn = false;
+    drop_graph(h);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    auto timeIt = [&](float& ms) -> fmmg_status {
+      fmmg_status r = evaluate_eager(h, k, dDen, dVal, precision, false);  // warm (allocations, caches)
+      if (r != FMMG_OK) return r;
+      cudaEventRecord(e0, st);
+      for (int i = 0; i < reps; i++) {
+        r = evaluate_eager(h, k, dDen, dVal, precision, false);
+        if (r != FMMG_OK) return r;
+      }
+      cudaEventRecord(e1, st);
+      cudaError_t ce = cudaEventSynchronize(e1);
+      if (ce != cudaSuccess) return fail(h, FMMG_CUDA_ERROR, cudaGetErrorString(ce));
+      cudaEventElapsedTime(&ms, e0, e1);
+      ms /= reps;
+      return FMMG_OK;
+    };
+    fmmg::DevState::Tune& T = h->dev.tune;
+    float best = 1e30f, ms = 0.f;
+    const bool mixed = precision == FMMG_PREC_MIXED;
+    int* rowsKnob = mixed ? &T.hadRows : &T.pqParents;
+    const int rowsCand[4] = {32, 64, 128, 256};
+    int bestRows = *rowsKnob;
+    for (int c : rowsCand) {
+      *rowsKnob = c;
+      if ((s = timeIt(ms)) != FMMG_OK) break;
+      if (ms < best) {
+        best = ms;
+        bestRows = c;
+      }
+    }
+    *rowsKnob = bestRows;
+    if (s == FMMG_OK && mixed) {
+      const int splitCand[4] = {0, 1, 2, 4};
+      int bestSplit = T.gemmSplitMul;
+      best = 1e30f;
+      for (int c : splitCand) {
+        T.gemmSplitMul = c;
+        if ((s = timeIt(ms)) != FMMG_OK) break;
+        if (ms < best) {
+          best = ms;
+          bestSplit = c;
+        }
+      }
+      T.gemmSplitMul = bestSplit;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    h->graphOn = wasGraph;
+    if (s != FMMG_OK) return s;
+    if (bestMs) *bestMs = best;
+  }
+  FMMG_GUARD(h)
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_tuning(fmmg_handle* h, int* vals, int n, int set) {
+  if (!h || !vals || n < 3) return fail(h, FMMG_INVALID_ARG, "need 3 values");
+  fmmg::DevState::Tune& T = h->dev.tune;
+  if (set) {
+    if (vals[0] < 1 || vals[1] < 1 || vals[2] < 0) return fail(h, FMMG_INVALID_ARG, "tuning values");
+    T.hadRows = vals[0];
+    T.pqParents = vals[1];
+    T.gemmSplitMul = vals[2];
+    drop_graph(h);
+  } else {
+    vals[0] = T.hadRows;
+    vals[1] = T.pqParents;
+    vals[2] = T.gemmSplitMul;
+  }
+  return FMMG_OK;
+}
+
 fmmg_status fmmg_graph_state(const fmmg_handle* h, int* active, const char** note) {
   if (!h) return FMMG_INVALID_ARG;
   if (active) *active = h->graphExec ? 1 : 0;

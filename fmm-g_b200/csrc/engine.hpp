@@ -86,6 +86,12 @@ struct DevState {
   double* gemmScratch = nullptr;
   size_t gemmScratchBytes = 0;
   int numSMs = 148;
+  // launch shapes chosen by fmmg_autotune (defaults otherwise): rows per CTA of
+  // the FP32 and FP64 Hadamard kernels, and split-K when a GEMM's tiles fill
+  // fewer than gemmSplitMul CTAs per SM (0: never split)
+  struct Tune {
+    int hadRows = 64, pqParents = 128, gemmSplitMul = 2;
+  } tune;
   bool gemmTC = false;     // M2M/L2L FP32 row GEMMs on the tensor cores (3xTF32), opt-in
   int* devErr = nullptr;   // set by kernels whose bounded waits gave up  // scalar Hadamard: parent-pair register-blocked kernel (else expanded lists)
   float adjMs = 0.f;

@@ -220,12 +220,12 @@ __global__ void __launch_bounds__(256)
 }
 
 // Launches the row GEMM; when the output tiles alone would leave the GPU
-// underfilled (fewer than two CTAs per SM) and K is long, K is split into up to
-// 8 chunks whose partial tiles go to `scratch` (scratchElems values) and are
+// underfilled (fewer than splitCtas CTAs: 2 per SM by default, set by the
+// autotuner, 0 never splits) and K is long, K is split into up to 8 chunks whose partial tiles go to `scratch` (scratchElems values) and are
 // summed in a fixed order by k_gemm_reduce_t, so results stay deterministic.
 // Returns the number of kernels launched.
 template <typename T, int BK>
-inline int launch_gemm_rows(cudaStream_t st, int numSMs, T* scratch, size_t scratchElems, int nrows, int nrhs,
+inline int launch_gemm_rows(cudaStream_t st, int splitCtas, T* scratch, size_t scratchElems, int nrows, int nrhs,
                             const int32_t* rows, const int32_t* chd, int xChild, int yChild, const T* X, int64_t ldx,
                             int64_t xRhs, const T* W, T* Y, int64_t ldy, int64_t yRhs, int K, int N, GrScale<T> xs,
                             GrScale<T> ys, T beta) {
@@ -233,8 +233,8 @@ inline int launch_gemm_rows(cudaStream_t st, int numSMs, T* scratch, size_t scra
   const int64_t M = (int64_t)nrows * nrhs;
   const int tiles = (int)((M + GR_BM - 1) / GR_BM) * ((N + GR_BN - 1) / GR_BN);
   int splits = 1;
-  if (scratch && tiles < 2 * numSMs && K >= 8 * BK) {
-    splits = std::min(8, (2 * numSMs + tiles - 1) / tiles);
+  if (scratch && tiles < splitCtas && K >= 8 * BK) {
+    splits = std::min(8, (splitCtas + tiles - 1) / tiles);
     splits = std::min(splits, K / (4 * BK));
     while (splits > 1 && (size_t)splits * M * N > scratchElems) splits--;
   }

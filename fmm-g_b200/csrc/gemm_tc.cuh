@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(TC_THREADS)
 // FP32 row GEMM launcher: the tensor-core kernel when useTC and the operands
 // have the 16-byte row layout, else the CUDA-core kernel; split K as in
 // launch_gemm_rows (chunks a multiple of 32 on the tensor-core path).
-inline int launch_gemm_rows_f32(cudaStream_t st, int numSMs, float* scratch, size_t scratchElems, bool useTC,
+inline int launch_gemm_rows_f32(cudaStream_t st, int splitCtas, float* scratch, size_t scratchElems, bool useTC,
                                 int* errFlag, int nrows, int nrhs, const int32_t* rows, const int32_t* chd,
                                 int xChild, int yChild, const float* X, int64_t ldx, int64_t xRhs, const float* W,
                                 float* Y, int64_t ldy, int64_t yRhs, int K, int N, GrScale<float> xs,
@@ -268,13 +268,13 @@ inline int launch_gemm_rows_f32(cudaStream_t st, int numSMs, float* scratch, siz
   const bool vec = ((uintptr_t)X % 16 == 0) && ((uintptr_t)W % 16 == 0) && ldx % 4 == 0 && xRhs % 4 == 0 &&
                    K % 4 == 0;
   if (!useTC || !vec || !errFlag)
-    return launch_gemm_rows<float, 16>(st, numSMs, scratch, scratchElems, nrows, nrhs, rows, chd, xChild, yChild, X,
+    return launch_gemm_rows<float, 16>(st, splitCtas, scratch, scratchElems, nrows, nrhs, rows, chd, xChild, yChild, X,
                                        ldx, xRhs, W, Y, ldy, yRhs, K, N, xs, ys, beta);
   const int64_t M = (int64_t)nrows * nrhs;
   const int tiles = (int)((M + TC_BM - 1) / TC_BM) * ((N + TC_BN - 1) / TC_BN);
   int splits = 1;
-  if (scratch && tiles < 2 * numSMs && K >= 4 * TC_BK) {
-    splits = std::min(8, (2 * numSMs + tiles - 1) / tiles);
+  if (scratch && tiles < splitCtas && K >= 4 * TC_BK) {
+    splits = std::min(8, (splitCtas + tiles - 1) / tiles);
     splits = std::min(splits, K / (2 * TC_BK));
     while (splits > 1 && (size_t)splits * M * N > scratchElems) splits--;
   }

@@ -89,7 +89,7 @@ __device__ __forceinline__ void pq_id_table(int16_t* sId, const int16_t* __restr
 // spectrum rows of the neighbour's 8 children nIn[8*e + c2] (or -1).  effIn /
 // effOut hold nrhs right-hand sides at strides inRhs / outRhs; transId maps
 // (rx+3)*49+(ry+3)*7+(rz+3) to a translation id or -1.  Grid (rows /
-// PQ_PARENTS, nEff / 32, ceil(nrhs / KB)); dynamic shared memory
+// rows per CTA, nEff / 32, ceil(nrhs / KB)) (PQ_PARENTS rows per CTA by default); dynamic shared memory
 // pq_smem_bytes<C>(32).  The child slots of the next entry are fetched while
 // the current one is applied, so each neighbour costs one dependent load.
 template <typename C, int KB, bool ADJ>
@@ -114,8 +114,9 @@ __global__ void __launch_bounds__(PQ_THREADS)
   __syncthreads();
   if (f >= nEff) return;
   const C* inF = effIn + (int64_t)rhs0 * inRhs + f;
-  const int bEnd = min(nRows, (int)(blockIdx.x + 1) * PQ_PARENTS);
-  for (int b = blockIdx.x * PQ_PARENTS + warp; b < bEnd; b += PQ_THREADS / 32) {
+  const int per = (nRows + gridDim.x - 1) / gridDim.x;  // rows per CTA: the grid sets it (tunable)
+  const int bEnd = min(nRows, (int)(blockIdx.x + 1) * per);
+  for (int b = blockIdx.x * per + warp; b < bEnd; b += PQ_THREADS / 32) {
     C acc[8][KB];
 #pragma unroll
     for (int c = 0; c < 8; c++)
@@ -225,7 +226,7 @@ __device__ __forceinline__ void pq_delta_x2(unsigned long long (&acc)[8], const 
 // right-hand side, FW = 4 for blocks of 8, where every translation value read
 // from shared memory serves 8 lanes and the CTA stages only 4 frequencies of
 // the 316 translations (10 KB), so residency is set by registers.  Grid (rows
-// / PQX_ROWS, nEff / FW, ceil(nrhs / (32 / FW))); blockIdx.z selects the
+// per CTA, nEff / FW, ceil(nrhs / (32 / FW))) (PQX_ROWS rows per CTA by default); blockIdx.z selects the
 // right-hand-side block of the layout below; dynamic shared memory
 // pqx_smem_bytes<FW>() (row 316 is the zero row of touching pairs).
 constexpr int PQX_THREADS = 256;
@@ -274,8 +275,9 @@ __global__ void __launch_bounds__(PQX_THREADS, 3)
   const int64_t lanePos = act ? (int64_t)f * fStride + (int64_t)rl * rStride : 0;
   const float2* inF = effIn + (act ? blockIdx.z * inL.blk : 0) + lanePos;
   float2* outF = effOut + blockIdx.z * outL.blk + lanePos;
-  const int bEnd = min(nRows, (int)(blockIdx.x + 1) * PQX_ROWS);
-  for (int b = blockIdx.x * PQX_ROWS + warp; b < bEnd; b += PQX_THREADS / 32) {
+  const int per = (nRows + gridDim.x - 1) / gridDim.x;  // rows per CTA: the grid sets it (tunable)
+  const int bEnd = min(nRows, (int)(blockIdx.x + 1) * per);
+  for (int b = blockIdx.x * per + warp; b < bEnd; b += PQX_THREADS / 32) {
     unsigned long long acc[8];
 #pragma unroll
     for (int c = 0; c < 8; c++) acc[c] = 0ull;
@@ -339,7 +341,7 @@ namespace fmmg {
 //   acc = fma2((t.x, t.x), u, acc);  acc = fma2((-t.y, t.y), s(u), acc).
 // The translations are read as 8-byte values (the kernel is bound by shared-
 // memory wavefronts: 16-byte reads cost 4 per warp, 8-byte ones 2).
-// Grid (rows / PQX_ROWS, nEff / 4, ceil(nrhs / 8)); dynamic shared memory
+// Grid (rows / rows per CTA, nEff / 4, ceil(nrhs / 8)); dynamic shared memory
 // 27 * 27 * 4 * 8 bytes.
 constexpr int W8_OFFS = 27;  // offset codes 0..26 (13 unused)
 
@@ -420,8 +422,9 @@ static __global__ void __launch_bounds__(PQX_THREADS, 2)
   const int64_t lanePos = act ? (int64_t)f * 8 + rl : 0;
   const float2* inF = effIn + (act ? blockIdx.z * inL.blk : 0) + lanePos;
   float2* outF = effOut + blockIdx.z * outL.blk + lanePos;
-  const int bEnd = min(nRows, (int)(blockIdx.x + 1) * PQX_ROWS);
-  for (int b = blockIdx.x * PQX_ROWS + warp; b < bEnd; b += PQX_THREADS / 32) {
+  const int per = (nRows + gridDim.x - 1) / gridDim.x;  // rows per CTA: the grid sets it (tunable)
+  const int bEnd = min(nRows, (int)(blockIdx.x + 1) * per);
+  for (int b = blockIdx.x * per + warp; b < bEnd; b += PQX_THREADS / 32) {
     unsigned long long acc[27];
 #pragma unroll
     for (int j = 0; j < 27; j++) acc[j] = 0ull;

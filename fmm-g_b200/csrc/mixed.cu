@@ -935,7 +935,7 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
       gx.v[k] = (float)xs.v[k];
       gy.v[k] = (float)ys.v[k];
     }
-    ls->launches += launch_gemm_rows_f32(st, D.numSMs, reinterpret_cast<float*>(D.gemmScratch),
+    ls->launches += launch_gemm_rows_f32(st, D.numSMs * D.tune.gemmSplitMul, reinterpret_cast<float*>(D.gemmScratch),
                                          D.gemmScratchBytes / sizeof(float), D.gemmTC && tc, D.devErr, nrows, kc, rows,
                                          D.chd, xChild, yChild, X, ldx, xR, W, Y, ldy, yR, K, N, gx, gy, beta);
   };
@@ -1030,20 +1030,20 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
       if (!r8) {  // planes of one right-hand side
         const size_t smem = pqx_smem_bytes<32>();
         cudaFuncSetAttribute(k_m2l_had_pqx2<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        dim3 g1((npar + PQX_ROWS - 1) / PQX_ROWS, (P.nEff + 31) / 32, kc);
+        dim3 g1((npar + D.tune.hadRows - 1) / D.tune.hadRows, (P.nEff + 31) / 32, kc);
         k_m2l_had_pqx2<32, false><<<g1, PQX_THREADS, smem, st>>>(
             npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen32, PqLayout{effDR, P.nEff}, D.m2lT32, D.effVal32,
             PqLayout{effVR, P.nEff}, 1, 0, P.nEff, kc, nrmfc, D.transIdDev);
       } else if (D.hadW && D.m2lTw32) {  // 27-product form
         const size_t smem = (size_t)W8_OFFS * 27 * 4 * sizeof(float2);
         cudaFuncSetAttribute(k_m2l_had_w8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        dim3 g8((npar + PQX_ROWS - 1) / PQX_ROWS, (P.nEff + 3) / 4, nblk);
+        dim3 g8((npar + D.tune.hadRows - 1) / D.tune.hadRows, (P.nEff + 3) / 4, nblk);
         k_m2l_had_w8<<<g8, PQX_THREADS, smem, st>>>(npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen32,
                                                      PqLayout{blkDen, (int64_t)P.nEff * 8}, D.m2lTw32, D.effVal32,
                                                      PqLayout{blkVal, (int64_t)P.nEff * 8}, P.nEff, kc, nrmfc);
       } else {
         const size_t smem = pqx_smem_bytes<4>();
-        dim3 g8((npar + PQX_ROWS - 1) / PQX_ROWS, (P.nEff + 3) / 4, nblk);
+        dim3 g8((npar + D.tune.hadRows - 1) / D.tune.hadRows, (P.nEff + 3) / 4, nblk);
         k_m2l_had_pqx2<4, false><<<g8, PQX_THREADS, smem, st>>>(
             npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen32, PqLayout{blkDen, (int64_t)P.nEff * 8}, D.m2lT32,
             D.effVal32, PqLayout{blkVal, (int64_t)P.nEff * 8}, 8, 1, P.nEff, kc, nrmfc, D.transIdDev);

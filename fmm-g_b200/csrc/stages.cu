@@ -829,7 +829,7 @@ static void launch_m2l_np(const Plan& P, DevState& D, LaunchStats* ls) {
     if (P.sdm == 1 && P.tdm == 1 && D.hadPQ) {
       const size_t smem = pq_smem_bytes<double2>(32);
       cudaFuncSetAttribute(k_m2l_had_pq<double2, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      dim3 g2((npar + PQ_PARENTS - 1) / PQ_PARENTS, (P.nEff + 31) / 32, 1);
+      dim3 g2((npar + D.tune.pqParents - 1) / D.tune.pqParents, (P.nEff + 31) / 32, 1);
       k_m2l_had_pq<double2, 1, false><<<g2, PQ_THREADS, smem, D.stream>>>(
           npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen, 0, D.m2lT, D.effVal, 0, P.nEff, 1, nrmfc,
           D.transIdDev);
@@ -902,7 +902,7 @@ void hadamard_pq64_adj(const Plan& P, DevState& D, const double2* in, double2* o
   if (nrow <= 0) return;
   const size_t smem = pq_smem_bytes<double2>(32);
   cudaFuncSetAttribute(k_m2l_had_pq<double2, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  dim3 g2((nrow + PQ_PARENTS - 1) / PQ_PARENTS, (P.nEff + 31) / 32, 1);
+  dim3 g2((nrow + D.tune.pqParents - 1) / D.tune.pqParents, (P.nEff + 31) / 32, 1);
   k_m2l_had_pq<double2, 1, true><<<g2, PQ_THREADS, smem, D.stream>>>(
       nrow, D.vRowOutT, D.vNbrTPtr, D.vNbrOffT, D.vNbrInT, in, 0, D.m2lT, out, 0, P.nEff, 1, 1.0 / double(P.nReg),
       D.transIdDev);

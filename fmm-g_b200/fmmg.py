@@ -81,6 +81,9 @@ SIGNATURES = {
     "fmmg_set_timing": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "fmmg_set_graph": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "fmmg_set_gemm_path": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "fmmg_autotune": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                       _dp], ctypes.c_int),
+    "fmmg_tuning": ([ctypes.c_void_p, _ip, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "fmmg_device_error": ([ctypes.c_void_p, _ip], ctypes.c_int),
     "fmmg_graph_state": ([ctypes.c_void_p, _ip, ctypes.POINTER(ctypes.c_char_p)], ctypes.c_int),
     "fmmg_tree": ([ctypes.c_void_p, _i32p, _i64p, _i64p], ctypes.c_int),
@@ -313,6 +316,26 @@ class FMM3d:
         v = ctypes.c_int()
         self._chk(lib().fmmg_device_error(self.h, ctypes.byref(v)))
         return v.value
+
+    def autotune(self, den, out, k=1, precision=PREC_FP64, reps=2):
+        """Pick the launch shapes for (k, precision) by timing evaluates on
+        these CUDA tensors; returns (best ms per evaluate, tuning dict)."""
+        self._order_after_torch()
+        ms = ctypes.c_double()
+        self._chk(lib().fmmg_autotune(self.h, k, precision, ctypes.c_void_p(den.data_ptr()),
+                                      ctypes.c_void_p(out.data_ptr()), reps, ctypes.byref(ms)))
+        return ms.value, self.tuning()
+
+    def tuning(self, values=None):
+        """Current launch shapes, or install `values` (a dict as returned)."""
+        v = (ctypes.c_int * 3)()
+        keys = ("had_rows_fp32", "had_rows_fp64", "gemm_split_ctas_per_sm")
+        if values is not None:
+            for i, key in enumerate(keys):
+                v[i] = int(values[key])
+            self._chk(lib().fmmg_tuning(self.h, v, 3, 1))
+        self._chk(lib().fmmg_tuning(self.h, v, 3, 0))
+        return dict(zip(keys, list(v)))
 
     def graph_state(self):
         act, note = ctypes.c_int(), ctypes.c_char_p()

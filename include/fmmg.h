@@ -212,6 +212,18 @@ fmmg_status fmmg_set_gemm_path(fmmg_handle* h, int tensor_cores);
  * results are then invalid), else 0; clears the flag.  Synchronises. */
 fmmg_status fmmg_device_error(fmmg_handle* h, int* flag);
 
+/* Autotuner (no counterpart in the reference): times `reps` evaluates of
+ * (k, precision) on the caller's device buffers for each candidate launch
+ * shape -- rows per CTA of the Hadamard kernel (32, 64, 128, 256), then for
+ * the mixed form the split-K threshold of the FP32 GEMMs (0, 1, 2, 4 CTAs per
+ * SM) -- keeps the fastest in the handle and returns its time in best_ms.
+ * d_trg_val is overwritten.  Synchronises. */
+fmmg_status fmmg_autotune(fmmg_handle* h, int k, int precision, const double* d_src_den, double* d_trg_val,
+                          int reps, double* best_ms);
+/* vals[0..2] = Hadamard rows per CTA (FP32 form), Hadamard rows per CTA (FP64
+ * form), split-K threshold (CTAs per SM); set != 0 installs them, else reads. */
+fmmg_status fmmg_tuning(fmmg_handle* h, int* vals, int n, int set);
+
 /* Host-plan introspection (valid after setup, also with device < 0).
  * which: 0 U, 1 V, 2 W, 3 X lists in the reference form.  node_rec receives
  * per node {depth, path x, path y, path z, parent, first child, tag bits,
