@@ -89,7 +89,12 @@ __device__ __forceinline__ void reduce_store(double* sRed, const double* acc, in
   }
 }
 
-// near field: U-list, direct W and X entries; grid (evaluator leaves, RHS blocks)
+// near field: U-list, direct W and X entries; grid (evaluator leaves, RHS blocks).
+// For the double-layer kernels (source normal, NRM) the offsets are formed from
+// hi/lo FP32 pairs of the box-centred coordinates, (x_hi - y_hi) + (x_lo - y_lo):
+// on densely sampled surfaces near-coincident pairs dominate the sum and
+// n.(x - y) cancels to curvature size, so plain FP32 offsets (rounded at box
+// scale) lose digits there; the hi difference of close points is exact.
 template <int KT, int KB>
 __global__ void __launch_bounds__(MX_THREADS)
     k_p2p_near32(const int32_t* __restrict__ rows, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
@@ -100,6 +105,7 @@ __global__ void __launch_bounds__(MX_THREADS)
                  double* __restrict__ val, int64_t valStride, int nrhs, float mu, float ve) {
   constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD, NRM = KTraits<KT>::NRM;
   __shared__ float sPos[MX_TILE * 3];
+  __shared__ float sPosLo[NRM ? MX_TILE * 3 : 1];
   __shared__ float sNrm[NRM ? MX_TILE * 3 : 1];
   __shared__ float sDen[MX_TILE * SD * KB];
   __shared__ int64_t eBeg[MX_MAXE];
@@ -118,11 +124,17 @@ __global__ void __launch_bounds__(MX_THREADS)
   for (int64_t t0 = 0; t0 < tn; t0 += TG) {
     const int64_t t = t0 + tl;
     const bool act = t < tn;
-    float tx = 0, ty = 0, tz = 0;
+    float tx = 0, ty = 0, tz = 0, txl = 0, tyl = 0, tzl = 0;
     if (act) {
-      tx = (float)(trg[3 * (tb + t)] - cx);
-      ty = (float)(trg[3 * (tb + t) + 1] - cy);
-      tz = (float)(trg[3 * (tb + t) + 2] - cz);
+      const double dx = trg[3 * (tb + t)] - cx, dy = trg[3 * (tb + t) + 1] - cy, dz = trg[3 * (tb + t) + 2] - cz;
+      tx = (float)dx;
+      ty = (float)dy;
+      tz = (float)dz;
+      if (NRM) {
+        txl = (float)(dx - tx);
+        tyl = (float)(dy - ty);
+        tzl = (float)(dz - tz);
+      }
     }
     double acc[TD * KB];
 #pragma unroll
@@ -135,10 +147,14 @@ __global__ void __launch_bounds__(MX_THREADS)
         __syncthreads();
         for (int i = tid; i < cnt; i += MX_THREADS) {
           const int64_t s = entry_source(base + i, ne, eBeg, ePre);
-          sPos[3 * i] = (float)(src[3 * s] - cx);
-          sPos[3 * i + 1] = (float)(src[3 * s + 1] - cy);
-          sPos[3 * i + 2] = (float)(src[3 * s + 2] - cz);
+          const double dx = src[3 * s] - cx, dy = src[3 * s + 1] - cy, dz = src[3 * s + 2] - cz;
+          sPos[3 * i] = (float)dx;
+          sPos[3 * i + 1] = (float)dy;
+          sPos[3 * i + 2] = (float)dz;
           if (NRM) {
+            sPosLo[3 * i] = (float)(dx - (float)dx);
+            sPosLo[3 * i + 1] = (float)(dy - (float)dy);
+            sPosLo[3 * i + 2] = (float)(dz - (float)dz);
             sNrm[3 * i] = (float)nrm[3 * s];
             sNrm[3 * i + 1] = (float)nrm[3 * s + 1];
             sNrm[3 * i + 2] = (float)nrm[3 * s + 2];
@@ -155,9 +171,16 @@ __global__ void __launch_bounds__(MX_THREADS)
           float part[TD * KB];
 #pragma unroll
           for (int c = 0; c < TD * KB; c++) part[c] = 0.f;
-          for (int i = sp; i < cnt; i += S)
-            kaccum_multi<KT, KB, float, float>(tx - sPos[3 * i], ty - sPos[3 * i + 1], tz - sPos[3 * i + 2],
-                                               NRM ? &sNrm[3 * i] : nullptr, &sDen[i * KB * SD], part, mu, ve);
+          for (int i = sp; i < cnt; i += S) {
+            float ox = tx - sPos[3 * i], oy = ty - sPos[3 * i + 1], oz = tz - sPos[3 * i + 2];
+            if (NRM) {
+              ox += txl - sPosLo[3 * i];
+              oy += tyl - sPosLo[3 * i + 1];
+              oz += tzl - sPosLo[3 * i + 2];
+            }
+            kaccum_multi<KT, KB, float, float>(ox, oy, oz, NRM ? &sNrm[3 * i] : nullptr, &sDen[i * KB * SD], part, mu,
+                                               ve);
+          }
 #pragma unroll
           for (int c = 0; c < TD * KB; c++) acc[c] += (double)part[c];
         }
