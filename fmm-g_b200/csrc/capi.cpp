@@ -337,9 +337,10 @@ fmmg_status fmmg_set_graph(fmmg_handle* h, int on) {
   return FMMG_OK;
 }
 
-fmmg_status fmmg_set_gemm_path(fmmg_handle* h, int tensor_cores) {
+fmmg_status fmmg_set_gemm_path(fmmg_handle* h, int path) {
   if (!h) return fail(nullptr, FMMG_INVALID_ARG, "handle is NULL");
-  h->dev.gemmTC = tensor_cores != 0;
+  if (path < 0 || path > 2) return fail(h, FMMG_INVALID_ARG, "gemm path must be 0, 1 or 2");
+  h->dev.gemmPath = path;
   drop_graph(h);
   return FMMG_OK;
 }

@@ -92,8 +92,17 @@ struct DevState {
   struct Tune {
     int hadRows = 64, pqParents = 128, gemmSplitMul = 2;
   } tune;
-  bool gemmTC = false;     // M2M/L2L FP32 row GEMMs on the tensor cores (3xTF32), opt-in
-  int* devErr = nullptr;   // set by kernels whose bounded waits gave up  // scalar Hadamard: parent-pair register-blocked kernel (else expanded lists)
+  // FP32 row GEMMs: 0 wide-tile CUDA-core kernel (default), 1 M2M/L2L on the
+  // tensor cores (3xTF32, opt-in), 2 the 128 x 64 CUDA-core kernel
+  int gemmPath = 0;
+  // FP32 operators transposed and zero padded for the wide-tile GEMM,
+  // Wt[k][n]: K to a multiple of 16, N to a multiple of 160 (ld)
+  struct OpT {
+    float* p = nullptr;
+    int ld = 0;
+  };
+  OpT tM2M, tL2L, tUpF1, tUpF2, tDnF1, tDnF2;
+  int* devErr = nullptr;  // set by kernels whose bounded waits gave up
   float adjMs = 0.f;
   // dense check scratch
   double *chkPos = nullptr, *chkOut = nullptr;

@@ -257,16 +257,21 @@ __global__ void __launch_bounds__(TC_THREADS)
 }
 
 // FP32 row GEMM launcher: the tensor-core kernel when useTC and the operands
-// have the 16-byte row layout, else the CUDA-core kernel; split K as in
+// have the 16-byte row layout; else the wide-tile CUDA-core kernel when the
+// transposed operator Wt (ldw per row) is given and the X rows allow 16-byte
+// fetches; else the 128 x 64 CUDA-core kernel.  Split K as in
 // launch_gemm_rows (chunks a multiple of 32 on the tensor-core path).
 inline int launch_gemm_rows_f32(cudaStream_t st, int splitCtas, float* scratch, size_t scratchElems, bool useTC,
                                 int* errFlag, int nrows, int nrhs, const int32_t* rows, const int32_t* chd,
                                 int xChild, int yChild, const float* X, int64_t ldx, int64_t xRhs, const float* W,
-                                float* Y, int64_t ldy, int64_t yRhs, int K, int N, GrScale<float> xs,
-                                GrScale<float> ys, float beta) {
+                                const float* Wt, int ldw, float* Y, int64_t ldy, int64_t yRhs, int K, int N,
+                                GrScale<float> xs, GrScale<float> ys, float beta) {
   if (nrows <= 0 || nrhs <= 0) return 0;
-  const bool vec = ((uintptr_t)X % 16 == 0) && ((uintptr_t)W % 16 == 0) && ldx % 4 == 0 && xRhs % 4 == 0 &&
-                   K % 4 == 0;
+  const bool xvec = ((uintptr_t)X % 16 == 0) && ldx % 4 == 0 && xRhs % 4 == 0 && K % 4 == 0;
+  const bool vec = xvec && ((uintptr_t)W % 16 == 0);
+  if ((!useTC || !vec || !errFlag) && Wt && xvec && ((uintptr_t)Wt % 16 == 0) && ldw % GW_BN == 0)
+    return launch_gemm_rows_w(st, splitCtas, scratch, scratchElems, nrows, nrhs, rows, chd, xChild, yChild, X, ldx,
+                              xRhs, Wt, ldw, Y, ldy, yRhs, K, N, xs, ys, beta);
   if (!useTC || !vec || !errFlag)
     return launch_gemm_rows<float, 16>(st, splitCtas, scratch, scratchElems, nrows, nrhs, rows, chd, xChild, yChild, X,
                                        ldx, xRhs, W, Y, ldy, yRhs, K, N, xs, ys, beta);

@@ -836,6 +836,17 @@ static std::vector<double> pad_cols(const std::vector<double>& F, int m, int k) 
   return r;
 }
 
+// W row-major n x k -> Wt[k][n] in FP32, K padded to a multiple of GW_BK and N
+// to a multiple of GW_BN (ld) with zeros: the wide-tile GEMM reads whole tiles
+static std::vector<float> transpose_pad(const std::vector<double>& W, int n, int k, int& ld) {
+  const int kp = (k + GW_BK - 1) / GW_BK * GW_BK;
+  ld = (n + GW_BN - 1) / GW_BN * GW_BN;
+  std::vector<float> t((size_t)kp * ld, 0.f);
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < k; j++) t[(size_t)j * ld + i] = (float)W[(size_t)i * k + j];
+  return t;
+}
+
 // Work arrays for a chunk of kc right-hand sides, and the FP32 operator copies.
 static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
   const size_t ue = (size_t)P.nUE * P.sdm, uc = (size_t)P.nUC * P.tdm;
@@ -884,6 +895,22 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
     FMMG_TRY(put(D.upF2, pad_cols(P.uc2ueF2, (int)ue, P.kUp)));
     FMMG_TRY(put(D.dnF1, pad_rows(P.dc2deF1, P.kDn, (int)dc)));
     FMMG_TRY(put(D.dnF2, pad_cols(P.dc2deF2, (int)de, P.kDn)));
+    // the same operators transposed and padded for the wide-tile GEMM
+    auto putT = [&](DevState::OpT& op, const std::vector<double>& W, int n, int k) -> std::string {
+      int ld = 0;
+      const std::vector<float> t = transpose_pad(W, n, k, ld);
+      if (!op.p) FMMG_TRY(dalloc(D, op.p, t.size()));
+      op.ld = ld;
+      FMMG_CK(cudaMemcpy(op.p, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice));
+      return std::string();
+    };
+    const int kUp4 = pad4(P.kUp), kDn4 = pad4(P.kDn);
+    FMMG_TRY(putT(D.tM2M, P.m2m, (int)uc, (int)(8 * ue)));
+    FMMG_TRY(putT(D.tL2L, P.l2l, (int)(8 * dc), (int)de));
+    FMMG_TRY(putT(D.tUpF1, pad_rows(P.uc2ueF1, P.kUp, (int)uc), kUp4, (int)uc));
+    FMMG_TRY(putT(D.tUpF2, pad_cols(P.uc2ueF2, (int)ue, P.kUp), (int)ue, kUp4));
+    FMMG_TRY(putT(D.tDnF1, pad_rows(P.dc2deF1, P.kDn, (int)dc), kDn4, (int)dc));
+    FMMG_TRY(putT(D.tDnF2, pad_cols(P.dc2deF2, (int)de, P.kDn), (int)de, kDn4));
     std::vector<float2> t(P.m2lT.size());
     for (size_t i = 0; i < t.size(); i++) t[i] = make_float2((float)P.m2lT[i].real(), (float)P.m2lT[i].imag());
     FMMG_CK(cudaMemcpy(D.m2lT32, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice));
@@ -948,8 +975,8 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
   // factor of the pseudo-inverse amplifies the tensor core's accumulation
   // rounding past the 1e-5 budget.
   auto gemm = [&](int nrows, const int32_t* rows, int xChild, int yChild, const float* X, int64_t ldx, int64_t xR,
-                  const float* W, float* Y, int64_t ldy, int64_t yR, int K, int N, Scale4 xs, Scale4 ys, float beta,
-                  bool tc) {
+                  const float* W, const DevState::OpT& wt, float* Y, int64_t ldy, int64_t yR, int K, int N, Scale4 xs,
+                  Scale4 ys, float beta, bool tc) {
     if (nrows <= 0) return;
     GrScale<float> gx, gy;
     gx.mod = xs.mod;
@@ -959,8 +986,9 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
       gy.v[k] = (float)ys.v[k];
     }
     ls->launches += launch_gemm_rows_f32(st, D.numSMs * D.tune.gemmSplitMul, reinterpret_cast<float*>(D.gemmScratch),
-                                         D.gemmScratchBytes / sizeof(float), D.gemmTC && tc, D.devErr, nrows, kc, rows,
-                                         D.chd, xChild, yChild, X, ldx, xR, W, Y, ldy, yR, K, N, gx, gy, beta);
+                                         D.gemmScratchBytes / sizeof(float), D.gemmPath == 1 && tc, D.devErr, nrows,
+                                         kc, rows, D.chd, xChild, yChild, X, ldx, xR, W,
+                                         D.gemmPath == 2 ? nullptr : wt.p, wt.ld, Y, ldy, yR, K, N, gx, gy, beta);
   };
   if ((mask & 1) && !P.s2mLeaves.empty()) {
     k_src2surf32<KT, KB><<<dim3((unsigned)P.s2mLeaves.size(), kb), MX_SURF, 0, st>>>(
@@ -972,14 +1000,14 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
   if (mask & 1) {
     for (int d = P.maxDepth; d >= 1; d--) {
       int64_t a = D.offUpM2M[d], b = D.offUpM2M[d + 1];
-      gemm((int)(b - a), D.levelRows + a, 1, 0, D.uden32, ue, nn * ue, D.m2m32, D.uchk32, uc, nn * uc, 8 * ue, uc,
+      gemm((int)(b - a), D.levelRows + a, 1, 0, D.uden32, ue, nn * ue, D.m2m32, D.tM2M, D.uchk32, uc, nn * uc, 8 * ue, uc,
            level_scale(P, d + 1 + rl, +1.0), unit_scale(), 0.f, true);
       a = D.offUpC2E[d];
       b = D.offUpC2E[d + 1];
       // C2E as F2 (F1 uchk): the large-norm pinv never multiplies in FP32
-      gemm((int)(b - a), D.levelRows + a, 0, 0, D.uchk32, uc, nn * uc, D.upF1, D.upT32, kUp4, nn * kUp4, uc,
+      gemm((int)(b - a), D.levelRows + a, 0, 0, D.uchk32, uc, nn * uc, D.upF1, D.tUpF1, D.upT32, kUp4, nn * kUp4, uc,
            kUp4, unit_scale(), unit_scale(), 0.f, false);
-      gemm((int)(b - a), D.levelRows + a, 0, 0, D.upT32, kUp4, nn * kUp4, D.upF2, D.uden32, ue, nn * ue, kUp4,
+      gemm((int)(b - a), D.levelRows + a, 0, 0, D.upT32, kUp4, nn * kUp4, D.upF2, D.tUpF2, D.uden32, ue, nn * ue, kUp4,
            ue, unit_scale(), level_scale(P, d + rl, -1.0), 0.f, false);
     }
   }
@@ -1151,13 +1179,13 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
     for (int d = 2; d <= P.maxDepth; d++) {
       if (d >= 3) {
         int64_t a = D.offDnL2L[d - 1], b = D.offDnL2L[d];
-        gemm((int)(b - a), D.levelRows + a, 0, 1, D.dden32, de, nn * de, D.l2l32, D.dchk32, dc, nn * dc, de, 8 * dc,
+        gemm((int)(b - a), D.levelRows + a, 0, 1, D.dden32, de, nn * de, D.l2l32, D.tL2L, D.dchk32, dc, nn * dc, de, 8 * dc,
              level_scale(P, d - 1 + rl, +1.0), unit_scale(), 1.f, true);
       }
       int64_t a = D.offDnC2E[d], b = D.offDnC2E[d + 1];
-      gemm((int)(b - a), D.levelRows + a, 0, 0, D.dchk32, dc, nn * dc, D.dnF1, D.dnT32, kDn4, nn * kDn4, dc,
+      gemm((int)(b - a), D.levelRows + a, 0, 0, D.dchk32, dc, nn * dc, D.dnF1, D.tDnF1, D.dnT32, kDn4, nn * kDn4, dc,
            kDn4, unit_scale(), unit_scale(), 0.f, false);
-      gemm((int)(b - a), D.levelRows + a, 0, 0, D.dnT32, kDn4, nn * kDn4, D.dnF2, D.dden32, de, nn * de, kDn4,
+      gemm((int)(b - a), D.levelRows + a, 0, 0, D.dnT32, kDn4, nn * kDn4, D.dnF2, D.tDnF2, D.dden32, de, nn * de, kDn4,
            de, unit_scale(), level_scale(P, d + rl, -1.0), 0.f, false);
     }
   }

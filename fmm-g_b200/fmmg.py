@@ -306,10 +306,17 @@ class FMM3d:
         with the same k, precision and tensors)."""
         self._chk(lib().fmmg_set_graph(self.h, 1 if on else 0))
 
-    def set_gemm_path(self, tensor_cores=True):
-        """M2M/L2L FP32 row GEMMs on the tensor cores (3xTF32, opt-in) or all on
-        the CUDA cores (default)."""
-        self._chk(lib().fmmg_set_gemm_path(self.h, 1 if tensor_cores else 0))
+    GEMM_PATHS = {"wide": 0, "tc": 1, "narrow": 2}
+
+    def set_gemm_path(self, path="wide"):
+        """Kernels of the FP32 row GEMMs: "wide" (CUDA cores, 128 x 160 tiles,
+        the default), "narrow" (CUDA cores, 128 x 64 tiles) or "tc" (M2M/L2L on
+        the tensor cores as 3xTF32, opt-in).  True/False mean "tc"/"wide"."""
+        if path is True or path is False:
+            path = "tc" if path else "wide"
+        if path not in self.GEMM_PATHS:
+            raise ValueError("gemm path must be one of %s" % sorted(self.GEMM_PATHS))
+        self._chk(lib().fmmg_set_gemm_path(self.h, self.GEMM_PATHS[path]))
 
     def device_error(self):
         """1 if a kernel gave up a bounded wait since the last call (clears it)."""

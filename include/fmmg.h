@@ -201,13 +201,16 @@ fmmg_status fmmg_set_graph(fmmg_handle* h, int on);
 /* active: 1 while a captured graph is cached; note: why capture was refused ("" if not). */
 fmmg_status fmmg_graph_state(const fmmg_handle* h, int* active, const char** note);
 
-/* tensor_cores != 0: the M2M and L2L FP32 row GEMMs of the mixed form run on
- * the tensor cores as 3xTF32 split products (tcgen05) where the operand rows
- * are 16-byte aligned; 0 (the default): all row GEMMs on the CUDA cores.  The
- * tensor-core accumulation rounding, amplified by the next check-to-equivalent
- * pseudo-inverse, lifts the error of the 1M-point Laplace np=6 workload to
- * 1.1e-5, above its 1e-5 budget.  No counterpart in the reference. */
-fmmg_status fmmg_set_gemm_path(fmmg_handle* h, int tensor_cores);
+/* The kernels of the mixed form's FP32 row GEMMs.  path 0 (the default): all
+ * on the CUDA cores with 128 x 160 tiles; 2: CUDA cores with 128 x 64 tiles;
+ * 1: the M2M and L2L GEMMs on the tensor cores as 3xTF32 split products
+ * (tcgen05) where the operand rows are 16-byte aligned, the rest as path 0.
+ * The TF32 rounding of the low parts and the tensor-core accumulation,
+ * amplified by the next check-to-equivalent pseudo-inverse, lift the error of
+ * the 1M-point Laplace np=6 workload to 1.1e-5 on path 1, above its 1e-5
+ * budget.  FMMG_INVALID_ARG for another path.  No counterpart in the
+ * reference. */
+fmmg_status fmmg_set_gemm_path(fmmg_handle* h, int path);
 /* flag = 1 if a kernel gave up a bounded wait since the last call (its
  * results are then invalid), else 0; clears the flag.  Synchronises. */
 fmmg_status fmmg_device_error(fmmg_handle* h, int* flag);

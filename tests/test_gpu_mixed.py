@@ -104,12 +104,15 @@ def test_mixed_multi_rhs_matches_single_rhs():
 
 
 @pytest.mark.parametrize("k", [1, 8])
-def test_tensor_core_gemms_match_cuda_core_gemms(k):
-    """The FP32 row GEMMs on the tensor cores (3xTF32, tcgen05) against the
-    CUDA-core FP32 GEMMs.  3xTF32 drops the lo*lo term and the tensor core
-    truncates lo, so its products carry a few FP32 roundings (the two paths
-    differ by ~4e-6 at np = 6); both meet the 1e-5 bound against the dense
-    FP64 sum, which is the accuracy gate of the mixed form."""
+def test_gemm_paths_agree(k):
+    """The three kernels of the FP32 row GEMMs on one evaluate: the 128 x 160
+    CUDA-core tiles (default), the 128 x 64 CUDA-core tiles, and the tensor
+    cores (3xTF32, tcgen05) on M2M/L2L.  The CUDA-core kernels differ only in
+    summation order (split K, where the uniform X scale is applied); 3xTF32
+    drops the lo*lo term and the tensor core truncates lo, so its products
+    carry a few FP32 roundings (~4e-6 from the others at np = 6).  All meet
+    the 1e-5 bound against the dense FP64 sum, the accuracy gate of the
+    mixed form."""
     import torch
     rng = np.random.default_rng(41 + k)
     n = 60000
@@ -118,21 +121,26 @@ def test_tensor_core_gemms_match_cuda_core_gemms(k):
     lib.setup(src)
     D = rng.normal(size=(k, n))
     outs = {}
-    for tc in (True, False):
-        lib.set_gemm_path(tc)
+    for path in ("tc", "narrow", "wide"):
+        lib.set_gemm_path(path)
         out = torch.zeros(k, n, dtype=torch.float64, device="cuda")
         torch.cuda.synchronize()
         lib.evaluate_device(torch.from_numpy(D).cuda(), out, k, fmmg.PREC_MIXED)
         lib.sync()
         assert lib.device_error() == 0
-        outs[tc] = out.cpu().numpy()
-    assert rel_l2(outs[True], outs[False]) <= 1e-5
+        outs[path] = out.cpu().numpy()
+    print("k %d wide vs narrow %.3e, wide vs tc %.3e" % (
+        k, rel_l2(outs["wide"], outs["narrow"]), rel_l2(outs["wide"], outs["tc"])))
+    assert rel_l2(outs["wide"], outs["narrow"]) <= 1e-6
+    assert rel_l2(outs["tc"], outs["wide"]) <= 1e-5
     idx = rng.choice(n, 2000, replace=False)
     for r in (0, k - 1):
-        for tc in (True, False):
-            rel, _, _ = lib.check(D[r], outs[tc][r], idx)
-            print("k %d rhs %d tensor-cores %s rel err vs dense %.3e" % (k, r, tc, rel))
+        for path in outs:
+            rel, _, _ = lib.check(D[r], outs[path][r], idx)
+            print("k %d rhs %d %s rel err vs dense %.3e" % (k, r, path, rel))
             assert rel <= 1e-5
+    with pytest.raises(ValueError):
+        lib.set_gemm_path("fast")
 
 
 @pytest.mark.parametrize("np_", [3, 4, 5, 8])
