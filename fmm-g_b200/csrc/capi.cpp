@@ -391,9 +391,23 @@ fmmg_status fmmg_autotune(fmmg_handle* h, int k, int precision, const double* dD
     float best = 1e30f, ms = 0.f;
     const bool mixed = precision == FMMG_PREC_MIXED;
     int* rowsKnob = mixed ? &T.hadRows : &T.pqParents;
+    if (mixed && k >= 2) {  // the 27-product Hadamard with 1 or 2 right-hand sides per thread
+      int bestForm = T.hadRhsPerThread;
+      for (int c : {2, 1}) {
+        T.hadRhsPerThread = c;
+        if ((s = timeIt(ms)) != FMMG_OK) break;
+        if (ms < best) {
+          best = ms;
+          bestForm = c;
+        }
+      }
+      T.hadRhsPerThread = bestForm;
+      best = 1e30f;
+    }
     const int rowsCand[4] = {32, 64, 128, 256};
     int bestRows = *rowsKnob;
     for (int c : rowsCand) {
+      if (s != FMMG_OK) break;
       *rowsKnob = c;
       if ((s = timeIt(ms)) != FMMG_OK) break;
       if (ms < best) {
@@ -430,15 +444,18 @@ fmmg_status fmmg_tuning(fmmg_handle* h, int* vals, int n, int set) {
   if (!h || !vals || n < 3) return fail(h, FMMG_INVALID_ARG, "need 3 values");
   fmmg::DevState::Tune& T = h->dev.tune;
   if (set) {
-    if (vals[0] < 1 || vals[1] < 1 || vals[2] < 0) return fail(h, FMMG_INVALID_ARG, "tuning values");
+    if (vals[0] < 1 || vals[1] < 1 || vals[2] < 0 || (n >= 4 && vals[3] != 1 && vals[3] != 2))
+      return fail(h, FMMG_INVALID_ARG, "tuning values");
     T.hadRows = vals[0];
     T.pqParents = vals[1];
     T.gemmSplitMul = vals[2];
+    if (n >= 4) T.hadRhsPerThread = vals[3];
     drop_graph(h);
   } else {
     vals[0] = T.hadRows;
     vals[1] = T.pqParents;
     vals[2] = T.gemmSplitMul;
+    if (n >= 4) vals[3] = T.hadRhsPerThread;
   }
   return FMMG_OK;
 }

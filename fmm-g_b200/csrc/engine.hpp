@@ -27,6 +27,11 @@ struct DBuf {
 struct DevState {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // second stream of an untimed pass: the near field and the W list run on it
+  // beside the upward pass and the V list (they only add into the target
+  // values); evFork/evUp/evSide order it against the main stream
+  cudaStream_t side = nullptr;
+  cudaEvent_t evFork = nullptr, evUp = nullptr, evSide = nullptr;
   bool ownStream = false;
   // geometry (permuted order)
   double *src = nullptr, *nrm = nullptr, *trg = nullptr;
@@ -89,8 +94,10 @@ struct DevState {
   // launch shapes chosen by fmmg_autotune (defaults otherwise): rows per CTA of
   // the FP32 and FP64 Hadamard kernels, and split-K when a GEMM's tiles fill
   // fewer than gemmSplitMul CTAs per SM (0: never split)
+  // fmmg_autotune (defaults otherwise), and the right-hand sides per thread
+  // of the FP32 27-product Hadamard (1 or 2)
   struct Tune {
-    int hadRows = 64, pqParents = 128, gemmSplitMul = 2;
+    int hadRows = 64, pqParents = 128, gemmSplitMul = 2, hadRhsPerThread = 1;
   } tune;
   // FP32 row GEMMs: 0 wide-tile CUDA-core kernel (default), 1 M2M/L2L on the
   // tensor cores (3xTF32, opt-in), 2 the 128 x 64 CUDA-core kernel

@@ -350,10 +350,6 @@ __device__ __forceinline__ unsigned long long w8_add(unsigned long long a, unsig
   asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
   return r;
 }
-__device__ __forceinline__ unsigned long long w8_swap(unsigned long long a) {
-  const float2 v = pq_unpk(a);
-  return pq_pk(v.y, v.x);
-}
 
 // Sum over the children (bx, by, bz) selected by the y and z combination
 // codes jy, jz (0: both, 1: b = 1, 2: b = 0) for a fixed bx.
@@ -373,11 +369,21 @@ __device__ __forceinline__ unsigned long long w8_yz(const unsigned long long (&x
   return s;
 }
 
-// one combined translation as the packed operands (t.x, t.x) and (-t.y, t.y),
-// from an 8-byte shared load (served per half-warp: 2 wavefronts)
-__device__ __forceinline__ ulonglong2 w8_t(const float2* __restrict__ Tw, int i) {
+// acc += t * u for the combined translation t = Tw[i] (8-byte shared load,
+// served per half-warp: 2 wavefronts) and u packed (re, im): the t.x terms as
+// one packed FMA on (t.x, t.x), the t.y terms (re -= t.y im, im += t.y re) as
+// two scalar FMAs, which take the negation and the crossed halves as operand
+// forms instead of a swapped copy of u and a (-t.y, t.y) pair.  Per component
+// the same two roundings as two packed FMAs.
+__device__ __forceinline__ void w8_cmac(unsigned long long& acc, const float2* __restrict__ Tw, int i,
+                                        unsigned long long u) {
   const float2 t = Tw[i];
-  return make_ulonglong2(pq_pk(t.x, t.x), pq_pk(-t.y, t.y));
+  pq_fma2(acc, pq_pk(t.x, t.x), u);
+  float2 a = pq_unpk(acc);
+  const float2 v = pq_unpk(u);
+  a.x = fmaf(-t.y, v.y, a.x);
+  a.y = fmaf(t.y, v.x, a.y);
+  acc = pq_pk(a.x, a.y);
 }
 
 template <int J>
@@ -386,17 +392,10 @@ __device__ __forceinline__ void w8_group(unsigned long long (&acc)[27], const un
   if constexpr (J < 9) {
     constexpr int JY = J / 3, JZ = J % 3;
     const unsigned long long p0 = w8_yz<JY, JZ>(x, 0), p1 = w8_yz<JY, JZ>(x, 1);
-    const unsigned long long q0 = w8_swap(p0), q1 = w8_swap(p1);
     // jx = m1 (x0 + x1), m2 (x1), m3 (x0); j = jx * 9 + jy * 3 + jz
-    const ulonglong2 t1 = w8_t(Tw, (0 * 9 + J) * 4 + fl), t2 = w8_t(Tw, (1 * 9 + J) * 4 + fl),
-                     t3 = w8_t(Tw, (2 * 9 + J) * 4 + fl);
-    const unsigned long long u1 = w8_add(p0, p1), s1 = w8_add(q0, q1);
-    pq_fma2(acc[0 * 9 + J], t1.x, u1);
-    pq_fma2(acc[0 * 9 + J], t1.y, s1);
-    pq_fma2(acc[1 * 9 + J], t2.x, p1);
-    pq_fma2(acc[1 * 9 + J], t2.y, q1);
-    pq_fma2(acc[2 * 9 + J], t3.x, p0);
-    pq_fma2(acc[2 * 9 + J], t3.y, q0);
+    w8_cmac(acc[0 * 9 + J], Tw, (0 * 9 + J) * 4 + fl, w8_add(p0, p1));
+    w8_cmac(acc[1 * 9 + J], Tw, (1 * 9 + J) * 4 + fl, p1);
+    w8_cmac(acc[2 * 9 + J], Tw, (2 * 9 + J) * 4 + fl, p0);
     w8_group<J + 1>(acc, x, Tw, fl);
   }
 }
@@ -483,6 +482,141 @@ static __global__ void __launch_bounds__(PQX_THREADS, 2)
       }
       const float2 a = pq_unpk(s);
       outF[(int64_t)t * outL.slot] = make_float2(a.x * nrmfc, a.y * nrmfc);
+    }
+  }
+}
+
+
+// k_m2l_had_w8x2: the 27-product form with two right-hand sides per thread.
+// Lanes = 8 frequencies x 4 pairs of right-hand sides (one block of 8), a
+// warp per target parent as in k_m2l_had_w8.  Each combined translation read
+// from shared memory feeds both right-hand sides, which halves the table
+// traffic per FMA (the L1 data path bounds the one-per-thread form); the two
+// right-hand sides of a lane are adjacent in the interleaved layout, so every
+// child spectrum is one 16-byte load.  Per right-hand side the arithmetic is
+// the same operations in the same order as k_m2l_had_w8, so the results are
+// identical.
+constexpr int W8X2_F = 8;  // frequencies per CTA
+
+template <int J>
+__device__ __forceinline__ void w8x2_group(unsigned long long (&acc)[2][27], const unsigned long long (&x)[2][8],
+                                           const float2* __restrict__ Tw, int fl) {
+  if constexpr (J < 9) {
+    constexpr int JY = J / 3, JZ = J % 3;
+#pragma unroll
+    for (int jx = 0; jx < 3; jx++) {
+      const float2 t = Tw[(jx * 9 + J) * W8X2_F + fl];
+      const unsigned long long tx = pq_pk(t.x, t.x);
+#pragma unroll
+      for (int r = 0; r < 2; r++) {
+        const unsigned long long p0 = w8_yz<JY, JZ>(x[r], 0), p1 = w8_yz<JY, JZ>(x[r], 1);
+        const unsigned long long u = jx == 0 ? w8_add(p0, p1) : (jx == 1 ? p1 : p0);
+        unsigned long long& a = acc[r][jx * 9 + J];
+        pq_fma2(a, tx, u);
+        float2 av = pq_unpk(a);
+        const float2 v = pq_unpk(u);
+        av.x = fmaf(-t.y, v.y, av.x);
+        av.y = fmaf(t.y, v.x, av.y);
+        a = pq_pk(av.x, av.y);
+      }
+    }
+    w8x2_group<J + 1>(acc, x, Tw, fl);
+  }
+}
+
+static __global__ void __launch_bounds__(PQX_THREADS, 1)
+    k_m2l_had_w8x2(int nRows, const int32_t* __restrict__ rowOut, const int64_t* __restrict__ nPtr,
+                   const int8_t* __restrict__ nOff, const int32_t* __restrict__ nIn, const float2* __restrict__ effIn,
+                   PqLayout inL, const float2* __restrict__ Tw, float2* __restrict__ effOut, PqLayout outL, int nEff,
+                   int nrhs, float nrmfc) {
+  extern __shared__ __align__(16) unsigned char w8x2_smem[];
+  float2* Ts = reinterpret_cast<float2*>(w8x2_smem);  // [27 offsets][27 combinations][8 frequencies]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int fl = lane & 7, rp = lane >> 3;
+  const int f0 = blockIdx.y * W8X2_F;
+  const int f = f0 + fl;
+  const int rhs = blockIdx.z * 8 + 2 * rp;  // this lane's two right-hand sides: rhs, rhs + 1
+  for (int i = threadIdx.x; i < W8_OFFS * 27 * W8X2_F; i += blockDim.x) {
+    const int oj = i / W8X2_F, ff = f0 + (i % W8X2_F);
+    Ts[i] = ff < nEff ? Tw[(int64_t)oj * nEff + ff] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  const bool act = f < nEff && rhs < nrhs;
+  const bool two = rhs + 1 < nrhs;
+  // the block holds 8 right-hand-side slots, so rhs + 1 is in the buffer
+  const int64_t lanePos = act ? (int64_t)f * 8 + 2 * rp : 0;
+  const float4* inF = reinterpret_cast<const float4*>(effIn + (act ? blockIdx.z * inL.blk : 0) + lanePos);
+  float2* outF = effOut + blockIdx.z * outL.blk + lanePos;
+  const int64_t inSlot4 = inL.slot / 2;  // float4 units (slot strides are multiples of 8 float2)
+  const int per = (nRows + gridDim.x - 1) / gridDim.x;
+  const int bEnd = min(nRows, (int)(blockIdx.x + 1) * per);
+  for (int b = blockIdx.x * per + warp; b < bEnd; b += PQX_THREADS / 32) {
+    unsigned long long acc[2][27];
+#pragma unroll
+    for (int r = 0; r < 2; r++)
+#pragma unroll
+      for (int j = 0; j < 27; j++) acc[r][j] = 0ull;
+    int64_t e = nPtr[b];
+    const int64_t e1 = nPtr[b + 1];
+    float4 raw[8];
+    int offNext = 13;
+    int4 sa = make_int4(-1, -1, -1, -1), sb = sa;
+    if (e < e1) {
+      const int4 a0 = reinterpret_cast<const int4*>(nIn)[2 * e];
+      const int4 b0 = reinterpret_cast<const int4*>(nIn)[2 * e + 1];
+      const int sl[8] = {a0.x, a0.y, a0.z, a0.w, b0.x, b0.y, b0.z, b0.w};
+#pragma unroll
+      for (int c2 = 0; c2 < 8; c2++)
+        raw[c2] = (act && sl[c2] >= 0) ? inF[(int64_t)sl[c2] * inSlot4] : make_float4(0.f, 0.f, 0.f, 0.f);
+      offNext = nOff[e];
+      if (e + 1 < e1) {
+        sa = reinterpret_cast<const int4*>(nIn)[2 * (e + 1)];
+        sb = reinterpret_cast<const int4*>(nIn)[2 * (e + 1) + 1];
+      }
+    }
+    for (; e < e1; e++) {
+      unsigned long long x[2][8];
+#pragma unroll
+      for (int c2 = 0; c2 < 8; c2++) {
+        x[0][c2] = pq_pk(raw[c2].x, raw[c2].y);
+        x[1][c2] = pq_pk(raw[c2].z, raw[c2].w);
+      }
+      const int offCur = offNext;
+      if (e + 1 < e1) {
+        const int sl[8] = {sa.x, sa.y, sa.z, sa.w, sb.x, sb.y, sb.z, sb.w};
+#pragma unroll
+        for (int c2 = 0; c2 < 8; c2++)
+          raw[c2] = (act && sl[c2] >= 0) ? inF[(int64_t)sl[c2] * inSlot4] : make_float4(0.f, 0.f, 0.f, 0.f);
+        offNext = nOff[e + 1];
+        if (e + 2 < e1) {
+          sa = reinterpret_cast<const int4*>(nIn)[2 * (e + 2)];
+          sb = reinterpret_cast<const int4*>(nIn)[2 * (e + 2) + 1];
+        }
+      }
+      w8x2_group<0>(acc, x, Ts + offCur * 27 * W8X2_F, fl);
+    }
+    if (!act) continue;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      const int t = rowOut[8 * b + c];
+      if (t < 0) continue;
+      const int cx = c >> 2, cy = (c >> 1) & 1, cz = c & 1;
+      unsigned long long s0 = 0ull, s1 = 0ull;
+#pragma unroll
+      for (int j = 0; j < 27; j++) {
+        const int jx = j / 9, jy = (j / 3) % 3, jz = j % 3;
+        const bool use = (jx == 0 || jx == 1 + cx) && (jy == 0 || jy == 1 + cy) && (jz == 0 || jz == 1 + cz);
+        if (use) {
+          s0 = w8_add(s0, acc[0][j]);
+          s1 = w8_add(s1, acc[1][j]);
+        }
+      }
+      const float2 a0 = pq_unpk(s0), a1 = pq_unpk(s1);
+      float2* o = outF + (int64_t)t * outL.slot;
+      if (two)
+        *reinterpret_cast<float4*>(o) = make_float4(a0.x * nrmfc, a0.y * nrmfc, a1.x * nrmfc, a1.y * nrmfc);
+      else
+        o[0] = make_float2(a0.x * nrmfc, a0.y * nrmfc);
     }
   }
 }

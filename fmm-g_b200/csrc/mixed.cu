@@ -35,6 +35,13 @@ __constant__ int16_t c_transId32[343];
 
 constexpr int MX_THREADS = 128;
 constexpr int MX_TILE = 128;
+// staged sources (or surface points) per round: 256 when a source carries at
+// most 8 density values and no normal (the static shared memory stays under
+// 48 KB), else 128
+template <int DEN, bool NRM>
+constexpr int mx_tile() {
+  return (DEN <= 8 && !NRM) ? 256 : 128;
+}
 constexpr int MX_MAXE = 256;
 
 // fill eBeg/ePre for entries [ec, ec+ne) and return the total source count
@@ -89,6 +96,34 @@ __device__ __forceinline__ void reduce_store(double* sRed, const double* acc, in
   }
 }
 
+// Lanes per target group of a leaf with tn targets: the smallest power of two
+// from gmin (8, 16 or 32) up to 128 that holds them (a leaf holds
+// ~ptsMax/4..ptsMax points), the rest of the CTA splitting the sources.
+__device__ __forceinline__ int mx_group(int64_t tn, int gmin = 8) {
+  int g = gmin;
+  while (g < 128 && g < tn) g *= 2;
+  return g;
+}
+
+// The N staged densities of one source from shared memory into registers,
+// as 16-byte vectors when N is a multiple of 4 (the row is 16-byte aligned).
+template <int N>
+__device__ __forceinline__ void mx_den(const float* __restrict__ s, float (&d)[N]) {
+  if constexpr (N % 4 == 0) {
+#pragma unroll
+    for (int c = 0; c < N; c += 4) {
+      const float4 v = *reinterpret_cast<const float4*>(s + c);
+      d[c] = v.x;
+      d[c + 1] = v.y;
+      d[c + 2] = v.z;
+      d[c + 3] = v.w;
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < N; c++) d[c] = s[c];
+  }
+}
+
 // near field: U-list, direct W and X entries; grid (evaluator leaves, RHS blocks).
 // For the double-layer kernels (source normal, NRM) the offsets are formed from
 // hi/lo FP32 pairs of the box-centred coordinates, (x_hi - y_hi) + (x_lo - y_lo):
@@ -104,10 +139,11 @@ __global__ void __launch_bounds__(MX_THREADS)
                  int64_t denStride, const double* __restrict__ trg, const double* __restrict__ ctr,
                  double* __restrict__ val, int64_t valStride, int nrhs, float mu, float ve) {
   constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD, NRM = KTraits<KT>::NRM;
-  __shared__ float sPos[MX_TILE * 3];
-  __shared__ float sPosLo[NRM ? MX_TILE * 3 : 1];
-  __shared__ float sNrm[NRM ? MX_TILE * 3 : 1];
-  __shared__ float sDen[MX_TILE * SD * KB];
+  constexpr int MX_TILE = mx_tile<SD * KB, NRM != 0>();
+  __shared__ float4 sPos[MX_TILE];
+  __shared__ float4 sPosLo[NRM ? MX_TILE : 1];
+  __shared__ float4 sNrm[NRM ? MX_TILE : 1];
+  __shared__ __align__(16) float sDen[MX_TILE * SD * KB];
   __shared__ int64_t eBeg[MX_MAXE];
   __shared__ int32_t ePre[MX_MAXE + 1];
   __shared__ double sRed[MX_THREADS * TD * KB];
@@ -118,7 +154,7 @@ __global__ void __launch_bounds__(MX_THREADS)
   const int64_t e0 = ptr[row], e1 = ptr[row + 1];
   const double cx = ctr[3 * g], cy = ctr[3 * g + 1], cz = ctr[3 * g + 2];
   const int tid = threadIdx.x;
-  const int TG = tn <= 32 ? 32 : (tn <= 64 ? 64 : 128);
+  const int TG = mx_group(tn);
   const int S = MX_THREADS / TG;
   const int tl = tid % TG, sp = tid / TG;
   for (int64_t t0 = 0; t0 < tn; t0 += TG) {
@@ -148,16 +184,10 @@ __global__ void __launch_bounds__(MX_THREADS)
         for (int i = tid; i < cnt; i += MX_THREADS) {
           const int64_t s = entry_source(base + i, ne, eBeg, ePre);
           const double dx = src[3 * s] - cx, dy = src[3 * s + 1] - cy, dz = src[3 * s + 2] - cz;
-          sPos[3 * i] = (float)dx;
-          sPos[3 * i + 1] = (float)dy;
-          sPos[3 * i + 2] = (float)dz;
+          sPos[i] = make_float4((float)dx, (float)dy, (float)dz, 0.f);
           if (NRM) {
-            sPosLo[3 * i] = (float)(dx - (float)dx);
-            sPosLo[3 * i + 1] = (float)(dy - (float)dy);
-            sPosLo[3 * i + 2] = (float)(dz - (float)dz);
-            sNrm[3 * i] = (float)nrm[3 * s];
-            sNrm[3 * i + 1] = (float)nrm[3 * s + 1];
-            sNrm[3 * i + 2] = (float)nrm[3 * s + 2];
+            sPosLo[i] = make_float4((float)(dx - (float)dx), (float)(dy - (float)dy), (float)(dz - (float)dz), 0.f);
+            sNrm[i] = make_float4((float)nrm[3 * s], (float)nrm[3 * s + 1], (float)nrm[3 * s + 2], 0.f);
           }
 #pragma unroll
           for (int r = 0; r < KB; r++)
@@ -172,14 +202,21 @@ __global__ void __launch_bounds__(MX_THREADS)
 #pragma unroll
           for (int c = 0; c < TD * KB; c++) part[c] = 0.f;
           for (int i = sp; i < cnt; i += S) {
-            float ox = tx - sPos[3 * i], oy = ty - sPos[3 * i + 1], oz = tz - sPos[3 * i + 2];
+            const float4 q = sPos[i];
+            float ox = tx - q.x, oy = ty - q.y, oz = tz - q.z;
+            float nv[3] = {0.f, 0.f, 0.f};
             if (NRM) {
-              ox += txl - sPosLo[3 * i];
-              oy += tyl - sPosLo[3 * i + 1];
-              oz += tzl - sPosLo[3 * i + 2];
+              const float4 ql = sPosLo[i], qn = sNrm[i];
+              ox += txl - ql.x;
+              oy += tyl - ql.y;
+              oz += tzl - ql.z;
+              nv[0] = qn.x;
+              nv[1] = qn.y;
+              nv[2] = qn.z;
             }
-            kaccum_multi<KT, KB, float, float>(ox, oy, oz, NRM ? &sNrm[3 * i] : nullptr, &sDen[i * KB * SD], part, mu,
-                                               ve);
+            float d[KB * SD];
+            mx_den<KB * SD>(&sDen[i * KB * SD], d);
+            kaccum_multi<KT, KB, float, float>(ox, oy, oz, NRM ? nv : nullptr, d, part, mu, ve);
           }
 #pragma unroll
           for (int c = 0; c < TD * KB; c++) acc[c] += (double)part[c];
@@ -200,10 +237,10 @@ __global__ void __launch_bounds__(MX_THREADS)
             const double* __restrict__ samDE, int nDE, const float* __restrict__ uden,
             const float* __restrict__ dden, int64_t rhsStrideU, int64_t rhsStrideD,
             const int64_t* __restrict__ trgBeg, const int64_t* __restrict__ trgCnt, const double* __restrict__ trg,
-            double* __restrict__ val, int64_t valStride, int nrhs, float mu, float ve) {
+            double* __restrict__ val, int64_t valStride, int nrhs, float mu, float ve, int gmin) {
   constexpr int SD = KTraits<KM>::SD, TD = KTraits<KM>::TD;
-  __shared__ float sPos[MX_TILE * 3];
-  __shared__ float sDen[MX_TILE * SD * KB];
+  __shared__ float4 sPos[MX_TILE];
+  __shared__ __align__(16) float sDen[MX_TILE * SD * KB];
   __shared__ double sRed[MX_THREADS * TD * KB];
   const int row = blockIdx.x;
   const int rhs0 = blockIdx.y * KB;
@@ -211,7 +248,7 @@ __global__ void __launch_bounds__(MX_THREADS)
   const int64_t tb = trgBeg[g], tn = trgCnt[g];
   const double gx = ctr[3 * g], gy = ctr[3 * g + 1], gz = ctr[3 * g + 2];
   const int tid = threadIdx.x;
-  const int TG = tn <= 32 ? 32 : (tn <= 64 ? 64 : 128);
+  const int TG = mx_group(tn, gmin);
   const int S = MX_THREADS / TG;
   const int tl = tid % TG, sp = tid / TG;
   const int own = (useOwn && depth[g] >= 2) ? 1 : 0;
@@ -242,9 +279,8 @@ __global__ void __launch_bounds__(MX_THREADS)
         __syncthreads();
         for (int i = tid; i < cnt; i += MX_THREADS) {
           const int j = base + i;
-          sPos[3 * i] = (float)(ox + r * sam[3 * j]);
-          sPos[3 * i + 1] = (float)(oy + r * sam[3 * j + 1]);
-          sPos[3 * i + 2] = (float)(oz + r * sam[3 * j + 2]);
+          sPos[i] = make_float4((float)(ox + r * sam[3 * j]), (float)(oy + r * sam[3 * j + 1]),
+                                (float)(oz + r * sam[3 * j + 2]), 0.f);
 #pragma unroll
           for (int q = 0; q < KB; q++)
 #pragma unroll
@@ -256,9 +292,12 @@ __global__ void __launch_bounds__(MX_THREADS)
           float part[TD * KB];
 #pragma unroll
           for (int c = 0; c < TD * KB; c++) part[c] = 0.f;
-          for (int i = sp; i < cnt; i += S)
-            kaccum_multi<KM, KB, float, float>(tx - sPos[3 * i], ty - sPos[3 * i + 1], tz - sPos[3 * i + 2], nullptr,
-                                               &sDen[i * KB * SD], part, mu, ve);
+          for (int i = sp; i < cnt; i += S) {
+            const float4 q = sPos[i];
+            float d[KB * SD];
+            mx_den<KB * SD>(&sDen[i * KB * SD], d);
+            kaccum_multi<KM, KB, float, float>(tx - q.x, ty - q.y, tz - q.z, nullptr, d, part, mu, ve);
+          }
 #pragma unroll
           for (int c = 0; c < TD * KB; c++) acc[c] += (double)part[c];
         }
@@ -269,9 +308,12 @@ __global__ void __launch_bounds__(MX_THREADS)
 }
 
 // point sources -> check surface of a box (S2M onto UC, S2L onto DC), FP32
-// out.  One thread per surface point (a CTA of MX_SURF threads, up to 512
-// points: np <= 8).
+// out.  One thread per surface point: a CTA of mx_surf_threads(nSurf) (the
+// surface rounded up to whole warps, at most 512 points: np <= 8).  With no
+// entry list (ptr == nullptr) the sources are the box's own, one contiguous
+// run, and need no prefix table.
 constexpr int MX_SURF = 512;
+static inline int mx_surf_threads(int nSurf) { return std::min(MX_SURF, (nSurf + 31) / 32 * 32); }
 template <int KT, int KB>
 __global__ void __launch_bounds__(MX_SURF)
     k_src2surf32(const int32_t* __restrict__ rows, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
@@ -281,9 +323,9 @@ __global__ void __launch_bounds__(MX_SURF)
                  const double* __restrict__ sam, int nSurf, float* __restrict__ out, int64_t ldo,
                  int64_t outRhsStride, int nrhs, float mu, float ve) {
   constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD, NRM = KTraits<KT>::NRM;
-  __shared__ float sPos[MX_TILE * 3];
-  __shared__ float sNrm[NRM ? MX_TILE * 3 : 1];
-  __shared__ float sDen[MX_TILE * SD * KB];
+  __shared__ float4 sPos[MX_TILE];
+  __shared__ float4 sNrm[NRM ? MX_TILE : 1];
+  __shared__ __align__(16) float sDen[MX_TILE * SD * KB];
   __shared__ int64_t eBeg[MX_MAXE];
   __shared__ int32_t ePre[MX_MAXE + 1];
   const int row = blockIdx.x;
@@ -295,26 +337,33 @@ __global__ void __launch_bounds__(MX_SURF)
   const float px = act ? (float)(r * sam[3 * tid]) : 0.f;
   const float py = act ? (float)(r * sam[3 * tid + 1]) : 0.f;
   const float pz = act ? (float)(r * sam[3 * tid + 2]) : 0.f;
-  double acc[TD * KB];
+  float acc[TD * KB];  // the check surface is FP32: one FP32 sum over all tiles
 #pragma unroll
-  for (int c = 0; c < TD * KB; c++) acc[c] = 0.0;
+  for (int c = 0; c < TD * KB; c++) acc[c] = 0.f;
   const int64_t e0 = ptr ? ptr[row] : 0, e1 = ptr ? ptr[row + 1] : 1;
   for (int64_t ec = e0; ec < e1; ec += MX_MAXE) {
     const int ne = (int)min((int64_t)MX_MAXE, e1 - ec);
-    const int total = load_entries(ptr ? idx : nullptr, ec, ne, g, srcBeg, srcCnt, eBeg, ePre);
+    int total;
+    if (ptr) {
+      total = load_entries(idx, ec, ne, g, srcBeg, srcCnt, eBeg, ePre);
+    } else {
+      __syncthreads();
+      if (tid == 0) {
+        eBeg[0] = srcBeg[g];
+        ePre[0] = 0;
+        ePre[1] = (int32_t)srcCnt[g];
+      }
+      __syncthreads();
+      total = ePre[1];
+    }
     for (int base = 0; base < total; base += MX_TILE) {
       const int cnt = min(MX_TILE, total - base);
       __syncthreads();
       for (int i = tid; i < cnt; i += blockDim.x) {
         const int64_t s = entry_source(base + i, ne, eBeg, ePre);
-        sPos[3 * i] = (float)(src[3 * s] - cx);
-        sPos[3 * i + 1] = (float)(src[3 * s + 1] - cy);
-        sPos[3 * i + 2] = (float)(src[3 * s + 2] - cz);
-        if (NRM) {
-          sNrm[3 * i] = (float)nrm[3 * s];
-          sNrm[3 * i + 1] = (float)nrm[3 * s + 1];
-          sNrm[3 * i + 2] = (float)nrm[3 * s + 2];
-        }
+        sPos[i] = make_float4((float)(src[3 * s] - cx), (float)(src[3 * s + 1] - cy), (float)(src[3 * s + 2] - cz),
+                              0.f);
+        if (NRM) sNrm[i] = make_float4((float)nrm[3 * s], (float)nrm[3 * s + 1], (float)nrm[3 * s + 2], 0.f);
 #pragma unroll
         for (int q = 0; q < KB; q++)
 #pragma unroll
@@ -324,14 +373,19 @@ __global__ void __launch_bounds__(MX_SURF)
       }
       __syncthreads();
       if (act) {
-        float part[TD * KB];
-#pragma unroll
-        for (int c = 0; c < TD * KB; c++) part[c] = 0.f;
-        for (int i = 0; i < cnt; i++)
-          kaccum_multi<KT, KB, float, float>(px - sPos[3 * i], py - sPos[3 * i + 1], pz - sPos[3 * i + 2],
-                                             NRM ? &sNrm[3 * i] : nullptr, &sDen[i * KB * SD], part, mu, ve);
-#pragma unroll
-        for (int c = 0; c < TD * KB; c++) acc[c] += (double)part[c];
+        for (int i = 0; i < cnt; i++) {
+          const float4 q = sPos[i];
+          float nv[3] = {0.f, 0.f, 0.f};
+          if (NRM) {
+            const float4 qn = sNrm[i];
+            nv[0] = qn.x;
+            nv[1] = qn.y;
+            nv[2] = qn.z;
+          }
+          float d[KB * SD];
+          mx_den<KB * SD>(&sDen[i * KB * SD], d);
+          kaccum_multi<KT, KB, float, float>(px - q.x, py - q.y, pz - q.z, NRM ? nv : nullptr, d, acc, mu, ve);
+        }
       }
     }
   }
@@ -341,7 +395,7 @@ __global__ void __launch_bounds__(MX_SURF)
       if (rhs0 + q >= nrhs) break;
 #pragma unroll
       for (int c = 0; c < TD; c++)
-        out[(rhs0 + q) * outRhsStride + (int64_t)g * ldo + (int64_t)tid * TD + c] += (float)acc[q * TD + c];
+        out[(rhs0 + q) * outRhsStride + (int64_t)g * ldo + (int64_t)tid * TD + c] += acc[q * TD + c];
     }
 }
 
@@ -589,6 +643,12 @@ __device__ __forceinline__ void r8_store(float2* p, const float2 (&v)[8]) {
 #pragma unroll
   for (int i = 0; i < 4; i++) q[i] = make_float4(v[2 * i].x, v[2 * i].y, v[2 * i + 1].x, v[2 * i + 1].y);
 }
+// (-1)^H v, H = NP / 2: the factor between the half-length partial sums of
+// outputs k and k + NP of a forward line transform
+template <int NP>
+__device__ __forceinline__ float2 r8_half_sign(float2 v) {
+  return (FftDims<NP>::H & 1) ? make_float2(-v.x, -v.y) : v;
+}
 template <int NP>
 __device__ __forceinline__ void r8_twiddles(float2* twb) {
   using F = FftDims<NP>;
@@ -648,22 +708,27 @@ __global__ void __launch_bounds__(256)
     }
   }
   __syncthreads();
-  // y pass: a thread owns one y line (kx, zb) of one right-hand side and all N ky outputs
+  // y pass: a thread owns one y line (kx, zb) of one right-hand side and all N
+  // ky outputs.  The twiddle of output k + NP is that of k times (-1)^(b + H)
+  // (W^NP = -1), so the even- and odd-b partial sums pe, po of output k give
+  // X[k] = pe + po and X[k + NP] = (-1)^H (pe - po): NP x NP products a line.
   for (int i = tid; i < NH * NP * 8; i += blockDim.x) {
     const int kx = i % NH, zb = (i / NH) % NP, r = i / (NH * NP);
     float2 c[NP];
 #pragma unroll
     for (int yb = 0; yb < NP; yb++) c[yb] = X1[r * S1 + (zb * NP + yb) * NH + kx];
 #pragma unroll 1
-    for (int ky = 0; ky < N; ky++) {
-      float2 s = make_float2(0.f, 0.f);
+    for (int ky = 0; ky < NP; ky++) {
+      float2 pe = make_float2(0.f, 0.f), po = pe;
 #pragma unroll
       for (int yb = 0; yb < NP; yb++) {
         const float2 t = cmul(c[yb], twb[ky * NP + yb]);
-        s.x += t.x;
-        s.y += t.y;
+        float2& a = (yb & 1) ? po : pe;
+        a.x += t.x;
+        a.y += t.y;
       }
-      X2[r * S2 + (zb * N + ky) * NH + kx] = s;
+      X2[r * S2 + (zb * N + ky) * NH + kx] = make_float2(pe.x + po.x, pe.y + po.y);
+      X2[r * S2 + (zb * N + ky + NP) * NH + kx] = r8_half_sign<NP>(make_float2(pe.x - po.x, pe.y - po.y));
     }
   }
   __syncthreads();
@@ -676,15 +741,17 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int zb = 0; zb < NP; zb++) c[zb] = X2[r * S2 + (zb * N + ky) * NH + kx];
 #pragma unroll 1
-    for (int kz = 0; kz < N; kz++) {
-      float2 s = make_float2(0.f, 0.f);
+    for (int kz = 0; kz < NP; kz++) {  // outputs kz and kz + NP, as in the y pass
+      float2 pe = make_float2(0.f, 0.f), po = pe;
 #pragma unroll
       for (int zb = 0; zb < NP; zb++) {
         const float2 t = cmul(c[zb], twb[kz * NP + zb]);
-        s.x += t.x;
-        s.y += t.y;
+        float2& a = (zb & 1) ? po : pe;
+        a.x += t.x;
+        a.y += t.y;
       }
-      out[((int64_t)(kz * N + ky) * NH + kx) * 8 + r] = s;
+      out[((int64_t)(kz * N + ky) * NH + kx) * 8 + r] = make_float2(pe.x + po.x, pe.y + po.y);
+      out[((int64_t)((kz + NP) * N + ky) * NH + kx) * 8 + r] = r8_half_sign<NP>(make_float2(pe.x - po.x, pe.y - po.y));
     }
   }
 }
@@ -754,18 +821,22 @@ __global__ void __launch_bounds__(256)
   }
   __syncthreads();
   // z pass, band outputs only: a thread owns one z line (kx, ky) of one
-  // right-hand side; right-hand side fastest, matching the staged layout
+  // right-hand side; right-hand side fastest, matching the staged layout.
+  // Inputs kz and kz + NP share the twiddle up to (-1)^(b + H), so output b
+  // takes S = X[kz] + X[kz + NP] (b + H even) or D = X[kz] - X[kz + NP]
+  // (b + H odd) against the twiddle of kz: NP x NP products a line.
   for (int i = tid; i < NH * N * 8; i += blockDim.x) {
     const int r = i & 7, kx = (i >> 3) % NH, ky = (i >> 3) / NH;
     float2 s[NP];
 #pragma unroll
     for (int zb = 0; zb < NP; zb++) s[zb] = make_float2(0.f, 0.f);
 #pragma unroll 1
-    for (int kz = 0; kz < N; kz++) {
-      const float2 c = X0[((kz * N + ky) * NH + kx) * 8 + r];
+    for (int kz = 0; kz < NP; kz++) {
+      const float2 c0 = X0[((kz * N + ky) * NH + kx) * 8 + r], c1 = X0[(((kz + NP) * N + ky) * NH + kx) * 8 + r];
+      const float2 cs = make_float2(c0.x + c1.x, c0.y + c1.y), cd = make_float2(c0.x - c1.x, c0.y - c1.y);
 #pragma unroll
       for (int zb = 0; zb < NP; zb++) {
-        const float2 t = cmulc(c, twb[kz * NP + zb]);
+        const float2 t = cmulc(((zb + F::H) & 1) ? cd : cs, twb[kz * NP + zb]);
         s[zb].x += t.x;
         s[zb].y += t.y;
       }
@@ -781,11 +852,12 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int yb = 0; yb < NP; yb++) s[yb] = make_float2(0.f, 0.f);
 #pragma unroll 1
-    for (int ky = 0; ky < N; ky++) {
-      const float2 c = Y2[r * S2 + (zb * N + ky) * NH + kx];
+    for (int ky = 0; ky < NP; ky++) {  // inputs ky and ky + NP, as in the z pass
+      const float2 c0 = Y2[r * S2 + (zb * N + ky) * NH + kx], c1 = Y2[r * S2 + (zb * N + ky + NP) * NH + kx];
+      const float2 cs = make_float2(c0.x + c1.x, c0.y + c1.y), cd = make_float2(c0.x - c1.x, c0.y - c1.y);
 #pragma unroll
       for (int yb = 0; yb < NP; yb++) {
-        const float2 t = cmulc(c, twb[ky * NP + yb]);
+        const float2 t = cmulc(((yb + F::H) & 1) ? cd : cs, twb[ky * NP + yb]);
         s[yb].x += t.x;
         s[yb].y += t.y;
       }
@@ -954,10 +1026,12 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
 }
 
 // one pass over a chunk of kc right-hand sides, KB of them per launch block
+// overlap: run the near field and the W list on D.side (an untimed pass; a
+// timed one keeps every stage on the main stream so the events bracket it)
 template <int KT, int KB>
-static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats* ls) {
+static void run_mixed(const Plan& P, DevState& D, int kc, int mask, bool overlap, LaunchStats* ls) {
   if constexpr (KTraits<KT>::TD != 1 && KB > 4) {
-    run_mixed<KT, 4>(P, D, kc, mask, ls);  // pick_kb never asks for this
+    run_mixed<KT, 4>(P, D, kc, mask, overlap, ls);  // pick_kb never asks for this
     return;
   }
   cudaStream_t st = D.stream;
@@ -990,8 +1064,13 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
                                          kc, rows, D.chd, xChild, yChild, X, ldx, xR, W,
                                          D.gemmPath == 2 ? nullptr : wt.p, wt.ld, Y, ldy, yR, K, N, gx, gy, beta);
   };
+  const bool ovl = overlap && D.side;
+  if (ovl) {  // fork: the densities are gathered and the target values cleared
+    cudaEventRecord(D.evFork, st);
+    cudaStreamWaitEvent(D.side, D.evFork, 0);
+  }
   if ((mask & 1) && !P.s2mLeaves.empty()) {
-    k_src2surf32<KT, KB><<<dim3((unsigned)P.s2mLeaves.size(), kb), MX_SURF, 0, st>>>(
+    k_src2surf32<KT, KB><<<dim3((unsigned)P.s2mLeaves.size(), kb), mx_surf_threads(P.nUC), 0, st>>>(
         D.s2mLeaves, nullptr, nullptr, D.srcBeg, D.srcCnt, D.src, D.nrm, D.denK, denStride, D.ctr, D.rad, D.sam[1],
         P.nUC, D.uchk32, uc, nn * uc, kc, mu, ve);
     ls->launches++;
@@ -1012,19 +1091,28 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
     }
   }
   cudaEventRecord(D.ev[EV_UP_GEMM], st);
-  auto near = [&](const int64_t* ptr, const int32_t* idx) {
+  auto near = [&](const int64_t* ptr, const int32_t* idx, cudaStream_t sn) {
     if (nl == 0) return;
-    k_p2p_near32<KT, KB><<<dim3(nl, kb), MX_THREADS, 0, st>>>(D.evtrLeaves, ptr, idx, D.srcBeg, D.srcCnt, D.trgBeg,
+    k_p2p_near32<KT, KB><<<dim3(nl, kb), MX_THREADS, 0, sn>>>(D.evtrLeaves, ptr, idx, D.srcBeg, D.srcCnt, D.trgBeg,
                                                              D.trgCnt, D.src, D.nrm, D.denK, denStride, D.trg, D.ctr,
                                                              D.valK, valStride, kc, mu, ve);
     ls->launches++;
   };
-  if ((mask & 2) && (mask & 8) && (mask & 16)) {
-    near(D.nearPtr, D.nearIdx);
+  auto nearAll = [&](cudaStream_t sn) {
+    if ((mask & 2) && (mask & 8) && (mask & 16)) {
+      near(D.nearPtr, D.nearIdx, sn);
+    } else {
+      if (mask & 2) near(D.nearUPtr, D.nearUIdx, sn);
+      if (mask & 8) near(D.nearWPtr, D.nearWIdx, sn);
+      if (mask & 16) near(D.nearXPtr, D.nearXIdx, sn);
+    }
+  };
+  if (ovl) {  // the up pass is done: the W list (own upward densities) joins the near field
+    nearAll(D.side);
+    cudaEventRecord(D.evUp, st);
+    cudaStreamWaitEvent(D.side, D.evUp, 0);
   } else {
-    if (mask & 2) near(D.nearUPtr, D.nearUIdx);
-    if (mask & 8) near(D.nearWPtr, D.nearWIdx);
-    if (mask & 16) near(D.nearXPtr, D.nearXIdx);
+    nearAll(st);
   }
   cudaEventRecord(D.ev[EV_NEAR], st);
   const int nsrc = (int)P.vSrcNodes.size(), ntrg = (int)P.vTrgNodes.size(), npar = (int)P.vParents.size();
@@ -1085,6 +1173,13 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
         k_m2l_had_pqx2<32, false><<<g1, PQX_THREADS, smem, st>>>(
             npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen32, PqLayout{effDR, P.nEff}, D.m2lT32, D.effVal32,
             PqLayout{effVR, P.nEff}, 1, 0, P.nEff, kc, nrmfc, D.transIdDev);
+      } else if (D.hadW && D.m2lTw32 && D.tune.hadRhsPerThread == 2) {  // 27-product form, 2 RHS a thread
+        const size_t smem = (size_t)W8_OFFS * 27 * W8X2_F * sizeof(float2);
+        cudaFuncSetAttribute(k_m2l_had_w8x2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        dim3 g8((npar + D.tune.hadRows - 1) / D.tune.hadRows, (P.nEff + W8X2_F - 1) / W8X2_F, nblk);
+        k_m2l_had_w8x2<<<g8, PQX_THREADS, smem, st>>>(npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen32,
+                                                       PqLayout{blkDen, (int64_t)P.nEff * 8}, D.m2lTw32, D.effVal32,
+                                                       PqLayout{blkVal, (int64_t)P.nEff * 8}, P.nEff, kc, nrmfc);
       } else if (D.hadW && D.m2lTw32) {  // 27-product form
         const size_t smem = (size_t)W8_OFFS * 27 * 4 * sizeof(float2);
         cudaFuncSetAttribute(k_m2l_had_w8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1147,17 +1242,20 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
     ls->launches++;
   }
   cudaEventRecord(D.ev[EV_M2L_INV], st);
-  auto e2t = [&](int own, int far) {
+  // target groups of at least 8 lanes for L2T (one surface per leaf), 32 for
+  // M2T (many small W-list surfaces per leaf, where narrower groups measured
+  // slower on B200)
+  auto e2t = [&](int own, int far, cudaStream_t se) {
     const int nr = far ? (int)P.farLeaves.size() : (int)P.l2tLeaves.size();
     const int32_t* rows = far ? D.farLeaves : D.l2tLeaves;
     if (nr == 0) return;
     switch (P.mm) {
 #define FMMG_E2T32(KM)                                                                                          \
   case KM:                                                                                                      \
-    k_e2t32<KM, KB><<<dim3(nr, kb), MX_THREADS, 0, st>>>(rows, D.farPtr, D.farIdx, own, far, D.depth, D.ctr,    \
+    k_e2t32<KM, KB><<<dim3(nr, kb), MX_THREADS, 0, se>>>(rows, D.farPtr, D.farIdx, own, far, D.depth, D.ctr,    \
                                                          D.rad, D.sam[0], P.nUE, D.sam[2], P.nDE, D.uden32,     \
                                                          D.dden32, nn * ue, nn * de, D.trgBeg, D.trgCnt, D.trg, \
-                                                         D.valK, valStride, kc, mu, ve);                        \
+                                                         D.valK, valStride, kc, mu, ve, far ? 32 : 8);          \
     break;
       FMMG_E2T32(LAP_S_U)
       FMMG_E2T32(STK_F_U)
@@ -1166,10 +1264,11 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
     }
     ls->launches++;
   };
-  if (mask & 8) e2t(0, 1);
+  if (mask & 8) e2t(0, 1, ovl ? D.side : st);
+  if (ovl) cudaEventRecord(D.evSide, D.side);
   cudaEventRecord(D.ev[EV_M2T], st);
   if ((mask & 16) && !P.s2lNodes.empty()) {
-    k_src2surf32<KT, KB><<<dim3((unsigned)P.s2lNodes.size(), kb), MX_SURF, 0, st>>>(
+    k_src2surf32<KT, KB><<<dim3((unsigned)P.s2lNodes.size(), kb), mx_surf_threads(P.nDC), 0, st>>>(
         D.s2lNodes, D.s2lPtr, D.s2lIdx, D.srcBeg, D.srcCnt, D.src, D.nrm, D.denK, denStride, D.ctr, D.rad, D.sam[3],
         P.nDC, D.dchk32, dc, nn * dc, kc, mu, ve);
     ls->launches++;
@@ -1190,7 +1289,8 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, LaunchStats*
     }
   }
   cudaEventRecord(D.ev[EV_DN_GEMM], st);
-  if (mask & 32) e2t(1, 0);
+  if (ovl) cudaStreamWaitEvent(st, D.evSide, 0);  // join: the target values are complete but for L2T
+  if (mask & 32) e2t(1, 0, st);
   cudaEventRecord(D.ev[EV_L2T], st);
 }
 
@@ -1252,7 +1352,7 @@ std::string dev_evaluate_mixed(const Plan& P, DevState& D, const double* dDen, d
     FMMG_CK(cudaMemsetAsync(D.dden32, 0, sizeof(float) * kk * P.nn * de, st));
     cudaEventRecord(D.ev[EV_PREP], st);
     const int KBv = pick_kb(kk, P.td);
-#define FMMG_RUN_KB(KBC) FMMG_DISPATCH_KT(P.o.kt, KT, run_mixed<KT, KBC>(P, D, kk, mask, ls))
+#define FMMG_RUN_KB(KBC) FMMG_DISPATCH_KT(P.o.kt, KT, run_mixed<KT, KBC>(P, D, kk, mask, !timed, ls))
     if (KBv == 8) { FMMG_RUN_KB(8); }
     else if (KBv == 4) { FMMG_RUN_KB(4); }
     else if (KBv == 2) { FMMG_RUN_KB(2); }

@@ -560,8 +560,13 @@ static std::string dput(DevState& D, T*& dst, const std::vector<T>& v) {
 void dev_free(DevState& D) {
   for (void* p : D.allocs) cudaFree(p);
   D.allocs.clear();
-  if (D.evReady)
+  if (D.evReady) {
     for (auto& e : D.ev) cudaEventDestroy(e);
+    for (cudaEvent_t e : {D.evFork, D.evUp, D.evSide}) cudaEventDestroy(e);
+    if (D.side) cudaStreamDestroy(D.side);
+    D.side = nullptr;
+    D.evFork = D.evUp = D.evSide = nullptr;
+  }
   D.evReady = false;
   D.uc2ue = D.m2m = D.dc2de = D.l2l = nullptr;
   D.m2lT = nullptr;
@@ -747,6 +752,8 @@ std::string dev_upload(const Plan& P, DevState& D, const double* src, const doub
   }
   if (!D.evReady) {
     for (auto& e : D.ev) FMMG_CK(cudaEventCreate(&e));
+    FMMG_CK(cudaStreamCreateWithFlags(&D.side, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&D.evFork, &D.evUp, &D.evSide}) FMMG_CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     D.evReady = true;
   }
   return std::string();

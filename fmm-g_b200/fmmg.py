@@ -335,13 +335,15 @@ class FMM3d:
 
     def tuning(self, values=None):
         """Current launch shapes, or install `values` (a dict as returned)."""
-        v = (ctypes.c_int * 3)()
-        keys = ("had_rows_fp32", "had_rows_fp64", "gemm_split_ctas_per_sm")
+        keys = ("had_rows_fp32", "had_rows_fp64", "gemm_split_ctas_per_sm", "had_fp32_rhs_per_thread")
+        v = (ctypes.c_int * len(keys))()
         if values is not None:
+            self._chk(lib().fmmg_tuning(self.h, v, len(keys), 0))
             for i, key in enumerate(keys):
-                v[i] = int(values[key])
-            self._chk(lib().fmmg_tuning(self.h, v, 3, 1))
-        self._chk(lib().fmmg_tuning(self.h, v, 3, 0))
+                if key in values:
+                    v[i] = int(values[key])
+            self._chk(lib().fmmg_tuning(self.h, v, len(keys), 1))
+        self._chk(lib().fmmg_tuning(self.h, v, len(keys), 0))
         return dict(zip(keys, list(v)))
 
     def graph_state(self):

@@ -224,7 +224,9 @@ fmmg_status fmmg_device_error(fmmg_handle* h, int* flag);
 fmmg_status fmmg_autotune(fmmg_handle* h, int k, int precision, const double* d_src_den, double* d_trg_val,
                           int reps, double* best_ms);
 /* vals[0..2] = Hadamard rows per CTA (FP32 form), Hadamard rows per CTA (FP64
- * form), split-K threshold (CTAs per SM); set != 0 installs them, else reads. */
+ * form), split-K threshold (CTAs per SM); with n >= 4, vals[3] = right-hand
+ * sides per thread of the FP32 27-product Hadamard (1 or 2).  set != 0
+ * installs them (FMMG_INVALID_ARG for values out of range), else reads. */
 fmmg_status fmmg_tuning(fmmg_handle* h, int* vals, int n, int set);
 
 /* Host-plan introspection (valid after setup, also with device < 0).

@@ -163,3 +163,30 @@ def test_mixed_rhs_blocks_at_other_np(np_):
     V = out.cpu().numpy()
     for r in range(k):
         assert rel_l2(V[r], _mixed_eval(lib, D[r])) <= 1e-6
+
+
+@pytest.mark.parametrize("k", [5, 8, 12])
+def test_hadamard_two_rhs_per_thread_identical(k):
+    """The 27-product Hadamard with two right-hand sides per thread does, per
+    right-hand side, the same operations in the same order as the kernel with
+    one per thread: the evaluates agree bit for bit (odd k leaves a lane with
+    one right-hand side, k = 12 spans two blocks of 8)."""
+    import torch
+    rng = np.random.default_rng(77 + k)
+    n = 40000
+    src = W.sphere_clusters(n, rng)
+    lib = fmmg.FMM3d(111, np_=6, pts_max=64)
+    lib.setup(src)
+    D = torch.from_numpy(rng.normal(size=(k, n))).cuda()
+    outs = []
+    for per in (1, 2):
+        assert lib.tuning({"had_fp32_rhs_per_thread": per})["had_fp32_rhs_per_thread"] == per
+        out = torch.zeros(k, n, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        lib.evaluate_device(D, out, k, fmmg.PREC_MIXED)
+        lib.sync()
+        assert lib.device_error() == 0
+        outs.append(out.cpu().numpy())
+    assert np.array_equal(outs[0], outs[1])
+    with pytest.raises(fmmg.FmmgError):
+        lib.tuning({"had_fp32_rhs_per_thread": 3})
