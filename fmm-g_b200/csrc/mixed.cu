@@ -311,7 +311,8 @@ __global__ void __launch_bounds__(MX_THREADS)
 // out.  One thread per surface point: a CTA of mx_surf_threads(nSurf) (the
 // surface rounded up to whole warps, at most 512 points: np <= 8).  With no
 // entry list (ptr == nullptr) the sources are the box's own, one contiguous
-// run, and need no prefix table.
+// run, and need no prefix table.  assign: store the sums (S2M, the only
+// writer of a leaf's check surface) instead of adding them (S2L).
 constexpr int MX_SURF = 512;
 static inline int mx_surf_threads(int nSurf) { return std::min(MX_SURF, (nSurf + 31) / 32 * 32); }
 template <int KT, int KB>
@@ -321,7 +322,7 @@ __global__ void __launch_bounds__(MX_SURF)
                  const double* __restrict__ src, const double* __restrict__ nrm, const double* __restrict__ den,
                  int64_t denStride, const double* __restrict__ ctr, const double* __restrict__ rad,
                  const double* __restrict__ sam, int nSurf, float* __restrict__ out, int64_t ldo,
-                 int64_t outRhsStride, int nrhs, float mu, float ve) {
+                 int64_t outRhsStride, int nrhs, float mu, float ve, int assign) {
   constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD, NRM = KTraits<KT>::NRM;
   __shared__ float4 sPos[MX_TILE];
   __shared__ float4 sNrm[NRM ? MX_TILE : 1];
@@ -394,8 +395,10 @@ __global__ void __launch_bounds__(MX_SURF)
     for (int q = 0; q < KB; q++) {
       if (rhs0 + q >= nrhs) break;
 #pragma unroll
-      for (int c = 0; c < TD; c++)
-        out[(rhs0 + q) * outRhsStride + (int64_t)g * ldo + (int64_t)tid * TD + c] += acc[q * TD + c];
+      for (int c = 0; c < TD; c++) {
+        float* o = &out[(rhs0 + q) * outRhsStride + (int64_t)g * ldo + (int64_t)tid * TD + c];
+        *o = assign ? acc[q * TD + c] : *o + acc[q * TD + c];
+      }
     }
 }
 
@@ -927,6 +930,9 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
     // grow: the old buffers stay in D.allocs until the handle is freed
     FMMG_TRY(dalloc(D, D.uchk32, (size_t)kc * P.nn * uc));
     FMMG_TRY(dalloc(D, D.uden32, (size_t)kc * P.nn * ue));
+    // rows of nodes without sources are read (M2M children, V and W sources)
+    // but never written: zero once here
+    FMMG_CK(cudaMemsetAsync(D.uden32, 0, sizeof(float) * kc * P.nn * ue, D.stream));
     FMMG_TRY(dalloc(D, D.dchk32, (size_t)kc * P.nn * dc));
     FMMG_TRY(dalloc(D, D.dden32, (size_t)kc * P.nn * de));
     const size_t kc8 = (size_t)(kc + 7) / 8 * 8;  // the scalar k >= 2 layout stores blocks of 8
@@ -1072,7 +1078,7 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, bool overlap
   if ((mask & 1) && !P.s2mLeaves.empty()) {
     k_src2surf32<KT, KB><<<dim3((unsigned)P.s2mLeaves.size(), kb), mx_surf_threads(P.nUC), 0, st>>>(
         D.s2mLeaves, nullptr, nullptr, D.srcBeg, D.srcCnt, D.src, D.nrm, D.denK, denStride, D.ctr, D.rad, D.sam[1],
-        P.nUC, D.uchk32, uc, nn * uc, kc, mu, ve);
+        P.nUC, D.uchk32, uc, nn * uc, kc, mu, ve, 1);
     ls->launches++;
   }
   cudaEventRecord(D.ev[EV_S2M], st);
@@ -1270,7 +1276,7 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, bool overlap
   if ((mask & 16) && !P.s2lNodes.empty()) {
     k_src2surf32<KT, KB><<<dim3((unsigned)P.s2lNodes.size(), kb), mx_surf_threads(P.nDC), 0, st>>>(
         D.s2lNodes, D.s2lPtr, D.s2lIdx, D.srcBeg, D.srcCnt, D.src, D.nrm, D.denK, denStride, D.ctr, D.rad, D.sam[3],
-        P.nDC, D.dchk32, dc, nn * dc, kc, mu, ve);
+        P.nDC, D.dchk32, dc, nn * dc, kc, mu, ve, 0);
     ls->launches++;
   }
   cudaEventRecord(D.ev[EV_S2L], st);
@@ -1345,11 +1351,16 @@ std::string dev_evaluate_mixed(const Plan& P, DevState& D, const double* dDen, d
     k_gather_den_k<<<(unsigned)((ns + 255) / 256), 256, 0, st>>>(ns, P.sd, kk, denStride, D.srcPerm,
                                                                   dDen + r0 * denStride, D.denK);
     ls->launches++;
+    // Cleared per pass: the accumulated target values and downward check
+    // potentials.  Every upward check row that C2E reads is assigned first
+    // (S2M for a leaf with sources, M2M for a parent), the upward densities of
+    // the nodes with sources are assigned by C2E and the others stay zero from
+    // allocation, and every downward density that L2L or L2T reads is assigned
+    // by C2E at its level before; with the upward stage masked off the
+    // densities are cleared so the V and W stages see zeros.
     FMMG_CK(cudaMemsetAsync(D.valK, 0, sizeof(double) * kk * valStride, st));
-    FMMG_CK(cudaMemsetAsync(D.uchk32, 0, sizeof(float) * kk * P.nn * uc, st));
-    FMMG_CK(cudaMemsetAsync(D.uden32, 0, sizeof(float) * kk * P.nn * ue, st));
     FMMG_CK(cudaMemsetAsync(D.dchk32, 0, sizeof(float) * kk * P.nn * dc, st));
-    FMMG_CK(cudaMemsetAsync(D.dden32, 0, sizeof(float) * kk * P.nn * de, st));
+    if (!(mask & 1)) FMMG_CK(cudaMemsetAsync(D.uden32, 0, sizeof(float) * kk * P.nn * ue, st));
     cudaEventRecord(D.ev[EV_PREP], st);
     const int KBv = pick_kb(kk, P.td);
 #define FMMG_RUN_KB(KBC) FMMG_DISPATCH_KT(P.o.kt, KT, run_mixed<KT, KBC>(P, D, kk, mask, !timed, ls))
