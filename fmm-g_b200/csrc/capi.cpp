@@ -791,7 +791,10 @@ fmmg_status fmmg_operator(fmmg_handle* h, int which, int idx, double* get, const
       return fail(h, FMMG_INVALID_ARG, "operator id");
   }
   if (count) *count = n;
-  if (set) h->opsDirty = true;
+  if (set) {
+    h->opsDirty = true;
+    if (which == 0 || which == 2) P.refactor_c2e(which);  // the FP32 pass applies the pinv factored
+  }
   return FMMG_OK;
 }
 

@@ -52,7 +52,7 @@ struct DevState {
   int32_t *s2lNodes = nullptr; int64_t *s2lPtr = nullptr; int32_t *s2lIdx = nullptr;
   int32_t *s2mLeaves = nullptr;
   int32_t *levelRows = nullptr;  // concatenated per-level row lists
-  std::vector<int64_t> offUpC2E, offUpM2M, offDnL2L, offDnC2E;  // host offsets into levelRows, size maxDepth+2
+  std::vector<int64_t> offUpC2E, offUpM2M, offDnL2L, offDnC2E, offUpLeaf;  // host offsets into levelRows, size maxDepth+2
   int32_t *vParents = nullptr; int64_t *vPtr = nullptr; int32_t *vIdx = nullptr; int8_t *vOff = nullptr;
   int32_t *vSrcSlot = nullptr, *vTrgSlot = nullptr, *vSrcNodes = nullptr, *vTrgNodes = nullptr;
   int64_t *vTrgPtr = nullptr, *vSrcPtr = nullptr;   // expanded V-lists per target / source slot
@@ -67,7 +67,7 @@ struct DevState {
   // mixed-precision work arrays and FP32 operator copies (allocated on first use)
   float *uchk32 = nullptr, *uden32 = nullptr, *dchk32 = nullptr, *dden32 = nullptr;
   float2 *effDen32 = nullptr, *effVal32 = nullptr;
-  float *uc2ue32 = nullptr, *m2m32 = nullptr, *dc2de32 = nullptr, *l2l32 = nullptr;
+  float* l2l32 = nullptr;
   float *upF1 = nullptr, *upF2 = nullptr, *dnF1 = nullptr, *dnF2 = nullptr;  // factored pinvs
   float *upT32 = nullptr, *dnT32 = nullptr;  // [k][nn][kUp|kDn] intermediate of the factored C2E
   float2* m2lT32 = nullptr;
@@ -107,8 +107,12 @@ struct DevState {
   struct OpT {
     float* p = nullptr;
     int ld = 0;
+    size_t cap = 0;  // allocated floats
   };
-  OpT tM2M, tL2L, tUpF1, tUpF2, tDnF1, tDnF2;
+  OpT tL2L, tUpF1, tUpF2, tDnF1, tDnF2, tM2MUp;
+  // C2E up x M2M folded (Plan fold_c2e_m2m), FP32 [ue][8 ue]: the FP32 pass
+  // takes a parent's upward density from its children's in one product
+  float* m2mUp32 = nullptr;
   int* devErr = nullptr;  // set by kernels whose bounded waits gave up
   float adjMs = 0.f;
   // dense check scratch

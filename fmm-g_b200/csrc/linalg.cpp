@@ -163,6 +163,72 @@ int pinv_factors(int m, int n, const double* A, double eps, std::vector<double>&
   return k;
 }
 
+// B (m x n, row-major) as F2 (m x k, row-major) times F1 (k x n, row-major):
+// F2 holds the left singular vectors and F1 = diag(s) times the right ones,
+// singular values below relCut * s_max dropped.  Applied to an explicit
+// truncated pseudo-inverse this recovers the factors of pinv_factors (the
+// singular vectors are shared and s = 1/s_A), for tables the caller replaces.
+int svd_factors(int m, int n, const double* B, double relCut, std::vector<double>& F1, std::vector<double>& F2) {
+  const bool tr = m < n;  // factor B^T (n x m) so the one-sided SVD sees M >= N
+  const int M = tr ? n : m, N = tr ? m : n;
+  std::vector<double> W((size_t)M * N), V;
+  if (tr) std::memcpy(W.data(), B, sizeof(double) * M * N);  // row-major B = column-major B^T
+  else
+    for (int i = 0; i < m; i++)
+      for (int j = 0; j < n; j++) W[(size_t)j * m + i] = B[(size_t)i * n + j];
+  svd_onesided(M, N, W, V);
+  std::vector<double> S(N);
+  for (int c = 0; c < N; c++) {
+    double s = 0;
+    for (int i = 0; i < M; i++) s += W[(size_t)c * M + i] * W[(size_t)c * M + i];
+    S[c] = std::sqrt(s);
+  }
+  const double smax = N ? *std::max_element(S.begin(), S.end()) : 0.0;
+  std::vector<int> keep;
+  for (int c = 0; c < N; c++)
+    if (S[c] > relCut * smax && S[c] > 0.0) keep.push_back(c);
+  const int k = (int)keep.size();
+  F1.assign((size_t)k * n, 0.0);
+  F2.assign((size_t)m * k, 0.0);
+  for (int r = 0; r < k; r++) {
+    const int c = keep[r];
+    const double s = S[c];
+    const double* w = &W[(size_t)c * M];  // U_c * s_c (length M)
+    const double* v = &V[(size_t)c * N];  // V_c (length N)
+    if (tr) {  // B^T = U S V^T: B = V S U^T, F2 column = V_c, F1 row = s U_c^T = w^T
+      for (int i = 0; i < m; i++) F2[(size_t)i * k + r] = v[i];
+      for (int j = 0; j < n; j++) F1[(size_t)r * n + j] = w[j];
+    } else {  // B = U S V^T: F2 column = U_c = w / s, F1 row = s V_c^T
+      for (int i = 0; i < m; i++) F2[(size_t)i * k + r] = w[i] / s;
+      for (int j = 0; j < n; j++) F1[(size_t)r * n + j] = s * v[j];
+    }
+  }
+  return k;
+}
+
+// C2E up x M2M through the factored pinv, in FP64: F2 (F1 M2M)
+std::vector<double> fold_c2e_m2m(const Plan& P) {
+  const int ue = P.nUE * P.sdm, uc = P.nUC * P.tdm, k = P.kUp, w = 8 * ue;
+  std::vector<double> T((size_t)k * w, 0.0), R((size_t)ue * w, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int r = 0; r < k; r++)
+    for (int c = 0; c < uc; c++) {
+      const double f = P.uc2ueF1[(size_t)r * uc + c];
+      const double* mrow = &P.m2m[(size_t)c * w];
+      double* trow = &T[(size_t)r * w];
+      for (int j = 0; j < w; j++) trow[j] += f * mrow[j];
+    }
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < ue; i++)
+    for (int r = 0; r < k; r++) {
+      const double f = P.uc2ueF2[(size_t)i * k + r];
+      const double* trow = &T[(size_t)r * w];
+      double* rrow = &R[(size_t)i * w];
+      for (int j = 0; j < w; j++) rrow[j] += f * trow[j];
+    }
+  return R;
+}
+
 // out[kz][ky][kx][h], kx in [0, n/2]; in[z][y][x][h] (x fastest), e^{-2 pi i}
 void rfft3_host(int n, int howmany, const double* in, std::complex<double>* out) {
   typedef std::complex<double> C;

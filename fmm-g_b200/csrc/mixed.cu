@@ -926,6 +926,9 @@ static std::vector<float> transpose_pad(const std::vector<double>& W, int n, int
 static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
   const size_t ue = (size_t)P.nUE * P.sdm, uc = (size_t)P.nUC * P.tdm;
   const size_t de = (size_t)P.nDE * P.sdm, dc = (size_t)P.nDC * P.tdm;
+  // rank-sized buffers take the largest rank a pinv can have, so factors
+  // recomputed for a replaced table (Plan::refactor_c2e) always fit
+  const int kUpMax = pad4((int)std::min(ue, uc)), kDnMax = pad4((int)std::min(de, dc));
   if (!D.mixedReady || kc > D.mixedK) {
     // grow: the old buffers stay in D.allocs until the handle is freed
     FMMG_TRY(dalloc(D, D.uchk32, (size_t)kc * P.nn * uc));
@@ -938,21 +941,19 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
     const size_t kc8 = (size_t)(kc + 7) / 8 * 8;  // the scalar k >= 2 layout stores blocks of 8
     FMMG_TRY(dalloc(D, D.effDen32, kc8 * P.vSrcNodes.size() * P.nEff * P.sdm));
     FMMG_TRY(dalloc(D, D.effVal32, kc8 * P.vTrgNodes.size() * P.nEff * P.tdm));
-    FMMG_TRY(dalloc(D, D.upT32, (size_t)kc * P.nn * std::max(pad4(P.kUp), 4)));
-    FMMG_TRY(dalloc(D, D.dnT32, (size_t)kc * P.nn * std::max(pad4(P.kDn), 4)));
+    FMMG_TRY(dalloc(D, D.upT32, (size_t)kc * P.nn * kUpMax));
+    FMMG_TRY(dalloc(D, D.dnT32, (size_t)kc * P.nn * kDnMax));
     FMMG_TRY(dalloc(D, D.denK, (size_t)kc * P.ns * P.sd));
     FMMG_TRY(dalloc(D, D.valK, (size_t)kc * std::max<int64_t>(P.nt, 1) * P.td));
-    if (!D.uc2ue32) {
-      FMMG_TRY(dalloc(D, D.uc2ue32, P.uc2ue.size()));
-      FMMG_TRY(dalloc(D, D.m2m32, P.m2m.size()));
-      FMMG_TRY(dalloc(D, D.dc2de32, P.dc2de.size()));
+    if (!D.l2l32) {
       FMMG_TRY(dalloc(D, D.l2l32, P.l2l.size()));
       FMMG_TRY(dalloc(D, D.m2lT32, P.m2lT.size()));
       if (P.sdm == 1 && P.tdm == 1) FMMG_TRY(dalloc(D, D.m2lTw32, (size_t)27 * 27 * P.nEff));
-      FMMG_TRY(dalloc(D, D.upF1, (size_t)pad4(P.kUp) * uc));
-      FMMG_TRY(dalloc(D, D.upF2, ue * pad4(P.kUp)));
-      FMMG_TRY(dalloc(D, D.dnF1, (size_t)pad4(P.kDn) * dc));
-      FMMG_TRY(dalloc(D, D.dnF2, de * pad4(P.kDn)));
+      FMMG_TRY(dalloc(D, D.upF1, (size_t)kUpMax * uc));
+      FMMG_TRY(dalloc(D, D.upF2, ue * kUpMax));
+      FMMG_TRY(dalloc(D, D.dnF1, (size_t)kDnMax * dc));
+      FMMG_TRY(dalloc(D, D.dnF2, de * kDnMax));
+      FMMG_TRY(dalloc(D, D.m2mUp32, ue * 8 * ue));
     }
     D.mixedReady = true;
     D.mixedK = kc;
@@ -963,9 +964,6 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
       FMMG_CK(cudaMemcpy(dst, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice));
       return std::string();
     };
-    FMMG_TRY(put(D.uc2ue32, P.uc2ue));
-    FMMG_TRY(put(D.m2m32, P.m2m));
-    FMMG_TRY(put(D.dc2de32, P.dc2de));
     FMMG_TRY(put(D.l2l32, P.l2l));
     // the factors padded to a rank that is a multiple of 4 (zero rows of F1,
     // zero columns of F2), so the intermediate rows allow 16-byte tile fetches
@@ -977,18 +975,24 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
     auto putT = [&](DevState::OpT& op, const std::vector<double>& W, int n, int k) -> std::string {
       int ld = 0;
       const std::vector<float> t = transpose_pad(W, n, k, ld);
-      if (!op.p) FMMG_TRY(dalloc(D, op.p, t.size()));
+      if (!op.p || t.size() > op.cap) {
+        FMMG_TRY(dalloc(D, op.p, t.size()));
+        op.cap = t.size();
+      }
       op.ld = ld;
       FMMG_CK(cudaMemcpy(op.p, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice));
       return std::string();
     };
     const int kUp4 = pad4(P.kUp), kDn4 = pad4(P.kDn);
-    FMMG_TRY(putT(D.tM2M, P.m2m, (int)uc, (int)(8 * ue)));
     FMMG_TRY(putT(D.tL2L, P.l2l, (int)(8 * dc), (int)de));
     FMMG_TRY(putT(D.tUpF1, pad_rows(P.uc2ueF1, P.kUp, (int)uc), kUp4, (int)uc));
     FMMG_TRY(putT(D.tUpF2, pad_cols(P.uc2ueF2, (int)ue, P.kUp), (int)ue, kUp4));
     FMMG_TRY(putT(D.tDnF1, pad_rows(P.dc2deF1, P.kDn, (int)dc), kDn4, (int)dc));
     FMMG_TRY(putT(D.tDnF2, pad_cols(P.dc2deF2, (int)de, P.kDn), (int)de, kDn4));
+    // a parent's upward density straight from its children's: C2E up x M2M
+    const std::vector<double> fold = fold_c2e_m2m(P);
+    FMMG_TRY(put(D.m2mUp32, fold));
+    FMMG_TRY(putT(D.tM2MUp, fold, (int)ue, (int)(8 * ue)));
     std::vector<float2> t(P.m2lT.size());
     for (size_t i = 0; i < t.size(); i++) t[i] = make_float2((float)P.m2lT[i].real(), (float)P.m2lT[i].imag());
     FMMG_CK(cudaMemcpy(D.m2lT32, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice));
@@ -1084,16 +1088,21 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, bool overlap
   cudaEventRecord(D.ev[EV_S2M], st);
   if (mask & 1) {
     for (int d = P.maxDepth; d >= 1; d--) {
-      int64_t a = D.offUpM2M[d], b = D.offUpM2M[d + 1];
-      gemm((int)(b - a), D.levelRows + a, 1, 0, D.uden32, ue, nn * ue, D.m2m32, D.tM2M, D.uchk32, uc, nn * uc, 8 * ue, uc,
-           level_scale(P, d + 1 + rl, +1.0), unit_scale(), 0.f, true);
-      a = D.offUpC2E[d];
-      b = D.offUpC2E[d + 1];
-      // C2E as F2 (F1 uchk): the large-norm pinv never multiplies in FP32
+      // leaves with sources: C2E as F2 (F1 uchk), so the large-norm pinv
+      // never multiplies in FP32
+      int64_t a = D.offUpLeaf[d], b = D.offUpLeaf[d + 1];
       gemm((int)(b - a), D.levelRows + a, 0, 0, D.uchk32, uc, nn * uc, D.upF1, D.tUpF1, D.upT32, kUp4, nn * kUp4, uc,
            kUp4, unit_scale(), unit_scale(), 0.f, false);
       gemm((int)(b - a), D.levelRows + a, 0, 0, D.upT32, kUp4, nn * kUp4, D.upF2, D.tUpF2, D.uden32, ue, nn * ue, kUp4,
            ue, unit_scale(), level_scale(P, d + rl, -1.0), 0.f, false);
+      // parents: C2E up x M2M folded on the host in FP64 (its norm is O(1)
+      // where the pinv's is ~1e6), one product from the children's upward
+      // densities (depth d + 1, done in the previous iteration) with no check
+      // surface in between
+      a = D.offUpM2M[d];
+      b = D.offUpM2M[d + 1];
+      gemm((int)(b - a), D.levelRows + a, 1, 0, D.uden32, ue, nn * ue, D.m2mUp32, D.tM2MUp, D.uden32, ue, nn * ue,
+           8 * ue, ue, level_scale(P, d + 1 + rl, +1.0), level_scale(P, d + rl, -1.0), 0.f, true);
     }
   }
   cudaEventRecord(D.ev[EV_UP_GEMM], st);
@@ -1352,12 +1361,12 @@ std::string dev_evaluate_mixed(const Plan& P, DevState& D, const double* dDen, d
                                                                   dDen + r0 * denStride, D.denK);
     ls->launches++;
     // Cleared per pass: the accumulated target values and downward check
-    // potentials.  Every upward check row that C2E reads is assigned first
-    // (S2M for a leaf with sources, M2M for a parent), the upward densities of
-    // the nodes with sources are assigned by C2E and the others stay zero from
-    // allocation, and every downward density that L2L or L2T reads is assigned
-    // by C2E at its level before; with the upward stage masked off the
-    // densities are cleared so the V and W stages see zeros.
+    // potentials.  The upward C2E reads only the check rows of leaves with
+    // sources, which S2M assigns; the upward densities of the nodes with
+    // sources are assigned (leaf C2E, the folded product for parents) and the
+    // others stay zero from allocation; every downward density that L2L or
+    // L2T reads is assigned by C2E at its level before.  With the upward stage
+    // masked off the densities are cleared so the V and W stages see zeros.
     FMMG_CK(cudaMemsetAsync(D.valK, 0, sizeof(double) * kk * valStride, st));
     FMMG_CK(cudaMemsetAsync(D.dchk32, 0, sizeof(float) * kk * P.nn * dc, st));
     if (!(mask & 1)) FMMG_CK(cudaMemsetAsync(D.uden32, 0, sizeof(float) * kk * P.nn * ue, st));

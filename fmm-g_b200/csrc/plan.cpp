@@ -251,13 +251,14 @@ void Plan::build_worklists() {
     }
   }
   // level lists for the batched equivalent-density GEMMs
-  upC2E.assign(maxDepth + 1, {}); upM2M.assign(maxDepth + 1, {});
+  upC2E.assign(maxDepth + 1, {}); upM2M.assign(maxDepth + 1, {}); upLeaf.assign(maxDepth + 1, {});
   dnL2L.assign(maxDepth + 1, {}); dnC2E.assign(maxDepth + 1, {});
   for (int g = 0; g < nn; g++) {
     int d = depth[g];
     if (flags[g] & NF_CBTR) {
       upC2E[d].push_back(g);
       if (!leaf(g)) upM2M[d].push_back(g);
+      else upLeaf[d].push_back(g);
     }
     if ((flags[g] & NF_EVTR) && d >= 2) {
       dnC2E[d].push_back(g);
@@ -519,6 +520,7 @@ std::string Plan::build_operators() {
   for (int r = 0; r < de; r++)
     for (int c = 0; c < dc; c++) dc2de[(size_t)r * dc + c] = Rm[(size_t)c * de + r];
   kDn = pinv_factors(dc, de, A.data(), eps, dc2deF1, dc2deF2);
+  // (refactor_c2e recovers these factors from the explicit tables)
   // M2M / L2L octant matrices
   m2m.assign((size_t)uc * 8 * ue, 0.0);
   l2l.assign((size_t)8 * dc * de, 0.0);
@@ -577,6 +579,16 @@ std::string Plan::build_operators() {
     rfft3_host(n, mdof, grid.data(), &m2lT[(size_t)id * nEff * mdof]);
   }
   return std::string();
+}
+
+void Plan::refactor_c2e(int which) {
+  // the kept singular values of a truncated pinv span at most 1/eps; the
+  // dropped ones are rounding noise
+  const double cut = 1e-13;
+  if (which == 0)
+    kUp = svd_factors(nUE * sdm, nUC * tdm, uc2ue.data(), cut, uc2ueF1, uc2ueF2);
+  else if (which == 2)
+    kDn = svd_factors(nDE * sdm, nDC * tdm, dc2de.data(), cut, dc2deF1, dc2deF2);
 }
 
 }  // namespace fmmg

@@ -80,6 +80,9 @@ struct Plan {
   // per level d: CBTR nodes (upward C2E), CBTR non-leaf parents at d (M2M
   // into them), EVTR non-leaves at d (L2L from them), EVTR nodes at d (C2E down)
   std::vector<std::vector<int32_t>> upC2E, upM2M, dnL2L, dnC2E;
+  // the leaves with sources per depth: the upward C2E rows of the FP32 pass,
+  // where a parent's upward density comes from the folded C2E x M2M product
+  std::vector<std::vector<int32_t>> upLeaf;
   // M2L grouped by parent pairs: for each target parent P (non-leaf, depth >=1,
   // with an EVTR child) the same-depth non-leaf neighbours Q and offset code
   std::vector<int32_t> vParents;  // rows
@@ -128,6 +131,9 @@ struct Plan {
   std::string build(const Options& opt, int64_t ns, const double* src, const double* nrm, int64_t nt,
                     const double* trg);
   std::string build_operators();
+  // refactor the pinv the caller replaced (0: C2E up, 2: C2E down) from its
+  // explicit table, so the FP32 pass applies the same operator
+  void refactor_c2e(int which);
   int child(int n, int o) const { return chd[n] + o; }
   bool leaf(int n) const { return chd[n] < 0; }
 
@@ -146,5 +152,11 @@ void pinv_jacobi(int m, int n, const double* A_colmajor, double eps, double* R_c
 int pinv_factors(int m, int n, const double* A_colmajor, double eps, std::vector<double>& F1,
                  std::vector<double>& F2);
 void rfft3_host(int n, int howmany, const double* in, std::complex<double>* out);
+int svd_factors(int m, int n, const double* B_rowmajor, double relCut, std::vector<double>& F1,
+                std::vector<double>& F2);
+// [nUE*sdm][8*nUE*sdm] row-major: C2E up times the 8 side-by-side M2M
+// matrices, F2 (F1 M2M) in FP64 -- a parent's upward equivalent density from
+// its children's in one product (the FP32 pass)
+std::vector<double> fold_c2e_m2m(const Plan& P);
 
 }  // namespace fmmg

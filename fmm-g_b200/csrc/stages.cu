@@ -574,8 +574,10 @@ void dev_free(DevState& D) {
   D.chkCap = 0;
   D.uchk32 = D.uden32 = D.dchk32 = D.dden32 = nullptr;
   D.effDen32 = D.effVal32 = nullptr;
-  D.uc2ue32 = D.m2m32 = D.dc2de32 = D.l2l32 = nullptr;
+  D.l2l32 = nullptr;
   D.upF1 = D.upF2 = D.dnF1 = D.dnF2 = D.upT32 = D.dnT32 = nullptr;
+  D.m2mUp32 = nullptr;
+  for (DevState::OpT* op : {&D.tL2L, &D.tUpF1, &D.tUpF2, &D.tDnF1, &D.tDnF2, &D.tM2MUp}) *op = DevState::OpT();
   D.transIdDev = nullptr;
   D.m2lT32 = nullptr;
   D.m2lTw32 = nullptr;
@@ -713,6 +715,7 @@ std::string dev_upload(const Plan& P, DevState& D, const double* src, const doub
     cat(P.upM2M, D.offUpM2M);
     cat(P.dnL2L, D.offDnL2L);
     cat(P.dnC2E, D.offDnC2E);
+    cat(P.upLeaf, D.offUpLeaf);
     FMMG_TRY(dput(D, D.levelRows, rows));
   }
   FMMG_TRY(dput(D, D.vParents, P.vParents));

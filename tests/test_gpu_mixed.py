@@ -190,3 +190,36 @@ def test_hadamard_two_rhs_per_thread_identical(k):
     assert np.array_equal(outs[0], outs[1])
     with pytest.raises(fmmg.FmmgError):
         lib.tuning({"had_fp32_rhs_per_thread": 3})
+
+
+def test_mixed_follows_replaced_pinv():
+    """fmmg_operator(set) replaces the pseudo-inverses: the FP32 pass refactors
+    each from its explicit table (SVD) and rebuilds the folded C2E x M2M
+    product, so the mixed form still matches the FP64 form on the replaced
+    operator set."""
+    import torch
+    rng = np.random.default_rng(91)
+    n = 30000
+    src = W.sphere_clusters(n, rng)
+    f = fmmg.FMM3d(111, np_=6, pts_max=64)
+    f.setup(src)
+    D = torch.from_numpy(rng.normal(size=(2, n))).cuda()
+
+    def both():
+        outs = []
+        for prec in (fmmg.PREC_FP64, fmmg.PREC_MIXED):
+            out = torch.zeros(2, n, dtype=torch.float64, device="cuda")
+            torch.cuda.synchronize()
+            f.evaluate_device(D, out, 2, prec)
+            f.sync()
+            outs.append(out.cpu().numpy())
+        return outs
+
+    d0, m0 = both()
+    assert rel_l2(m0, d0) <= 1e-5
+    for which in (0, 2):
+        f.set_operator(which, 0, 0.5 * f.operator(which))
+    d1, m1 = both()
+    print("replaced pinv: fp64 change %.3e, mixed vs fp64 %.3e" % (rel_l2(d1, d0), rel_l2(m1, d1)))
+    assert rel_l2(d1, d0) > 1e-2  # the replacement is visible
+    assert rel_l2(m1, d1) <= 1e-5
