@@ -134,7 +134,11 @@ fmmg_status fmmg_create(const fmmg_options* o, fmmg_handle** out) {
         if (o->stream) {
           h->dev.stream = (cudaStream_t)o->stream;
         } else {
-          ce = cudaStreamCreateWithFlags(&h->dev.stream, cudaStreamNonBlocking);
+          // the highest priority: the side stream of the mixed pass (lowest)
+          // then fills the gaps of the main stream's kernels
+          int least = 0, greatest = 0;
+          cudaDeviceGetStreamPriorityRange(&least, &greatest);
+          ce = cudaStreamCreateWithPriority(&h->dev.stream, cudaStreamNonBlocking, greatest);
           h->dev.ownStream = true;
         }
       }
@@ -313,7 +317,8 @@ fmmg_status fmmg_evaluate_device(fmmg_handle* h, int k, const double* dDen, doub
     h->graphOn = false;  // stay eager from now on
     return evaluate_eager(h, k, dDen, dVal, precision, false);
   }
-  ce = cudaGraphInstantiate(&h->graphExec, g, 0);
+  // keep the captured streams' priorities (the side stream yields to the main one)
+  ce = cudaGraphInstantiateWithFlags(&h->graphExec, g, cudaGraphInstantiateFlagUseNodePriority);
   cudaGraphDestroy(g);
   if (ce != cudaSuccess) {
     h->graphExec = nullptr;

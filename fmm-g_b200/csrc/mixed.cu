@@ -628,8 +628,8 @@ constexpr size_t r8_fwd_smem() {  // cube + X1 + X2 (padded planes) + twiddles
          sizeof(float2) * (8 * r8_pad(NP * NP * (NP + 1)) + 8 * r8_pad(NP * 2 * NP * (NP + 1)) + 2 * NP * NP);
 }
 template <int NP>
-constexpr size_t r8_inv_smem() {  // staged input (later reused for Y1) + Y2 + twiddles
-  return sizeof(float2) * (8 * (2 * NP * 2 * NP * (NP + 1)) + 8 * r8_pad(NP * 2 * NP * (NP + 1)) + 2 * NP * NP);
+constexpr size_t r8_inv_smem() {  // Y1 + Y2 (padded planes) + twiddles
+  return sizeof(float2) * (8 * r8_pad(NP * NP * (NP + 1)) + 8 * r8_pad(NP * 2 * NP * (NP + 1)) + 2 * NP * NP);
 }
 
 __device__ __forceinline__ void r8_load(const float2* p, float2 (&v)[8]) {
@@ -684,8 +684,8 @@ __global__ void __launch_bounds__(256)
   const float scl = (float)exp2((double)(depth[v] + rootLevel) * deg);
   for (int i = tid; i < S3 * 8; i += blockDim.x) cube[i] = 0.f;
   __syncthreads();
-  for (int i = tid; i < nUE * 8; i += blockDim.x) {
-    const int j = i >> 3, r = i & 7;
+  for (int i = tid; i < nUE * 8; i += blockDim.x) {  // surface point fastest: coalesced reads of each plane
+    const int j = i % nUE, r = i / nUE;
     if (r0 + r >= kc) continue;
     const int p = ijk[j];
     cube[r * S3 + ((p >> 16) * NP + ((p >> 8) & 255)) * NP + (p & 255)] =
@@ -759,84 +759,48 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// The node's spectra block (contiguous in global memory: [frequency][8]) is
-// brought into shared memory by the bulk-copy (TMA) engine in one
-// cp.async.bulk completed on an mbarrier; the wait is bounded and, if it gives
-// up, sets *errFlag and still waits (bounded) before the CTA exits.
-constexpr long long R8_WAIT_LIMIT = 1ll << 24;
-
-__device__ __forceinline__ bool r8_bar_wait(uint32_t bar, uint32_t parity) {
-  for (long long i = 0; i < R8_WAIT_LIMIT; i++) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, P1;\n\t}"
-        : "=r"(done)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
+// The z pass reads the node's spectra from global memory directly: a warp's
+// 32 lanes read 256 contiguous bytes and every element is read once, so the
+// CTA needs no staging space (4 CTAs per SM at np = 6; staging the 64.5 KB
+// block in shared memory first allowed 2 and measured 1.3x slower).
 template <int NP>
 __global__ void __launch_bounds__(256)
     k_m2l_inv32r8(const int32_t* __restrict__ nodes, const float2* __restrict__ effVal, int64_t blkStride, int nEff,
-                  const int32_t* __restrict__ ijk, int nDC, float* __restrict__ dchk, int64_t dchkRhs, int kc,
-                  int* __restrict__ errFlag) {
+                  const int32_t* __restrict__ ijk, int nDC, float* __restrict__ dchk, int64_t dchkRhs, int kc) {
   using F = FftDims<NP>;
   constexpr int N = F::N, NH = F::NH;
-  constexpr int NF = N * N * NH;  // frequencies
   constexpr int S1 = r8_pad(NP * NP * NH), S2 = r8_pad(NP * N * NH);
   extern __shared__ __align__(16) unsigned char r8_smem[];
-  float2* X0 = reinterpret_cast<float2*>(r8_smem);  // [N][N][NH][8]: the node's spectra, interleaved as in HBM
-  float2* Y2 = X0 + NF * 8;                          // [8][NP][N][NH]
+  float2* Y1 = reinterpret_cast<float2*>(r8_smem);  // [8][NP][NP][NH]
+  float2* Y2 = Y1 + S1 * 8;                          // [8][NP][N][NH]
   float2* twb = Y2 + S2 * 8;                         // [N][NP]
-  float2* Y1 = X0;                                   // [8][NP][NP][NH], reuses the staging space
-  __shared__ __align__(8) uint64_t bar;
   const int slot = blockIdx.x;
   const int node = nodes[slot];
   const int r0 = blockIdx.y * 8;
   const int tid = threadIdx.x;
-  const uint32_t barA = (uint32_t)__cvta_generic_to_shared(&bar);
-  if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(barA), "r"(1));
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  if (tid == 0) {
-    const uint32_t bytes = (uint32_t)(NF * 8 * sizeof(float2));
-    const float2* src = effVal + blockIdx.y * blkStride + (int64_t)slot * nEff * 8;
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(barA), "r"(bytes) : "memory");
-    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(X0);
-    for (uint32_t off = 0; off < bytes; off += 32768u) {  // pieces of at most 32 KB, multiples of 16 bytes
-      const uint32_t piece = bytes - off < 32768u ? bytes - off : 32768u;
-      asm volatile(
-          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst + off),
-          "l"(reinterpret_cast<const char*>(src) + off), "r"(piece), "r"(barA)
-          : "memory");
-    }
-  }
+  const float2* Xg = effVal + blockIdx.y * blkStride + (int64_t)slot * nEff * 8;
   r8_twiddles<NP>(twb);
-  if (!r8_bar_wait(barA, 0)) {
-    if (tid == 0) atomicExch(errFlag, 1);
-    r8_bar_wait(barA, 0);
-  }
   __syncthreads();
   // z pass, band outputs only: a thread owns one z line (kx, ky) of one
-  // right-hand side; right-hand side fastest, matching the staged layout.
-  // Inputs kz and kz + NP share the twiddle up to (-1)^(b + H), so output b
-  // takes S = X[kz] + X[kz + NP] (b + H even) or D = X[kz] - X[kz + NP]
-  // (b + H odd) against the twiddle of kz: NP x NP products a line.
+  // right-hand side, right-hand side fastest as in HBM.  Inputs kz and kz + NP
+  // share the twiddle up to (-1)^(b + H), so output b takes
+  // S = X[kz] + X[kz + NP] (b + H even) or D = X[kz] - X[kz + NP] (b + H odd)
+  // against the twiddle of kz: NP x NP products a line.
   for (int i = tid; i < NH * N * 8; i += blockDim.x) {
     const int r = i & 7, kx = (i >> 3) % NH, ky = (i >> 3) / NH;
+    float2 c0[NP], c1[NP];
+#pragma unroll
+    for (int kz = 0; kz < NP; kz++) {  // all loads of the line first
+      c0[kz] = Xg[((kz * N + ky) * NH + kx) * 8 + r];
+      c1[kz] = Xg[(((kz + NP) * N + ky) * NH + kx) * 8 + r];
+    }
     float2 s[NP];
 #pragma unroll
     for (int zb = 0; zb < NP; zb++) s[zb] = make_float2(0.f, 0.f);
-#pragma unroll 1
+#pragma unroll
     for (int kz = 0; kz < NP; kz++) {
-      const float2 c0 = X0[((kz * N + ky) * NH + kx) * 8 + r], c1 = X0[(((kz + NP) * N + ky) * NH + kx) * 8 + r];
-      const float2 cs = make_float2(c0.x + c1.x, c0.y + c1.y), cd = make_float2(c0.x - c1.x, c0.y - c1.y);
+      const float2 cs = make_float2(c0[kz].x + c1[kz].x, c0[kz].y + c1[kz].y);
+      const float2 cd = make_float2(c0[kz].x - c1[kz].x, c0[kz].y - c1[kz].y);
 #pragma unroll
       for (int zb = 0; zb < NP; zb++) {
         const float2 t = cmulc(((zb + F::H) & 1) ? cd : cs, twb[kz * NP + zb]);
@@ -1229,7 +1193,7 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, bool overlap
     constexpr size_t sm = r8_inv_smem<NP_>();                                                                  \
     cudaFuncSetAttribute(k_m2l_inv32r8<NP_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);            \
     k_m2l_inv32r8<NP_><<<dim3(ntrg, nblk), 256, sm, st>>>(D.vTrgNodes, D.effVal32, blkVal, P.nEff, D.surfIJK,  \
-                                                          P.nDC, D.dchk32, nn * dc, kc, D.devErr);             \
+                                                          P.nDC, D.dchk32, nn * dc, kc);                       \
   } while (0)
     switch (P.o.np) {
       case 3: FMMG_INV32R8(3); break;

@@ -755,7 +755,11 @@ std::string dev_upload(const Plan& P, DevState& D, const double* src, const doub
   }
   if (!D.evReady) {
     for (auto& e : D.ev) FMMG_CK(cudaEventCreate(&e));
-    FMMG_CK(cudaStreamCreateWithFlags(&D.side, cudaStreamNonBlocking));
+    {
+      int least = 0, greatest = 0;
+      FMMG_CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+      FMMG_CK(cudaStreamCreateWithPriority(&D.side, cudaStreamNonBlocking, least));
+    }
     for (cudaEvent_t* e : {&D.evFork, &D.evUp, &D.evSide}) FMMG_CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     D.evReady = true;
   }
