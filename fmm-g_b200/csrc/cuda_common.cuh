@@ -48,6 +48,13 @@ template <int NP>
 struct FftDims {
   static constexpr int N = 2 * NP, NH = NP + 1, H = NP / 2;
 };
+// The FP32 pass's grid: 2np - 1 points per axis, the smallest on which the
+// band-to-band convolution of M2L does not wrap (offsets -(np-1)..np-1);
+// odd, so the r2c half spectrum has no Nyquist term.
+template <int NP>
+struct FftDims32 {
+  static constexpr int N = 2 * NP - 1, NH = NP, H = NP / 2;
+};
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);

@@ -409,7 +409,7 @@ __global__ void __launch_bounds__(128)
     k_m2l_fwd32(const int32_t* __restrict__ nodes, const int32_t* __restrict__ depth, int rootLevel, Scale4 deg,
                 int sdm, const float* __restrict__ uden, int64_t udenRhs, const int32_t* __restrict__ ijk, int nUE,
                 float2* __restrict__ effDen, int64_t effRhs, int nEff) {
-  using F = FftDims<NP>;
+  using F = FftDims32<NP>;
   constexpr int N = F::N, NH = F::NH, H = F::H;
   __shared__ float cube[NP * NP * NP];
   __shared__ float2 X1[NP * NP * NH];
@@ -550,7 +550,7 @@ template <int NP>
 __global__ void __launch_bounds__(128)
     k_m2l_inv32(const int32_t* __restrict__ nodes, const float2* __restrict__ effVal, int64_t valRhs, int nEff,
                 int tdm, const int32_t* __restrict__ ijk, int nDC, float* __restrict__ dchk, int64_t dchkRhs) {
-  using F = FftDims<NP>;
+  using F = FftDims32<NP>;
   constexpr int N = F::N, NH = F::NH, H = F::H;
   __shared__ float2 Y2[NP * N * NH];
   __shared__ float2 Y1[NP * NP * NH];
@@ -600,7 +600,7 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
       for (int kx = 0; kx < NH; kx++) {
         float2 t = cmulc(y1[kx], tw[(kx * x) % N]);
-        s += (kx == 0 || kx == N / 2) ? t.x : 2.f * t.x;
+        s += (kx == 0 || 2 * kx == N) ? t.x : 2.f * t.x;  // the Nyquist term only for even N
       }
       dc[(int64_t)i * tdm + m] += s;
     }
@@ -611,25 +611,28 @@ __global__ void __launch_bounds__(128)
 // Scalar equivalent kernels, blocks of 8 right-hand sides: one CTA per
 // (slot, block) transforms the 8 densities together.  Each pass is a set of
 // 1-D DFTs along one axis: a thread owns one line of one right-hand side,
-// reads its np (or 2np) inputs from shared memory once and produces all the
+// reads its np (or N) inputs from shared memory once and produces all the
 // line's outputs, so shared-memory traffic is one read per input (the kernels
 // are bound by it otherwise).  Shared staging arrays are planes [8][...]
 // padded against bank conflicts; in global memory the spectra are written
 // (and read back by k_m2l_inv32r8) as [block][slot][frequency][8], the
-// forward's last pass ordered right-hand side fastest for contiguous writes.  The twiddles of every pass come from one table
-// twb[k][b] = exp(-2 pi i k (b + np/2) / 2np).  Dynamic shared memory
-// r8_fwd_smem<NP>() / r8_inv_smem<NP>().
+// forward's last pass ordered right-hand side fastest for contiguous writes.
+// The grid is FftDims32 (N = 2np - 1 points per axis); the twiddles of every
+// pass come from one table twb[k][b] = exp(-2 pi i k (b + np/2) / N).  Dynamic
+// shared memory r8_fwd_smem<NP>() / r8_inv_smem<NP>().
 // plane length rounded so that consecutive planes start 8 words apart modulo
 // the 32 shared-memory banks (2-way conflicts at most across right-hand sides)
 constexpr int r8_pad(int s) { return s + ((4 - s % 16) + 16) % 16; }
 template <int NP>
 constexpr size_t r8_fwd_smem() {  // cube + X1 + X2 (padded planes) + twiddles
+  using F = FftDims32<NP>;
   return sizeof(float) * NP * NP * NP * 8 +
-         sizeof(float2) * (8 * r8_pad(NP * NP * (NP + 1)) + 8 * r8_pad(NP * 2 * NP * (NP + 1)) + 2 * NP * NP);
+         sizeof(float2) * (8 * r8_pad(NP * NP * F::NH) + 8 * r8_pad(NP * F::N * F::NH) + F::N * NP);
 }
 template <int NP>
 constexpr size_t r8_inv_smem() {  // Y1 + Y2 (padded planes) + twiddles
-  return sizeof(float2) * (8 * r8_pad(NP * NP * (NP + 1)) + 8 * r8_pad(NP * 2 * NP * (NP + 1)) + 2 * NP * NP);
+  using F = FftDims32<NP>;
+  return sizeof(float2) * (8 * r8_pad(NP * NP * F::NH) + 8 * r8_pad(NP * F::N * F::NH) + F::N * NP);
 }
 
 __device__ __forceinline__ void r8_load(const float2* p, float2 (&v)[8]) {
@@ -646,15 +649,9 @@ __device__ __forceinline__ void r8_store(float2* p, const float2 (&v)[8]) {
 #pragma unroll
   for (int i = 0; i < 4; i++) q[i] = make_float4(v[2 * i].x, v[2 * i].y, v[2 * i + 1].x, v[2 * i + 1].y);
 }
-// (-1)^H v, H = NP / 2: the factor between the half-length partial sums of
-// outputs k and k + NP of a forward line transform
-template <int NP>
-__device__ __forceinline__ float2 r8_half_sign(float2 v) {
-  return (FftDims<NP>::H & 1) ? make_float2(-v.x, -v.y) : v;
-}
 template <int NP>
 __device__ __forceinline__ void r8_twiddles(float2* twb) {
-  using F = FftDims<NP>;
+  using F = FftDims32<NP>;
   for (int i = threadIdx.x; i < F::N * NP; i += blockDim.x) {
     const int k = i / NP, b = i % NP;
     double sn, cs;
@@ -668,7 +665,7 @@ __global__ void __launch_bounds__(256)
     k_m2l_fwd32r8(const int32_t* __restrict__ nodes, const int32_t* __restrict__ depth, int rootLevel, float deg,
                   const float* __restrict__ uden, int64_t udenRhs, const int32_t* __restrict__ ijk, int nUE,
                   float2* __restrict__ effDen, int64_t blkStride, int nEff, int kc) {
-  using F = FftDims<NP>;
+  using F = FftDims32<NP>;
   constexpr int N = F::N, NH = F::NH;
   constexpr int S1 = r8_pad(NP * NP * NH), S2 = r8_pad(NP * N * NH), S3 = NP * NP * NP;
   extern __shared__ __align__(16) unsigned char r8_smem[];
@@ -712,26 +709,22 @@ __global__ void __launch_bounds__(256)
   }
   __syncthreads();
   // y pass: a thread owns one y line (kx, zb) of one right-hand side and all N
-  // ky outputs.  The twiddle of output k + NP is that of k times (-1)^(b + H)
-  // (W^NP = -1), so the even- and odd-b partial sums pe, po of output k give
-  // X[k] = pe + po and X[k + NP] = (-1)^H (pe - po): NP x NP products a line.
+  // ky outputs
   for (int i = tid; i < NH * NP * 8; i += blockDim.x) {
     const int kx = i % NH, zb = (i / NH) % NP, r = i / (NH * NP);
     float2 c[NP];
 #pragma unroll
     for (int yb = 0; yb < NP; yb++) c[yb] = X1[r * S1 + (zb * NP + yb) * NH + kx];
 #pragma unroll 1
-    for (int ky = 0; ky < NP; ky++) {
-      float2 pe = make_float2(0.f, 0.f), po = pe;
+    for (int ky = 0; ky < N; ky++) {
+      float2 s = make_float2(0.f, 0.f);
 #pragma unroll
       for (int yb = 0; yb < NP; yb++) {
         const float2 t = cmul(c[yb], twb[ky * NP + yb]);
-        float2& a = (yb & 1) ? po : pe;
-        a.x += t.x;
-        a.y += t.y;
+        s.x += t.x;
+        s.y += t.y;
       }
-      X2[r * S2 + (zb * N + ky) * NH + kx] = make_float2(pe.x + po.x, pe.y + po.y);
-      X2[r * S2 + (zb * N + ky + NP) * NH + kx] = r8_half_sign<NP>(make_float2(pe.x - po.x, pe.y - po.y));
+      X2[r * S2 + (zb * N + ky) * NH + kx] = s;
     }
   }
   __syncthreads();
@@ -744,17 +737,15 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int zb = 0; zb < NP; zb++) c[zb] = X2[r * S2 + (zb * N + ky) * NH + kx];
 #pragma unroll 1
-    for (int kz = 0; kz < NP; kz++) {  // outputs kz and kz + NP, as in the y pass
-      float2 pe = make_float2(0.f, 0.f), po = pe;
+    for (int kz = 0; kz < N; kz++) {
+      float2 s = make_float2(0.f, 0.f);
 #pragma unroll
       for (int zb = 0; zb < NP; zb++) {
         const float2 t = cmul(c[zb], twb[kz * NP + zb]);
-        float2& a = (zb & 1) ? po : pe;
-        a.x += t.x;
-        a.y += t.y;
+        s.x += t.x;
+        s.y += t.y;
       }
-      out[((int64_t)(kz * N + ky) * NH + kx) * 8 + r] = make_float2(pe.x + po.x, pe.y + po.y);
-      out[((int64_t)((kz + NP) * N + ky) * NH + kx) * 8 + r] = r8_half_sign<NP>(make_float2(pe.x - po.x, pe.y - po.y));
+      out[((int64_t)(kz * N + ky) * NH + kx) * 8 + r] = s;
     }
   }
 }
@@ -767,7 +758,7 @@ template <int NP>
 __global__ void __launch_bounds__(256)
     k_m2l_inv32r8(const int32_t* __restrict__ nodes, const float2* __restrict__ effVal, int64_t blkStride, int nEff,
                   const int32_t* __restrict__ ijk, int nDC, float* __restrict__ dchk, int64_t dchkRhs, int kc) {
-  using F = FftDims<NP>;
+  using F = FftDims32<NP>;
   constexpr int N = F::N, NH = F::NH;
   constexpr int S1 = r8_pad(NP * NP * NH), S2 = r8_pad(NP * N * NH);
   extern __shared__ __align__(16) unsigned char r8_smem[];
@@ -782,28 +773,20 @@ __global__ void __launch_bounds__(256)
   r8_twiddles<NP>(twb);
   __syncthreads();
   // z pass, band outputs only: a thread owns one z line (kx, ky) of one
-  // right-hand side, right-hand side fastest as in HBM.  Inputs kz and kz + NP
-  // share the twiddle up to (-1)^(b + H), so output b takes
-  // S = X[kz] + X[kz + NP] (b + H even) or D = X[kz] - X[kz + NP] (b + H odd)
-  // against the twiddle of kz: NP x NP products a line.
+  // right-hand side, right-hand side fastest as in HBM
   for (int i = tid; i < NH * N * 8; i += blockDim.x) {
     const int r = i & 7, kx = (i >> 3) % NH, ky = (i >> 3) / NH;
-    float2 c0[NP], c1[NP];
+    float2 c[N];
 #pragma unroll
-    for (int kz = 0; kz < NP; kz++) {  // all loads of the line first
-      c0[kz] = Xg[((kz * N + ky) * NH + kx) * 8 + r];
-      c1[kz] = Xg[(((kz + NP) * N + ky) * NH + kx) * 8 + r];
-    }
+    for (int kz = 0; kz < N; kz++) c[kz] = Xg[((kz * N + ky) * NH + kx) * 8 + r];  // all loads of the line first
     float2 s[NP];
 #pragma unroll
     for (int zb = 0; zb < NP; zb++) s[zb] = make_float2(0.f, 0.f);
 #pragma unroll
-    for (int kz = 0; kz < NP; kz++) {
-      const float2 cs = make_float2(c0[kz].x + c1[kz].x, c0[kz].y + c1[kz].y);
-      const float2 cd = make_float2(c0[kz].x - c1[kz].x, c0[kz].y - c1[kz].y);
+    for (int kz = 0; kz < N; kz++) {
 #pragma unroll
       for (int zb = 0; zb < NP; zb++) {
-        const float2 t = cmulc(((zb + F::H) & 1) ? cd : cs, twb[kz * NP + zb]);
+        const float2 t = cmulc(c[kz], twb[kz * NP + zb]);
         s[zb].x += t.x;
         s[zb].y += t.y;
       }
@@ -819,12 +802,11 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int yb = 0; yb < NP; yb++) s[yb] = make_float2(0.f, 0.f);
 #pragma unroll 1
-    for (int ky = 0; ky < NP; ky++) {  // inputs ky and ky + NP, as in the z pass
-      const float2 c0 = Y2[r * S2 + (zb * N + ky) * NH + kx], c1 = Y2[r * S2 + (zb * N + ky + NP) * NH + kx];
-      const float2 cs = make_float2(c0.x + c1.x, c0.y + c1.y), cd = make_float2(c0.x - c1.x, c0.y - c1.y);
+    for (int ky = 0; ky < N; ky++) {
+      const float2 c = Y2[r * S2 + (zb * N + ky) * NH + kx];
 #pragma unroll
       for (int yb = 0; yb < NP; yb++) {
-        const float2 t = cmulc(((yb + F::H) & 1) ? cd : cs, twb[ky * NP + yb]);
+        const float2 t = cmulc(c, twb[ky * NP + yb]);
         s[yb].x += t.x;
         s[yb].y += t.y;
       }
@@ -843,7 +825,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int kx = 0; kx < NH; kx++) {
       const float2 w = twb[kx * NP + a];
-      s += ((kx == 0 || kx == N / 2) ? 1.f : 2.f) * cmulc(y1[kx], w).x;
+      s += ((kx == 0 || 2 * kx == N) ? 1.f : 2.f) * cmulc(y1[kx], w).x;
     }
     dchk[(int64_t)(r0 + r) * dchkRhs + (int64_t)node * nDC + j] += s;
   }
@@ -903,16 +885,16 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
     FMMG_TRY(dalloc(D, D.dchk32, (size_t)kc * P.nn * dc));
     FMMG_TRY(dalloc(D, D.dden32, (size_t)kc * P.nn * de));
     const size_t kc8 = (size_t)(kc + 7) / 8 * 8;  // the scalar k >= 2 layout stores blocks of 8
-    FMMG_TRY(dalloc(D, D.effDen32, kc8 * P.vSrcNodes.size() * P.nEff * P.sdm));
-    FMMG_TRY(dalloc(D, D.effVal32, kc8 * P.vTrgNodes.size() * P.nEff * P.tdm));
+    FMMG_TRY(dalloc(D, D.effDen32, kc8 * P.vSrcNodes.size() * P.nEff32 * P.sdm));
+    FMMG_TRY(dalloc(D, D.effVal32, kc8 * P.vTrgNodes.size() * P.nEff32 * P.tdm));
     FMMG_TRY(dalloc(D, D.upT32, (size_t)kc * P.nn * kUpMax));
     FMMG_TRY(dalloc(D, D.dnT32, (size_t)kc * P.nn * kDnMax));
     FMMG_TRY(dalloc(D, D.denK, (size_t)kc * P.ns * P.sd));
     FMMG_TRY(dalloc(D, D.valK, (size_t)kc * std::max<int64_t>(P.nt, 1) * P.td));
     if (!D.l2l32) {
       FMMG_TRY(dalloc(D, D.l2l32, P.l2l.size()));
-      FMMG_TRY(dalloc(D, D.m2lT32, P.m2lT.size()));
-      if (P.sdm == 1 && P.tdm == 1) FMMG_TRY(dalloc(D, D.m2lTw32, (size_t)27 * 27 * P.nEff));
+      FMMG_TRY(dalloc(D, D.m2lT32, P.m2lT32.size()));
+      if (P.sdm == 1 && P.tdm == 1) FMMG_TRY(dalloc(D, D.m2lTw32, (size_t)27 * 27 * P.nEff32));
       FMMG_TRY(dalloc(D, D.upF1, (size_t)kUpMax * uc));
       FMMG_TRY(dalloc(D, D.upF2, ue * kUpMax));
       FMMG_TRY(dalloc(D, D.dnF1, (size_t)kDnMax * dc));
@@ -957,8 +939,8 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
     const std::vector<double> fold = fold_c2e_m2m(P);
     FMMG_TRY(put(D.m2mUp32, fold));
     FMMG_TRY(putT(D.tM2MUp, fold, (int)ue, (int)(8 * ue)));
-    std::vector<float2> t(P.m2lT.size());
-    for (size_t i = 0; i < t.size(); i++) t[i] = make_float2((float)P.m2lT[i].real(), (float)P.m2lT[i].imag());
+    std::vector<float2> t(P.m2lT32.size());
+    for (size_t i = 0; i < t.size(); i++) t[i] = make_float2((float)P.m2lT32[i].real(), (float)P.m2lT32[i].imag());
     FMMG_CK(cudaMemcpy(D.m2lT32, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice));
     if (D.m2lTw32) {  // combined translations of the 27-product Hadamard (had_pq.cuh), FP64 sums
       auto w = [](int code, int d) -> double {
@@ -966,7 +948,7 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
         if (code == 1) return d == 1 ? 1.0 : (d == 0 ? -1.0 : 0.0);
         return d == -1 ? 1.0 : (d == 0 ? -1.0 : 0.0);
       };
-      const int ne = P.nEff;
+      const int ne = P.nEff32;
       std::vector<float2> tw((size_t)27 * 27 * ne, make_float2(0.f, 0.f));
       std::vector<std::complex<double>> acc(ne);
       for (int o = 0; o < 27; o++) {
@@ -982,7 +964,7 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
                 if (wt == 0.0) continue;
                 const int id = P.transId[2 * ox + dx + 3][2 * oy + dy + 3][2 * oz + dz + 3];
                 if (id < 0) continue;  // touching pair
-                const std::complex<double>* Tt = &P.m2lT[(size_t)id * ne];
+                const std::complex<double>* Tt = &P.m2lT32[(size_t)id * ne];
                 for (int f = 0; f < ne; f++) acc[f] += wt * Tt[f];
               }
           float2* dst = &tw[((size_t)o * 27 + j) * ne];
@@ -1095,10 +1077,10 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, bool overlap
   }
   cudaEventRecord(D.ev[EV_NEAR], st);
   const int nsrc = (int)P.vSrcNodes.size(), ntrg = (int)P.vTrgNodes.size(), npar = (int)P.vParents.size();
-  const int64_t effDR = (int64_t)nsrc * P.nEff * P.sdm, effVR = (int64_t)ntrg * P.nEff * P.tdm;
+  const int64_t effDR = (int64_t)nsrc * P.nEff32 * P.sdm, effVR = (int64_t)ntrg * P.nEff32 * P.tdm;
   const bool r8 = P.sdm == 1 && P.tdm == 1 && kc >= 2 && D.hadPQ;  // blocks of 8 interleaved right-hand sides
   const int nblk = (kc + 7) / 8;
-  const int64_t blkDen = (int64_t)nsrc * P.nEff * 8, blkVal = (int64_t)ntrg * P.nEff * 8;
+  const int64_t blkDen = (int64_t)nsrc * P.nEff32 * 8, blkVal = (int64_t)ntrg * P.nEff32 * 8;
   if ((mask & 4) && nsrc > 0 && r8) {
 #define FMMG_FWD32R8(NP_)                                                                                      \
   do {                                                                                                         \
@@ -1106,7 +1088,7 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, bool overlap
     cudaFuncSetAttribute(k_m2l_fwd32r8<NP_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);            \
     k_m2l_fwd32r8<NP_><<<dim3(nsrc, nblk), 256, sm, st>>>(D.vSrcNodes, D.depth, rl, (float)P.deg[0], D.uden32, \
                                                           nn * ue, D.surfIJK, P.nUE, D.effDen32, blkDen,       \
-                                                          P.nEff, kc);                                         \
+                                                          P.nEff32, kc);                                         \
   } while (0)
     switch (P.o.np) {
       case 3: FMMG_FWD32R8(3); break;
@@ -1124,7 +1106,7 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, bool overlap
     for (int k = 0; k < 4; k++) deg.v[k] = P.deg[k];
 #define FMMG_FWD32(NP_)                                                                                         \
   k_m2l_fwd32<NP_><<<dim3(nsrc, kc), 128, 0, st>>>(D.vSrcNodes, D.depth, rl, deg, P.sdm, D.uden32, nn * ue,    \
-                                                    D.surfIJK, P.nUE, D.effDen32, effDR, P.nEff)
+                                                    D.surfIJK, P.nUE, D.effDen32, effDR, P.nEff32)
     switch (P.o.np) {
       case 3: FMMG_FWD32(3); break;
       case 4: FMMG_FWD32(4); break;
@@ -1138,48 +1120,48 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, bool overlap
   }
   cudaEventRecord(D.ev[EV_M2L_FWD], st);
   if ((mask & 4) && npar > 0 && ntrg > 0) {
-    dim3 grid(npar, (P.nEff + 31) / 32, kb);
-    const float nrmfc = 1.0f / float(P.nReg);
+    dim3 grid(npar, (P.nEff32 + 31) / 32, kb);
+    const float nrmfc = 1.0f / float(P.nReg32);
 #define FMMG_HAD32(SD_, TD_)                                                                                   \
   k_m2l_had32<SD_, TD_, KB><<<grid, 256, 0, st>>>(D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot,      \
                                                    D.vTrgSlot, D.effDen32, effDR, D.m2lT32, D.effVal32, effVR, \
-                                                   P.nEff, kc, nrmfc)
+                                                   P.nEff32, kc, nrmfc)
     if (P.sdm == 1 && P.tdm == 1 && D.hadPQ) {
       if (!r8) {  // planes of one right-hand side
         const size_t smem = pqx_smem_bytes<32>();
         cudaFuncSetAttribute(k_m2l_had_pqx2<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        dim3 g1((npar + D.tune.hadRows - 1) / D.tune.hadRows, (P.nEff + 31) / 32, kc);
+        dim3 g1((npar + D.tune.hadRows - 1) / D.tune.hadRows, (P.nEff32 + 31) / 32, kc);
         k_m2l_had_pqx2<32, false><<<g1, PQX_THREADS, smem, st>>>(
-            npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen32, PqLayout{effDR, P.nEff}, D.m2lT32, D.effVal32,
-            PqLayout{effVR, P.nEff}, 1, 0, P.nEff, kc, nrmfc, D.transIdDev);
+            npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen32, PqLayout{effDR, P.nEff32}, D.m2lT32, D.effVal32,
+            PqLayout{effVR, P.nEff32}, 1, 0, P.nEff32, kc, nrmfc, D.transIdDev);
       } else if (D.hadW && D.m2lTw32 && D.tune.hadRhsPerThread == 2) {  // 27-product form, 2 RHS a thread
         const size_t smem = (size_t)W8_OFFS * 27 * W8X2_F * sizeof(float2);
         cudaFuncSetAttribute(k_m2l_had_w8x2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        dim3 g8((npar + D.tune.hadRows - 1) / D.tune.hadRows, (P.nEff + W8X2_F - 1) / W8X2_F, nblk);
+        dim3 g8((npar + D.tune.hadRows - 1) / D.tune.hadRows, (P.nEff32 + W8X2_F - 1) / W8X2_F, nblk);
         k_m2l_had_w8x2<<<g8, PQX_THREADS, smem, st>>>(npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen32,
-                                                       PqLayout{blkDen, (int64_t)P.nEff * 8}, D.m2lTw32, D.effVal32,
-                                                       PqLayout{blkVal, (int64_t)P.nEff * 8}, P.nEff, kc, nrmfc);
+                                                       PqLayout{blkDen, (int64_t)P.nEff32 * 8}, D.m2lTw32, D.effVal32,
+                                                       PqLayout{blkVal, (int64_t)P.nEff32 * 8}, P.nEff32, kc, nrmfc);
       } else if (D.hadW && D.m2lTw32) {  // 27-product form
         const size_t smem = (size_t)W8_OFFS * 27 * 4 * sizeof(float2);
         cudaFuncSetAttribute(k_m2l_had_w8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        dim3 g8((npar + D.tune.hadRows - 1) / D.tune.hadRows, (P.nEff + 3) / 4, nblk);
+        dim3 g8((npar + D.tune.hadRows - 1) / D.tune.hadRows, (P.nEff32 + 3) / 4, nblk);
         k_m2l_had_w8<<<g8, PQX_THREADS, smem, st>>>(npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen32,
-                                                     PqLayout{blkDen, (int64_t)P.nEff * 8}, D.m2lTw32, D.effVal32,
-                                                     PqLayout{blkVal, (int64_t)P.nEff * 8}, P.nEff, kc, nrmfc);
+                                                     PqLayout{blkDen, (int64_t)P.nEff32 * 8}, D.m2lTw32, D.effVal32,
+                                                     PqLayout{blkVal, (int64_t)P.nEff32 * 8}, P.nEff32, kc, nrmfc);
       } else {
         const size_t smem = pqx_smem_bytes<4>();
-        dim3 g8((npar + D.tune.hadRows - 1) / D.tune.hadRows, (P.nEff + 3) / 4, nblk);
+        dim3 g8((npar + D.tune.hadRows - 1) / D.tune.hadRows, (P.nEff32 + 3) / 4, nblk);
         k_m2l_had_pqx2<4, false><<<g8, PQX_THREADS, smem, st>>>(
-            npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen32, PqLayout{blkDen, (int64_t)P.nEff * 8}, D.m2lT32,
-            D.effVal32, PqLayout{blkVal, (int64_t)P.nEff * 8}, 8, 1, P.nEff, kc, nrmfc, D.transIdDev);
+            npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen32, PqLayout{blkDen, (int64_t)P.nEff32 * 8}, D.m2lT32,
+            D.effVal32, PqLayout{blkVal, (int64_t)P.nEff32 * 8}, 8, 1, P.nEff32, kc, nrmfc, D.transIdDev);
       }
     } else if (P.sdm == 1 && P.tdm == 1) {
       const size_t smem = had_smem_bytes<float2>();
       cudaFuncSetAttribute(k_m2l_had_list<float2, KB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
-      dim3 g2((ntrg + HS_BOXES - 1) / HS_BOXES, (P.nEff + 31) / 32, kb);
+      dim3 g2((ntrg + HS_BOXES - 1) / HS_BOXES, (P.nEff32 + 31) / 32, kb);
       k_m2l_had_list<float2, KB, false><<<g2, HS_THREADS, smem, st>>>(
-          ntrg, D.vTrgPtr, (const int2*)D.vTrgEnt, D.effDen32, effDR, D.m2lT32, D.effVal32, effVR, P.nEff, kc,
+          ntrg, D.vTrgPtr, (const int2*)D.vTrgEnt, D.effDen32, effDR, D.m2lT32, D.effVal32, effVR, P.nEff32, kc,
           nrmfc);
     } else if (P.sdm == 4 && P.tdm == 3) FMMG_HAD32(4, 3);
     else FMMG_HAD32(3, 3);
@@ -1192,7 +1174,7 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, bool overlap
   do {                                                                                                         \
     constexpr size_t sm = r8_inv_smem<NP_>();                                                                  \
     cudaFuncSetAttribute(k_m2l_inv32r8<NP_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);            \
-    k_m2l_inv32r8<NP_><<<dim3(ntrg, nblk), 256, sm, st>>>(D.vTrgNodes, D.effVal32, blkVal, P.nEff, D.surfIJK,  \
+    k_m2l_inv32r8<NP_><<<dim3(ntrg, nblk), 256, sm, st>>>(D.vTrgNodes, D.effVal32, blkVal, P.nEff32, D.surfIJK,  \
                                                           P.nDC, D.dchk32, nn * dc, kc);                       \
   } while (0)
     switch (P.o.np) {
@@ -1207,7 +1189,7 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, bool overlap
     ls->launches++;
   } else if ((mask & 4) && npar > 0 && ntrg > 0) {
 #define FMMG_INV32(NP_)                                                                                   \
-  k_m2l_inv32<NP_><<<dim3(ntrg, kc), 128, 0, st>>>(D.vTrgNodes, D.effVal32, effVR, P.nEff, P.tdm, D.surfIJK, \
+  k_m2l_inv32<NP_><<<dim3(ntrg, kc), 128, 0, st>>>(D.vTrgNodes, D.effVal32, effVR, P.nEff32, P.tdm, D.surfIJK, \
                                                     P.nDC, D.dchk32, nn * dc)
     switch (P.o.np) {
       case 3: FMMG_INV32(3); break;
@@ -1310,7 +1292,7 @@ std::string dev_evaluate_mixed(const Plan& P, DevState& D, const double* dDen, d
   // right-hand sides per pass, bounded by a device-memory budget for the
   // per-density work arrays (node rows and M2L spectra)
   const double perRhs = 4.0 * P.nn * (ue + uc + de + dc + pad4(P.kUp) + pad4(P.kDn)) +
-                        8.0 * P.nEff * (P.vSrcNodes.size() * P.sdm + P.vTrgNodes.size() * P.tdm) +
+                        8.0 * P.nEff32 * (P.vSrcNodes.size() * P.sdm + P.vTrgNodes.size() * P.tdm) +
                         8.0 * (ns * P.sd + nt * P.td);
   const double budget = D.mixedBudgetBytes;
   int kmax = (int)std::max(1.0, std::floor(budget / std::max(perRhs, 1.0)));

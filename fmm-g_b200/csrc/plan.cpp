@@ -501,6 +501,11 @@ std::string Plan::build_operators() {
   const int n = 2 * np;
   nReg = n * n * n;
   nEff = n * n * (n / 2 + 1);
+  {
+    const int n32 = 2 * np - 1;
+    nReg32 = n32 * n32 * n32;
+    nEff32 = n32 * n32 * (n32 / 2 + 1);
+  }
   const double eps = std::pow(0.1, np + 1);  // matmgnt3d_mpi.cpp:37-40
   const int ue = nUE * sdm, uc = nUC * tdm, de = nDE * sdm, dc = nDC * tdm;
   std::vector<double> A, Rm;
@@ -549,35 +554,40 @@ std::string Plan::build_operators() {
       for (int i3 = -3; i3 <= 3; i3++)
         transId[i1 + 3][i2 + 3][i3 + 3] =
             (std::abs(i1) > 1 || std::abs(i2) > 1 || std::abs(i3) > 1) ? cnt++ : -1;
-  std::vector<double> reg(3 * (size_t)nReg);
-  {
+  // the translations sampled on the n^3 regular grid (offsets
+  // (i < np ? i : i - n) steps per axis), r2c transformed
+  const int mdof = sdm * tdm;
+  auto spectra = [&](int n_, int nEff_, std::vector<std::complex<double>>& out) {
+    const int nReg_ = n_ * n_ * n_;
+    std::vector<double> reg(3 * (size_t)nReg_);
     double step = 2.0 / (np - 1);
     size_t c = 0;
-    for (int k = 0; k < n; k++)
-      for (int j = 0; j < n; j++)
-        for (int i = 0; i < n; i++, c++) {
-          reg[3 * c + 0] = (i < np ? i : i - n) * step;
-          reg[3 * c + 1] = (j < np ? j : j - n) * step;
-          reg[3 * c + 2] = (k < np ? k : k - n) * step;
+    for (int k = 0; k < n_; k++)
+      for (int j = 0; j < n_; j++)
+        for (int i = 0; i < n_; i++, c++) {
+          reg[3 * c + 0] = (i < np ? i : i - n_) * step;
+          reg[3 * c + 1] = (j < np ? j : j - n_) * step;
+          reg[3 * c + 2] = (k < np ? k : k - n_) * step;
         }
-  }
-  const int mdof = sdm * tdm;
-  m2lT.assign((size_t)316 * nEff * mdof, std::complex<double>(0, 0));
+    out.assign((size_t)316 * nEff_ * mdof, std::complex<double>(0, 0));
 #pragma omp parallel for schedule(dynamic, 2)
-  for (int t = 0; t < 343; t++) {
-    int i1 = t / 49 - 3, i2 = (t / 7) % 7 - 3, i3 = t % 7 - 3;
-    int id = transId[i1 + 3][i2 + 3][i3 + 3];
-    if (id < 0) continue;
-    double sp[3] = {i1 * 2.0, i2 * 2.0, i3 * 2.0};
-    std::vector<double> tt;
-    mm_matrix_rt(mm, o.coefs, 1, sp, nReg, reg.data(), tt);  // (nReg*tdm) x sdm
-    std::vector<double> grid((size_t)nReg * mdof);
-    for (int k = 0; k < nReg; k++)
-      for (int i = 0; i < tdm; i++)
-        for (int j = 0; j < sdm; j++)
-          grid[(size_t)k * mdof + j * tdm + i] = tt[(size_t)j * nReg * tdm + i + (size_t)k * tdm];
-    rfft3_host(n, mdof, grid.data(), &m2lT[(size_t)id * nEff * mdof]);
-  }
+    for (int t = 0; t < 343; t++) {
+      int i1 = t / 49 - 3, i2 = (t / 7) % 7 - 3, i3 = t % 7 - 3;
+      int id = transId[i1 + 3][i2 + 3][i3 + 3];
+      if (id < 0) continue;
+      double sp[3] = {i1 * 2.0, i2 * 2.0, i3 * 2.0};
+      std::vector<double> tt;
+      mm_matrix_rt(mm, o.coefs, 1, sp, nReg_, reg.data(), tt);  // (nReg*tdm) x sdm
+      std::vector<double> grid((size_t)nReg_ * mdof);
+      for (int k = 0; k < nReg_; k++)
+        for (int i = 0; i < tdm; i++)
+          for (int j = 0; j < sdm; j++)
+            grid[(size_t)k * mdof + j * tdm + i] = tt[(size_t)j * nReg_ * tdm + i + (size_t)k * tdm];
+      rfft3_host(n_, mdof, grid.data(), &out[(size_t)id * nEff_ * mdof]);
+    }
+  };
+  spectra(n, nEff, m2lT);
+  spectra(2 * np - 1, nEff32, m2lT32);
   return std::string();
 }
 
@@ -589,6 +599,49 @@ void Plan::refactor_c2e(int which) {
     kUp = svd_factors(nUE * sdm, nUC * tdm, uc2ue.data(), cut, uc2ueF1, uc2ueF2);
   else if (which == 2)
     kDn = svd_factors(nDE * sdm, nDC * tdm, dc2de.data(), cut, dc2deF1, dc2deF2);
+}
+
+void Plan::m2l_spectrum32(int id) {
+  typedef std::complex<double> C;
+  const int n = 2 * o.np, m = 2 * o.np - 1, nh = n / 2 + 1, mdof = sdm * tdm;
+  const C* X = &m2lT[(size_t)id * nEff * mdof];
+  std::vector<C> w(n);
+  for (int j = 0; j < n; j++) w[j] = C(std::cos(2.0 * M_PI * j / n), std::sin(2.0 * M_PI * j / n));
+  // z and y complex inverse transforms: B[z][y][kx][h]
+  std::vector<C> A((size_t)n * n * nh * mdof), B((size_t)n * n * nh * mdof);
+  for (int z = 0; z < n; z++)
+    for (int ky = 0; ky < n; ky++)
+      for (int kx = 0; kx < nh; kx++)
+        for (int h = 0; h < mdof; h++) {
+          C s(0, 0);
+          for (int kz = 0; kz < n; kz++) s += X[(((size_t)kz * n + ky) * nh + kx) * mdof + h] * w[(kz * z) % n];
+          A[(((size_t)z * n + ky) * nh + kx) * mdof + h] = s;
+        }
+  for (int z = 0; z < n; z++)
+    for (int y = 0; y < n; y++)
+      for (int kx = 0; kx < nh; kx++)
+        for (int h = 0; h < mdof; h++) {
+          C s(0, 0);
+          for (int ky = 0; ky < n; ky++) s += A[(((size_t)z * n + ky) * nh + kx) * mdof + h] * w[(ky * y) % n];
+          B[(((size_t)z * n + y) * nh + kx) * mdof + h] = s;
+        }
+  // x c2r at the offsets the odd grid keeps, written into the m^3 grid
+  std::vector<double> grid((size_t)m * m * m * mdof);
+  auto src = [&](int i) { return i < o.np ? i : i - m + n; };  // odd-grid index -> even-grid index
+  const double scale = 1.0 / ((double)n * n * n);
+  for (int z = 0; z < m; z++)
+    for (int y = 0; y < m; y++)
+      for (int x = 0; x < m; x++)
+        for (int h = 0; h < mdof; h++) {
+          const int zz = src(z), yy = src(y), xx = src(x);
+          double s = 0;
+          for (int kx = 0; kx < nh; kx++) {
+            const C v = B[(((size_t)zz * n + yy) * nh + kx) * mdof + h] * w[(kx * xx) % n];
+            s += (kx == 0 || kx == n / 2 ? 1.0 : 2.0) * v.real();
+          }
+          grid[(((size_t)z * m + y) * m + x) * mdof + h] = s * scale;
+        }
+  rfft3_host(m, mdof, grid.data(), &m2lT32[(size_t)id * nEff32 * mdof]);
 }
 
 }  // namespace fmmg

@@ -51,6 +51,9 @@ struct Plan {
   bool nrm = false;
   // surfaces and grid (matmgnt3d_mpi.cpp:451-499)
   int nUE = 0, nUC = 0, nDE = 0, nDC = 0, nReg = 0, nEff = 0;
+  // the FP32 pass transforms on the (2np-1)^3 grid, the smallest on which the
+  // band-to-band M2L convolution does not wrap (offsets -(np-1)..np-1)
+  int nReg32 = 0, nEff32 = 0;
   std::vector<double> sam[4];  // UE, UC, DE, DC templates at unit radius scale, [n][3]
 
   // ---- tree
@@ -122,6 +125,7 @@ struct Plan {
   std::vector<double> dc2de;     // [nDE*sdm][nDC*tdm]       C2E down (pinv)
   std::vector<double> l2l;       // [8*nDC*tdm][nDE*sdm]     8 octant DE->DC matrices stacked
   std::vector<std::complex<double>> m2lT;  // [316][nEff][sdm*tdm] (FFTW r2c layout)
+  std::vector<std::complex<double>> m2lT32;  // [316][nEff32][sdm*tdm]: the same translations, (2np-1)^3 grid
   // the two pseudo-inverses in factored form for the FP32 path:
   // C2E = F2 (F1 x), F1 = diag(1/s) U^T [k][check], F2 = V [equiv][k]
   int kUp = 0, kDn = 0;
@@ -134,6 +138,9 @@ struct Plan {
   // refactor the pinv the caller replaced (0: C2E up, 2: C2E down) from its
   // explicit table, so the FP32 pass applies the same operator
   void refactor_c2e(int which);
+  // m2lT32[id] from m2lT[id] (after the caller replaced it): inverse r2c to
+  // the kernel samples, keep the offsets -(np-1)..np-1, r2c on the odd grid
+  void m2l_spectrum32(int id);
   int child(int n, int o) const { return chd[n] + o; }
   bool leaf(int n) const { return chd[n] < 0; }
 

@@ -223,3 +223,40 @@ def test_mixed_follows_replaced_pinv():
     print("replaced pinv: fp64 change %.3e, mixed vs fp64 %.3e" % (rel_l2(d1, d0), rel_l2(m1, d1)))
     assert rel_l2(d1, d0) > 1e-2  # the replacement is visible
     assert rel_l2(m1, d1) <= 1e-5
+
+
+@pytest.mark.parametrize("np_", [5, 6])
+def test_mixed_follows_replaced_translation_spectra(np_):
+    """The FP32 pass transforms on the (2np-1)^3 grid, the reference's tables
+    live on the (2np)^3 grid: a translation spectrum the caller replaces is
+    converted exactly (inverse r2c to the kernel samples, the offsets
+    -(np-1)..np-1 the band-to-band convolution reads, r2c on the odd grid), so
+    the mixed form still matches the FP64 form.  Two translations are swapped,
+    which changes the V list visibly."""
+    import torch
+    rng = np.random.default_rng(92 + np_)
+    n = 30000
+    src = W.sphere_clusters(n, rng)
+    f = fmmg.FMM3d(111, np_=np_, pts_max=64)
+    f.setup(src)
+    D = torch.from_numpy(rng.normal(size=(2, n))).cuda()
+
+    def both():
+        outs = []
+        for prec in (fmmg.PREC_FP64, fmmg.PREC_MIXED):
+            out = torch.zeros(2, n, dtype=torch.float64, device="cuda")
+            torch.cuda.synchronize()
+            f.evaluate_device(D, out, 2, prec)
+            f.sync()
+            outs.append(out.cpu().numpy())
+        return outs
+
+    d0, m0 = both()
+    assert rel_l2(m0, d0) <= 1e-5
+    a, b = f.operator(4, 0), f.operator(4, 315)
+    f.set_operator(4, 0, b)
+    f.set_operator(4, 315, a)
+    d1, m1 = both()
+    print("np %d swapped spectra: fp64 change %.3e, mixed vs fp64 %.3e" % (np_, rel_l2(d1, d0), rel_l2(m1, d1)))
+    assert rel_l2(d1, d0) > 1e-4
+    assert rel_l2(m1, d1) <= 1e-5
