@@ -681,11 +681,21 @@ fmmg_status fmmg_plan_stats(const fmmg_handle* h, int64_t* st, int n) {
     if (d >= 3) dnFlops += (int64_t)P.dnL2L[d - 1].size() * 2 * 8 * dc * de;
     dnFlops += (int64_t)P.dnC2E[d].size() * 2 * de * dc;
   }
-  int64_t v[16] = {nearPairs, s2mPairs, s2lPairs, m2tPairs, l2tPairs,
+  // the FP32 pass: parents take the folded C2E x M2M product, leaves and the
+  // downward pass the factored pseudo-inverses (ranks padded to 4)
+  const int64_t kUp4 = (P.kUp + 3) & ~3, kDn4 = (P.kDn + 3) & ~3;
+  int64_t upFlops32 = 0, dnFlops32 = 0;
+  for (int d = 0; d <= P.maxDepth; d++) {
+    upFlops32 += (int64_t)P.upM2M[d].size() * 2 * ue * 8 * ue + (int64_t)P.upLeaf[d].size() * 2 * kUp4 * (uc + ue);
+    if (d >= 3) dnFlops32 += (int64_t)P.dnL2L[d - 1].size() * 2 * 8 * dc * de;
+    dnFlops32 += (int64_t)P.dnC2E[d].size() * 2 * kDn4 * (dc + de);
+  }
+  int64_t v[19] = {nearPairs, s2mPairs, s2lPairs, m2tPairs, l2tPairs,
                    (int64_t)P.vSrcNodes.size(), (int64_t)P.vTrgNodes.size(), (int64_t)P.vParents.size(),
                    (int64_t)P.vNbr.idx.size(), (int64_t)P.V.idx.size(), upFlops, dnFlops,
-                   (int64_t)P.nEff, (int64_t)P.sdm, (int64_t)P.tdm, (int64_t)P.nn};
-  std::copy(v, v + 16, st);
+                   (int64_t)P.nEff, (int64_t)P.sdm, (int64_t)P.tdm, (int64_t)P.nn,
+                   (int64_t)P.nEff32, upFlops32, dnFlops32};
+  std::copy(v, v + std::min(n, 19), st);
   return FMMG_OK;
 }
 

@@ -254,24 +254,29 @@ class FMM3d:
 
     PLAN_STATS = ("near_pairs", "s2m_pairs", "s2l_pairs", "m2t_pairs", "l2t_pairs", "v_src", "v_trg",
                   "v_parents", "v_parent_pairs", "v_interactions", "up_gemm_flops", "dn_gemm_flops", "n_eff",
-                  "sdm", "tdm", "nodes")
+                  "sdm", "tdm", "nodes", "n_eff_mixed", "up_gemm_flops_mixed", "dn_gemm_flops_mixed")
     # FLOPs counted per kernel pair for the FP64 direct sums: offset (3),
     # r^2 (5), inverse square root (1), scale and accumulate per component
     PAIR_FLOPS = {111: 11, 121: 16, 311: 40, 312: 20, 321: 36, 322: 26, 511: 40, 521: 60, 301: 46}
 
     def plan_stats(self):
-        st = np.zeros(16, dtype=np.int64)
-        self._chk(lib().fmmg_plan_stats(self.h, st.ctypes.data_as(_i64p), 16))
+        st = np.zeros(len(self.PLAN_STATS), dtype=np.int64)
+        self._chk(lib().fmmg_plan_stats(self.h, st.ctypes.data_as(_i64p), len(self.PLAN_STATS)))
         return dict(zip(self.PLAN_STATS, st.tolist()))
 
     def algorithmic_work(self, k=1, precision="fp64"):
         """Per kernel class: the roofline that bounds it and its algorithmic work
         for one evaluate of k right-hand sides (pairs x FLOPs per pair x k, GEMM
-        FLOPs x k, or the minimum memory bytes of the spectral M2L steps)."""
+        FLOPs x k, or the minimum memory bytes of the spectral M2L steps), for
+        the algorithm the given form runs: the mixed form transforms on the
+        (2np-1)^3 grid and folds the upward C2E into M2M for parents."""
         s = self.plan_stats()
         mm = {111: 111, 121: 111, 312: 111, 322: 111, 311: 301, 321: 301, 511: 511, 521: 511}[self.kt]
         fp, fpm = self.PAIR_FLOPS[self.kt], self.PAIR_FLOPS[mm]
-        ne, sdm, tdm = s["n_eff"], s["sdm"], s["tdm"]
+        mixed = precision != "fp64"
+        ne, sdm, tdm = s["n_eff_mixed" if mixed else "n_eff"], s["sdm"], s["tdm"]
+        upf = s["up_gemm_flops_mixed" if mixed else "up_gemm_flops"]
+        dnf = s["dn_gemm_flops_mixed" if mixed else "dn_gemm_flops"]
         cb = 16 if precision == "fp64" else 8  # bytes per complex value
         pipe = "fp64" if precision == "fp64" else "fp32"
         return {
@@ -280,8 +285,8 @@ class FMM3d:
             "s2l": {"bound": pipe, "flops": k * s["s2l_pairs"] * fp, "pairs": s["s2l_pairs"]},
             "m2t": {"bound": pipe, "flops": k * s["m2t_pairs"] * fpm, "pairs": s["m2t_pairs"]},
             "l2t": {"bound": pipe, "flops": k * s["l2t_pairs"] * fpm, "pairs": s["l2t_pairs"]},
-            "up_gemm": {"bound": pipe, "flops": k * s["up_gemm_flops"]},
-            "dn_gemm": {"bound": pipe, "flops": k * s["dn_gemm_flops"]},
+            "up_gemm": {"bound": pipe, "flops": k * upf},
+            "dn_gemm": {"bound": pipe, "flops": k * dnf},
             "m2l_had": {"bound": pipe,
                         "bytes": cb * ne * (k * s["v_src"] * sdm + k * s["v_trg"] * tdm + 316 * sdm * tdm),
                         "flops": 8 * ne * sdm * tdm * s["v_interactions"] * k},

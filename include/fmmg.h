@@ -175,7 +175,10 @@ fmmg_status fmmg_kernel_times(const fmmg_handle* h, double* ms, int n);
  * kernel-pair counts of the near-field P2P, S2M, S2L, M2T and L2T sums;
  * M2L source spectra, target spectra, target parents, (parent, neighbour)
  * pairs and V-list interactions; FLOPs of the upward and downward GEMMs;
- * spectrum length, equivalent-kernel source and target DOF, node count. */
+ * spectrum length, equivalent-kernel source and target DOF, node count.  With
+ * n >= 19 also the mixed form's own figures: spectrum length on its
+ * (2np-1)^3 grid and the FLOPs of its upward GEMMs (parents through the folded
+ * C2E x M2M product) and downward GEMMs (factored pseudo-inverses). */
 fmmg_status fmmg_plan_stats(const fmmg_handle* h, int64_t* stats, int n);
 
 /* Number of this library's kernels launched by the last evaluate call. */

@@ -189,3 +189,22 @@ def test_degenerate_inputs_build_a_plan():
     h.setup(edge)
     _, ps, _ = h.tree()
     assert sorted(ps.tolist()) == [0, 1, 2, 3]
+
+
+@pytest.mark.parametrize("np_", [4, 5, 6])
+def test_plan_stats_of_the_mixed_form(np_):
+    """The mixed form's own work figures: its spectra live on the
+    (2np-1)^3 grid (r2c half spectrum, no Nyquist term), and folding the
+    upward C2E into M2M for parents needs fewer upward FLOPs than the
+    reference's M2M + C2E."""
+    rng = np.random.default_rng(31 + np_)
+    lib = fmmg.FMM3d(111, np_=np_, pts_max=20, device=-1)
+    lib.setup(_clustered(rng, 6000))
+    s = lib.plan_stats()
+    n, m = 2 * np_, 2 * np_ - 1
+    assert s["n_eff"] == n * n * (n // 2 + 1)
+    assert s["n_eff_mixed"] == m * m * (m // 2 + 1) == m * m * np_
+    assert 0 < s["up_gemm_flops_mixed"] < s["up_gemm_flops"]
+    assert s["dn_gemm_flops_mixed"] > 0
+    w64, w32 = lib.algorithmic_work(k=8, precision="fp64"), lib.algorithmic_work(k=8, precision="fp32")
+    assert w32["m2l_had"]["flops"] * s["n_eff"] == w64["m2l_had"]["flops"] * s["n_eff_mixed"]
