@@ -51,7 +51,7 @@ inline int kernel_trg_dof(int kt) {
   }
   return 0;
 }
-inline int kernel_mm(int kt) {
+constexpr int kernel_mm(int kt) {
   switch (kt) {
     case LAP_S_U: case LAP_D_U: case STK_S_P: case STK_D_P: return LAP_S_U;
     case STK_S_U: case STK_D_U: return STK_F_U;

@@ -34,6 +34,7 @@ namespace fmmg {
 __constant__ int16_t c_transId32[343];
 
 constexpr int MX_THREADS = 128;
+constexpr int MX_THREADS_FAR = 192;  // M2T: 2^6 x 3 also allows target groups of 24, 48, 96
 constexpr int MX_TILE = 128;
 // staged sources (or surface points) per round: 256 when a source carries at
 // most 8 density values and no normal (the static shared memory stays under
@@ -96,13 +97,23 @@ __device__ __forceinline__ void reduce_store(double* sRed, const double* acc, in
   }
 }
 
-// Lanes per target group of a leaf with tn targets: the smallest power of two
-// from gmin (8, 16 or 32) up to 128 that holds them (a leaf holds
-// ~ptsMax/4..ptsMax points), the rest of the CTA splitting the sources.
+// Lanes per target group of a leaf with tn targets: the smallest of 8, 16,
+// 24, 32, 48, 64, 96, 128 that divides the CTA size, is at least gmin and
+// holds them, else the whole CTA (a leaf holds ~ptsMax/4..ptsMax points); the
+// rest of the CTA splits the sources.
+template <int THREADS>
 __device__ __forceinline__ int mx_group(int64_t tn, int gmin = 8) {
-  int g = gmin;
-  while (g < 128 && g < tn) g *= 2;
-  return g;
+  if constexpr ((THREADS & (THREADS - 1)) == 0) {  // power of two: 8, 16, 32, ...
+    int g = gmin;
+    while (g < THREADS && g < tn) g *= 2;
+    return g;
+  } else {
+    constexpr int G[7] = {8, 16, 24, 32, 48, 64, 96};
+#pragma unroll
+    for (int i = 0; i < 7; i++)
+      if (THREADS % G[i] == 0 && G[i] >= gmin && G[i] >= tn) return G[i];
+    return THREADS;
+  }
 }
 
 // The N staged densities of one source from shared memory into registers,
@@ -154,7 +165,7 @@ __global__ void __launch_bounds__(MX_THREADS)
   const int64_t e0 = ptr[row], e1 = ptr[row + 1];
   const double cx = ctr[3 * g], cy = ctr[3 * g + 1], cz = ctr[3 * g + 2];
   const int tid = threadIdx.x;
-  const int TG = mx_group(tn);
+  const int TG = mx_group<MX_THREADS>(tn);
   const int S = MX_THREADS / TG;
   const int tl = tid % TG, sp = tid / TG;
   for (int64_t t0 = 0; t0 < tn; t0 += TG) {
@@ -229,8 +240,8 @@ __global__ void __launch_bounds__(MX_THREADS)
 
 // equivalent surfaces -> targets: L2T (own DE surface, downward density) and
 // M2T (UE surfaces of the W nodes, upward densities), equivalent kernel
-template <int KM, int KB>
-__global__ void __launch_bounds__(MX_THREADS)
+template <int KM, int KB, int THREADS>
+__global__ void __launch_bounds__(THREADS)
     k_e2t32(const int32_t* __restrict__ rows, const int64_t* __restrict__ farPtr, const int32_t* __restrict__ farIdx,
             int useOwn, int useFar, const int32_t* __restrict__ depth, const double* __restrict__ ctr,
             const double* __restrict__ rad, const double* __restrict__ samUE, int nUE,
@@ -241,15 +252,15 @@ __global__ void __launch_bounds__(MX_THREADS)
   constexpr int SD = KTraits<KM>::SD, TD = KTraits<KM>::TD;
   __shared__ float4 sPos[MX_TILE];
   __shared__ __align__(16) float sDen[MX_TILE * SD * KB];
-  __shared__ double sRed[MX_THREADS * TD * KB];
+  __shared__ double sRed[THREADS * TD * KB];
   const int row = blockIdx.x;
   const int rhs0 = blockIdx.y * KB;
   const int g = rows[row];
   const int64_t tb = trgBeg[g], tn = trgCnt[g];
   const double gx = ctr[3 * g], gy = ctr[3 * g + 1], gz = ctr[3 * g + 2];
   const int tid = threadIdx.x;
-  const int TG = mx_group(tn, gmin);
-  const int S = MX_THREADS / TG;
+  const int TG = mx_group<THREADS>(tn, gmin);
+  const int S = THREADS / TG;
   const int tl = tid % TG, sp = tid / TG;
   const int own = (useOwn && depth[g] >= 2) ? 1 : 0;
   const int64_t f0 = useFar ? farPtr[row] : 0, nf = useFar ? farPtr[row + 1] - f0 : 0;
@@ -277,7 +288,7 @@ __global__ void __launch_bounds__(MX_THREADS)
       for (int base = 0; base < ns; base += MX_TILE) {
         const int cnt = min(MX_TILE, ns - base);
         __syncthreads();
-        for (int i = tid; i < cnt; i += MX_THREADS) {
+        for (int i = tid; i < cnt; i += THREADS) {
           const int j = base + i;
           sPos[i] = make_float4((float)(ox + r * sam[3 * j]), (float)(oy + r * sam[3 * j + 1]),
                                 (float)(oz + r * sam[3 * j + 2]), 0.f);
@@ -985,11 +996,7 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
 // overlap: run the near field and the W list on D.side (an untimed pass; a
 // timed one keeps every stage on the main stream so the events bracket it)
 template <int KT, int KB>
-static void run_mixed(const Plan& P, DevState& D, int kc, int mask, bool overlap, LaunchStats* ls) {
-  if constexpr (KTraits<KT>::TD != 1 && KB > 4) {
-    run_mixed<KT, 4>(P, D, kc, mask, overlap, ls);  // pick_kb never asks for this
-    return;
-  }
+static void run_mixed_blocks(const Plan& P, DevState& D, int kc, int mask, bool overlap, LaunchStats* ls) {
   cudaStream_t st = D.stream;
   const int64_t ue = (int64_t)P.nUE * P.sdm, uc = (int64_t)P.nUC * P.tdm;
   const int64_t de = (int64_t)P.nDE * P.sdm, dc = (int64_t)P.nDC * P.tdm;
@@ -1203,26 +1210,22 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, bool overlap
     ls->launches++;
   }
   cudaEventRecord(D.ev[EV_M2L_INV], st);
-  // target groups of at least 8 lanes for L2T (one surface per leaf), 32 for
-  // M2T (many small W-list surfaces per leaf, where narrower groups measured
-  // slower on B200)
+  // L2T (one surface per leaf): 128-thread CTAs, target groups from 8 lanes;
+  // M2T (many small W-list surfaces per leaf): 192-thread CTAs, groups from
+  // 32 lanes -- the choices that measured fastest on B200
   auto e2t = [&](int own, int far, cudaStream_t se) {
     const int nr = far ? (int)P.farLeaves.size() : (int)P.l2tLeaves.size();
     const int32_t* rows = far ? D.farLeaves : D.l2tLeaves;
     if (nr == 0) return;
-    switch (P.mm) {
-#define FMMG_E2T32(KM)                                                                                          \
-  case KM:                                                                                                      \
-    k_e2t32<KM, KB><<<dim3(nr, kb), MX_THREADS, 0, se>>>(rows, D.farPtr, D.farIdx, own, far, D.depth, D.ctr,    \
-                                                         D.rad, D.sam[0], P.nUE, D.sam[2], P.nDE, D.uden32,     \
-                                                         D.dden32, nn * ue, nn * de, D.trgBeg, D.trgCnt, D.trg, \
-                                                         D.valK, valStride, kc, mu, ve, far ? 32 : 8);          \
-    break;
-      FMMG_E2T32(LAP_S_U)
-      FMMG_E2T32(STK_F_U)
-      FMMG_E2T32(NAV_S_U)
-#undef FMMG_E2T32
-    }
+    constexpr int KM = kernel_mm(KT) < 0 ? KT : kernel_mm(KT);  // the equivalent kernel of KT (301 is its own)
+    if (far)
+      k_e2t32<KM, KB, MX_THREADS_FAR><<<dim3(nr, kb), MX_THREADS_FAR, 0, se>>>(
+          rows, D.farPtr, D.farIdx, own, far, D.depth, D.ctr, D.rad, D.sam[0], P.nUE, D.sam[2], P.nDE, D.uden32,
+          D.dden32, nn * ue, nn * de, D.trgBeg, D.trgCnt, D.trg, D.valK, valStride, kc, mu, ve, 32);
+    else
+      k_e2t32<KM, KB, MX_THREADS><<<dim3(nr, kb), MX_THREADS, 0, se>>>(
+          rows, D.farPtr, D.farIdx, own, far, D.depth, D.ctr, D.rad, D.sam[0], P.nUE, D.sam[2], P.nDE, D.uden32,
+          D.dden32, nn * ue, nn * de, D.trgBeg, D.trgCnt, D.trg, D.valK, valStride, kc, mu, ve, 8);
     ls->launches++;
   };
   if (mask & 8) e2t(0, 1, ovl ? D.side : st);
@@ -1253,6 +1256,16 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, bool overlap
   if (ovl) cudaStreamWaitEvent(st, D.evSide, 0);  // join: the target values are complete but for L2T
   if (mask & 32) e2t(1, 0, st);
   cudaEventRecord(D.ev[EV_L2T], st);
+}
+
+// blocks of KB right-hand sides; vector targets take at most 4 a block (pick_kb
+// never asks for more), so those instantiations are never built
+template <int KT, int KB>
+static void run_mixed(const Plan& P, DevState& D, int kc, int mask, bool overlap, LaunchStats* ls) {
+  if constexpr (KTraits<KT>::TD != 1 && KB > 4)
+    run_mixed_blocks<KT, 4>(P, D, kc, mask, overlap, ls);
+  else
+    run_mixed_blocks<KT, KB>(P, D, kc, mask, overlap, ls);
 }
 
 __global__ void k_gather_den_k(int64_t n, int sd, int kc, int64_t stride, const int64_t* __restrict__ perm,
