@@ -260,3 +260,29 @@ def test_mixed_follows_replaced_translation_spectra(np_):
     print("np %d swapped spectra: fp64 change %.3e, mixed vs fp64 %.3e" % (np_, rel_l2(d1, d0), rel_l2(m1, d1)))
     assert rel_l2(d1, d0) > 1e-4
     assert rel_l2(m1, d1) <= 1e-5
+
+
+@pytest.mark.parametrize("np_", [3, 4, 5, 6, 7, 8])
+def test_mixed_matches_fp64_form_every_np(np_):
+    """The mixed form transforms on the (2np-1)^3 grid, the FP64 form on the
+    reference's (2np)^3 grid: for every order both compute the same operator,
+    so they agree to the FP32 rounding of the mixed form (k = 1 and a block of
+    8 right-hand sides)."""
+    import torch
+    rng = np.random.default_rng(60 + np_)
+    n = 30000
+    src = W.sphere_clusters(n, rng)
+    lib = fmmg.FMM3d(111, np_=np_, pts_max=64)
+    lib.setup(src)
+    for k in (1, 8):
+        D = torch.from_numpy(rng.normal(size=(k, n))).cuda()
+        outs = []
+        for prec in (fmmg.PREC_FP64, fmmg.PREC_MIXED):
+            out = torch.zeros(k, n, dtype=torch.float64, device="cuda")
+            torch.cuda.synchronize()
+            lib.evaluate_device(D, out, k, prec)
+            lib.sync()
+            outs.append(out.cpu().numpy())
+        err = rel_l2(outs[1], outs[0])
+        print("np %d k %d mixed vs fp64 %.3e" % (np_, k, err))
+        assert err <= 2e-5
