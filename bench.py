@@ -162,14 +162,34 @@ def run_reference(args):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "points": args.n, "sample_points": n, "kernel": "laplace_s_u", "np": 6,
                    "pts_max": 64, "k_rhs": 1},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
+        "cpu_baseline": dict({"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
+                             **host_cpu()),
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
 
+_PEAKS = {}
+
+
+def host_cpu():
+    """The host CPU model and the threads this process may use."""
+    model = "unknown"
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"cpu_model": model, "nproc": os.cpu_count() or 1}
+
+
 def measure_peak(torch, kind):
     """cuBLAS GEMM 8192^3 best of 3 (TFLOP/s) in FP64 or FP32 (TF32 off): the
-    roof for the CUDA-core kernels, which MEASURED_PEAKS.json does not hold."""
+    roof for the CUDA-core kernels, which MEASURED_PEAKS.json does not hold.
+    Measured once per process."""
+    if kind in _PEAKS:
+        return _PEAKS[kind]
     torch.backends.cuda.matmul.allow_tf32 = False
     dt = torch.float64 if kind == "fp64" else torch.float32
     a = torch.randn(8192, 8192, dtype=dt, device="cuda")
@@ -183,7 +203,34 @@ def measure_peak(torch, kind):
         e.synchronize()
         best = min(best, s.elapsed_time(e))
     del a, b
-    return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+    _PEAKS[kind] = 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+    return _PEAKS[kind]
+
+
+def stage_rooflines(f, kern, torch, k, precision):
+    """Every stage of one step against the roof that bounds it: the pair sums
+    and GEMMs in FLOP/s of the FP32 (FP64) pipe, the spectral transforms in
+    bytes/s of HBM, with the pair rate of the pair sums."""
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    work = f.algorithmic_work(k=k, precision="fp64" if precision == "fp64" else "fp32")
+    out = {}
+    for name, ms in kern.items():
+        w = work.get(name)
+        if w is None or ms <= 0:
+            continue
+        t = ms * 1e-3
+        if w["bound"] == "hbm":
+            ach = w["bytes"] / t / 1e9
+            out[name] = {"ms": ms, "bound": "hbm", "achieved": ach, "unit": "GB/s", "frac": ach / hbm_peak}
+        else:
+            peak = measure_peak(torch, w["bound"])
+            ach = w["flops"] / t / 1e12
+            out[name] = {"ms": ms, "bound": w["bound"], "achieved": ach, "unit": "TFLOP/s", "frac": ach / peak}
+            if w.get("pairs"):
+                out[name]["pairs_per_s"] = k * w["pairs"] / t
+    return out
 
 
 def time_form(f, torch, stream, den_dev, out_dev, n, k, prec, steps, warmup, flush):
@@ -277,6 +324,8 @@ def run_ours(args):
         forms = forms[:1]
     if args.only:
         forms = [forms[["fp64", "mixed1", "mixedk"].index(args.only)]]
+    elif K > 1 and args.precision != "fp64":
+        forms.append(("fp64", fmmg.PREC_FP64, K))  # the FP64 form at equal k
     results = []
     if dist:
         tdist.barrier()
@@ -301,8 +350,8 @@ def run_ours(args):
         adj["ms_per_step"] = FD.max_over_ranks(adj["ms_per_step"], device="cuda")
         adj["target_grad_ms_per_step"] = FD.max_over_ranks(adj["target_grad_ms_per_step"], device="cuda")
     clk = clocks.stop()
-    fp64 = next((r for r in results if r["precision"] == "fp64"), None)
-    fp64_ms = [r["ms_per_step"] for r in results if r["precision"] == "fp64"]
+    fp64 = next((r for r in results if r["precision"] == "fp64" and r["k"] == 1), None)
+    fp64_ms = [r["ms_per_step"] for r in results if r["precision"] == "fp64" and r["k"] == 1]
     if adj and fp64_ms:
         adj["ratio_vs_fp64_forward"] = adj["ms_per_step"] / fp64_ms[0]
     ok = [r for r in results if r["rel_err_vs_dense"] <= 1e-5]
@@ -331,9 +380,9 @@ def run_ours(args):
         cpu = None
         if not args.no_cpu_baseline and not dist:
             rate, times = oracle_rate(CPU_SAMPLE, 1)
-            cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
-                   "sample": "%d-point sample of the workload distribution, 1 thread (one MPI rank), "
-                             "tree/operators prebuilt, %.1f s" % (CPU_SAMPLE, times[0])}
+            cpu = dict({"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
+                        "sample": "%d-point sample of the workload distribution, 1 thread (one MPI rank), "
+                                  "tree/operators prebuilt, %.1f s" % (CPU_SAMPLE, times[0])}, **host_cpu())
         line = {
             "metric": METRIC, "value": head["points_per_s"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
@@ -349,6 +398,8 @@ def run_ours(args):
             "rel_err_vs_dense": head["rel_err_vs_dense"], "check_targets": CHECK_TARGETS,
             "fp64_points_per_s": fp64["points_per_s"] if fp64 else None,
             "speedup_vs_fp64": head["points_per_s"] / fp64["points_per_s"] if fp64 else None,
+            "speedups": speedups(results),
+            "stage_roofline": stage_rooflines(f, head["kernel_ms"], torch, kh, head["precision"]),
             "forms": results, "adjoint": adj, "setup_s": setup_s, "roofline": roof, "clocks": clk,
         }
         if cpu:
@@ -407,6 +458,21 @@ def roofline(f, kern, torch, k, precision):
         out["traffic_source"] = "ncu on the 262,144-point case, scaled by algorithmic bytes; " + tr["profile"]
     else:
         out["traffic"] = None
+    return out
+
+
+def speedups(results):
+    """points/s ratios of the mixed form to the FP64 form: the headline block
+    of k against FP64 at k = 1, at equal k, and k = 1 against k = 1."""
+    pts = {(r["precision"], r["k"]): r["points_per_s"] for r in results}
+    out = {}
+    for (p, k), v in pts.items():
+        if p != "mixed":
+            continue
+        if ("fp64", 1) in pts:
+            out["mixed_k%d_vs_fp64_k1" % k] = v / pts[("fp64", 1)]
+        if k > 1 and ("fp64", k) in pts:
+            out["mixed_k%d_vs_fp64_k%d" % (k, k)] = v / pts[("fp64", k)]
     return out
 
 

@@ -279,12 +279,17 @@ class FMM3d:
         dnf = s["dn_gemm_flops_mixed" if mixed else "dn_gemm_flops"]
         cb = 16 if precision == "fp64" else 8  # bytes per complex value
         pipe = "fp64" if precision == "fp64" else "fp32"
+        # a pair's kernel block is evaluated once for all k right-hand sides;
+        # the multiply-add per (source, target) component repeats per one
+        sd, td = KERNELS[self.kt]
+        pair = fp + (k - 1) * 2 * sd * td
+        pairm = fpm + (k - 1) * 2 * sdm * tdm
         return {
-            "p2p_near": {"bound": pipe, "flops": k * s["near_pairs"] * fp, "pairs": s["near_pairs"]},
-            "s2m": {"bound": pipe, "flops": k * s["s2m_pairs"] * fp, "pairs": s["s2m_pairs"]},
-            "s2l": {"bound": pipe, "flops": k * s["s2l_pairs"] * fp, "pairs": s["s2l_pairs"]},
-            "m2t": {"bound": pipe, "flops": k * s["m2t_pairs"] * fpm, "pairs": s["m2t_pairs"]},
-            "l2t": {"bound": pipe, "flops": k * s["l2t_pairs"] * fpm, "pairs": s["l2t_pairs"]},
+            "p2p_near": {"bound": pipe, "flops": s["near_pairs"] * pair, "pairs": s["near_pairs"]},
+            "s2m": {"bound": pipe, "flops": s["s2m_pairs"] * pair, "pairs": s["s2m_pairs"]},
+            "s2l": {"bound": pipe, "flops": s["s2l_pairs"] * pair, "pairs": s["s2l_pairs"]},
+            "m2t": {"bound": pipe, "flops": s["m2t_pairs"] * pairm, "pairs": s["m2t_pairs"]},
+            "l2t": {"bound": pipe, "flops": s["l2t_pairs"] * pairm, "pairs": s["l2t_pairs"]},
             "up_gemm": {"bound": pipe, "flops": k * upf},
             "dn_gemm": {"bound": pipe, "flops": k * dnf},
             "m2l_had": {"bound": pipe,
