@@ -233,10 +233,11 @@ def stage_rooflines(f, kern, torch, k, precision):
     return out
 
 
-def time_form(f, torch, stream, den_dev, out_dev, n, k, prec, steps, warmup, flush):
+def time_form(f, torch, stream, den_dev, out_dev, n, k, prec, steps, warmup, flush, barrier=None):
     """Device time per step of one evaluate form, replayed as a CUDA graph
     (eager first call, captured second call, replays after); then one eager
-    step with per-kernel events for the breakdown (not part of the timing)."""
+    step with per-kernel events for the breakdown (not part of the timing).
+    With several ranks, barrier() brackets the timed steps."""
     f.set_timing(False)
     f.set_graph(True)
     for _ in range(max(warmup, 3)):
@@ -244,12 +245,17 @@ def time_form(f, torch, stream, den_dev, out_dev, n, k, prec, steps, warmup, flu
     torch.cuda.synchronize()
     graph_active, graph_note = f.graph_state()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    if barrier:
+        barrier()
+    torch.cuda.synchronize()
     for i in range(steps):
         flush.zero_()
         ev[i][0].record(stream)
         f.evaluate_device(den_dev, out_dev, k, prec)
         ev[i][1].record(stream)
     torch.cuda.synchronize()
+    if barrier:
+        barrier()
     launches = f.launch_count() * steps
     ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
     f.set_graph(False)
@@ -337,7 +343,7 @@ def run_ours(args):
         if not args.no_autotune:  # launch shapes for this (kernel, np, k, precision), timed on this GPU
             _, tuned = f.autotune(den, out, k, prec, reps=2)
         ms, kern, stage, launches, graph = time_form(f, torch, stream, den, out, n, k, prec, args.steps, args.warmup,
-                                                     flush)
+                                                     flush, barrier=tdist.barrier if dist else None)
         if dist:
             ms = FD.max_over_ranks(ms, device="cuda")
         vals = out[0].cpu().numpy()
