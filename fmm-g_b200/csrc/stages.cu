@@ -786,10 +786,11 @@ void gemm_rows(DevState& D, int nrows, const int32_t* rows, const int32_t* chd, 
 }
 
 template <int KT>
-static void launch_near(const Plan& P, DevState& D, const int64_t* ptr, const int32_t* idx, LaunchStats* ls) {
+static void launch_near(const Plan& P, DevState& D, const int64_t* ptr, const int32_t* idx, LaunchStats* ls,
+                        cudaStream_t sn) {
   int n = (int)P.evtrLeaves.size();
   if (n == 0) return;
-  k_p2p_near<KT><<<n, P2P_THREADS, 0, D.stream>>>(D.evtrLeaves, ptr, idx, D.srcBeg, D.srcCnt, D.trgBeg, D.trgCnt,
+  k_p2p_near<KT><<<n, P2P_THREADS, 0, sn>>>(D.evtrLeaves, ptr, idx, D.srcBeg, D.srcCnt, D.trgBeg, D.trgCnt,
                                                   D.src, D.nrm, D.den, D.trg, D.val, P.o.coefs[0], P.o.coefs[1]);
   if (ls) ls->launches++;
 }
@@ -805,7 +806,7 @@ static void launch_s2surf(const Plan& P, DevState& D, int nrows, const int32_t* 
   if (ls) ls->launches++;
 }
 
-static void launch_e2t(const Plan& P, DevState& D, int useOwn, int useFar, LaunchStats* ls) {
+static void launch_e2t(const Plan& P, DevState& D, int useOwn, int useFar, LaunchStats* ls, cudaStream_t se) {
   // L2T runs over the leaves at depth >= 2, M2T over the leaves with W nodes
   const int n = useFar ? (int)P.farLeaves.size() : (int)P.l2tLeaves.size();
   const int32_t* rows = useFar ? D.farLeaves : D.l2tLeaves;
@@ -813,7 +814,7 @@ static void launch_e2t(const Plan& P, DevState& D, int useOwn, int useFar, Launc
   switch (P.mm) {
 #define FMMG_E2T(KM)                                                                                          \
   case KM:                                                                                                    \
-    k_e2t<KM><<<n, P2P_THREADS, 0, D.stream>>>(rows, D.farPtr, D.farIdx, useOwn, useFar, D.depth, D.ctr, D.rad, \
+    k_e2t<KM><<<n, P2P_THREADS, 0, se>>>(rows, D.farPtr, D.farIdx, useOwn, useFar, D.depth, D.ctr, D.rad,       \
                                                D.sam[0], P.nUE, D.sam[2], P.nDE, D.uden, D.dden, D.trgBeg,     \
                                                D.trgCnt, D.trg, D.val, P.o.coefs[0], P.o.coefs[1]);            \
     break;
@@ -950,11 +951,20 @@ static void launch_m2l(const Plan& P, DevState& D, LaunchStats* ls) {
 }
 
 template <int KT>
-static void run_stages(const Plan& P, DevState& D, int mask, LaunchStats* ls) {
+// overlap: the near field and the W list run on D.side (an untimed pass; a
+// timed one keeps every stage on the main stream so the events bracket it);
+// the target values still receive near field, M2T and L2T in that order
+static void run_stages(const Plan& P, DevState& D, int mask, LaunchStats* ls, bool overlap) {
   cudaStream_t st = D.stream;
   const int ue = P.nUE * P.sdm, uc = P.nUC * P.tdm, de = P.nDE * P.sdm, dc = P.nDC * P.tdm;
   const int rl = P.o.rootLevel;
   const bool trgOut = !(mask & STAGE_NO_TARGETS);
+  const bool ovl = overlap && trgOut && D.side;
+  if (ovl) {  // fork: the densities are gathered and the target values cleared
+    cudaEventRecord(D.evFork, st);
+    cudaStreamWaitEvent(D.side, D.evFork, 0);
+  }
+  cudaStream_t sn = ovl ? D.side : st;
   if (mask & 1)  // upward: S2M
     launch_s2surf<KT>(P, D, (int)P.s2mLeaves.size(), D.s2mLeaves, nullptr, nullptr, D.sam[1], P.nUC, D.uchk, uc, ls);
   cudaEventRecord(D.ev[EV_S2M], st);
@@ -971,11 +981,15 @@ static void run_stages(const Plan& P, DevState& D, int mask, LaunchStats* ls) {
   cudaEventRecord(D.ev[EV_UP_GEMM], st);
   if (!trgOut) {
   } else if ((mask & 2) && (mask & 8) && (mask & 16)) {
-    launch_near<KT>(P, D, D.nearPtr, D.nearIdx, ls);
+    launch_near<KT>(P, D, D.nearPtr, D.nearIdx, ls, sn);
   } else {
-    if (mask & 2) launch_near<KT>(P, D, D.nearUPtr, D.nearUIdx, ls);
-    if (mask & 8) launch_near<KT>(P, D, D.nearWPtr, D.nearWIdx, ls);
-    if (mask & 16) launch_near<KT>(P, D, D.nearXPtr, D.nearXIdx, ls);
+    if (mask & 2) launch_near<KT>(P, D, D.nearUPtr, D.nearUIdx, ls, sn);
+    if (mask & 8) launch_near<KT>(P, D, D.nearWPtr, D.nearWIdx, ls, sn);
+    if (mask & 16) launch_near<KT>(P, D, D.nearXPtr, D.nearXIdx, ls, sn);
+  }
+  if (ovl) {  // the up pass is done: the W list (upward densities) follows the near field
+    cudaEventRecord(D.evUp, st);
+    cudaStreamWaitEvent(D.side, D.evUp, 0);
   }
   cudaEventRecord(D.ev[EV_NEAR], st);
   if (mask & 4) {
@@ -985,7 +999,8 @@ static void run_stages(const Plan& P, DevState& D, int mask, LaunchStats* ls) {
     cudaEventRecord(D.ev[EV_M2L_HAD], st);
   }
   cudaEventRecord(D.ev[EV_M2L_INV], st);
-  if ((mask & 8) && trgOut) launch_e2t(P, D, 0, 1, ls);
+  if ((mask & 8) && trgOut) launch_e2t(P, D, 0, 1, ls, sn);
+  if (ovl) cudaEventRecord(D.evSide, D.side);
   cudaEventRecord(D.ev[EV_M2T], st);
   if (mask & 16)
     launch_s2surf<KT>(P, D, (int)P.s2lNodes.size(), D.s2lNodes, D.s2lPtr, D.s2lIdx, D.sam[3], P.nDC, D.dchk, dc, ls);
@@ -1003,7 +1018,8 @@ static void run_stages(const Plan& P, DevState& D, int mask, LaunchStats* ls) {
     }
   }
   cudaEventRecord(D.ev[EV_DN_GEMM], st);
-  if ((mask & 32) && trgOut) launch_e2t(P, D, 1, 0, ls);  // L2T
+  if (ovl) cudaStreamWaitEvent(st, D.evSide, 0);  // join before the last writer of the target values
+  if ((mask & 32) && trgOut) launch_e2t(P, D, 1, 0, ls, st);  // L2T
   cudaEventRecord(D.ev[EV_L2T], st);
 }
 
@@ -1025,7 +1041,7 @@ std::string dev_evaluate(const Plan& P, DevState& D, const double* dDen, double*
   FMMG_CK(cudaMemsetAsync(D.dchk, 0, sizeof(double) * (size_t)P.nn * dc, st));
   FMMG_CK(cudaMemsetAsync(D.dden, 0, sizeof(double) * (size_t)P.nn * de, st));
   cudaEventRecord(D.ev[EV_PREP], st);
-  FMMG_DISPATCH_KT(P.o.kt, KT, run_stages<KT>(P, D, mask, ls));
+  FMMG_DISPATCH_KT(P.o.kt, KT, run_stages<KT>(P, D, mask, ls, !timed));
   if (nt > 0) {
     k_scatter_val<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(nt, P.td, D.trgPerm, D.val, dVal);
     if (ls) ls->launches++;
@@ -1074,7 +1090,7 @@ std::string dev_far_field(const Plan& P, DevState& D, const double* dDen) {
   FMMG_CK(cudaMemsetAsync(D.uden, 0, sizeof(double) * (size_t)P.nn * ue, st));
   FMMG_CK(cudaMemsetAsync(D.dchk, 0, sizeof(double) * (size_t)P.nn * dc, st));
   FMMG_CK(cudaMemsetAsync(D.dden, 0, sizeof(double) * (size_t)P.nn * de, st));
-  FMMG_DISPATCH_KT(P.o.kt, KT, run_stages<KT>(P, D, 63 | STAGE_NO_TARGETS, nullptr));
+  FMMG_DISPATCH_KT(P.o.kt, KT, run_stages<KT>(P, D, 63 | STAGE_NO_TARGETS, nullptr, false));
   FMMG_CK(cudaGetLastError());
   return std::string();
 }
