@@ -808,8 +808,11 @@ fmmg_status fmmg_operator(fmmg_handle* h, int which, int idx, double* get, const
   if (count) *count = n;
   if (set) {
     h->opsDirty = true;
-    if (which == 0 || which == 2) P.refactor_c2e(which);  // the FP32 pass applies the pinv factored
-    if (which == 4) P.m2l_spectrum32(idx);                 // and transforms on the (2np-1)^3 grid
+    try {
+      if (which == 0 || which == 2) P.refactor_c2e(which);  // the FP32 pass applies the pinv factored
+      if (which == 4) P.m2l_spectrum32(idx);                 // and transforms on the (2np-1)^3 grid
+    }
+    FMMG_GUARD(h)
   }
   return FMMG_OK;
 }
