@@ -180,9 +180,12 @@ FMMG_UNROLL
   for (int r = 0; r < KB; r++)
 FMMG_UNROLL
     for (int t = 0; t < TD; t++) {
-      R s = R(0);
+      // the first product starts the sum: an explicit 0 + x cannot be dropped
+      // under IEEE rules and would cost an add per term (with SD = 1 the
+      // product and the accumulate fuse into one FMA)
+      R s = K[t * SD] * den[r * SD];
 FMMG_UNROLL
-      for (int c = 0; c < SD; c++) s += K[t * SD + c] * den[r * SD + c];
+      for (int c = 1; c < SD; c++) s += K[t * SD + c] * den[r * SD + c];
       acc[r * TD + t] += s;
     }
 }
