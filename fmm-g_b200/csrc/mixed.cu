@@ -660,6 +660,22 @@ __device__ __forceinline__ void r8_store(float2* p, const float2 (&v)[8]) {
 #pragma unroll
   for (int i = 0; i < 4; i++) q[i] = make_float4(v[2 * i].x, v[2 * i].y, v[2 * i + 1].x, v[2 * i + 1].y);
 }
+// s += a b and s += a conj(b) as four FMAs into the accumulator (a product
+// formed first and then added costs a multiply and an add more: IEEE rules
+// keep the compiler from reassociating it)
+__device__ __forceinline__ void r8_cmac(float2& s, float2 a, float2 b) {
+  s.x = fmaf(a.x, b.x, s.x);
+  s.x = fmaf(-a.y, b.y, s.x);
+  s.y = fmaf(a.x, b.y, s.y);
+  s.y = fmaf(a.y, b.x, s.y);
+}
+__device__ __forceinline__ void r8_cmacc(float2& s, float2 a, float2 b) {
+  s.x = fmaf(a.x, b.x, s.x);
+  s.x = fmaf(a.y, b.y, s.x);
+  s.y = fmaf(a.y, b.x, s.y);
+  s.y = fmaf(-a.x, b.y, s.y);
+}
+
 template <int NP>
 __device__ __forceinline__ void r8_twiddles(float2* twb) {
   using F = FftDims32<NP>;
@@ -730,11 +746,7 @@ __global__ void __launch_bounds__(256)
     for (int ky = 0; ky < N; ky++) {
       float2 s = make_float2(0.f, 0.f);
 #pragma unroll
-      for (int yb = 0; yb < NP; yb++) {
-        const float2 t = cmul(c[yb], twb[ky * NP + yb]);
-        s.x += t.x;
-        s.y += t.y;
-      }
+      for (int yb = 0; yb < NP; yb++) r8_cmac(s, c[yb], twb[ky * NP + yb]);
       X2[r * S2 + (zb * N + ky) * NH + kx] = s;
     }
   }
@@ -751,11 +763,7 @@ __global__ void __launch_bounds__(256)
     for (int kz = 0; kz < N; kz++) {
       float2 s = make_float2(0.f, 0.f);
 #pragma unroll
-      for (int zb = 0; zb < NP; zb++) {
-        const float2 t = cmul(c[zb], twb[kz * NP + zb]);
-        s.x += t.x;
-        s.y += t.y;
-      }
+      for (int zb = 0; zb < NP; zb++) r8_cmac(s, c[zb], twb[kz * NP + zb]);
       out[((int64_t)(kz * N + ky) * NH + kx) * 8 + r] = s;
     }
   }
@@ -796,11 +804,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int kz = 0; kz < N; kz++) {
 #pragma unroll
-      for (int zb = 0; zb < NP; zb++) {
-        const float2 t = cmulc(c[kz], twb[kz * NP + zb]);
-        s[zb].x += t.x;
-        s[zb].y += t.y;
-      }
+      for (int zb = 0; zb < NP; zb++) r8_cmacc(s[zb], c[kz], twb[kz * NP + zb]);
     }
 #pragma unroll
     for (int zb = 0; zb < NP; zb++) Y2[r * S2 + (zb * N + ky) * NH + kx] = s[zb];
@@ -816,11 +820,7 @@ __global__ void __launch_bounds__(256)
     for (int ky = 0; ky < N; ky++) {
       const float2 c = Y2[r * S2 + (zb * N + ky) * NH + kx];
 #pragma unroll
-      for (int yb = 0; yb < NP; yb++) {
-        const float2 t = cmulc(c, twb[ky * NP + yb]);
-        s[yb].x += t.x;
-        s[yb].y += t.y;
-      }
+      for (int yb = 0; yb < NP; yb++) r8_cmacc(s[yb], c, twb[ky * NP + yb]);
     }
 #pragma unroll
     for (int yb = 0; yb < NP; yb++) Y1[r * S1 + (zb * NP + yb) * NH + kx] = s[yb];
