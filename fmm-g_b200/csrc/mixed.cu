@@ -413,6 +413,22 @@ __global__ void __launch_bounds__(MX_SURF)
     }
 }
 
+// s += a b and s += a conj(b) as four FMAs into the accumulator (a product
+// formed first and then added costs a multiply and an add more: IEEE rules
+// keep the compiler from reassociating it)
+__device__ __forceinline__ void r8_cmac(float2& s, float2 a, float2 b) {
+  s.x = fmaf(a.x, b.x, s.x);
+  s.x = fmaf(-a.y, b.y, s.x);
+  s.y = fmaf(a.x, b.y, s.y);
+  s.y = fmaf(a.y, b.x, s.y);
+}
+__device__ __forceinline__ void r8_cmacc(float2& s, float2 a, float2 b) {
+  s.x = fmaf(a.x, b.x, s.x);
+  s.x = fmaf(a.y, b.y, s.x);
+  s.y = fmaf(a.y, b.x, s.y);
+  s.y = fmaf(-a.x, b.y, s.y);
+}
+
 // ------------------------------------------------------------------ FP32 M2L
 // grid (source slots, right-hand sides)
 template <int NP>
@@ -464,9 +480,7 @@ __global__ void __launch_bounds__(128)
       float2 s = make_float2(0.f, 0.f);
 #pragma unroll
       for (int yb = 0; yb < NP; yb++) {
-        float2 t = cmul(X1[(zb * NP + yb) * NH + kx], tw[(ky * (yb + H)) % N]);
-        s.x += t.x;
-        s.y += t.y;
+        r8_cmac(s, X1[(zb * NP + yb) * NH + kx], tw[(ky * (yb + H)) % N]);
       }
       X2[e] = s;
     }
@@ -476,9 +490,7 @@ __global__ void __launch_bounds__(128)
       float2 s = make_float2(0.f, 0.f);
 #pragma unroll
       for (int zb = 0; zb < NP; zb++) {
-        float2 t = cmul(X2[(zb * N + ky) * NH + kx], tw[(kz * (zb + H)) % N]);
-        s.x += t.x;
-        s.y += t.y;
+        r8_cmac(s, X2[(zb * N + ky) * NH + kx], tw[(kz * (zb + H)) % N]);
       }
       out[(int64_t)e * sdm + m] = s;
     }
@@ -583,9 +595,7 @@ __global__ void __launch_bounds__(128)
       float2 s = make_float2(0.f, 0.f);
 #pragma unroll 4
       for (int kz = 0; kz < N; kz++) {
-        float2 t = cmulc(in[((int64_t)(kz * N + ky) * NH + kx) * tdm + m], tw[(kz * (zb + H)) % N]);
-        s.x += t.x;
-        s.y += t.y;
+        r8_cmacc(s, in[((int64_t)(kz * N + ky) * NH + kx) * tdm + m], tw[(kz * (zb + H)) % N]);
       }
       Y2[e] = s;
     }
@@ -595,9 +605,7 @@ __global__ void __launch_bounds__(128)
       float2 s = make_float2(0.f, 0.f);
 #pragma unroll
       for (int ky = 0; ky < N; ky++) {
-        float2 t = cmulc(Y2[(zb * N + ky) * NH + kx], tw[(ky * (yb + H)) % N]);
-        s.x += t.x;
-        s.y += t.y;
+        r8_cmacc(s, Y2[(zb * N + ky) * NH + kx], tw[(ky * (yb + H)) % N]);
       }
       Y1[e] = s;
     }
@@ -660,22 +668,6 @@ __device__ __forceinline__ void r8_store(float2* p, const float2 (&v)[8]) {
 #pragma unroll
   for (int i = 0; i < 4; i++) q[i] = make_float4(v[2 * i].x, v[2 * i].y, v[2 * i + 1].x, v[2 * i + 1].y);
 }
-// s += a b and s += a conj(b) as four FMAs into the accumulator (a product
-// formed first and then added costs a multiply and an add more: IEEE rules
-// keep the compiler from reassociating it)
-__device__ __forceinline__ void r8_cmac(float2& s, float2 a, float2 b) {
-  s.x = fmaf(a.x, b.x, s.x);
-  s.x = fmaf(-a.y, b.y, s.x);
-  s.y = fmaf(a.x, b.y, s.y);
-  s.y = fmaf(a.y, b.x, s.y);
-}
-__device__ __forceinline__ void r8_cmacc(float2& s, float2 a, float2 b) {
-  s.x = fmaf(a.x, b.x, s.x);
-  s.x = fmaf(a.y, b.y, s.x);
-  s.y = fmaf(a.y, b.x, s.y);
-  s.y = fmaf(-a.x, b.y, s.y);
-}
-
 template <int NP>
 __device__ __forceinline__ void r8_twiddles(float2* twb) {
   using F = FftDims32<NP>;
