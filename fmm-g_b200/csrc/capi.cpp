@@ -802,6 +802,25 @@ fmmg_status fmmg_operator(fmmg_handle* h, int which, int idx, double* get, const
       if (get) std::memcpy(get, base, sizeof(double) * n);
       if (set) std::memcpy(base, set, sizeof(double) * n);
     } break;
+    case 5: {  // the mixed form's translation spectra on the (2np-1)^3 grid, read only
+      if (idx < 0 || idx > 315) return fail(h, FMMG_INVALID_ARG, "translation index");
+      if (set) return fail(h, FMMG_INVALID_ARG, "operator 5 is read only (set operator 4)");
+      const int64_t m = (int64_t)P.nEff32 * P.sdm * P.tdm;
+      n = 2 * m;
+      if (get) std::memcpy(get, (const double*)(P.m2lT32.data() + (size_t)idx * m), sizeof(double) * n);
+    } break;
+    case 6: {  // the mixed form's folded C2E up x M2M, (ue x 8 ue) column-major, read only
+      if (set) return fail(h, FMMG_INVALID_ARG, "operator 6 is read only (set operators 0 and 1)");
+      n = ue * 8 * ue;
+      if (get) {
+        try {
+          const std::vector<double> f = fmmg::fold_c2e_m2m(P);  // row-major [ue][8 ue]
+          for (int64_t i = 0; i < ue; i++)
+            for (int64_t j = 0; j < 8 * ue; j++) get[j * ue + i] = f[i * 8 * ue + j];
+        }
+        FMMG_GUARD(h)
+      }
+    } break;
     default:
       return fail(h, FMMG_INVALID_ARG, "operator id");
   }

@@ -248,7 +248,12 @@ fmmg_status fmmg_lists(const fmmg_handle* h, int which, int64_t* ptr, int32_t* i
  * column-major as the reference NumMat (common/nummat.hpp:96-105); spectra use
  * the FFTW r2c layout.  *count receives the number of doubles.  With set != NULL
  * the table is replaced (before the next evaluate) -- used to run the GPU path
- * on an externally supplied operator set. */
+ * on an externally supplied operator set.  Read only, the mixed form's own
+ * tables: 5 the translation spectra on its (2np-1)^3 grid (idx 0..315, derived
+ * from table 4), 6 the folded upward operator C2E x M2M, (ue x 8 ue)
+ * column-major with the 8 octants side by side (derived from tables 0 and 1);
+ * set on 5 or 6 returns FMMG_INVALID_ARG.  No counterpart in the reference
+ * for 5 and 6. */
 fmmg_status fmmg_operator(fmmg_handle* h, int which, int idx, double* get, const double* set,
                           int64_t* count);
 
