@@ -4,6 +4,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <list>
+#include <memory>
+#include <mutex>
 #include <numeric>
 #include <queue>
 
@@ -479,10 +482,66 @@ static void mm_matrix_rt(int kt, const double* coefs, int ns, const double* sp, 
   }
 }
 
+// The operator tables depend on the kernel, its two coefficients and np only.
+// The process keeps the most recent sets, so that new handles and repeated
+// setups of one handle (points that move between evaluations) copy them
+// instead of rebuilding them, as the reference shares one operator manager per
+// kernel and order among its FMM objects (fmm3d_mpi/matmgnt3d_mpi.cpp:526-543).
+namespace {
+struct OpKey {
+  int kt, np;
+  double c0, c1;
+  bool operator==(const OpKey& b) const { return kt == b.kt && np == b.np && c0 == b.c0 && c1 == b.c1; }
+};
+constexpr size_t kOperatorSetsKept = 4;
+std::mutex gOpMu;
+std::list<std::pair<OpKey, std::shared_ptr<const Plan>>> gOps;  // most recent first
+}  // namespace
+
+std::string Plan::build_operators() {
+  const OpKey key{o.kt, o.np, o.coefs[0], o.coefs[1]};
+  std::shared_ptr<const Plan> set;
+  {
+    std::lock_guard<std::mutex> g(gOpMu);
+    for (auto it = gOps.begin(); it != gOps.end(); ++it)
+      if (it->first == key) {
+        set = it->second;
+        gOps.splice(gOps.begin(), gOps, it);
+        break;
+      }
+  }
+  if (!set) {
+    auto fresh = std::make_shared<Plan>();
+    fresh->o = o;
+    std::string e = fresh->build_operators_uncached();
+    if (!e.empty()) return e;
+    std::lock_guard<std::mutex> g(gOpMu);
+    gOps.emplace_front(key, fresh);
+    if (gOps.size() > kOperatorSetsKept) gOps.pop_back();
+    set = fresh;
+  }
+  copy_operators(*set);
+  return std::string();
+}
+
+void Plan::copy_operators(const Plan& s) {
+  sd = s.sd; td = s.td; mm = s.mm; sdm = s.sdm; tdm = s.tdm;
+  std::memcpy(deg, s.deg, sizeof(deg));
+  nrm = s.nrm;
+  nUE = s.nUE; nUC = s.nUC; nDE = s.nDE; nDC = s.nDC; nReg = s.nReg; nEff = s.nEff;
+  nReg32 = s.nReg32; nEff32 = s.nEff32;
+  for (int i = 0; i < 4; i++) sam[i] = s.sam[i];
+  uc2ue = s.uc2ue; m2m = s.m2m; dc2de = s.dc2de; l2l = s.l2l;
+  m2lT = s.m2lT; m2lT32 = s.m2lT32;
+  kUp = s.kUp; kDn = s.kDn;
+  uc2ueF1 = s.uc2ueF1; uc2ueF2 = s.uc2ueF2; dc2deF1 = s.dc2deF1; dc2deF2 = s.dc2deF2;
+  std::memcpy(transId, s.transId, sizeof(transId));
+}
+
 // The operator set of MatMgnt3d_MPI (fmm3d_mpi/matmgnt3d_mpi.cpp:52-71,
 // 107-274, 373-411) for a homogeneous equivalent kernel: unit-radius tables,
 // level scaling 2^(+-l*deg) applied by the GPU stages.
-std::string Plan::build_operators() {
+std::string Plan::build_operators_uncached() {
   sd = kernel_src_dof(o.kt);
   td = kernel_trg_dof(o.kt);
   mm = kernel_mm(o.kt);
@@ -512,19 +571,17 @@ std::string Plan::build_operators() {
   // C2E up: pinv of the UE -> UC matrix
   mm_matrix_rt(mm, o.coefs, nUE, sam[0].data(), nUC, sam[1].data(), A);
   Rm.assign((size_t)ue * uc, 0.0);
-  pinv_jacobi(uc, ue, A.data(), eps, Rm.data());
+  kUp = pinv_truncated(uc, ue, A.data(), eps, Rm.data(), uc2ueF1, uc2ueF2);
   uc2ue.resize((size_t)ue * uc);
   for (int r = 0; r < ue; r++)
     for (int c = 0; c < uc; c++) uc2ue[(size_t)r * uc + c] = Rm[(size_t)c * ue + r];
-  kUp = pinv_factors(uc, ue, A.data(), eps, uc2ueF1, uc2ueF2);
   // C2E down
   mm_matrix_rt(mm, o.coefs, nDE, sam[2].data(), nDC, sam[3].data(), A);
   Rm.assign((size_t)de * dc, 0.0);
-  pinv_jacobi(dc, de, A.data(), eps, Rm.data());
+  kDn = pinv_truncated(dc, de, A.data(), eps, Rm.data(), dc2deF1, dc2deF2);
   dc2de.resize((size_t)de * dc);
   for (int r = 0; r < de; r++)
     for (int c = 0; c < dc; c++) dc2de[(size_t)r * dc + c] = Rm[(size_t)c * de + r];
-  kDn = pinv_factors(dc, de, A.data(), eps, dc2deF1, dc2deF2);
   // (refactor_c2e recovers these factors from the explicit tables)
   // M2M / L2L octant matrices
   m2m.assign((size_t)uc * 8 * ue, 0.0);

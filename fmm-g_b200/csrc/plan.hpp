@@ -134,6 +134,8 @@ struct Plan {
 
   std::string build(const Options& opt, int64_t ns, const double* src, const double* nrm, int64_t nt,
                     const double* trg);
+  // the operator tables of (kt, coefs, np), copied from the process's most
+  // recent sets when they hold it
   std::string build_operators();
   // refactor the pinv the caller replaced (0: C2E up, 2: C2E down) from its
   // explicit table, so the FP32 pass applies the same operator
@@ -145,6 +147,8 @@ struct Plan {
   bool leaf(int n) const { return chd[n] < 0; }
 
  private:
+  std::string build_operators_uncached();
+  void copy_operators(const Plan& s);
   void build_tree(const double* src);
   void bin_targets(const double* trg);
   void build_lists();
@@ -155,9 +159,12 @@ struct Plan {
 };
 
 // linear algebra used by the operator builder (linalg.cpp)
-void pinv_jacobi(int m, int n, const double* A_colmajor, double eps, double* R_colmajor);
-int pinv_factors(int m, int n, const double* A_colmajor, double eps, std::vector<double>& F1,
-                 std::vector<double>& F2);
+// the truncated pseudo-inverse of A (m x n column-major) from one SVD, both as
+// the explicit table R (n x m column-major; skipped when R is NULL) and in
+// factored form R = F2 F1, F1 = diag(1/s) U^T (k x m, row-major), F2 = V
+// (n x k, row-major); returns k, the singular values kept (s >= eps s_max)
+int pinv_truncated(int m, int n, const double* A_colmajor, double eps, double* R_colmajor,
+                   std::vector<double>& F1, std::vector<double>& F2);
 void rfft3_host(int n, int howmany, const double* in, std::complex<double>* out);
 int svd_factors(int m, int n, const double* B_rowmajor, double relCut, std::vector<double>& F1,
                 std::vector<double>& F2);

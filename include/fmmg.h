@@ -89,14 +89,20 @@ typedef struct fmmg_handle fmmg_handle;
  * device 0. */
 fmmg_status fmmg_default_options(fmmg_options* opt);
 
-/* new FMM3d_MPI + knl()/np()/ctr()/rootLevel() setters. */
+/* new FMM3d_MPI + knl()/np()/ctr()/rootLevel() setters.  Builds the operator
+ * tables of (kernel_type, coefs, np), or copies them from the sets the process
+ * keeps: the 4 most recently used, as the reference shares one operator
+ * manager per kernel and order (fmm3d_mpi/matmgnt3d_mpi.cpp:526-543). */
 fmmg_status fmmg_create(const fmmg_options* opt, fmmg_handle** out);
 
 /* FMM3d_MPI::setup() (fmm3d_mpi/fmm3d_setup_mpi.cpp:41-567): builds the
  * adaptive octree over the sources, bins the targets, builds the U/V/W/X lists
  * (fmm3d_mpi/let3d_mpi.cpp:1637-1768) and their device CSR forms, the
  * operators, and uploads everything.  src_nrm may be NULL for single-layer
- * kernels.  All points must lie in the closed root box; n_src >= 1, n_trg >= 0. */
+ * kernels.  All points must lie in the closed root box; n_src >= 1, n_trg >= 0.
+ * May be called again on the same handle with new points (points that moved):
+ * the tree, lists and device data are rebuilt and the operator tables reset to
+ * the built ones (tables replaced through fmmg_operator are dropped). */
 fmmg_status fmmg_setup(fmmg_handle* h, int64_t n_src, const double* src_xyz, const double* src_nrm,
                        int64_t n_trg, const double* trg_xyz);
 

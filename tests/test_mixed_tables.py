@@ -7,7 +7,8 @@ steps of 2/(np-1) per axis and r2c transformed -- the construction of
 fmm3d_mpi/matmgnt3d_mpi.cpp:385-411 on the odd grid.  A replaced (2np)^3
 spectrum (table 4) is converted exactly: inverse transform, keep the offsets
 -(np-1)..np-1, forward transform on the odd grid.  Table 6 is the parent
-upward operator pinv(UC->UE) x M2M with the 8 octants side by side.
+upward operator pinv(UC->UE) x M2M with the 8 octants side by side.  The
+operator sets a process keeps are shared between handles.
 """
 import numpy as np
 import pytest
@@ -137,3 +138,25 @@ def test_mixed_tables_are_read_only():
         f.set_operator(6, 0, f.operator(6))
     with pytest.raises(fmmg.FmmgError):
         f.operator(5, 316)
+
+
+def test_operator_sets_are_shared_between_handles_not_their_replacements():
+    """A process keeps the operator sets it built (the reference shares one
+    operator manager per kernel and order, fmm3d_mpi/matmgnt3d_mpi.cpp:526-543):
+    a second handle gets bit-identical tables; a table one handle replaces stays
+    its own, and a new setup of that handle resets it."""
+    a = _handle(111, 5)
+    b = _handle(111, 5)
+    for which, idx in ((0, 0), (1, 3), (2, 0), (3, 5), (4, 100), (5, 100), (6, 0)):
+        np.testing.assert_array_equal(a.operator(which, idx), b.operator(which, idx))
+    orig = a.operator(0)
+    a.set_operator(0, 0, 2.0 * orig)
+    np.testing.assert_array_equal(_handle(111, 5).operator(0), orig)
+    np.testing.assert_array_equal(a.operator(0), 2.0 * orig)
+    rng = np.random.default_rng(5)
+    a.setup(rng.random((400, 3)))
+    np.testing.assert_array_equal(a.operator(0), orig)
+    # other coefficients are another set (Navier's Poisson ratio enters the kernel)
+    n1 = fmmg.FMM3d(511, np_=3, pts_max=60, coefs=(1.0, 0.25), device=-1)
+    n2 = fmmg.FMM3d(511, np_=3, pts_max=60, coefs=(1.0, 0.3), device=-1)
+    assert not np.array_equal(n1.operator(1, 0), n2.operator(1, 0))
