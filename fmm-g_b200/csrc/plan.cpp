@@ -8,7 +8,6 @@
 #include <memory>
 #include <mutex>
 #include <numeric>
-#include <queue>
 
 #include "kernels.hpp"
 
@@ -157,63 +156,89 @@ bool Plan::adjacent(int a, int b) const {
 // U/V/W/X lists of every evaluator node (fmm3d_mpi/let3d_mpi.cpp:1637-1768):
 // the candidates are the children of the parent's neighbours at the node's
 // depth, resolved to the deepest existing box; lists hold sorted unique ids.
+// A candidate's box is found from the parent's 27 neighbour boxes (its parent
+// position is one of them), one level down when that box has children; nodes
+// go in chunks whose lists are appended to per-chunk arrays in node order.
 void Plan::build_lists() {
-  std::vector<std::vector<int32_t>> Lu(nn), Lv(nn), Lw(nn), Lx(nn);
-#pragma omp parallel for schedule(dynamic, 32)
-  for (int g = 0; g < nn; g++) {
-    if (!(flags[g] & NF_EVTR)) continue;
-    std::vector<int32_t>& Us = Lu[g];
-    std::vector<int32_t>& Vs = Lv[g];
-    std::vector<int32_t>& Ws = Lw[g];
-    std::vector<int32_t>& Xs = Lx[g];
-    const bool term = leaf(g);
-    if (g != 0) {
-      const int P = par[g], dg = depth[g];
-      const int lim = 1 << dg;
-      const int* pp = &path[3 * (size_t)P];
-      const int* pg = &path[3 * (size_t)g];
-      for (int i = -2; i < 4; i++)
-        for (int j = -2; j < 4; j++)
-          for (int k = -2; k < 4; k++) {
-            int tp[3] = {2 * pp[0] + i, 2 * pp[1] + j, 2 * pp[2] + k};
-            if (tp[0] < 0 || tp[1] < 0 || tp[2] < 0 || tp[0] >= lim || tp[1] >= lim || tp[2] >= lim) continue;
-            if (tp[0] == pg[0] && tp[1] == pg[1] && tp[2] == pg[2]) continue;
-            int res = find_node(dg, tp);
-            bool adj = adjacent(res, g);
-            if (depth[res] < dg) {
-              if (adj) { if (term) Us.push_back(res); }
-              else Xs.push_back(res);
-            } else if (!adj) {
-              Vs.push_back(res);
-            } else if (term) {
-              std::queue<int> rest;
-              rest.push(res);
-              while (!rest.empty()) {
-                int f = rest.front();
-                rest.pop();
-                if (!adjacent(f, g)) Ws.push_back(f);
-                else if (leaf(f)) Us.push_back(f);
-                else for (int c = 0; c < 8; c++) rest.push(chd[f] + c);
-              }
-            }
+  constexpr int CH = 128;
+  const int nch = (nn + CH - 1) / CH;
+  std::vector<std::vector<int32_t>> part[4];
+  for (auto& pv : part) pv.assign(nch, {});
+  std::vector<int64_t> cnt[4];
+  for (auto& c : cnt) c.assign(nn, 0);
+#pragma omp parallel
+  {
+    std::vector<int32_t> L[4], rest;  // U, V, W, X of one node; W descent work
+#pragma omp for schedule(dynamic, 1)
+    for (int ch = 0; ch < nch; ch++)
+      for (int g = ch * CH; g < std::min(nn, (ch + 1) * CH); g++) {
+        if (!(flags[g] & NF_EVTR)) continue;
+        for (auto& l : L) l.clear();
+        std::vector<int32_t>&Us = L[0], &Vs = L[1], &Ws = L[2], &Xs = L[3];
+        const bool term = leaf(g);
+        if (g != 0) {
+          const int P = par[g], dg = depth[g];
+          const int lim = 1 << dg, plim = lim >> 1;
+          const int* pp = &path[3 * (size_t)P];
+          const int* pg = &path[3 * (size_t)g];
+          int nb[27];  // the box holding each neighbour position of P at depth dg - 1
+          for (int a = 0; a < 27; a++) {
+            const int q[3] = {pp[0] + a / 9 - 1, pp[1] + (a / 3) % 3 - 1, pp[2] + a % 3 - 1};
+            nb[a] = (q[0] < 0 || q[1] < 0 || q[2] < 0 || q[0] >= plim || q[1] >= plim || q[2] >= plim)
+                        ? -1 : find_node(dg - 1, q);
           }
-    }
-    if (term) Us.push_back(g);
-    auto fin = [&](std::vector<int32_t>& L, uint8_t need) {
-      std::sort(L.begin(), L.end());
-      L.erase(std::unique(L.begin(), L.end()), L.end());
-      L.erase(std::remove_if(L.begin(), L.end(), [&](int32_t s) { return !(flags[s] & need); }), L.end());
-    };
-    fin(Us, NF_LSRC); fin(Vs, NF_SRCE); fin(Ws, NF_SRCE); fin(Xs, NF_LSRC);
+          for (int i = -2; i < 4; i++)
+            for (int j = -2; j < 4; j++)
+              for (int k = -2; k < 4; k++) {
+                int tp[3] = {2 * pp[0] + i, 2 * pp[1] + j, 2 * pp[2] + k};
+                if (tp[0] < 0 || tp[1] < 0 || tp[2] < 0 || tp[0] >= lim || tp[1] >= lim || tp[2] >= lim) continue;
+                if (tp[0] == pg[0] && tp[1] == pg[1] && tp[2] == pg[2]) continue;
+                // i, j, k in [-2, 4): the parent-level offset floor(i / 2) is -1, 0 or 1,
+                // and an in-range position has an in-range parent position
+                const int a = ((i + 2) / 2) * 9 + ((j + 2) / 2) * 3 + (k + 2) / 2;
+                int res = nb[a];
+                if (depth[res] == dg - 1 && !leaf(res)) res = chd[res] + (tp[0] & 1) * 4 + (tp[1] & 1) * 2 + (tp[2] & 1);
+                bool adj = adjacent(res, g);
+                if (depth[res] < dg) {
+                  if (adj) { if (term) Us.push_back(res); }
+                  else Xs.push_back(res);
+                } else if (!adj) {
+                  Vs.push_back(res);
+                } else if (term) {
+                  rest.assign(1, res);
+                  while (!rest.empty()) {
+                    int f = rest.back();
+                    rest.pop_back();
+                    if (!adjacent(f, g)) Ws.push_back(f);
+                    else if (leaf(f)) Us.push_back(f);
+                    else for (int c = 0; c < 8; c++) rest.push_back(chd[f] + c);
+                  }
+                }
+              }
+        }
+        if (term) Us.push_back(g);
+        const uint8_t need[4] = {NF_LSRC, NF_SRCE, NF_SRCE, NF_LSRC};
+        for (int l = 0; l < 4; l++) {
+          std::sort(L[l].begin(), L[l].end());
+          L[l].erase(std::unique(L[l].begin(), L[l].end()), L[l].end());
+          L[l].erase(std::remove_if(L[l].begin(), L[l].end(), [&](int32_t s) { return !(flags[s] & need[l]); }),
+                     L[l].end());
+          part[l][ch].insert(part[l][ch].end(), L[l].begin(), L[l].end());
+          cnt[l][g] = (int64_t)L[l].size();
+        }
+      }
   }
-  auto flat = [&](std::vector<std::vector<int32_t>>& L, CSR& out) {
-    out.ptr.assign(nn + 1, 0);
-    for (int n = 0; n < nn; n++) out.ptr[n + 1] = out.ptr[n] + (int64_t)L[n].size();
-    out.idx.resize(out.ptr[nn]);
-    for (int n = 0; n < nn; n++) std::copy(L[n].begin(), L[n].end(), out.idx.begin() + out.ptr[n]);
-    for (int32_t s : out.idx) flags[s] |= NF_USER;
-  };
-  flat(Lu, U); flat(Lv, V); flat(Lw, W); flat(Lx, X);
+  CSR* out[4] = {&U, &V, &W, &X};
+  for (int l = 0; l < 4; l++) {
+    CSR& o = *out[l];
+    o.ptr.assign(nn + 1, 0);
+    for (int n = 0; n < nn; n++) o.ptr[n + 1] = o.ptr[n] + cnt[l][n];
+    o.idx.resize(o.ptr[nn]);
+#pragma omp parallel for schedule(static)
+    for (int ch = 0; ch < nch; ch++)
+      std::copy(part[l][ch].begin(), part[l][ch].end(), o.idx.begin() + o.ptr[ch * CH]);
+    for (int32_t s : o.idx) flags[s] |= NF_USER;
+  }
 }
 
 // Flattened work for the GPU stages, following the per-node decisions of
@@ -314,44 +339,63 @@ void Plan::build_worklists() {
       }
     }
   }
-  // expanded per-target lists: v = child c2 of Q, c = child of P, idx = v - c
-  vTrgPtr.assign(vTrgNodes.size() + 1, 0);
-  vTrgEnt.clear();
-  std::vector<std::vector<std::pair<int32_t, int32_t>>> bySrc(vSrcNodes.size());
-  for (size_t r = 0; r < vParents.size(); r++) {
-    const int P = vParents[r];
-    for (int c = 0; c < 8; c++) {
-      const int t = chd[P] + c;
-      const int ts = vTrgSlot[t];
-      if (ts < 0) continue;
-      for (int64_t e = vNbr.ptr[r]; e < vNbr.ptr[r + 1]; e++) {
-        const int Q = vNbr.idx[e], off = vNbrOff[e];
-        const int dx = off / 9 - 1, dy = (off / 3) % 3 - 1, dz = off % 3 - 1;
-        for (int c2 = 0; c2 < 8; c2++) {
-          const int s = vSrcSlot[chd[Q] + c2];
-          if (s < 0) continue;
-          const int rx = 2 * dx + (c2 >> 2) - (c >> 2), ry = 2 * dy + ((c2 >> 1) & 1) - ((c >> 1) & 1),
-                    rz = 2 * dz + (c2 & 1) - (c & 1);
-          if (std::max(std::abs(rx), std::max(std::abs(ry), std::abs(rz))) <= 1) continue;
-          const int id = transId[rx + 3][ry + 3][rz + 3];
-          vTrgEnt.push_back(s);
-          vTrgEnt.push_back(id);
-          bySrc[s].push_back({ts, id});
-        }
+  // expanded per-target lists: v = child c2 of Q, c = child of P, idx = v - c.
+  // A target slot is one child c of one row P, so the slots are counted, then
+  // filled, row by row in parallel; each keeps its entries neighbour by
+  // neighbour, child by child.
+  const size_t nTrgSlots = vTrgNodes.size(), nSrcSlots = vSrcNodes.size();
+  auto expand = [&](size_t r, int c, auto&& emit) {
+    for (int64_t e = vNbr.ptr[r]; e < vNbr.ptr[r + 1]; e++) {
+      const int Q = vNbr.idx[e], off = vNbrOff[e];
+      const int dx = off / 9 - 1, dy = (off / 3) % 3 - 1, dz = off % 3 - 1;
+      for (int c2 = 0; c2 < 8; c2++) {
+        const int s = vSrcSlot[chd[Q] + c2];
+        if (s < 0) continue;
+        const int rx = 2 * dx + (c2 >> 2) - (c >> 2), ry = 2 * dy + ((c2 >> 1) & 1) - ((c >> 1) & 1),
+                  rz = 2 * dz + (c2 & 1) - (c & 1);
+        if (std::max(std::abs(rx), std::max(std::abs(ry), std::abs(rz))) <= 1) continue;
+        emit(s, transId[rx + 3][ry + 3][rz + 3]);
       }
-      vTrgPtr[ts + 1] = (int64_t)vTrgEnt.size() / 2;
     }
-  }
-  for (size_t t = 1; t < vTrgPtr.size(); t++) vTrgPtr[t] = std::max(vTrgPtr[t], vTrgPtr[t - 1]);
-  vSrcPtr.assign(vSrcNodes.size() + 1, 0);
-  vSrcEnt.clear();
-  for (size_t s2 = 0; s2 < bySrc.size(); s2++) {
-    for (auto& pr : bySrc[s2]) {
-      vSrcEnt.push_back(pr.first);
-      vSrcEnt.push_back(pr.second);
+  };
+  vTrgPtr.assign(nTrgSlots + 1, 0);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (size_t r = 0; r < vParents.size(); r++)
+    for (int c = 0; c < 8; c++) {
+      const int ts = vTrgSlot[chd[vParents[r]] + c];
+      if (ts < 0) continue;
+      int64_t n = 0;
+      expand(r, c, [&](int, int) { n++; });
+      vTrgPtr[ts + 1] = n;
     }
-    vSrcPtr[s2 + 1] = (int64_t)vSrcEnt.size() / 2;
-  }
+  for (size_t t = 0; t < nTrgSlots; t++) vTrgPtr[t + 1] += vTrgPtr[t];
+  vTrgEnt.resize(2 * (size_t)vTrgPtr[nTrgSlots]);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (size_t r = 0; r < vParents.size(); r++)
+    for (int c = 0; c < 8; c++) {
+      const int ts = vTrgSlot[chd[vParents[r]] + c];
+      if (ts < 0) continue;
+      int64_t o = vTrgPtr[ts];
+      expand(r, c, [&](int s, int id) {
+        vTrgEnt[2 * o] = s;
+        vTrgEnt[2 * o + 1] = id;
+        o++;
+      });
+    }
+  // inverted per source slot, in the order of the target-slot lists (a stable
+  // counting sort)
+  const int64_t nEnt = vTrgPtr[nTrgSlots];
+  vSrcPtr.assign(nSrcSlots + 1, 0);
+  for (int64_t i = 0; i < nEnt; i++) vSrcPtr[vTrgEnt[2 * i] + 1]++;
+  for (size_t t = 0; t < nSrcSlots; t++) vSrcPtr[t + 1] += vSrcPtr[t];
+  vSrcEnt.resize(2 * (size_t)nEnt);
+  std::vector<int64_t> fill(vSrcPtr.begin(), vSrcPtr.end() - 1);
+  for (size_t ts = 0; ts < nTrgSlots; ts++)
+    for (int64_t i = vTrgPtr[ts]; i < vTrgPtr[ts + 1]; i++) {
+      const int64_t o = fill[vTrgEnt[2 * i]]++;
+      vSrcEnt[2 * o] = (int32_t)ts;
+      vSrcEnt[2 * o + 1] = vTrgEnt[2 * i + 1];
+    }
 }
 
 // Inverse of a CSR (rows -> column ids): for every id that occurs, the rows

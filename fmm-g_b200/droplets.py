@@ -28,6 +28,7 @@ restated as Morton order with z the most significant axis on every level).
 """
 import math
 import os
+import time
 
 import numpy as np
 import torch
@@ -155,12 +156,17 @@ class FmmVelocity:
         self.f = fmmg.FMM3d(KERNEL, np_=np_, pts_max=pts_max, coefs=(1.0, 0.25), device=device)
         self.precision = precision
         self.device = torch.device("cuda", device)
+        self.setup_s = self.evaluate_s = 0.0  # wall time spent in each, summed over calls
 
     def __call__(self, xs, den):
+        t0 = time.perf_counter()
         self.f.setup(xs.detach().cpu().numpy())
+        t1 = time.perf_counter()
         out = torch.empty(den.numel(), dtype=torch.float64, device=self.device)
         self.f.evaluate_device(den, out, 1, self.precision)
         self.f.sync()
+        self.setup_s += t1 - t0
+        self.evaluate_s += time.perf_counter() - t1
         return out.view(-1, 3)
 
 
@@ -227,7 +233,7 @@ def main(argv=None):
     p.add_argument("--np", type=int, default=6)
     p.add_argument("--pts_max", type=int, default=64)
     p.add_argument("--mixed", action="store_true", help="evaluate in the mixed-precision form")
-    p.add_argument("--out", default="droplets_out")
+    p.add_argument("--out", default=None, help="folder for the coord<i>.txt files (none: not written)")
     a = p.parse_args(argv)
     x = initial_positions(a.numsrc, a.distribution)
     if not a.skip_initial_sort:
@@ -236,7 +242,11 @@ def main(argv=None):
     vel = FmmVelocity(a.np, a.pts_max, fmmg.PREC_MIXED if a.mixed else fmmg.PREC_FP64)
     d = Droplets(x, eps, a.time_step, vel)
     print("particles %d, particle size %g, time step %g, iterations %d" % (x.shape[0], eps, a.time_step, a.num_iter))
+    t0 = time.perf_counter()
     d.run(a.num_iter, a.write_fraction, a.out)
+    wall = time.perf_counter() - t0
+    print("%d steps (%d right-hand sides) in %.3f s: setup %.3f s, evaluate %.3f s, the rest %.3f s"
+          % (a.num_iter, d.evaluations, wall, vel.setup_s, vel.evaluate_s, wall - vel.setup_s - vel.evaluate_s))
 
 
 if __name__ == "__main__":
