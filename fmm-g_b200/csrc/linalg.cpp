@@ -2,9 +2,9 @@
 //
 // pinv_truncated: the truncated pseudo-inverse of common/vecmatop.cpp:129-164
 // (common/svdrep.cpp:38-80 keeps the singular values >= eps * s_max), computed
-// from a Jacobi SVD preconditioned by a pivoted QR, which is accurate in the
-// small singular values that the truncation tests (LAPACK dgesvd, which the
-// reference calls, is not installed here).  rfft3_host: the r2c transform with FFTW's rank-3
+// from a one-sided Jacobi SVD, which is accurate in the small singular values
+// that the truncation tests (LAPACK dgesvd, which the reference calls, is not
+// installed here).  rfft3_host: the r2c transform with FFTW's rank-3
 // layout used for the M2L translation tables (fmm3d_mpi/matmgnt3d_mpi.cpp:408).
 #include <algorithm>
 #include <cmath>
@@ -43,7 +43,6 @@ static void svd_onesided(int m, int n, std::vector<double>& W /* m x n, becomes 
         double* wp = &W[(size_t)p * m];
         double* wq = &W[(size_t)q * m];
         double a = 0, b = 0, g = 0;
-#pragma omp simd reduction(+ : a, b, g)
         for (int i = 0; i < m; i++) {
           a += wp[i] * wp[i];
           b += wq[i] * wq[i];
@@ -55,7 +54,6 @@ static void svd_onesided(int m, int n, std::vector<double>& W /* m x n, becomes 
         double zeta = (b - a) / (2.0 * g);
         double t = std::copysign(1.0, zeta) / (std::fabs(zeta) + std::hypot(1.0, zeta));
         double c = 1.0 / std::hypot(1.0, t), s = c * t;
-#pragma omp simd
         for (int i = 0; i < m; i++) {
           double x = wp[i], y = wq[i];
           wp[i] = c * x - s * y;
@@ -63,7 +61,6 @@ static void svd_onesided(int m, int n, std::vector<double>& W /* m x n, becomes 
         }
         double* vp = &V[(size_t)p * n];
         double* vq = &V[(size_t)q * n];
-#pragma omp simd
         for (int i = 0; i < n; i++) {
           double x = vp[i], y = vq[i];
           vp[i] = c * x - s * y;
@@ -83,154 +80,70 @@ static void svd_onesided(int m, int n, std::vector<double>& W /* m x n, becomes 
   }
 }
 
-// Householder QR with column pivoting of A (M x N column-major, M >= N):
-// A P = Q R.  On return W holds R on and above the diagonal and the reflector
-// tails below it (H_k = I - tau_k v v^T, v = [1, W[k+1.., k]]), and column j of
-// A P is column perm[j] of A.  The pivot is the trailing column of largest
-// remaining norm, recomputed exactly at every step.
-static void qr_pivoted(int M, int N, std::vector<double>& W, std::vector<double>& tau, std::vector<int>& perm) {
-  tau.assign(N, 0.0);
-  perm.resize(N);
-  for (int j = 0; j < N; j++) perm[j] = j;
-  std::vector<double> nrm(N);
-  for (int k = 0; k < N; k++) {
-#pragma omp parallel for schedule(static)
-    for (int j = k; j < N; j++) {
-      const double* w = &W[(size_t)j * M];
-      double s = 0;
-      for (int i = k; i < M; i++) s += w[i] * w[i];
-      nrm[j] = s;
-    }
-    int p = k;
-    for (int j = k + 1; j < N; j++)
-      if (nrm[j] > nrm[p]) p = j;
-    if (p != k) {
-      std::swap_ranges(W.begin() + (size_t)k * M, W.begin() + (size_t)(k + 1) * M, W.begin() + (size_t)p * M);
-      std::swap(perm[k], perm[p]);
-    }
-    double* v = &W[(size_t)k * M];
-    double xn = 0;
-    for (int i = k + 1; i < M; i++) xn += v[i] * v[i];
-    if (xn == 0.0) continue;  // nothing below the diagonal: H_k = I
-    const double alpha = v[k];
-    const double beta = -std::copysign(std::sqrt(alpha * alpha + xn), alpha);
-    const double t = (beta - alpha) / beta, sc = 1.0 / (alpha - beta);
-    tau[k] = t;
-    for (int i = k + 1; i < M; i++) v[i] *= sc;
-    v[k] = beta;
-#pragma omp parallel for schedule(static)
-    for (int j = k + 1; j < N; j++) {
-      double* w = &W[(size_t)j * M];
-      double d = w[k];
-      for (int i = k + 1; i < M; i++) d += v[i] * w[i];
-      d *= t;
-      w[k] -= d;
-      for (int i = k + 1; i < M; i++) w[i] -= d * v[i];
-    }
-  }
-}
-
-// Thin SVD A = U diag(S) V^T of A (M x N column-major, M >= N); U is M x N
-// and V N x N, column-major, with unit columns where S > 0.  Pivoted QR first,
-// then one-sided Jacobi on X = R^T, which the pivoting leaves close to
-// column-orthogonal so that few sweeps remain (Z. Drmac and K. Veselic, "New
-// fast and accurate Jacobi SVD algorithm", SIAM J. Matrix Anal. Appl. 29,
-// 2008): with X = Ux S Vx^T, R = Vx S Ux^T and A = (Q Vx) S (P Ux)^T.
-static void svd_thin(int M, int N, const double* A, std::vector<double>& U, std::vector<double>& S,
-                     std::vector<double>& V) {
-  std::vector<double> W(A, A + (size_t)M * N), tau, Vx;
-  std::vector<int> perm;
-  qr_pivoted(M, N, W, tau, perm);
-  std::vector<double> X((size_t)N * N, 0.0);
-  for (int j = 0; j < N; j++)  // column j of X = row j of R
-    for (int i = j; i < N; i++) X[(size_t)j * N + i] = W[(size_t)i * M + j];
-  svd_onesided(N, N, X, Vx);  // X becomes Ux S
-  S.assign(N, 0.0);
-  V.assign((size_t)N * N, 0.0);
-  for (int c = 0; c < N; c++) {
-    double s = 0;
-    const double* x = &X[(size_t)c * N];
-    for (int i = 0; i < N; i++) s += x[i] * x[i];
-    S[c] = std::sqrt(s);
-    if (S[c] > 0.0)
-      for (int j = 0; j < N; j++) V[(size_t)c * N + perm[j]] = x[j] / S[c];
-  }
-  U.assign((size_t)M * N, 0.0);
-#pragma omp parallel for schedule(dynamic, 4)
-  for (int c = 0; c < N; c++) {  // U_c = Q (Vx_c, 0) = H_0 H_1 .. H_{N-1} (Vx_c, 0)
-    double* y = &U[(size_t)c * M];
-    for (int i = 0; i < N; i++) y[i] = Vx[(size_t)c * N + i];
-    for (int k = N - 1; k >= 0; k--) {
-      if (tau[k] == 0.0) continue;
-      const double* v = &W[(size_t)k * M];
-      double d = y[k];
-      for (int i = k + 1; i < M; i++) d += v[i] * y[i];
-      d *= tau[k];
-      y[k] -= d;
-      for (int i = k + 1; i < M; i++) y[i] -= d * v[i];
-    }
-  }
-}
-
-// The singular triplets of A (m x n column-major) as left/right vector arrays
-// of lengths m and n: the SVD is taken of A or, when m < n, of A^T.
-struct Svd {
-  std::vector<double> U, S, V;
-  const double* left = nullptr;   // column c: the left singular vector c (length m)
-  const double* right = nullptr;  // column c: the right singular vector c (length n)
-  int lstride = 0, rstride = 0, N = 0;
-  Svd(int m, int n, const double* A_colmajor) {
-    const bool tr = m < n;
-    const int M = tr ? n : m;
-    N = tr ? m : n;
-    std::vector<double> B((size_t)M * N);
-    if (!tr) std::memcpy(B.data(), A_colmajor, sizeof(double) * M * N);
-    else
-      for (int i = 0; i < m; i++)
-        for (int j = 0; j < n; j++) B[(size_t)i * n + j] = A_colmajor[(size_t)j * m + i];
-    svd_thin(M, N, B.data(), U, S, V);
-    left = tr ? V.data() : U.data();
-    right = tr ? U.data() : V.data();
-    lstride = tr ? N : M;
-    rstride = tr ? M : N;
-  }
-  std::vector<int> keep(double relCut, bool inclusive) const {
-    const double smax = N ? *std::max_element(S.begin(), S.end()) : 0.0;
-    std::vector<int> k;
-    for (int c = 0; c < N; c++)
-      if ((inclusive ? S[c] >= relCut * smax : S[c] > relCut * smax) && S[c] > 0.0) k.push_back(c);
-    return k;
-  }
-};
-
+// One SVD gives both forms: the explicit table R (n x m column-major, skipped
+// when R is NULL) and the factors F1 = diag(1/s_k) U_k^T (k x m, row-major)
+// and F2 = V_k (n x k, row-major).  Applying F1 then F2 keeps the rounding
+// error of each factor relative to the size of its own result, which a single
+// product with the large-norm explicit pinv does not (used by the FP32 path).
 int pinv_truncated(int m, int n, const double* A, double eps, double* R, std::vector<double>& F1,
                    std::vector<double>& F2) {
-  const Svd d(m, n, A);
-  const std::vector<int> keep = d.keep(eps, true);  // svdrep.cpp:38-80: s >= eps * s_max
+  bool tr = m < n;
+  int M = tr ? n : m, N = tr ? m : n;
+  std::vector<double> W((size_t)M * N), V;
+  if (!tr) std::memcpy(W.data(), A, sizeof(double) * M * N);
+  else
+    for (int i = 0; i < m; i++)
+      for (int j = 0; j < n; j++) W[(size_t)i * n + j] = A[(size_t)j * m + i];
+  svd_onesided(M, N, W, V);
+  std::vector<double> S(N);
+  for (int j = 0; j < N; j++) {
+    double s = 0;
+    for (int i = 0; i < M; i++) s += W[(size_t)j * M + i] * W[(size_t)j * M + i];
+    S[j] = std::sqrt(s);
+  }
+  double smax = *std::max_element(S.begin(), S.end());
+  double cutoff = eps * smax;
+  if (R) {
+    std::fill(R, R + (size_t)n * m, 0.0);
+    // For A = W V^T with W = U S: pinv(A) = V S^-2 W^T restricted to kept columns.
+    for (int c = 0; c < N; c++) {
+      if (!(S[c] >= cutoff) || S[c] == 0.0) continue;
+      double inv2 = 1.0 / (S[c] * S[c]);
+      const double* w = &W[(size_t)c * M];
+      const double* v = &V[(size_t)c * N];
+      if (!tr) {  // R(i, j) += v_i w_j / s^2, R is n x m
+        for (int j = 0; j < m; j++) {
+          double f = w[j] * inv2;
+          double* r = R + (size_t)j * n;
+          for (int i = 0; i < n; i++) r[i] += v[i] * f;
+        }
+      } else {  // A^T = W V^T  ->  pinv(A) = W S^-2 V^T : R(i, j) += w_i v_j / s^2
+        for (int j = 0; j < m; j++) {
+          double f = v[j] * inv2;
+          double* r = R + (size_t)j * n;
+          for (int i = 0; i < n; i++) r[i] += w[i] * f;
+        }
+      }
+    }
+  }
+  std::vector<int> keep;
+  for (int c = 0; c < N; c++)
+    if (S[c] >= cutoff && S[c] > 0.0) keep.push_back(c);
   const int k = (int)keep.size();
   F1.assign((size_t)k * m, 0.0);
   F2.assign((size_t)n * k, 0.0);
   for (int r = 0; r < k; r++) {
     const int c = keep[r];
-    const double s = d.S[c];
-    const double* u = d.left + (size_t)c * d.lstride;
-    const double* v = d.right + (size_t)c * d.rstride;
-    for (int j = 0; j < m; j++) F1[(size_t)r * m + j] = u[j] / s;
-    for (int i = 0; i < n; i++) F2[(size_t)i * k + r] = v[i];
-  }
-  if (R) {  // R = F2 F1, n x m column-major
-    std::vector<double> F1t((size_t)m * k);
-    for (int r = 0; r < k; r++)
-      for (int j = 0; j < m; j++) F1t[(size_t)j * k + r] = F1[(size_t)r * m + j];
-#pragma omp parallel for schedule(static)
-    for (int j = 0; j < m; j++)
-      for (int i = 0; i < n; i++) {
-        double s = 0;
-        const double* a = &F2[(size_t)i * k];
-        const double* b = &F1t[(size_t)j * k];
-        for (int r = 0; r < k; r++) s += a[r] * b[r];
-        R[(size_t)j * n + i] = s;
-      }
+    const double s = S[c];
+    const double* w = &W[(size_t)c * M];  // U_c * s_c (length M)
+    const double* v = &V[(size_t)c * N];  // V_c (length N)
+    if (!tr) {  // A = U S V^T: F1 row = U_c^T / s = w^T / s^2, F2 column = v
+      for (int j = 0; j < m; j++) F1[(size_t)r * m + j] = w[j] / (s * s);
+      for (int i = 0; i < n; i++) F2[(size_t)i * k + r] = v[i];
+    } else {  // A^T = W V^T: A = V S U'^T with U' = W / s: F1 row = v^T / s, F2 column = w / s
+      for (int j = 0; j < m; j++) F1[(size_t)r * m + j] = v[j] / s;
+      for (int i = 0; i < n; i++) F2[(size_t)i * k + r] = w[i] / s;
+    }
   }
   return k;
 }
@@ -241,20 +154,39 @@ int pinv_truncated(int m, int n, const double* A, double eps, double* R, std::ve
 // truncated pseudo-inverse this recovers the factors of pinv_truncated (the
 // singular vectors are shared and s = 1/s_A), for tables the caller replaces.
 int svd_factors(int m, int n, const double* B, double relCut, std::vector<double>& F1, std::vector<double>& F2) {
-  std::vector<double> Bc((size_t)m * n);
-  for (int i = 0; i < m; i++)
-    for (int j = 0; j < n; j++) Bc[(size_t)j * m + i] = B[(size_t)i * n + j];
-  const Svd d(m, n, Bc.data());
-  const std::vector<int> keep = d.keep(relCut, false);
+  const bool tr = m < n;  // factor B^T (n x m) so the one-sided SVD sees M >= N
+  const int M = tr ? n : m, N = tr ? m : n;
+  std::vector<double> W((size_t)M * N), V;
+  if (tr) std::memcpy(W.data(), B, sizeof(double) * M * N);  // row-major B = column-major B^T
+  else
+    for (int i = 0; i < m; i++)
+      for (int j = 0; j < n; j++) W[(size_t)j * m + i] = B[(size_t)i * n + j];
+  svd_onesided(M, N, W, V);
+  std::vector<double> S(N);
+  for (int c = 0; c < N; c++) {
+    double s = 0;
+    for (int i = 0; i < M; i++) s += W[(size_t)c * M + i] * W[(size_t)c * M + i];
+    S[c] = std::sqrt(s);
+  }
+  const double smax = N ? *std::max_element(S.begin(), S.end()) : 0.0;
+  std::vector<int> keep;
+  for (int c = 0; c < N; c++)
+    if (S[c] > relCut * smax && S[c] > 0.0) keep.push_back(c);
   const int k = (int)keep.size();
   F1.assign((size_t)k * n, 0.0);
   F2.assign((size_t)m * k, 0.0);
   for (int r = 0; r < k; r++) {
     const int c = keep[r];
-    const double* u = d.left + (size_t)c * d.lstride;
-    const double* v = d.right + (size_t)c * d.rstride;
-    for (int i = 0; i < m; i++) F2[(size_t)i * k + r] = u[i];
-    for (int j = 0; j < n; j++) F1[(size_t)r * n + j] = d.S[c] * v[j];
+    const double s = S[c];
+    const double* w = &W[(size_t)c * M];  // U_c * s_c (length M)
+    const double* v = &V[(size_t)c * N];  // V_c (length N)
+    if (tr) {  // B^T = U S V^T: B = V S U^T, F2 column = V_c, F1 row = s U_c^T = w^T
+      for (int i = 0; i < m; i++) F2[(size_t)i * k + r] = v[i];
+      for (int j = 0; j < n; j++) F1[(size_t)r * n + j] = w[j];
+    } else {  // B = U S V^T: F2 column = U_c = w / s, F1 row = s V_c^T
+      for (int i = 0; i < m; i++) F2[(size_t)i * k + r] = w[i] / s;
+      for (int j = 0; j < n; j++) F1[(size_t)r * n + j] = s * v[j];
+    }
   }
   return k;
 }
