@@ -21,6 +21,7 @@ struct fmmg_handle {
   bool hostOnly = false;
   bool setupDone = false;
   bool opsDirty = false;
+  bool tablesReplaced = false;  // fmmg_operator replaced a table since the last setup
   bool timing = false;
   int64_t launches = 0;
   int hostPrecision = FMMG_PREC_FP64;
@@ -189,9 +190,14 @@ fmmg_status fmmg_setup(fmmg_handle* h, int64_t ns, const double* src, const doub
       h->ioK = 0;
       fmmg::Plan fresh;
       fresh.o = h->opt;
-      std::string e = fresh.build_operators();
-      if (!e.empty()) return fail(h, FMMG_NOT_SUPPORTED, e);
+      if (h->tablesReplaced) {  // back to the built tables
+        std::string e = fresh.build_operators();
+        if (!e.empty()) return fail(h, FMMG_NOT_SUPPORTED, e);
+      } else {
+        fresh.take_operators(std::move(h->plan));  // the handle's own, never replaced
+      }
       h->plan = std::move(fresh);
+      h->tablesReplaced = false;
       h->setupDone = false;
     }
     std::string e = h->plan.build(h->opt, ns, src, nrm, nt, nt > 0 ? trg : src);
@@ -827,6 +833,7 @@ fmmg_status fmmg_operator(fmmg_handle* h, int which, int idx, double* get, const
   if (count) *count = n;
   if (set) {
     h->opsDirty = true;
+    h->tablesReplaced = true;
     try {
       if (which == 0 || which == 2) P.refactor_c2e(which);  // the FP32 pass applies the pinv factored
       if (which == 4) P.m2l_spectrum32(idx);                 // and transforms on the (2np-1)^3 grid

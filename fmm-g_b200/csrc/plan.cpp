@@ -8,6 +8,7 @@
 #include <memory>
 #include <mutex>
 #include <numeric>
+#include <utility>
 
 #include "kernels.hpp"
 
@@ -564,23 +565,29 @@ std::string Plan::build_operators() {
     if (gOps.size() > kOperatorSetsKept) gOps.pop_back();
     set = fresh;
   }
-  copy_operators(*set);
+  assign_operators(*set);
   return std::string();
 }
 
-void Plan::copy_operators(const Plan& s) {
+// Every member build_operators sets: copied from a const set, moved from an
+// rvalue one.
+template <class S> void Plan::assign_operators(S&& s) {
   sd = s.sd; td = s.td; mm = s.mm; sdm = s.sdm; tdm = s.tdm;
   std::memcpy(deg, s.deg, sizeof(deg));
   nrm = s.nrm;
   nUE = s.nUE; nUC = s.nUC; nDE = s.nDE; nDC = s.nDC; nReg = s.nReg; nEff = s.nEff;
   nReg32 = s.nReg32; nEff32 = s.nEff32;
-  for (int i = 0; i < 4; i++) sam[i] = s.sam[i];
-  uc2ue = s.uc2ue; m2m = s.m2m; dc2de = s.dc2de; l2l = s.l2l;
-  m2lT = s.m2lT; m2lT32 = s.m2lT32;
+  for (int i = 0; i < 4; i++) sam[i] = std::forward<S>(s).sam[i];
+  uc2ue = std::forward<S>(s).uc2ue; m2m = std::forward<S>(s).m2m;
+  dc2de = std::forward<S>(s).dc2de; l2l = std::forward<S>(s).l2l;
+  m2lT = std::forward<S>(s).m2lT; m2lT32 = std::forward<S>(s).m2lT32;
   kUp = s.kUp; kDn = s.kDn;
-  uc2ueF1 = s.uc2ueF1; uc2ueF2 = s.uc2ueF2; dc2deF1 = s.dc2deF1; dc2deF2 = s.dc2deF2;
+  uc2ueF1 = std::forward<S>(s).uc2ueF1; uc2ueF2 = std::forward<S>(s).uc2ueF2;
+  dc2deF1 = std::forward<S>(s).dc2deF1; dc2deF2 = std::forward<S>(s).dc2deF2;
   std::memcpy(transId, s.transId, sizeof(transId));
 }
+
+void Plan::take_operators(Plan&& s) { assign_operators(std::move(s)); }
 
 // The operator set of MatMgnt3d_MPI (fmm3d_mpi/matmgnt3d_mpi.cpp:52-71,
 // 107-274, 373-411) for a homogeneous equivalent kernel: unit-radius tables,

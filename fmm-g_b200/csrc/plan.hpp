@@ -137,6 +137,8 @@ struct Plan {
   // the operator tables of (kt, coefs, np), copied from the process's most
   // recent sets when they hold it
   std::string build_operators();
+  // the operator tables of s (built by build_operators), moved into this plan
+  void take_operators(Plan&& s);
   // refactor the pinv the caller replaced (0: C2E up, 2: C2E down) from its
   // explicit table, so the FP32 pass applies the same operator
   void refactor_c2e(int which);
@@ -148,7 +150,7 @@ struct Plan {
 
  private:
   std::string build_operators_uncached();
-  void copy_operators(const Plan& s);
+  template <class S> void assign_operators(S&& s);  // copies or moves, as S is
   void build_tree(const double* src);
   void bin_targets(const double* trg);
   void build_lists();

@@ -156,6 +156,13 @@ def test_operator_sets_are_shared_between_handles_not_their_replacements():
     rng = np.random.default_rng(5)
     a.setup(rng.random((400, 3)))
     np.testing.assert_array_equal(a.operator(0), orig)
+    # a handle with no replaced table keeps its own tables through new setups
+    before = [b.operator(w, i) for w, i in ((0, 0), (1, 7), (3, 2), (4, 315), (5, 0), (6, 0))]
+    b.setup(rng.random((500, 3)))
+    b.setup(rng.random((600, 3)))
+    after = [b.operator(w, i) for w, i in ((0, 0), (1, 7), (3, 2), (4, 315), (5, 0), (6, 0))]
+    for x, y in zip(before, after):
+        np.testing.assert_array_equal(x, y)
     # other coefficients are another set (Navier's Poisson ratio enters the kernel)
     n1 = fmmg.FMM3d(511, np_=3, pts_max=60, coefs=(1.0, 0.25), device=-1)
     n2 = fmmg.FMM3d(511, np_=3, pts_max=60, coefs=(1.0, 0.3), device=-1)
