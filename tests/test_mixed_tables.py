@@ -167,3 +167,35 @@ def test_operator_sets_are_shared_between_handles_not_their_replacements():
     n1 = fmmg.FMM3d(511, np_=3, pts_max=60, coefs=(1.0, 0.25), device=-1)
     n2 = fmmg.FMM3d(511, np_=3, pts_max=60, coefs=(1.0, 0.3), device=-1)
     assert not np.array_equal(n1.operator(1, 0), n2.operator(1, 0))
+
+
+def test_operator_sets_under_concurrent_creation():
+    """Handles created from several threads at once (the foreign calls run
+    without the interpreter lock) get the same tables as handles created one
+    at a time, also while the process's sets are evicted (more keys than it
+    keeps)."""
+    import threading
+    keys = [(111, 3), (111, 4), (121, 5), (312, 3), (111, 3), (511, 3), (111, 4), (321, 3)]
+    ref = {}
+    for kt, np_ in set(keys):
+        f = fmmg.FMM3d(kt, np_=np_, pts_max=60, device=-1)
+        ref[(kt, np_)] = [f.operator(w, i) for w, i in ((0, 0), (2, 0), (4, 7), (5, 300), (6, 0))]
+    got, errors = {}, []
+
+    def make(j, kt, np_):
+        try:
+            f = fmmg.FMM3d(kt, np_=np_, pts_max=60, device=-1)
+            got[j] = ((kt, np_), [f.operator(w, i) for w, i in ((0, 0), (2, 0), (4, 7), (5, 300), (6, 0))])
+        except Exception as e:  # reported below
+            errors.append(e)
+
+    for _ in range(2):
+        th = [threading.Thread(target=make, args=(j, kt, np_)) for j, (kt, np_) in enumerate(keys)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        assert not errors, errors
+        for j, (key, tabs) in got.items():
+            for a, b in zip(tabs, ref[key]):
+                np.testing.assert_array_equal(a, b)
