@@ -218,7 +218,7 @@ class Droplets:
 def main(argv=None):
     """Command line of the reference driver: -numsrc, -distribution,
     -time_step, -particle_size or -volume_ratio, -num_iter, -write_fraction,
-    -skip_initial_sort (droplets.cpp:176-410)."""
+    -skip_initial_sort, -preserve_order, -isogranular (droplets.cpp:176-410)."""
     import argparse
     p = argparse.ArgumentParser(description=main.__doc__)
     p.add_argument("--numsrc", type=int, required=True)
@@ -230,6 +230,11 @@ def main(argv=None):
     p.add_argument("--num_iter", type=int, required=True)
     p.add_argument("--write_fraction", type=int, required=True)
     p.add_argument("--skip_initial_sort", action="store_true")
+    # at one process these change nothing: the evaluator returns values in the
+    # caller's order (-preserve_order, droplets.cpp:407) and -numsrc is the
+    # process's own count either way (-isogranular, :221-247)
+    p.add_argument("--preserve_order", action="store_true")
+    p.add_argument("--isogranular", action="store_true")
     p.add_argument("--np", type=int, default=6)
     p.add_argument("--pts_max", type=int, default=64)
     p.add_argument("--mixed", action="store_true", help="evaluate in the mixed-precision form")
