@@ -19,52 +19,74 @@ namespace fmmg {
 // A is m x n column-major with m >= n after an optional transpose.  Columns
 // are orthogonalised pairwise in tournament order (n/2 disjoint pairs per
 // round, so rounds parallelise and the result is thread-count independent).
+// Each column of V is kept right below its column of W, so one pass applies a
+// rotation to both.
 static void svd_onesided(int m, int n, std::vector<double>& W /* m x n, becomes U*S */,
                          std::vector<double>& V /* n x n */) {
-  V.assign((size_t)n * n, 0.0);
-  for (int i = 0; i < n; i++) V[(size_t)i * n + i] = 1.0;
+  const size_t ld = (size_t)m + n;
+  std::vector<double> Z(ld * n, 0.0);  // column j: W_j (m) then V_j (n), V = I
+  for (int j = 0; j < n; j++) {
+    std::copy(W.begin() + (size_t)j * m, W.begin() + (size_t)(j + 1) * m, Z.begin() + j * ld);
+    Z[j * ld + m + j] = 1.0;
+  }
   const int nn = n + (n & 1);
   std::vector<int> top(nn / 2), bot(nn / 2);
   for (int i = 0; i < nn / 2; i++) { top[i] = 2 * i; bot[i] = 2 * i + 1; }
-  std::vector<double> norms(n);
   for (int sweep = 0; sweep < 80; sweep++) {
     int rotated = 0;
-    for (int j = 0; j < n; j++) {
-      double s = 0;
-      const double* w = &W[(size_t)j * m];
-      for (int i = 0; i < m; i++) s += w[i] * w[i];
-      norms[j] = s;
-    }
     for (int round = 0; round < nn - 1; round++) {
+      // two pairs per iteration: their dot products share one loop (six
+      // independent sums hide the add latency; each pair sums in its own order)
+      const int npair = nn / 2;
 #pragma omp parallel for schedule(static) reduction(+ : rotated)
-      for (int k = 0; k < nn / 2; k++) {
-        int p = std::min(top[k], bot[k]), q = std::max(top[k], bot[k]);
-        if (q >= n) continue;
-        double* wp = &W[(size_t)p * m];
-        double* wq = &W[(size_t)q * m];
-        double a = 0, b = 0, g = 0;
-        for (int i = 0; i < m; i++) {
-          a += wp[i] * wp[i];
-          b += wq[i] * wq[i];
-          g += wp[i] * wq[i];
+      for (int k2 = 0; k2 < (npair + 1) / 2; k2++) {
+        double* zp[2] = {nullptr, nullptr};
+        double* zq[2] = {nullptr, nullptr};
+        for (int h = 0; h < 2; h++) {
+          const int k = 2 * k2 + h;
+          if (k >= npair) break;
+          int p = std::min(top[k], bot[k]), q = std::max(top[k], bot[k]);
+          if (q >= n) continue;
+          zp[h] = &Z[p * ld];
+          zq[h] = &Z[q * ld];
         }
-        if (a == 0.0 || b == 0.0) continue;
-        if (std::fabs(g) <= 1e-15 * std::sqrt(a * b)) continue;
-        rotated++;
-        double zeta = (b - a) / (2.0 * g);
-        double t = std::copysign(1.0, zeta) / (std::fabs(zeta) + std::hypot(1.0, zeta));
-        double c = 1.0 / std::hypot(1.0, t), s = c * t;
-        for (int i = 0; i < m; i++) {
-          double x = wp[i], y = wq[i];
-          wp[i] = c * x - s * y;
-          wq[i] = s * x + c * y;
+        double a[2] = {0, 0}, b[2] = {0, 0}, g[2] = {0, 0};
+        if (zp[0] && zp[1]) {
+          const double *p0 = zp[0], *q0 = zq[0], *p1 = zp[1], *q1 = zq[1];
+          for (int i = 0; i < m; i++) {
+            a[0] += p0[i] * p0[i];
+            b[0] += q0[i] * q0[i];
+            g[0] += p0[i] * q0[i];
+            a[1] += p1[i] * p1[i];
+            b[1] += q1[i] * q1[i];
+            g[1] += p1[i] * q1[i];
+          }
+        } else {
+          for (int h = 0; h < 2; h++) {
+            if (!zp[h]) continue;
+            const double *ph = zp[h], *qh = zq[h];
+            for (int i = 0; i < m; i++) {
+              a[h] += ph[i] * ph[i];
+              b[h] += qh[i] * qh[i];
+              g[h] += ph[i] * qh[i];
+            }
+          }
         }
-        double* vp = &V[(size_t)p * n];
-        double* vq = &V[(size_t)q * n];
-        for (int i = 0; i < n; i++) {
-          double x = vp[i], y = vq[i];
-          vp[i] = c * x - s * y;
-          vq[i] = s * x + c * y;
+        for (int h = 0; h < 2; h++) {
+          if (!zp[h]) continue;
+          if (a[h] == 0.0 || b[h] == 0.0) continue;
+          if (std::fabs(g[h]) <= 1e-15 * std::sqrt(a[h] * b[h])) continue;
+          rotated++;
+          double zeta = (b[h] - a[h]) / (2.0 * g[h]);
+          double t = std::copysign(1.0, zeta) / (std::fabs(zeta) + std::hypot(1.0, zeta));
+          double c = 1.0 / std::hypot(1.0, t), s = c * t;
+          double *zph = zp[h], *zqh = zq[h];
+#pragma omp simd
+          for (size_t i = 0; i < ld; i++) {  // element-wise: the same arithmetic vectorised
+            double x = zph[i], y = zqh[i];
+            zph[i] = c * x - s * y;
+            zqh[i] = s * x + c * y;
+          }
         }
       }
       // tournament rotation (player 0 stays)
@@ -77,6 +99,11 @@ static void svd_onesided(int m, int n, std::vector<double>& W /* m x n, becomes 
       }
     }
     if (!rotated) break;
+  }
+  V.resize((size_t)n * n);
+  for (int j = 0; j < n; j++) {
+    std::copy(Z.begin() + j * ld, Z.begin() + j * ld + m, W.begin() + (size_t)j * m);
+    std::copy(Z.begin() + j * ld + m, Z.begin() + (j + 1) * ld, V.begin() + (size_t)j * n);
   }
 }
 
