@@ -8,6 +8,7 @@
 #include <memory>
 #include <mutex>
 #include <numeric>
+#include <omp.h>
 #include <utility>
 
 #include "kernels.hpp"
@@ -23,6 +24,61 @@ void Plan::node_center(int d, const int* p, double* c) const {
   int tmp = 1 << d;
   for (int k = 0; k < 3; k++) c[k] = ll[k] + (2 * R) * (p[k] + 0.5) / double(tmp);
 }
+
+// Stable partition of perm[b, e) into the 8 octants about centre c (code
+// (p >= c) per axis, x most significant); cnt receives the octant sizes.
+// With `chunked` (called outside a parallel region, for big ranges) the range
+// is cut into one chunk per thread: each chunk counts its codes, then places
+// its points after the earlier chunks' points of the same octant, which gives
+// the order of the sequential pass.
+static void octant_partition(const double* pts, int64_t* perm, int64_t* tmp, int64_t b, int64_t e,
+                             const double* c, int64_t cnt[8], bool chunked) {
+  auto code_of = [&](int64_t i) {
+    const double* p = pts + 3 * perm[i];
+    return (p[0] >= c[0]) * 4 + (p[1] >= c[1]) * 2 + (p[2] >= c[2]);
+  };
+  if (!chunked) {
+    for (int k = 0; k < 8; k++) cnt[k] = 0;
+    for (int64_t i = b; i < e; i++) cnt[code_of(i)]++;
+    int64_t off[8];
+    off[0] = b;
+    for (int k = 1; k < 8; k++) off[k] = off[k - 1] + cnt[k - 1];
+    for (int64_t i = b; i < e; i++) tmp[off[code_of(i)]++] = perm[i];
+    std::memcpy(&perm[b], &tmp[b], sizeof(int64_t) * (e - b));
+    return;
+  }
+  const int T = std::max(1, omp_get_max_threads());
+  const int64_t chunk = (e - b + T - 1) / T;
+  std::vector<int64_t> pos((size_t)T * 8, 0);
+  std::vector<uint8_t> code(e - b);
+#pragma omp parallel for schedule(static)
+  for (int t = 0; t < T; t++)
+    for (int64_t i = b + t * chunk; i < std::min(e, b + (t + 1) * chunk); i++) {
+      const int k = code_of(i);
+      code[i - b] = (uint8_t)k;
+      pos[(size_t)t * 8 + k]++;
+    }
+  int64_t at = b;
+  for (int k = 0; k < 8; k++) {
+    cnt[k] = 0;
+    for (int t = 0; t < T; t++) {
+      const int64_t n = pos[(size_t)t * 8 + k];
+      pos[(size_t)t * 8 + k] = at;
+      at += n;
+      cnt[k] += n;
+    }
+  }
+#pragma omp parallel for schedule(static)
+  for (int t = 0; t < T; t++)
+    for (int64_t i = b + t * chunk; i < std::min(e, b + (t + 1) * chunk); i++)
+      tmp[pos[(size_t)t * 8 + code[i - b]]++] = perm[i];
+#pragma omp parallel for schedule(static)
+  for (int64_t i = b; i < e; i++) perm[i] = tmp[i];
+}
+
+// Ranges at least this long are partitioned by all threads at once (the top
+// levels hold few nodes with many points each).
+constexpr int64_t kChunkedPartition = 1 << 16;
 
 // Adaptive octree (stands in for DENDRO points2Octree + CreateAncestors,
 // fmm3d_mpi/let3d_mpi.cpp:268-288, 611-726): an octant is split while it
@@ -50,40 +106,30 @@ void Plan::build_tree(const double* src) {
     int total = next;
     depth.resize(total); par.resize(total); chd.resize(total); path.resize(3 * (size_t)total);
     srcBeg.resize(total); srcCnt.resize(total);
-#pragma omp parallel for schedule(dynamic, 8)
-    for (int n = lvS; n < lvE; n++) {
-      int f = first[n - lvS];
-      if (f < 0) continue;
+    auto split_node = [&](int n, bool chunked) {
+      const int f = first[n - lvS];
       chd[n] = f;
       double c[3];
       node_center(d, &path[3 * (size_t)n], c);
-      int64_t b = srcBeg[n], e = b + srcCnt[n];
-      int64_t cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      for (int64_t i = b; i < e; i++) {
-        const double* p = src + 3 * srcPerm[i];
-        int code = (p[0] >= c[0]) * 4 + (p[1] >= c[1]) * 2 + (p[2] >= c[2]);
-        cnt[code]++;
-      }
-      int64_t off[8];
-      off[0] = b;
-      for (int k = 1; k < 8; k++) off[k] = off[k - 1] + cnt[k - 1];
+      const int64_t b = srcBeg[n], e = b + srcCnt[n];
+      int64_t cnt[8];
+      octant_partition(src, srcPerm.data(), tmp.data(), b, e, c, cnt, chunked);
+      int64_t off = b;
       for (int k = 0; k < 8; k++) {
         int ch = f + k;
         depth[ch] = d + 1; par[ch] = n; chd[ch] = -1;
         path[3 * (size_t)ch + 0] = 2 * path[3 * (size_t)n + 0] + (k >> 2);
         path[3 * (size_t)ch + 1] = 2 * path[3 * (size_t)n + 1] + ((k >> 1) & 1);
         path[3 * (size_t)ch + 2] = 2 * path[3 * (size_t)n + 2] + (k & 1);
-        srcBeg[ch] = off[k]; srcCnt[ch] = cnt[k];
+        srcBeg[ch] = off; srcCnt[ch] = cnt[k];
+        off += cnt[k];
       }
-      int64_t w[8];
-      std::memcpy(w, off, sizeof(w));
-      for (int64_t i = b; i < e; i++) {
-        const double* p = src + 3 * srcPerm[i];
-        int code = (p[0] >= c[0]) * 4 + (p[1] >= c[1]) * 2 + (p[2] >= c[2]);
-        tmp[w[code]++] = srcPerm[i];
-      }
-      std::memcpy(&srcPerm[b], &tmp[b], sizeof(int64_t) * (e - b));
-    }
+    };
+    for (int n = lvS; n < lvE; n++)
+      if (first[n - lvS] >= 0 && srcCnt[n] >= kChunkedPartition) split_node(n, true);
+#pragma omp parallel for schedule(dynamic, 8)
+    for (int n = lvS; n < lvE; n++)
+      if (first[n - lvS] >= 0 && srcCnt[n] < kChunkedPartition) split_node(n, false);
     levelBeg.push_back(lvE);
     lvS = lvE; lvE = total; d++;
   }
@@ -102,28 +148,24 @@ void Plan::bin_targets(const double* trg) {
   std::vector<int64_t> tmp(nt);
   trgCnt[0] = nt;
   for (int d = 0; d <= maxDepth; d++) {
-#pragma omp parallel for schedule(dynamic, 8)
-    for (int n = levelBeg[d]; n < levelBeg[d + 1]; n++) {
-      if (chd[n] < 0) continue;
+    auto bin_node = [&](int n, bool chunked) {
       double c[3];
       node_center(d, &path[3 * (size_t)n], c);
-      int64_t b = trgBeg[n], e = b + trgCnt[n];
-      int64_t cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      for (int64_t i = b; i < e; i++) {
-        const double* p = trg + 3 * trgPerm[i];
-        cnt[(p[0] >= c[0]) * 4 + (p[1] >= c[1]) * 2 + (p[2] >= c[2])]++;
+      const int64_t b = trgBeg[n], e = b + trgCnt[n];
+      int64_t cnt[8];
+      octant_partition(trg, trgPerm.data(), tmp.data(), b, e, c, cnt, chunked);
+      int64_t off = b;
+      for (int k = 0; k < 8; k++) {
+        trgBeg[chd[n] + k] = off;
+        trgCnt[chd[n] + k] = cnt[k];
+        off += cnt[k];
       }
-      int64_t off[8];
-      off[0] = b;
-      for (int k = 1; k < 8; k++) off[k] = off[k - 1] + cnt[k - 1];
-      for (int k = 0; k < 8; k++) { trgBeg[chd[n] + k] = off[k]; trgCnt[chd[n] + k] = cnt[k]; }
-      for (int64_t i = b; i < e; i++) {
-        const double* p = trg + 3 * trgPerm[i];
-        int code = (p[0] >= c[0]) * 4 + (p[1] >= c[1]) * 2 + (p[2] >= c[2]);
-        tmp[off[code]++] = trgPerm[i];
-      }
-      std::memcpy(&trgPerm[b], &tmp[b], sizeof(int64_t) * (e - b));
-    }
+    };
+    for (int n = levelBeg[d]; n < levelBeg[d + 1]; n++)
+      if (chd[n] >= 0 && trgCnt[n] >= kChunkedPartition) bin_node(n, true);
+#pragma omp parallel for schedule(dynamic, 8)
+    for (int n = levelBeg[d]; n < levelBeg[d + 1]; n++)
+      if (chd[n] >= 0 && trgCnt[n] < kChunkedPartition) bin_node(n, false);
   }
 }
 
@@ -383,20 +425,41 @@ void Plan::build_worklists() {
         o++;
       });
     }
-  // inverted per source slot, in the order of the target-slot lists (a stable
-  // counting sort)
+  // inverted per source slot, in the order of the target-slot lists: a stable
+  // counting sort over chunks of target slots, each chunk placing its entries
+  // after the earlier chunks' entries of the same source slot
   const int64_t nEnt = vTrgPtr[nTrgSlots];
+  const int T = std::max(1, omp_get_max_threads());
+  const size_t tchunk = (nTrgSlots + T - 1) / T;
+  std::vector<int64_t> pos((size_t)T * nSrcSlots, 0);
+#pragma omp parallel for schedule(static)
+  for (int t = 0; t < T; t++) {
+    int64_t* pc = &pos[(size_t)t * nSrcSlots];
+    for (size_t ts = t * tchunk; ts < std::min(nTrgSlots, (t + 1) * tchunk); ts++)
+      for (int64_t i = vTrgPtr[ts]; i < vTrgPtr[ts + 1]; i++) pc[vTrgEnt[2 * i]]++;
+  }
   vSrcPtr.assign(nSrcSlots + 1, 0);
-  for (int64_t i = 0; i < nEnt; i++) vSrcPtr[vTrgEnt[2 * i] + 1]++;
-  for (size_t t = 0; t < nSrcSlots; t++) vSrcPtr[t + 1] += vSrcPtr[t];
-  vSrcEnt.resize(2 * (size_t)nEnt);
-  std::vector<int64_t> fill(vSrcPtr.begin(), vSrcPtr.end() - 1);
-  for (size_t ts = 0; ts < nTrgSlots; ts++)
-    for (int64_t i = vTrgPtr[ts]; i < vTrgPtr[ts + 1]; i++) {
-      const int64_t o = fill[vTrgEnt[2 * i]]++;
-      vSrcEnt[2 * o] = (int32_t)ts;
-      vSrcEnt[2 * o + 1] = vTrgEnt[2 * i + 1];
+  int64_t at = 0;
+  for (size_t sl = 0; sl < nSrcSlots; sl++) {
+    vSrcPtr[sl] = at;
+    for (int t = 0; t < T; t++) {
+      const int64_t n = pos[(size_t)t * nSrcSlots + sl];
+      pos[(size_t)t * nSrcSlots + sl] = at;
+      at += n;
     }
+  }
+  vSrcPtr[nSrcSlots] = at;
+  vSrcEnt.resize(2 * (size_t)nEnt);
+#pragma omp parallel for schedule(static)
+  for (int t = 0; t < T; t++) {
+    int64_t* pc = &pos[(size_t)t * nSrcSlots];
+    for (size_t ts = t * tchunk; ts < std::min(nTrgSlots, (t + 1) * tchunk); ts++)
+      for (int64_t i = vTrgPtr[ts]; i < vTrgPtr[ts + 1]; i++) {
+        const int64_t o = pc[vTrgEnt[2 * i]]++;
+        vSrcEnt[2 * o] = (int32_t)ts;
+        vSrcEnt[2 * o + 1] = vTrgEnt[2 * i + 1];
+      }
+  }
 }
 
 // Inverse of a CSR (rows -> column ids): for every id that occurs, the rows
