@@ -820,7 +820,7 @@ fmmg_status fmmg_operator(fmmg_handle* h, int which, int idx, double* get, const
       n = ue * 8 * ue;
       if (get) {
         try {
-          const std::vector<double> f = fmmg::fold_c2e_m2m(P);  // row-major [ue][8 ue]
+          const std::vector<double>& f = P.folded_upward();  // row-major [ue][8 ue]
           for (int64_t i = 0; i < ue; i++)
             for (int64_t j = 0; j < 8 * ue; j++) get[j * ue + i] = f[i * 8 * ue + j];
         }
@@ -834,6 +834,7 @@ fmmg_status fmmg_operator(fmmg_handle* h, int which, int idx, double* get, const
   if (set) {
     h->opsDirty = true;
     h->tablesReplaced = true;
+    if (which == 0 || which == 1) P.drop_folded_upward();
     try {
       if (which == 0 || which == 2) P.refactor_c2e(which);  // the FP32 pass applies the pinv factored
       if (which == 4) P.m2l_spectrum32(idx);                 // and transforms on the (2np-1)^3 grid

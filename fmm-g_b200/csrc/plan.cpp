@@ -648,6 +648,12 @@ template <class S> void Plan::assign_operators(S&& s) {
   uc2ueF1 = std::forward<S>(s).uc2ueF1; uc2ueF2 = std::forward<S>(s).uc2ueF2;
   dc2deF1 = std::forward<S>(s).dc2deF1; dc2deF2 = std::forward<S>(s).dc2deF2;
   std::memcpy(transId, s.transId, sizeof(transId));
+  upFold = std::forward<S>(s).upFold;
+}
+
+const std::vector<double>& Plan::folded_upward() const {
+  if (upFold.empty()) upFold = fold_c2e_m2m(*this);
+  return upFold;
 }
 
 void Plan::take_operators(Plan&& s) { assign_operators(std::move(s)); }

@@ -131,6 +131,10 @@ struct Plan {
   int kUp = 0, kDn = 0;
   std::vector<double> uc2ueF1, uc2ueF2, dc2deF1, dc2deF2;
   int transId[7][7][7];
+  // fold_c2e_m2m of these tables, formed on first use (the FP32 pass and
+  // fmmg_operator 6); cleared when the caller replaces C2E up or M2M
+  const std::vector<double>& folded_upward() const;
+  void drop_folded_upward() { upFold.clear(); }
 
   std::string build(const Options& opt, int64_t ns, const double* src, const double* nrm, int64_t nt,
                     const double* trg);
@@ -149,6 +153,7 @@ struct Plan {
   bool leaf(int n) const { return chd[n] < 0; }
 
  private:
+  mutable std::vector<double> upFold;  // [nUE*sdm][8*nUE*sdm], empty until formed
   std::string build_operators_uncached();
   template <class S> void assign_operators(S&& s);  // copies or moves, as S is
   void build_tree(const double* src);
