@@ -199,3 +199,27 @@ def test_operator_sets_under_concurrent_creation():
         for j, (key, tabs) in got.items():
             for a, b in zip(tabs, ref[key]):
                 np.testing.assert_array_equal(a, b)
+
+
+def test_failed_setup_leaves_a_handle_usable():
+    """A setup refused for its input (a point outside the root box) changes
+    nothing; the next valid setup of the same handle builds the same plan and
+    keeps the same tables as a fresh handle."""
+    rng = np.random.default_rng(9)
+    x = rng.random((800, 3))
+    f = _handle(321, 4)
+    tabs = [f.operator(w, i) for w, i in ((0, 0), (2, 0), (4, 9), (6, 0))]
+    bad = x.copy()
+    bad[17, 1] = 1.5
+    with pytest.raises(fmmg.FmmgError):
+        f.setup(bad, bad)
+    f.setup(x, x)
+    g = fmmg.FMM3d(321, np_=4, pts_max=60, device=-1)
+    g.setup(x, x)
+    for a, b in zip(f.tree(), g.tree()):
+        np.testing.assert_array_equal(a, b)
+    for which in range(4):
+        for a, b in zip(f.lists(which), g.lists(which)):
+            np.testing.assert_array_equal(a, b)
+    for t, (w, i) in zip(tabs, ((0, 0), (2, 0), (4, 9), (6, 0))):
+        np.testing.assert_array_equal(f.operator(w, i), t)
