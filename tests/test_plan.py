@@ -36,12 +36,14 @@ def _keymaps(lib, orc):
     return rec, nd, lk, ok
 
 
-@pytest.mark.parametrize("dist,pts,sep", [("uniform", 40, False), ("clustered", 25, False), ("clustered", 30, True)])
-def test_tree_and_lists_identical_to_oracle(dist, pts, sep):
+# the 150,000-point case has top-level nodes above the size at which the
+# library partitions a node's points with all threads (sources and targets)
+@pytest.mark.parametrize("dist,pts,sep,n", [("uniform", 40, False, 6000), ("clustered", 25, False, 6000),
+                                            ("clustered", 30, True, 6000), ("uniform", 60, True, 150000)])
+def test_tree_and_lists_identical_to_oracle(dist, pts, sep, n):
     rng = np.random.default_rng(5)
-    n = 6000
     src = rng.random((n, 3)) if dist == "uniform" else _clustered(rng, n)
-    trg = rng.random((2500, 3)) if sep else src
+    trg = rng.random((2500 if n <= 6000 else n // 2, 3)) if sep else src
     lib, orc = _pair(111, 4, pts, src, trg)
     rec, nd, lk, ok = _keymaps(lib, orc)
     assert set(lk) == set(ok)
