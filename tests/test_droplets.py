@@ -150,3 +150,24 @@ def test_run_writes_positions(tmp_path):
     assert np.loadtxt(tmp_path / "coord2.txt").shape == (200, 3)
     assert d.evaluations == 12
     assert d.x[:, 2].mean().item() < z0  # the particles sink
+
+
+def test_command_line(tmp_path, monkeypatch, capsys):
+    """main() with the reference's options, a dense CPU stand-in for the GPU
+    evaluator: eps from -volume_ratio, positions written every
+    -write_fraction steps, the timing line printed."""
+    class Stand(_DenseVelocity):
+        def __init__(self, np_, pts_max, precision):
+            self.setup_s = self.evaluate_s = 0.0
+
+    monkeypatch.setattr(D, "FmmVelocity", Stand)
+    D.main(["--numsrc", "150", "--distribution", "ball", "--time_step", "0.1", "--volume_ratio", "0.2",
+            "--num_iter", "2", "--write_fraction", "1", "--out", str(tmp_path), "--preserve_order"])
+    out = capsys.readouterr().out
+    n = D.snap_and_dedup(D.initial_positions(150, "ball")).shape[0]
+    assert "particles %d, particle size %g" % (n, D.particle_size(n, 0.2)) in out
+    assert "2 steps (8 right-hand sides)" in out
+    assert sorted(p.name for p in tmp_path.iterdir()) == ["coord0.txt", "coord1.txt", "coord2.txt"]
+    with pytest.raises(SystemExit):  # -particle_size and -volume_ratio exclude each other
+        D.main(["--numsrc", "10", "--distribution", "ball", "--time_step", "0.1", "--volume_ratio", "0.2",
+                "--particle_size", "0.01", "--num_iter", "1", "--write_fraction", "1"])
