@@ -41,7 +41,10 @@ struct Kernel3d {
 
 class FMM3d {
  public:
-  FMM3d() { fmmg_default_options(&opt_); }
+  FMM3d() {
+    fmmg_default_options(&opt_);
+    made_ = opt_;
+  }
   ~FMM3d() { fmmg_destroy(h_); }
   FMM3d(const FMM3d&) = delete;
   FMM3d& operator=(const FMM3d&) = delete;
@@ -61,16 +64,21 @@ class FMM3d {
   const char* lastError() const { return fmmg_last_error(h_); }
   fmmg_handle* handle() { return h_; }
 
-  // FMM3d_MPI::setup(): tree, lists, operators, device upload
+  // FMM3d_MPI::setup(): tree, lists, operators, device upload.  Called again
+  // with the same kernel and options (points that moved), the handle is set
+  // up again in place: it keeps its operator tables and device context.
   int setup() {
-    fmmg_destroy(h_);
-    h_ = nullptr;
     opt_.kernel_type = knl_.type;
     opt_.coefs[0] = knl_.coefs.size() > 0 ? knl_.coefs[0] : 1.0;
     opt_.coefs[1] = knl_.coefs.size() > 1 ? knl_.coefs[1] : 0.25;
     for (int d = 0; d < 3; d++) opt_.ctr[d] = ctr_[d];
-    fmmg_status s = fmmg_create(&opt_, &h_);
-    if (s != FMMG_OK) return s;
+    if (!h_ || !same_options(opt_, made_)) {
+      fmmg_destroy(h_);
+      h_ = nullptr;
+      fmmg_status s = fmmg_create(&opt_, &h_);
+      if (s != FMMG_OK) return s;
+      made_ = opt_;
+    }
     if (src_.size() % 3 || trg_.size() % 3) return FMMG_INVALID_ARG;
     return fmmg_setup(h_, (int64_t)src_.size() / 3, src_.data(), nrm_.empty() ? nullptr : nrm_.data(),
                       (int64_t)trg_.size() / 3, trg_.data());
@@ -101,7 +109,14 @@ class FMM3d {
   }
 
  private:
+  static bool same_options(const fmmg_options& a, const fmmg_options& b) {
+    return a.kernel_type == b.kernel_type && a.coefs[0] == b.coefs[0] && a.coefs[1] == b.coefs[1] &&
+           a.np == b.np && a.pts_max == b.pts_max && a.max_level == b.max_level && a.ctr[0] == b.ctr[0] &&
+           a.ctr[1] == b.ctr[1] && a.ctr[2] == b.ctr[2] && a.root_level == b.root_level && a.device == b.device &&
+           a.stream == b.stream;
+  }
   fmmg_options opt_;
+  fmmg_options made_;  // the options h_ was created with
   fmmg_handle* h_ = nullptr;
   Kernel3d knl_;
   std::array<double, 3> ctr_{0.5, 0.5, 0.5};

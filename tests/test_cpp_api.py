@@ -27,13 +27,28 @@ int main(int argc, char** argv) {
   if (s) { printf("setup %d %s\n", s, fmm.lastError()); return 1; }
   std::vector<double> den(n), val;
   for (auto& d : den) d = u(g) * 2 - 1;
-  s = fmm.evaluate(den, val);
-  if (device < 0) { printf("evaluate status %d\n", s); return s == FMMG_STATE ? 0 : 2; }
-  if (s) { printf("evaluate %d %s\n", s, fmm.lastError()); return 3; }
-  double rerr = 1;
-  s = fmm.check(den, val, 500, rerr);
-  printf("rerr %.3e\n", rerr);
-  return (s == 0 && rerr < 1e-3) ? 0 : 4;
+  // the points move: the same object set up again (same options: the handle
+  // is kept), then with another order (a new handle)
+  for (int pass = 0; pass < 3; pass++) {
+    if (pass > 0) {
+      for (auto& x : fmm.srcPos()) x = 0.9 * x + 0.05;
+      fmm.trgPos() = fmm.srcPos();
+      if (pass == 2) fmm.np() = 5;
+      s = fmm.setup();
+      if (s) { printf("setup again %d %s\n", s, fmm.lastError()); return 5; }
+    }
+    s = fmm.evaluate(den, val);
+    if (device < 0) {
+      if (s != FMMG_STATE) { printf("evaluate status %d\n", s); return 2; }
+      continue;
+    }
+    if (s) { printf("evaluate %d %s\n", s, fmm.lastError()); return 3; }
+    double rerr = 1;
+    s = fmm.check(den, val, 500, rerr);
+    printf("rerr %.3e\n", rerr);
+    if (s != 0 || rerr >= 1e-3) return 4;
+  }
+  return 0;
 }
 """
 
