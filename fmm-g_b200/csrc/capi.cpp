@@ -758,6 +758,31 @@ fmmg_status fmmg_lists(const fmmg_handle* h, int which, int64_t* ptr, int32_t* i
   return FMMG_OK;
 }
 
+fmmg_status fmmg_worklist(const fmmg_handle* h, int which, int32_t* rows, int64_t* ptr, int32_t* idx,
+                          int64_t* n_rows, int64_t* total) {
+  if (!h || which < 0 || which > 5) return FMMG_INVALID_ARG;
+  if (!h->setupDone) return FMMG_STATE;
+  const fmmg::Plan& P = h->plan;
+  static const fmmg::CSR none;
+  const std::vector<int32_t>* R = nullptr;
+  const fmmg::CSR* L = &none;
+  switch (which) {
+    case 0: R = &P.evtrLeaves; L = &P.nearSrc; break;
+    case 1: R = &P.farLeaves; L = &P.farUE; break;
+    case 2: R = &P.s2lNodes; L = &P.s2lSrc; break;
+    case 3: R = &P.vParents; L = &P.vNbr; break;
+    case 4: R = &P.s2mLeaves; break;
+    default: R = &P.l2tLeaves; break;
+  }
+  if (rows) std::copy(R->begin(), R->end(), rows);
+  if (n_rows) *n_rows = (int64_t)R->size();
+  const bool csr = which <= 3;
+  if (ptr && csr) std::copy(L->ptr.begin(), L->ptr.end(), ptr);
+  if (idx && csr) std::copy(L->idx.begin(), L->idx.end(), idx);
+  if (total) *total = csr ? (int64_t)L->idx.size() : 0;
+  return FMMG_OK;
+}
+
 fmmg_status fmmg_operator(fmmg_handle* h, int which, int idx, double* get, const double* set, int64_t* count) {
   if (!h) return FMMG_INVALID_ARG;
   if (set) drop_graph(h);  // a captured graph holds the FP32 operator copies of the old tables

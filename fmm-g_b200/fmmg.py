@@ -88,6 +88,7 @@ SIGNATURES = {
     "fmmg_graph_state": ([ctypes.c_void_p, _ip, ctypes.POINTER(ctypes.c_char_p)], ctypes.c_int),
     "fmmg_tree": ([ctypes.c_void_p, _i32p, _i64p, _i64p], ctypes.c_int),
     "fmmg_lists": ([ctypes.c_void_p, ctypes.c_int, _i64p, _i32p, _i64p], ctypes.c_int),
+    "fmmg_worklist": ([ctypes.c_void_p, ctypes.c_int, _i32p, _i64p, _i32p, _i64p, _i64p], ctypes.c_int),
     "fmmg_operator": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp, _i64p], ctypes.c_int),
     "fmmg_dense_noalloc": ([ctypes.c_int, _dp, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                             ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
@@ -387,6 +388,20 @@ class FMM3d:
         idx = np.zeros(max(tot.value, 1), dtype=np.int32)
         self._chk(lib().fmmg_lists(self.h, which, ptr.ctypes.data_as(_i64p), idx.ctypes.data_as(_i32p), None))
         return ptr, idx[: tot.value]
+
+    def worklist(self, which):
+        """(rows, ptr, idx) of GPU work list `which` (fmmg_worklist); ptr and
+        idx are None for the row-only lists 4 and 5."""
+        nr, tot = ctypes.c_int64(), ctypes.c_int64()
+        self._chk(lib().fmmg_worklist(self.h, which, None, None, None, ctypes.byref(nr), ctypes.byref(tot)))
+        rows = np.zeros(max(nr.value, 1), dtype=np.int32)
+        ptr = np.zeros(nr.value + 1, dtype=np.int64)
+        idx = np.zeros(max(tot.value, 1), dtype=np.int32)
+        self._chk(lib().fmmg_worklist(self.h, which, rows.ctypes.data_as(_i32p), ptr.ctypes.data_as(_i64p),
+                                      idx.ctypes.data_as(_i32p), None, None))
+        if which >= 4:
+            return rows[: nr.value], None, None
+        return rows[: nr.value], ptr, idx[: tot.value]
 
     def operator(self, which, idx=0):
         n = ctypes.c_int64()

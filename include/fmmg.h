@@ -248,6 +248,21 @@ fmmg_status fmmg_tuning(fmmg_handle* h, int* vals, int n, int set);
 fmmg_status fmmg_tree(const fmmg_handle* h, int32_t* node_rec, int64_t* perm_src, int64_t* perm_trg);
 fmmg_status fmmg_lists(const fmmg_handle* h, int which, int64_t* ptr, int32_t* idx, int64_t* total);
 
+/* The GPU work lists derived from those lists at setup (valid after setup,
+ * also with device < 0), following the per-node decisions of the reference
+ * evaluate() (fmm3d_mpi/fmm3d_eval_mpi.cpp:1146, 1249): which 0 the direct
+ * sources of each evaluator leaf (its U list, the W boxes with fewer than
+ * |UE| x srcDOF source values, and its X list when the leaf has fewer than
+ * |DC| x trgDOF target values), 1 the other W boxes (applied from their UE
+ * surface), 2 the X sources of the other nodes (summed onto their DC
+ * surface), 3 per target parent the same-depth non-leaf neighbours whose
+ * children feed its children's V lists, 4 the leaves with sources (S2M),
+ * 5 the evaluator leaves at depth >= 2 (L2T).  rows receives *n_rows node
+ * ids; for which 0-3 ptr (n_rows + 1 entries) and idx (*total entries) hold
+ * each row's node ids, for 4 and 5 *total is 0.  NULL buffers only size. */
+fmmg_status fmmg_worklist(const fmmg_handle* h, int which, int32_t* rows, int64_t* ptr, int32_t* idx,
+                          int64_t* n_rows, int64_t* total);
+
 /* Operator tables built by this handle.  which: 0 UC->UE pseudo-inverse,
  * 1 UE->UC (octant idx 0..7), 2 DC->DE pseudo-inverse, 3 DE->DC (octant 0..7),
  * 4 UE->DC translation spectrum (idx 0..315, complex as pairs).  Matrices are

@@ -1,0 +1,116 @@
+"""The GPU work lists (fmmg_worklist) rebuilt on the host from the tree and
+the U/V/W/X lists (which tests/test_plan.py checks against the oracle), by the
+per-node decisions of the reference evaluate(): W boxes with fewer than
+|UE| x srcDOF source values and the X list of a leaf with fewer than
+|DC| x trgDOF target values are summed directly (fmm3d_mpi/fmm3d_eval_mpi.cpp:1146,
+1249), the others go through the UE / DC surfaces; M2L is grouped by target
+parent and same-depth neighbour parent (let3d_mpi.cpp:1687-1698)."""
+import numpy as np
+import pytest
+
+import fmmg
+
+EVTR, SRCE = 4, 16
+
+
+def _points(kind, n, rng):
+    if kind == "uniform":
+        return rng.random((n, 3))
+    c = rng.uniform(0.2, 0.8, size=(6, 3))
+    p = c[rng.integers(0, 6, n)] + 0.03 * rng.normal(size=(n, 3))
+    return np.clip(p, 0.0, 1.0)
+
+
+def _case(kt, np_, pts, kind, n, n_trg):
+    rng = np.random.default_rng(kt + np_)
+    src = _points(kind, n, rng)
+    trg = _points("uniform", n_trg, rng) if n_trg else None
+    f = fmmg.FMM3d(kt, np_=np_, pts_max=pts, device=-1)
+    f.setup(src, src, trg)
+    return f
+
+
+def _csr_rows(ptr, idx):
+    return [idx[ptr[r]:ptr[r + 1]].tolist() for r in range(len(ptr) - 1)]
+
+
+@pytest.mark.parametrize("kt,np_,pts,kind,n,n_trg", [
+    (111, 4, 40, "uniform", 6000, 0),
+    (121, 4, 25, "clustered", 6000, 3000),
+    (321, 4, 30, "clustered", 5000, 2500),
+    (511, 5, 60, "uniform", 8000, 0),
+    (111, 6, 12, "clustered", 4000, 4000),
+])
+def test_worklists_follow_the_lists(kt, np_, pts, kind, n, n_trg):
+    f = _case(kt, np_, pts, kind, n, n_trg)
+    rec, _, _ = f.tree()
+    nn = rec.shape[0]
+    depth, chd, tag, scnt, tcnt = rec[:, 0], rec[:, 5], rec[:, 6], rec[:, 7], rec[:, 8]
+    leaf = chd < 0
+    lsrc = leaf & (scnt > 0)
+    info, st = f.info(), f.plan_stats()
+    sd, td = info["src_dof"], info["trg_dof"]
+    n_surf = np_ ** 3 - (np_ - 2) ** 3
+    ue_size, dc_size = n_surf * st["sdm"], n_surf * st["tdm"]
+    U, V, W, X = (_csr_rows(*f.lists(w)) for w in range(4))
+
+    w_direct = lambda w: bool(lsrc[w]) and scnt[w] * sd < ue_size
+    x_direct = lambda g: bool(leaf[g]) and tcnt[g] * td < dc_size
+    evtr_leaves = [g for g in range(nn) if tag[g] & EVTR and leaf[g]]
+    near = [U[g] + [w for w in W[g] if w_direct(w)] + (X[g] if x_direct(g) else []) for g in evtr_leaves]
+    far_rows = [g for g in evtr_leaves if any(not w_direct(w) for w in W[g])]
+    far = [[w for w in W[g] if not w_direct(w)] for g in far_rows]
+    s2l_rows = [g for g in range(nn) if tag[g] & EVTR and not x_direct(g) and X[g]]
+
+    rows, ptr, idx = f.worklist(0)
+    assert rows.tolist() == evtr_leaves and _csr_rows(ptr, idx) == near
+    rows, ptr, idx = f.worklist(1)
+    assert rows.tolist() == far_rows and _csr_rows(ptr, idx) == far
+    rows, ptr, idx = f.worklist(2)
+    assert rows.tolist() == s2l_rows and _csr_rows(ptr, idx) == [X[g] for g in s2l_rows]
+    assert f.worklist(4)[0].tolist() == [g for g in range(nn) if lsrc[g]]
+    assert f.worklist(5)[0].tolist() == [g for g in evtr_leaves if depth[g] >= 2]
+    # every direct or surface sum of a leaf's lists is in exactly one work list
+    assert sum(len(r) for r in near) + sum(len(r) for r in far) == \
+        sum(len(U[g]) + len(W[g]) + (len(X[g]) if x_direct(g) else 0) for g in evtr_leaves)
+
+    # M2L parent pairs: same-depth non-leaf neighbours, in (dx, dy, dz) order
+    at = {(int(depth[g]), *map(int, rec[g, 1:4])): g for g in range(nn)}
+    want_rows, want_nbr = [], []
+    for P in range(nn):
+        d = int(depth[P])
+        if d < 1 or leaf[P] or not any(tag[chd[P] + o] & EVTR for o in range(8)):
+            continue
+        q = []
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    key = (d, rec[P, 1] + dx, rec[P, 2] + dy, rec[P, 3] + dz)
+                    if (dx, dy, dz) != (0, 0, 0) and key in at and not leaf[at[key]]:
+                        q.append(at[key])
+        if q:
+            want_rows.append(P)
+            want_nbr.append(q)
+    rows, ptr, idx = f.worklist(3)
+    assert rows.tolist() == want_rows and _csr_rows(ptr, idx) == want_nbr
+    # and they give each evaluator child exactly its V list
+    for P, qs in zip(want_rows, want_nbr):
+        for o in range(8):
+            c = chd[P] + o
+            if not tag[c] & EVTR:
+                continue
+            got = {v for Q in qs for v in range(chd[Q], chd[Q] + 8)
+                   if np.abs(rec[v, 1:4] - rec[c, 1:4]).max() > 1 and tag[v] & SRCE}
+            assert got == set(V[c]), (P, c)
+    # V lists only arise this way
+    assert sum(len(V[g]) for g in range(nn)) == sum(
+        len(V[chd[P] + o]) for P in want_rows for o in range(8) if tag[chd[P] + o] & EVTR)
+
+
+def test_worklist_arguments():
+    f = fmmg.FMM3d(111, np_=4, pts_max=40, device=-1)
+    with pytest.raises(fmmg.FmmgError):
+        f.worklist(0)  # before setup
+    f.setup(np.random.default_rng(0).random((500, 3)))
+    with pytest.raises(fmmg.FmmgError):
+        f.worklist(6)
