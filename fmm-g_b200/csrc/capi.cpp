@@ -760,9 +760,20 @@ fmmg_status fmmg_lists(const fmmg_handle* h, int which, int64_t* ptr, int32_t* i
 
 fmmg_status fmmg_worklist(const fmmg_handle* h, int which, int32_t* rows, int64_t* ptr, int32_t* idx,
                           int64_t* n_rows, int64_t* total) {
-  if (!h || which < 0 || which > 5) return FMMG_INVALID_ARG;
+  if (!h || which < 0 || which > 7) return FMMG_INVALID_ARG;
   if (!h->setupDone) return FMMG_STATE;
   const fmmg::Plan& P = h->plan;
+  if (which >= 6) {  // expanded V lists: (slot, translation id) pairs per slot
+    const std::vector<int32_t>& R = which == 6 ? P.vTrgNodes : P.vSrcNodes;
+    const std::vector<int64_t>& Lp = which == 6 ? P.vTrgPtr : P.vSrcPtr;
+    const std::vector<int32_t>& Le = which == 6 ? P.vTrgEnt : P.vSrcEnt;
+    if (rows) std::copy(R.begin(), R.end(), rows);
+    if (n_rows) *n_rows = (int64_t)R.size();
+    if (ptr) std::copy(Lp.begin(), Lp.end(), ptr);
+    if (idx) std::copy(Le.begin(), Le.end(), idx);
+    if (total) *total = (int64_t)Le.size();
+    return FMMG_OK;
+  }
   static const fmmg::CSR none;
   const std::vector<int32_t>* R = nullptr;
   const fmmg::CSR* L = &none;

@@ -391,7 +391,8 @@ class FMM3d:
 
     def worklist(self, which):
         """(rows, ptr, idx) of GPU work list `which` (fmmg_worklist); ptr and
-        idx are None for the row-only lists 4 and 5."""
+        idx are None for the row-only lists 4 and 5, idx holds (slot,
+        translation id) pairs as an [n, 2] array for 6 and 7."""
         nr, tot = ctypes.c_int64(), ctypes.c_int64()
         self._chk(lib().fmmg_worklist(self.h, which, None, None, None, ctypes.byref(nr), ctypes.byref(tot)))
         rows = np.zeros(max(nr.value, 1), dtype=np.int32)
@@ -399,8 +400,10 @@ class FMM3d:
         idx = np.zeros(max(tot.value, 1), dtype=np.int32)
         self._chk(lib().fmmg_worklist(self.h, which, rows.ctypes.data_as(_i32p), ptr.ctypes.data_as(_i64p),
                                       idx.ctypes.data_as(_i32p), None, None))
-        if which >= 4:
+        if which in (4, 5):
             return rows[: nr.value], None, None
+        if which >= 6:
+            return rows[: nr.value], ptr, idx[: tot.value].reshape(-1, 2)
         return rows[: nr.value], ptr, idx[: tot.value]
 
     def operator(self, which, idx=0):

@@ -257,9 +257,13 @@ fmmg_status fmmg_lists(const fmmg_handle* h, int which, int64_t* ptr, int32_t* i
  * surface), 2 the X sources of the other nodes (summed onto their DC
  * surface), 3 per target parent the same-depth non-leaf neighbours whose
  * children feed its children's V lists, 4 the leaves with sources (S2M),
- * 5 the evaluator leaves at depth >= 2 (L2T).  rows receives *n_rows node
- * ids; for which 0-3 ptr (n_rows + 1 entries) and idx (*total entries) hold
- * each row's node ids, for 4 and 5 *total is 0.  NULL buffers only size. */
+ * 5 the evaluator leaves at depth >= 2 (L2T), 6 the V lists expanded per
+ * target spectrum slot, 7 the same inverted per source spectrum slot.  rows
+ * receives *n_rows node ids; for which 0-3 ptr (n_rows + 1 entries) and idx
+ * (*total entries) hold each row's node ids, for 4 and 5 *total is 0; for 6
+ * and 7 the rows are the slots' nodes and each entry of a row is a pair
+ * (slot on the other side, translation id 0..315) in idx, ptr counting pairs.
+ * NULL buffers only size. */
 fmmg_status fmmg_worklist(const fmmg_handle* h, int which, int32_t* rows, int64_t* ptr, int32_t* idx,
                           int64_t* n_rows, int64_t* total);
 

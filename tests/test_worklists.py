@@ -4,7 +4,9 @@ per-node decisions of the reference evaluate(): W boxes with fewer than
 |UE| x srcDOF source values and the X list of a leaf with fewer than
 |DC| x trgDOF target values are summed directly (fmm3d_mpi/fmm3d_eval_mpi.cpp:1146,
 1249), the others go through the UE / DC surfaces; M2L is grouped by target
-parent and same-depth neighbour parent (let3d_mpi.cpp:1687-1698)."""
+parent and same-depth neighbour parent (let3d_mpi.cpp:1687-1698), and the V
+lists are expanded per spectrum slot with their translation ids
+(matmgnt3d_mpi.cpp:385-411 numbers the 316 offsets)."""
 import numpy as np
 import pytest
 
@@ -113,4 +115,58 @@ def test_worklist_arguments():
         f.worklist(0)  # before setup
     f.setup(np.random.default_rng(0).random((500, 3)))
     with pytest.raises(fmmg.FmmgError):
-        f.worklist(6)
+        f.worklist(8)
+
+
+@pytest.mark.parametrize("kt,np_,pts,kind,n,n_trg", [
+    (111, 4, 30, "clustered", 6000, 0),
+    (321, 4, 25, "uniform", 5000, 3000),
+])
+def test_expanded_v_lists(kt, np_, pts, kind, n, n_trg):
+    """Lists 6 and 7: every V entry of a target slot once, as (source slot,
+    translation id of the source-minus-target offset), neighbour parent by
+    neighbour parent and child by child; list 7 the same entries sorted
+    stably by source slot."""
+    f = _case(kt, np_, pts, kind, n, n_trg)
+    rec, _, _ = f.tree()
+    chd, tag = rec[:, 5], rec[:, 6]
+    V = _csr_rows(*f.lists(1))
+    prow, pptr, pidx = f.worklist(3)
+    nbr = _csr_rows(pptr, pidx)
+    tid = {}
+    for a in range(-3, 4):
+        for b in range(-3, 4):
+            for c in range(-3, 4):
+                if max(abs(a), abs(b), abs(c)) > 1:
+                    tid[(a, b, c)] = len(tid)
+    # slots: target children of the rows in order; source children of their
+    # neighbours in first-seen order
+    tnodes, tptr, tent = f.worklist(6)
+    snodes, sptr, sent = f.worklist(7)
+    assert tnodes.tolist() == [chd[P] + o for P in prow for o in range(8) if tag[chd[P] + o] & EVTR]
+    seen = []
+    for qs in nbr:
+        for Q in qs:
+            for v in range(chd[Q], chd[Q] + 8):
+                if tag[v] & 1 and v not in seen:
+                    seen.append(v)
+    assert snodes.tolist() == seen
+    slot_of = {int(v): s for s, v in enumerate(snodes)}
+    parent_row = {int(P): r for r, P in enumerate(prow)}
+    pairs = []
+    for ts, t in enumerate(tnodes):
+        want = []
+        for Q in nbr[parent_row[int(rec[t, 4])]]:
+            for v in range(chd[Q], chd[Q] + 8):
+                if v in V[t]:
+                    off = tuple(int(x) for x in rec[v, 1:4] - rec[t, 1:4])
+                    want.append((slot_of[v], tid[off]))
+        got = [tuple(e) for e in tent[tptr[ts]:tptr[ts + 1]].tolist()]
+        assert got == want, t
+        assert sorted(snodes[s] for s, _ in got) == sorted(V[t])
+        pairs += [(s, ts, i) for s, i in got]
+    assert sum(len(V[int(t)]) for t in tnodes) == len(pairs)
+    inv = [(ts, i) for s, ts, i in sorted(pairs, key=lambda e: e[0])]  # stable
+    assert [tuple(e) for e in sent.tolist()] == inv
+    assert sptr.tolist() == np.concatenate([[0], np.cumsum(np.bincount([p[0] for p in pairs],
+                                                                        minlength=len(snodes)))]).tolist()
