@@ -18,7 +18,10 @@
 // capture.  Every call on a device shares the one array: calls that overlap on
 // the GPU (different streams, no ordering between them) race and give wrong
 // results.  The array keeps the last call's contents; each call clears the
-// part it accumulates into before use.
+// part it accumulates into before use.  The cached address belongs to the
+// device's current context: after cudaDeviceReset() (or any destruction of
+// the primary context) the module is loaded again and the array may move, so
+// this entry point must not be used across such a reset in one process.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -64,7 +67,7 @@ fmmg_status fmmg_dense_noalloc(int kernel_type, const double* coefs, int64_t n_s
   if (kernel_mm(kernel_type) < 0 || td == 0) {
     return FMMG_NOT_SUPPORTED;
   }
-  if (n_src < 1 || n_trg < 1 || !d_src || !d_den || !d_trg || !d_val ||
+  if (n_src < 1 || n_trg < 0 || !d_src || !d_den || (n_trg > 0 && (!d_trg || !d_val)) ||
       (kernel_has_normal(kernel_type) && !d_nrm)) {
     return FMMG_INVALID_ARG;
   }
@@ -74,6 +77,13 @@ fmmg_status fmmg_dense_noalloc(int kernel_type, const double* coefs, int64_t n_s
   const double mu = coefs ? coefs[0] : 1.0, ve = coefs ? coefs[1] : 0.25;
   if (!std::isfinite(mu) || !std::isfinite(ve) || mu == 0.0) {
     return FMMG_INVALID_ARG;
+  }
+  // the Navier kernels divide by 1 - nu (kernels.hpp), as fmmg_create refuses
+  if (kernel_mm(kernel_type) == NAV_S_U && ve == 1.0) {
+    return FMMG_INVALID_ARG;
+  }
+  if (n_trg == 0) {  // no targets: nothing to sum (fmmg_setup accepts zero targets too)
+    return FMMG_OK;
   }
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);

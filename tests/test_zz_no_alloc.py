@@ -56,6 +56,42 @@ def test_noalloc_matches_check_dense_sums_twice(kt):
         assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= TOL, call
 
 
+@pytest.mark.parametrize("kt", [111, 121, 321])
+def test_noalloc_matches_the_oracle_dense_sum(kt):
+    """An independent check of the kernel formulas and the normal indexing:
+    the CPU oracle's FP64 dense sum (the reference check()'s Dense3d sum) at a
+    few hundred targets, on two calls in a row."""
+    import oracle as O
+    rng = np.random.default_rng(5 + kt)
+    n = 6000
+    src = rng.random((n, 3))
+    nrm = rng.normal(size=(n, 3))
+    nrm /= np.linalg.norm(nrm, axis=1)[:, None]
+    sd = O.src_dof(kt)
+    for call in range(2):
+        den = rng.normal(size=n * sd)
+        trg = rng.random((300, 3))
+        st, got = _noalloc(kt, src, nrm, den, trg)
+        assert st == fmmg.FMMG_OK
+        ref = O.dense(kt, src, nrm, den, trg)
+        assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= TOL, call
+
+
+def test_noalloc_zero_targets_and_navier_nu_one():
+    rng = np.random.default_rng(4)
+    src = rng.random((10, 3))
+    # no targets: nothing to sum, like fmmg_setup with zero targets
+    import torch
+    ds = torch.from_numpy(src).cuda()
+    dd = torch.from_numpy(rng.normal(size=10)).cuda()
+    st = fmmg.lib().fmmg_dense_noalloc(111, None, 10, ds.data_ptr(), None, dd.data_ptr(), 0, None, None, None)
+    torch.cuda.synchronize()
+    assert st == fmmg.FMMG_OK
+    # the Navier kernels divide by 1 - nu: refused as fmmg_create refuses them
+    st, _ = _noalloc(511, src, src, rng.normal(size=30), src, coefs=(1.0, 1.0))
+    assert st == fmmg.FMMG_INVALID_ARG
+
+
 def test_noalloc_rejects_sizes_beyond_the_fixed_scratch():
     rng = np.random.default_rng(3)
     src = rng.random((10, 3))
