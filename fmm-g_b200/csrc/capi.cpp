@@ -64,6 +64,16 @@ static fmmg_status fail(fmmg_handle* h, fmmg_status s, const std::string& msg) {
   return s;
 }
 
+// After a synchronised call: FMMG_TIMEOUT if a kernel of the handle gave up a
+// bounded device wait (its results are then invalid), else FMMG_OK.
+static fmmg_status take_timeout(fmmg_handle* h) {
+  int flag = 0;
+  std::string e = fmmg::dev_take_error(h->dev, &flag);
+  if (!e.empty()) return fail(h, FMMG_CUDA_ERROR, e);
+  if (flag) return fail(h, FMMG_TIMEOUT, "a bounded device wait ran out; the results of this call are invalid");
+  return FMMG_OK;
+}
+
 #define FMMG_GUARD(h)                                                    \
   catch (const std::bad_alloc&) { return fail(h, FMMG_OOM, "host allocation failed"); } \
   catch (const std::exception& ex) { return fail(h, FMMG_INVALID_ARG, ex.what()); }
@@ -356,6 +366,14 @@ fmmg_status fmmg_set_gemm_path(fmmg_handle* h, int path) {
   return FMMG_OK;
 }
 
+fmmg_status fmmg_selftest_wait(int device, int arrive, int64_t limit_ns) {
+  if (device < 0 || limit_ns < 0 || limit_ns > 2000000000ll) return FMMG_INVALID_ARG;
+  int flag = 0;
+  std::string e = fmmg::dev_wait_selftest(device, arrive, (long long)limit_ns, &flag);
+  if (!e.empty()) return fail(nullptr, FMMG_CUDA_ERROR, e);
+  return flag ? FMMG_TIMEOUT : FMMG_OK;
+}
+
 fmmg_status fmmg_device_error(fmmg_handle* h, int* flag) {
   if (!h || !flag) return fail(h, FMMG_INVALID_ARG, "NULL argument");
   *flag = 0;
@@ -533,9 +551,9 @@ fmmg_status fmmg_adjoint_host(fmmg_handle* h, int k, const double* den, const do
     if (ce == cudaSuccess && gradT && bg) ce = cudaMemcpyAsync(gradT, h->dAdjGrad, bg * k, cudaMemcpyDeviceToHost, st);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
     if (ce != cudaSuccess) return fail(h, FMMG_CUDA_ERROR, cudaGetErrorString(ce));
+    return take_timeout(h);
   }
   FMMG_GUARD(h)
-  return FMMG_OK;
 }
 
 fmmg_status fmmg_synchronize(fmmg_handle* h) {
@@ -565,9 +583,9 @@ fmmg_status fmmg_evaluate(fmmg_handle* h, const double* den, double* val) {
     }
     ce = cudaStreamSynchronize(st);
     if (ce != cudaSuccess) return fail(h, FMMG_CUDA_ERROR, cudaGetErrorString(ce));
+    return take_timeout(h);
   }
   FMMG_GUARD(h)
-  return FMMG_OK;
 }
 
 fmmg_status fmmg_evaluate_host(fmmg_handle* h, int k, const double* den, double* val, int precision) {
@@ -598,9 +616,9 @@ fmmg_status fmmg_evaluate_host(fmmg_handle* h, int k, const double* den, double*
     }
     ce = cudaStreamSynchronize(st);
     if (ce != cudaSuccess) return fail(h, FMMG_CUDA_ERROR, cudaGetErrorString(ce));
+    return take_timeout(h);
   }
   FMMG_GUARD(h)
-  return FMMG_OK;
 }
 
 fmmg_status fmmg_check(fmmg_handle* h, const double* den, const double* val, int64_t nchk, const int64_t* idx,

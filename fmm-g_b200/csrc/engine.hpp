@@ -165,6 +165,9 @@ void scatter_rows(cudaStream_t st, int64_t n, int dof, const int64_t* perm, cons
 std::string dev_far_field(const Plan& P, DevState& D, const double* dDen);
 // reads and clears the device error flag (synchronises the handle's stream)
 std::string dev_take_error(DevState& D, int* flag);
+// Runs the bounded-wait error path on `device` (k_wait_selftest); *flag = 1
+// when the wait ran out.
+std::string dev_wait_selftest(int device, int arrive, long long limitNs, int* flag);
 // transposed FMM: g = A^T w for one right-hand side (caller order), and with
 // gradT != nullptr the target-position gradient of <w, A sigma> ([nt][3])
 std::string dev_adjoint(const Plan& P, DevState& D, const double* dDen, const double* dW, double* dG,

@@ -39,7 +39,7 @@ constexpr int TC_B_BYTES = TC_BN * TC_BK * 4;                    // 8 KB per B p
 constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;  // hi + lo of both
 constexpr size_t TC_SMEM_BYTES = (size_t)TC_STAGES * TC_STAGE_BYTES + 1024;  // + alignment slack
 constexpr uint32_t TC_TMEM_COLS = 64;
-constexpr long long TC_WAIT_LIMIT = 1ll << 26;  // mbarrier polls before giving up
+constexpr long long TC_WAIT_NS = 1000000000ll;  // a bounded mbarrier wait gives up after 1 s
 
 __device__ __forceinline__ uint32_t tc_smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -54,8 +54,17 @@ __device__ __forceinline__ uint64_t tc_desc(uint32_t addr) {
 constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
                               ((uint32_t)(TC_BM >> 4) << 24);
 
-__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity) {
-  for (long long i = 0; i < TC_WAIT_LIMIT; i++) {
+__device__ __forceinline__ uint64_t tc_clock_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Waits for the phase of the mbarrier at `bar` with the given parity to
+// complete; gives up (returns false) once limitNs nanoseconds have passed.
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity, long long limitNs = TC_WAIT_NS) {
+  const uint64_t t0 = tc_clock_ns();
+  for (;;) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
@@ -64,8 +73,8 @@ __device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity) {
         : "r"(bar), "r"(parity)
         : "memory");
     if (done) return true;
+    if ((long long)(tc_clock_ns() - t0) >= limitNs) return false;
   }
-  return false;
 }
 
 __device__ __forceinline__ void tc_split(float x, float& hi, float& lo) {
@@ -125,7 +134,7 @@ __global__ void __launch_bounds__(TC_THREADS)
 
   const int kBeg = blockIdx.z * kChunk, kEnd = min(K, kBeg + kChunk);
   const int nKB = (kEnd - kBeg + TC_BK - 1) / TC_BK;
-  bool ok = true;
+  bool ok;
   int issued = -1;  // last K block whose MMAs were issued (the same on every thread)
   // the next K block's raw operands travel in registers while the current block multiplies
   float4 ra[8], rb[4];
@@ -153,10 +162,9 @@ __global__ void __launch_bounds__(TC_THREADS)
     const uint32_t sAl = sA + TC_A_BYTES, sB = sA + 2 * TC_A_BYTES, sBl = sB + TC_B_BYTES;
     unsigned char* pA = baseP + s * TC_STAGE_BYTES;
     if (kb >= TC_STAGES) {  // the MMAs of block kb - 2 read this stage
-      if (!tc_wait(tc_smem_u32(&mbar[s]), (uint32_t)(((kb - TC_STAGES) / TC_STAGES) & 1))) {
-        ok = false;
-        atomicExch(&abortFlag, 1);
-      }
+      if (!tc_wait(tc_smem_u32(&mbar[s]), (uint32_t)(((kb - TC_STAGES) / TC_STAGES) & 1))) atomicExch(&abortFlag, 1);
+      __syncthreads();  // every thread's wait has ended: abortFlag is final for this block
+      if (abortFlag) break;  // the tensor core may still read this stage: nobody writes it
     }
     const int k0 = kBeg + kb * TC_BK;
 #pragma unroll
@@ -186,10 +194,6 @@ __global__ void __launch_bounds__(TC_THREADS)
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (abortFlag) {
-      ok = false;
-      break;
-    }
     issued = kb;
     if (tid == 0) {
 #pragma unroll
@@ -212,16 +216,29 @@ __global__ void __launch_bounds__(TC_THREADS)
     }
     if (kb + 1 < nKB) fetch(kb + 1);
   }
-  // wait for the last issued block (its commit covers every earlier MMA)
-  if (issued >= 0 && !tc_wait(tc_smem_u32(&mbar[issued & 1]), (uint32_t)((issued / TC_STAGES) & 1))) ok = false;
+  // wait for the last issued block (its commit covers every earlier MMA); if
+  // that wait runs out, wait once more (bounded) so that the MMAs are done
+  // before the accumulator's TMEM is freed, and skip the epilogue
+  if (issued >= 0) {
+    const uint32_t lb = tc_smem_u32(&mbar[issued & 1]), lp = (uint32_t)((issued / TC_STAGES) & 1);
+    if (!tc_wait(lb, lp)) {
+      atomicExch(&abortFlag, 1);
+      tc_wait(lb, lp);
+    }
+  }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  __syncthreads();
+  ok = abortFlag == 0;
   if (!ok && tid == 0) atomicExch(errFlag, 1);
   // epilogue: warp w reads TMEM lanes 32w..32w+31 (tile rows), 64 columns in 4 loads of 16
   const int m = warp * 32 + lane;
   float* yr = yrow[m];
   const int64_t M = (int64_t)nrows * nrhs;
+  // every thread reads the same abortFlag after the barrier: the warps skip
+  // the (warp-collective) TMEM loads together
 #pragma unroll
   for (int cb = 0; cb < TC_BN / 16; cb++) {
+    if (!ok || issued < 0) break;
     uint32_t v[16];
     const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cb * 16);
     asm volatile(
@@ -230,7 +247,6 @@ __global__ void __launch_bounds__(TC_THREADS)
           "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
         : "r"(addr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-    if (!ok || issued < 0) continue;
     if (part) {
       if (r0 + m < M) {
         float* pr = part + ((int64_t)blockIdx.z * M + r0 + m) * N;
@@ -254,6 +270,41 @@ __global__ void __launch_bounds__(TC_THREADS)
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS));
+}
+
+// The error path of the bounded waits, on its own: one CTA allocates TMEM
+// like the GEMM, inits an mbarrier and waits for its first phase with a wait
+// limit of limitNs.  With arrive != 0 thread 0 arrives first and the wait
+// completes; otherwise nothing arrives (no MMA is ever issued), the wait runs
+// out, the kernel sets *errFlag, frees its TMEM and returns.
+__global__ void __launch_bounds__(TC_THREADS) k_wait_selftest(int arrive, long long limitNs, int* errFlag) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmemSlot;
+  __shared__ int abortFlag;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  if (tid == 0) {
+    abortFlag = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tc_smem_u32(&bar)), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc_smem_u32(&tmemSlot)),
+                 "r"(TC_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (arrive && tid == 0) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(tc_smem_u32(&bar))
+                 : "memory");
+  }
+  if (!tc_wait(tc_smem_u32(&bar), 0u, limitNs)) atomicExch(&abortFlag, 1);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (abortFlag && tid == 0) atomicExch(errFlag, 1);
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmemSlot), "r"(TC_TMEM_COLS));
 }
 
 // FP32 row GEMM launcher: the tensor-core kernel when useTC and the operands

@@ -1285,6 +1285,23 @@ static int pick_kb(int kc, int td) {
   return kb;
 }
 
+std::string dev_wait_selftest(int device, int arrive, long long limitNs, int* flag) {
+  *flag = 0;
+  FMMG_CK(cudaSetDevice(device));
+  int* d = nullptr;
+  FMMG_CK(cudaMalloc(&d, sizeof(int)));
+  cudaError_t e = cudaMemset(d, 0, sizeof(int));
+  if (e == cudaSuccess) {
+    k_wait_selftest<<<1, TC_THREADS>>>(arrive, limitNs, d);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(flag, d, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return std::string("wait self-test: ") + cudaGetErrorString(e);
+  return std::string();
+}
+
 std::string dev_evaluate_mixed(const Plan& P, DevState& D, const double* dDen, double* dVal, int k, int mask,
                                bool timed, LaunchStats* lsIn) {
   LaunchStats local;

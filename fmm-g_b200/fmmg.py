@@ -85,6 +85,7 @@ SIGNATURES = {
                        _dp], ctypes.c_int),
     "fmmg_tuning": ([ctypes.c_void_p, _ip, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "fmmg_device_error": ([ctypes.c_void_p, _ip], ctypes.c_int),
+    "fmmg_selftest_wait": ([ctypes.c_int, ctypes.c_int, ctypes.c_int64], ctypes.c_int),
     "fmmg_graph_state": ([ctypes.c_void_p, _ip, ctypes.POINTER(ctypes.c_char_p)], ctypes.c_int),
     "fmmg_tree": ([ctypes.c_void_p, _i32p, _i64p, _i64p], ctypes.c_int),
     "fmmg_lists": ([ctypes.c_void_p, ctypes.c_int, _i64p, _i32p, _i64p], ctypes.c_int),

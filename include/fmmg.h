@@ -40,7 +40,7 @@ typedef enum {
   FMMG_INVALID_ARG = 1,   /* bad option, size, pointer or non-finite input */
   FMMG_OOM = 2,           /* host or device allocation failed */
   FMMG_CUDA_ERROR = 3,    /* a CUDA call or kernel launch failed */
-  FMMG_TIMEOUT = 4,       /* reserved: a bounded device wait ran out */
+  FMMG_TIMEOUT = 4,       /* a bounded device wait ran out (results invalid) */
   FMMG_NOT_SUPPORTED = 5, /* kernel type / np / mode not built */
   FMMG_STATE = 6          /* call order violated (e.g. evaluate before setup) */
 } fmmg_status;
@@ -221,8 +221,18 @@ fmmg_status fmmg_graph_state(const fmmg_handle* h, int* active, const char** not
  * reference. */
 fmmg_status fmmg_set_gemm_path(fmmg_handle* h, int path);
 /* flag = 1 if a kernel gave up a bounded wait since the last call (its
- * results are then invalid), else 0; clears the flag.  Synchronises. */
+ * results are then invalid), else 0; clears the flag.  Synchronises.  The
+ * synchronising calls (fmmg_evaluate, fmmg_evaluate_host, fmmg_adjoint_host)
+ * read and clear the flag themselves and return FMMG_TIMEOUT when it was set. */
 fmmg_status fmmg_device_error(fmmg_handle* h, int* flag);
+/* The error path of the bounded device waits, for tests: one CTA allocates
+ * tensor memory, waits on an mbarrier with a limit of limit_ns nanoseconds
+ * (0 .. 2e9) and frees it.  arrive != 0: the mbarrier is arrived on first and
+ * the call returns FMMG_OK; arrive == 0: nothing arrives (no tensor-core work
+ * is ever issued), the wait runs out and the call returns FMMG_TIMEOUT with
+ * the device still usable.  Synchronises the device.  No counterpart in the
+ * reference. */
+fmmg_status fmmg_selftest_wait(int device, int arrive, int64_t limit_ns);
 
 /* Autotuner (no counterpart in the reference): times `reps` evaluates of
  * (k, precision) on the caller's device buffers for each candidate launch
@@ -293,12 +303,15 @@ fmmg_status fmmg_operator(fmmg_handle* h, int which, int idx, double* get, const
  * densities/values); d_nrm may be NULL for single-layer kernels.  The
  * accumulation scratch is a fixed array of 2^20 doubles inside the library on
  * every GPU that loads it (held until the process exits): n_trg * trgDOF above
- * 1,048,576 is rejected with FMMG_INVALID_ARG.  The first call on a device
- * resolves the scratch address for that device and should come before any
- * stream capture.  All calls on a device share the scratch: calls that overlap
- * on the GPU race.  Work is enqueued on `stream` (a cudaStream_t, NULL = the
- * default stream) and the call returns without synchronising.  Errors are
- * reported by the status code only. */
+ * 1,048,576 is rejected with FMMG_INVALID_ARG, and so are the Navier kernels
+ * with nu == 1 (as fmmg_create does); n_trg == 0 does nothing and returns
+ * FMMG_OK.  The first call on a device resolves the scratch address for that
+ * device and should come before any stream capture; the address is kept for
+ * the process, so the entry point must not be used across a cudaDeviceReset.
+ * All calls on a device share the scratch: calls that overlap on the GPU race.
+ * Work is enqueued on `stream` (a cudaStream_t, NULL = the default stream) and
+ * the call returns without synchronising.  Errors are reported by the status
+ * code only. */
 fmmg_status fmmg_dense_noalloc(int kernel_type, const double* coefs, int64_t n_src, const double* d_src,
                                const double* d_nrm, const double* d_den, int64_t n_trg, const double* d_trg,
                                double* d_val, void* stream);
