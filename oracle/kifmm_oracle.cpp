@@ -827,8 +827,17 @@ struct Oracle {
     for (size_t j = 0; j < bas.size() / 3; j++)
       for (int d = 0; d < 3; d++) pos[3 * j + d] = c[d] + r * bas[3 * j + d];
   }
-  static void dgemv_acc(long m, long n, const double* A, const double* x, double* y) {
-    for (long j = 0; j < n; j++) {  // reference BLAS column order
+  // gemvOrder: bit b set sums the columns of operator class b in reverse
+  // (b = 0 upward C2E, 1 M2M, 2 downward C2E, 3 L2L); clear bits keep the
+  // reference BLAS column order (j = 0 .. n-1).  Reversed is an equally valid
+  // summation order, used by the tests to measure how far two FP64
+  // evaluations of the same operators that only sum in another order drift
+  // apart (the pseudo-inverses amplify rounding).
+  int gemvOrder = 0;
+  void dgemv_acc(long m, long n, const double* A, const double* x, double* y, int cls) const {
+    const bool rev = (gemvOrder >> cls) & 1;
+    for (long jj = 0; jj < n; jj++) {
+      const long j = rev ? n - 1 - jj : jj;
       double t = x[j];
       const double* a = A + j * m;
       for (long i = 0; i < m; i++) y[i] += t * a[i];
@@ -838,7 +847,7 @@ struct Oracle {
   void upwChk2UpwEqu(int l, const double* chk, double* den) const {
     long m = (long)nUE * sdm, n = (long)nUC * tdm;
     std::vector<double> tmp(m, 0.0);
-    dgemv_acc(m, n, uc2ue.data(), chk, tmp.data());
+    dgemv_acc(m, n, uc2ue.data(), chk, tmp.data(), 0);
     for (int i = 0; i < nUE; i++)
       for (int s = 0; s < sdm; s++) den[i * sdm + s] += tmp[i * sdm + s] * std::pow(2.0, -l * deg[s]);
   }
@@ -848,13 +857,13 @@ struct Oracle {
     std::vector<double> tmp(n);
     for (int i = 0; i < nUE; i++)
       for (int s = 0; s < sdm; s++) tmp[i * sdm + s] = den[i * sdm + s] * std::pow(2.0, l * deg[s]);
-    dgemv_acc(m, n, ue2uc[o].data(), tmp.data(), chk);
+    dgemv_acc(m, n, ue2uc[o].data(), tmp.data(), chk, 1);
   }
   // :196-229
   void dwnChk2DwnEqu(int l, const double* chk, double* den) const {
     long m = (long)nDE * sdm, n = (long)nDC * tdm;
     std::vector<double> tmp(m, 0.0);
-    dgemv_acc(m, n, dc2de.data(), chk, tmp.data());
+    dgemv_acc(m, n, dc2de.data(), chk, tmp.data(), 2);
     for (int i = 0; i < nDE; i++)
       for (int s = 0; s < sdm; s++) den[i * sdm + s] += tmp[i * sdm + s] * std::pow(2.0, -l * deg[s]);
   }
@@ -864,7 +873,7 @@ struct Oracle {
     std::vector<double> tmp(n);
     for (int i = 0; i < nDE; i++)
       for (int s = 0; s < sdm; s++) tmp[i * sdm + s] = den[i * sdm + s] * std::pow(2.0, l * deg[s]);
-    dgemv_acc(m, n, de2dc[o].data(), tmp.data(), chk);
+    dgemv_acc(m, n, de2dc[o].data(), tmp.data(), chk, 3);
   }
   // :276-331
   void plnDen2EffDen(int l, const double* plnDen, cplx* effDen) const {
@@ -1111,6 +1120,33 @@ void orc_destroy(void* h) { delete (Oracle*)h; }
 int orc_setup(void* h, long ns, const double* src, const double* nrm, long nt, const double* trg) {
   Oracle* o = (Oracle*)h;
   o->setup(ns, src, nrm, nt, trg);
+  return 0;
+}
+
+// One V-list interaction at level l through the oracle's M2L helpers: UE
+// density den (|UE| srcDOF values) -> DC check values accumulated into val
+// (|DC| trgDOF values), translation id tid (0..315).
+int orc_m2l_single(void* h, int l, int tid, const double* den, double* val) {
+  Oracle* o = (Oracle*)h;
+  int idx[3] = {0, 0, 0};
+  bool found = false;
+  for (int t = 0; t < 343 && !found; t++)
+    if (o->trans_id[t / 49][(t / 7) % 7][t % 7] == tid) {
+      idx[0] = t / 49 - 3;
+      idx[1] = (t / 7) % 7 - 3;
+      idx[2] = t % 7 - 3;
+      found = true;
+    }
+  if (!found) return -1;
+  std::vector<cplx> effDen((long)o->nEff * o->sdm), effVal((long)o->nEff * o->tdm, cplx(0.0, 0.0));
+  o->plnDen2EffDen(l, den, effDen.data());
+  o->upwEqu2DwnChk(idx, effDen.data(), effVal.data());
+  o->effVal2PlnVal(effVal.data(), val);
+  return 0;
+}
+
+int orc_set_gemv_order(void* h, int order) {
+  ((Oracle*)h)->gemvOrder = order & 15;
   return 0;
 }
 

@@ -40,6 +40,8 @@ def lib():
         L.orc_destroy.argtypes = [ctypes.c_void_p]
         L.orc_setup.argtypes = [ctypes.c_void_p, ctypes.c_long, _dp, _dp, ctypes.c_long, _dp]
         L.orc_evaluate.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int]
+        L.orc_set_gemv_order.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_m2l_single.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp]
         L.orc_dense.argtypes = [ctypes.c_int, _dp, ctypes.c_long, _dp, _dp, _dp, ctypes.c_long, _dp,
                                 _dp, ctypes.c_int]
         L.orc_num_nodes.restype = ctypes.c_long
@@ -173,6 +175,24 @@ class Oracle:
         out = np.zeros(self.nt * self.td)
         lib().orc_evaluate(self.h, _d(den), _d(out), stages)
         return out
+
+    GEMV_UP_C2E, GEMV_M2M, GEMV_DN_C2E, GEMV_L2L = 1, 2, 4, 8
+
+    def m2l_single(self, level, tid, den):
+        """One V-list interaction at `level` through the oracle's M2L helpers
+        (embed and r2c, Hadamard with translation tid, c2r and gather): the DC
+        check values of the UE density den."""
+        den = _c(den).ravel()
+        s = self.sizes()
+        out = np.zeros(s["DC"] * trg_dof(mm_type(self.kt)))
+        assert lib().orc_m2l_single(self.h, level, tid, _d(den), _d(out)) == 0
+        return out
+
+    def set_gemv_order(self, reverse):
+        """Sum the columns of the selected operator GEMVs in reverse: a mask of
+        GEMV_UP_C2E, GEMV_M2M, GEMV_DN_C2E and GEMV_L2L (True = all of them);
+        0 / False keeps the reference BLAS order for all (the default)."""
+        lib().orc_set_gemv_order(self.h, 15 if reverse is True else int(reverse))
 
     def sizes(self):
         out = np.zeros(6, dtype=np.int32)

@@ -6,6 +6,8 @@ side's own tables the two pseudo-inverses come from different SVD codes and the
 bound is looser (tested separately).  Accuracy against the FP64 dense sum (the
 reference check(), fmm3d_mpi/fmm3d_check_mpi.cpp:122-165) is stated per case.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -26,7 +28,7 @@ def _case(kt, np_, n, kind="uniform", pts=40, seed=0, sep_targets=0):
     trg = rng.random((sep_targets, 3)) if sep_targets else src
     lib = fmmg.FMM3d(kt, np_=np_, pts_max=pts)
     lib.setup(src, nrm, trg)
-    orc = O.Oracle(kt, np_=np_, pts_max=pts)
+    orc = O.Oracle(kt, np_=np_, pts_max=pts, nthreads=os.cpu_count() or 1)
     orc.setup(src, nrm, trg)
     share_operators(lib, orc)
     den = rng.uniform(-1, 1, n * lib.sd)
@@ -41,24 +43,45 @@ def test_fp64_parity_all_kernels_np4(kt):
     assert rel_l2(g, c) <= PARITY
 
 
-def parity_tol(np_):
-    # The C2E pseudo-inverse keeps singular values down to 0.1^(np+1) of the
-    # largest (matmgnt3d_mpi.cpp:37-40), so two FP64 codes that sum in a
-    # different order agree to about eps_mach * 10^(np+1) at worst: within
-    # 1e-10 up to np = 7; at np = 8 (cutoff 1e-9) the bound is 1e-8.
-    return PARITY if np_ <= 7 else 1e-8
+def self_noise(orc, den, stages=O.STAGE_ALL):
+    """How far the oracle drifts from itself when every operator GEMV sums its
+    columns in reverse, an equally valid FP64 order.  The C2E pseudo-inverse
+    keeps singular values down to 0.1^(np+1) of the largest
+    (matmgnt3d_mpi.cpp:37-40) and amplifies any reordering upstream of it, so
+    this floor grows tenfold per np: ~1e-11 at np=6, ~1e-10 at np=7, ~1e-9 at
+    np=8.  No FP64 code that does not repeat the reference's exact operation
+    order can agree with it more closely than this."""
+    a = orc.evaluate(den, stages=stages)
+    orc.set_gemv_order(True)
+    b = orc.evaluate(den, stages=stages)
+    orc.set_gemv_order(False)
+    return rel_l2(b, a) if np.linalg.norm(a) > 0 else 0.0
 
 
-@pytest.mark.parametrize("kt,np_", [(111, 6), (111, 8), (121, 6), (321, 6), (511, 6), (312, 5), (111, 3), (111, 7)])
+def parity_gate(orc, den, stages=O.STAGE_ALL):
+    """1e-10, or twice the oracle's own reordering floor where that is larger
+    (np >= 7)."""
+    return max(PARITY, 2.0 * self_noise(orc, den, stages))
+
+
+@pytest.mark.parametrize("kt,np_", [(111, 6), (111, 8), (121, 6), (321, 6), (511, 6), (312, 5), (111, 3), (111, 7),
+                                    (321, 7), (511, 8)])
 def test_fp64_parity_np(kt, np_):
     lib, orc, *_, den = _case(kt, np_, 5000, "uniform", pts=40, seed=np_)
     g = gpu_eval(lib, den)
     c = orc.evaluate(den)
-    assert rel_l2(g, c) <= parity_tol(np_)
+    gate = parity_gate(orc, den)
+    print("kt=%d np=%d rel_l2=%.3e gate=%.3e" % (kt, np_, rel_l2(g, c), gate))
+    assert rel_l2(g, c) <= gate
+    if np_ <= 6:
+        assert gate == PARITY
 
 
-@pytest.mark.parametrize("stages", [O.STAGE_U, O.STAGE_W | O.STAGE_UP, O.STAGE_X, O.STAGE_X | O.STAGE_DOWN,
-                                    O.STAGE_UP | O.STAGE_V | O.STAGE_DOWN, O.STAGE_UP | O.STAGE_DOWN])
+STAGE_MASKS = [O.STAGE_U, O.STAGE_W | O.STAGE_UP, O.STAGE_X, O.STAGE_X | O.STAGE_DOWN,
+               O.STAGE_UP | O.STAGE_V | O.STAGE_DOWN, O.STAGE_UP | O.STAGE_DOWN, O.STAGE_ALL]
+
+
+@pytest.mark.parametrize("stages", STAGE_MASKS)
 def test_stage_parity(stages):
     lib, orc, *_, den = _case(111, 4, 8000, "sphere_clusters", pts=20, seed=3)
     g = gpu_eval(lib, den, stages)
@@ -67,6 +90,67 @@ def test_stage_parity(stages):
         assert np.linalg.norm(g) == 0
     else:
         assert rel_l2(g, c) <= PARITY
+
+
+@pytest.mark.parametrize("np_", [7, 8])
+@pytest.mark.parametrize("stages", STAGE_MASKS)
+def test_stage_parity_high_np(np_, stages):
+    """Each stage alone at np = 7 and 8 on an adaptive tree (W and X lists
+    present): the stages without a pseudo-inverse (U list, S2T/M2T, X direct)
+    agree to FP64 rounding; the ones through C2E agree within twice the
+    oracle's own reordering floor, which is what carries the np=8 difference."""
+    lib, orc, *_, den = _case(111, np_, 12000, "sphere_clusters", pts=30, seed=20 + np_)
+    g = gpu_eval(lib, den, stages)
+    c = orc.evaluate(den, stages=stages)
+    if np.linalg.norm(c) == 0:
+        assert np.linalg.norm(g) == 0
+        return
+    err = rel_l2(g, c)
+    gate = parity_gate(orc, den, stages)
+    print("np=%d stages=%d rel_l2=%.3e self_noise=%.3e" % (np_, stages, err, gate / 2))
+    assert err <= gate
+    if stages in (O.STAGE_U, O.STAGE_X):  # no operator GEMV on the path
+        assert err <= 1e-13
+
+
+@pytest.mark.parametrize("kt,np_", [(111, 6), (321, 5), (511, 4)])
+def test_fp64_parity_on_reference_built_tables(kt, np_):
+    """The GPU path run on the operator tables that the reference's own
+    MatMgnt3d_MPI builds (compiled from its sources, LAPACK pseudo-inverses;
+    oracle/ref_code.py), against the oracle on the same tables."""
+    import ref_code as R
+    if not R.available():
+        pytest.skip("the reference's code is not built here")
+    mm = {111: 111, 321: 301, 511: 511}[kt]
+    lib, orc, *_, den = _case(kt, np_, 6000, "sphere_clusters", pts=30, seed=40 + np_)
+    for which, idxs in ((0, [0]), (1, range(8)), (2, [0]), (3, range(8)), (4, range(316))):
+        for i in idxs:
+            t = R.operator(mm, np_, which, i)
+            lib.set_operator(which, i, t)
+            orc.set_operator(which, i, t)
+    g = gpu_eval(lib, den)
+    c = orc.evaluate(den)
+    assert rel_l2(g, c) <= PARITY
+
+
+def test_headline_1m_fp64_parity():
+    """The benchmark workload itself: 1,048,576 points (half on a sphere, half
+    in 8 Gaussian clusters), Laplace single layer, np=6, ptsMax=64.  The FP64
+    GPU evaluate against the oracle on the same tree and operators, the oracle
+    on every host thread."""
+    import workloads as W
+    cfg = W.config2(1 << 20)
+    src, den = cfg["src"], cfg["den"]
+    lib = fmmg.FMM3d(111, np_=6, pts_max=64)
+    lib.setup(src)
+    orc = O.Oracle(111, np_=6, pts_max=64, nthreads=os.cpu_count() or 1)
+    orc.setup(src, src, src)
+    share_operators(lib, orc)
+    g = gpu_eval(lib, den)
+    c = orc.evaluate(den)
+    err = rel_l2(g, c)
+    print("1M headline: rel_l2(gpu fp64 vs oracle) = %.3e" % err)
+    assert err <= PARITY
 
 
 def test_config1_laplace_65536_np4():

@@ -205,3 +205,32 @@ def test_separate_targets_binned_into_source_tree():
     val = o.evaluate(den)
     ref = O.dense(111, src, src, den, trg)
     assert np.linalg.norm(val - ref) / np.linalg.norm(ref) < 1e-3
+
+
+@pytest.mark.parametrize("np_", [6, 8])
+def test_reordering_floor_of_the_reference_arithmetic(np_):
+    """The FP64 evaluate() of the reference sums every operator GEMV in BLAS
+    column order.  Summing the columns of any one operator class in reverse
+    (an equally valid order) moves the result by the reordering floor that the
+    GPU/oracle parity gate allows for: rounding upstream of a C2E
+    pseudo-inverse (cutoff 0.1^(np+1), matmgnt3d_mpi.cpp:37-40) is amplified,
+    ~1e-11 at np=6 and ~1e-9 at np=8, from M2M and L2L as much as from the
+    pseudo-inverses themselves."""
+    rng = np.random.default_rng(20261203 + np_)
+    n = 5000
+    src = rng.random((n, 3))
+    den = rng.uniform(-1, 1, n)
+    o = O.Oracle(111, np_=np_, pts_max=40, nthreads=8)
+    o.setup(src, src, src)
+    a = o.evaluate(den)
+    floors = {}
+    for mask in (O.Oracle.GEMV_UP_C2E, O.Oracle.GEMV_M2M, O.Oracle.GEMV_DN_C2E, O.Oracle.GEMV_L2L, True):
+        o.set_gemv_order(mask)
+        floors[mask] = np.linalg.norm(o.evaluate(den) - a) / np.linalg.norm(a)
+    o.set_gemv_order(False)
+    assert np.array_equal(o.evaluate(den), a)  # the reference order again, bit for bit
+    if np_ <= 6:
+        assert max(floors.values()) < 1e-10
+    else:
+        assert min(floors.values()) > 1e-10  # every class alone reaches it
+        assert max(floors.values()) < 1e-8
