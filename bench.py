@@ -15,8 +15,8 @@ evaluates its own right-hand side (multi-RHS sharding, weak scaling, no
 collective on the data path); the step time is the max over ranks.
 
 --impl reference: the CPU restatement of the reference evaluate() (oracle/),
-timed on the host cores with all threads, on a bounded sample of the same
-workload.
+timed on the host cores with all threads, on the same 1,048,576-point workload
+(one evaluate per step, tree and operators prebuilt).
 """
 import argparse
 import json
@@ -37,8 +37,6 @@ METRIC = json.load(open(os.path.join(ROOT, "BASELINE.json")))["metric"] if os.pa
     os.path.join(ROOT, "BASELINE.json")) else "Laplace 1M-pt points/s"
 UNIT = "points/s"
 WORKLOAD = "laplace_s_1M_sphere_clusters_np6_ptsmax64"
-CPU_SAMPLE = 1 << 17      # single-thread oracle sample (about 10-30 s on one core)
-REF_SAMPLE = 1 << 18      # all-threads oracle sample per reference-arm step
 CHECK_TARGETS = 4096
 
 
@@ -119,12 +117,12 @@ class ClockSampler:
 
 
 def oracle_rate(n, nthreads, reps=1):
-    """Oracle (CPU restatement of the reference evaluate) points/s on an n-point sample."""
+    """Oracle (CPU restatement of the reference evaluate) points/s on the
+    n-point benchmark workload."""
     import oracle as O
     import workloads as W
-    rng = np.random.default_rng(W.SEED + 2)
-    src = W.sphere_clusters(n, rng)
-    den = rng.normal(size=n)
+    cfg = W.config2(n)
+    src, den = cfg["src"], cfg["den"]
     o = O.Oracle(111, np_=6, pts_max=64, nthreads=nthreads)
     o.setup(src, src, src)
     times = []
@@ -142,10 +140,9 @@ def run_reference(args):
     nthreads = os.cpu_count() or 1
     import oracle as O
     import workloads as W
-    rng = np.random.default_rng(W.SEED + 2)
-    n = min(args.n, REF_SAMPLE)
-    src = W.sphere_clusters(n, rng)
-    den = rng.normal(size=n)
+    cfg = W.config2(args.n)  # the benchmark workload itself, full size
+    n = args.n
+    src, den = cfg["src"], cfg["den"]
     o = O.Oracle(111, np_=6, pts_max=64, nthreads=nthreads)
     o.setup(src, src, src)
     for _ in range(args.warmup):
@@ -155,13 +152,13 @@ def run_reference(args):
         o.evaluate(den)
     dt = (time.perf_counter() - t0) / max(args.steps, 1)
     v = n / dt
-    sample = "%d-point sample of the workload's distribution per step, tree and operators prebuilt" % n
+    sample = "the full %d-point workload, one evaluate per step, tree and operators prebuilt" % n
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "points": args.n, "sample_points": n, "kernel": "laplace_s_u", "np": 6,
-                   "pts_max": 64, "k_rhs": 1},
+        "config": {"workload": WORKLOAD, "points": n, "kernel": "laplace_s_u", "np": 6, "pts_max": 64,
+                   "k_rhs_per_gpu": 1, "precision": "fp64", "parallelism": "host threads x%d" % nthreads},
         "cpu_baseline": dict({"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
                              **host_cpu()),
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -394,10 +391,11 @@ def run_ours(args):
             print("setup again failed: %s" % e, file=sys.stderr)
         cpu = None
         if not args.no_cpu_baseline and not dist:
-            rate, times = oracle_rate(CPU_SAMPLE, 1)
-            cpu = dict({"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
-                        "sample": "%d-point sample of the workload distribution, 1 thread (one MPI rank), "
-                                  "tree/operators prebuilt, %.1f s" % (CPU_SAMPLE, times[0])}, **host_cpu())
+            nthr = os.cpu_count() or 1
+            rate, times = oracle_rate(n, nthr)
+            cpu = dict({"value": rate, "unit": UNIT, "cores": nthr, "kind": "port",
+                        "sample": "the full %d-point workload, one evaluate on %d host threads (one MPI rank, "
+                                  "OpenMP), tree/operators prebuilt, %.1f s" % (n, nthr, times[0])}, **host_cpu())
         line = {
             "metric": METRIC, "value": head["points_per_s"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
