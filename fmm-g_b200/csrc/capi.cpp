@@ -473,18 +473,23 @@ fmmg_status fmmg_tuning(fmmg_handle* h, int* vals, int n, int set) {
   if (!h || !vals || n < 3) return fail(h, FMMG_INVALID_ARG, "need 3 values");
   fmmg::DevState::Tune& T = h->dev.tune;
   if (set) {
-    if (vals[0] < 1 || vals[1] < 1 || vals[2] < 0 || (n >= 4 && vals[3] != 1 && vals[3] != 2))
+    if (vals[0] < 1 || vals[1] < 1 || vals[2] < 0 || (n >= 4 && vals[3] != 1 && vals[3] != 2) ||
+        (n >= 5 && (vals[4] < 0 || vals[4] > 63)) || (n >= 6 && vals[5] != 3 && vals[5] != 4))
       return fail(h, FMMG_INVALID_ARG, "tuning values");
     T.hadRows = vals[0];
     T.pqParents = vals[1];
     T.gemmSplitMul = vals[2];
     if (n >= 4) T.hadRhsPerThread = vals[3];
+    if (n >= 5) T.tcMask = vals[4];
+    if (n >= 6) T.tcProducts = vals[5];
     drop_graph(h);
   } else {
     vals[0] = T.hadRows;
     vals[1] = T.pqParents;
     vals[2] = T.gemmSplitMul;
     if (n >= 4) vals[3] = T.hadRhsPerThread;
+    if (n >= 5) vals[4] = T.tcMask;
+    if (n >= 6) vals[5] = T.tcProducts;
   }
   return FMMG_OK;
 }

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "plan.hpp"
+#include "tc_op.hpp"
 
 namespace fmmg {
 
@@ -96,12 +97,17 @@ struct DevState {
   // fewer than gemmSplitMul CTAs per SM (0: never split)
   // fmmg_autotune (defaults otherwise), and the right-hand sides per thread
   // of the FP32 27-product Hadamard (1 or 2)
+  // tcMask: which FP32 GEMM classes the tensor-core path takes (bit 0 leaf
+  // C2E F1, 1 leaf C2E F2, 2 folded C2E x M2M, 3 L2L, 4 downward C2E F1,
+  // 5 downward C2E F2); tcProducts: 3 (hi*hi + hi*lo + lo*hi) or 4 (+ lo*lo)
   struct Tune {
-    int hadRows = 64, pqParents = 128, gemmSplitMul = 2, hadRhsPerThread = 1;
+    int hadRows = 64, pqParents = 128, gemmSplitMul = 2, hadRhsPerThread = 1, tcMask = 63, tcProducts = 3;
   } tune;
-  // FP32 row GEMMs: 0 wide-tile CUDA-core kernel (default), 1 M2M/L2L on the
-  // tensor cores (3xTF32, opt-in), 2 the 128 x 64 CUDA-core kernel
+  // FP32 row GEMMs: 0 wide-tile CUDA-core kernel (default), 1 on the tensor
+  // cores (3xTF32), 2 the 128 x 64 CUDA-core kernel
   int gemmPath = 0;
+  // the same operators split and laid out for the tensor-core kernel
+  TcOp cL2L, cUpF1, cUpF2, cDnF1, cDnF2, cM2MUp;
   // FP32 operators transposed and zero padded for the wide-tile GEMM,
   // Wt[k][n]: K to a multiple of 16, N to a multiple of 160 (ld)
   struct OpT {

@@ -942,6 +942,14 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
     const std::vector<double>& fold = P.folded_upward();
     FMMG_TRY(put(D.m2mUp32, fold));
     FMMG_TRY(putT(D.tM2MUp, fold, (int)ue, (int)(8 * ue)));
+    // the same six operators split into TF32 hi / lo parts for the tensor cores
+    auto tcAlloc = [&](float*& p, size_t n) { return dalloc(D, p, n); };
+    FMMG_TRY(tc_prepare_operator(D.cL2L, P.l2l, (int)(8 * dc), (int)de, tcAlloc));
+    FMMG_TRY(tc_prepare_operator(D.cUpF1, pad_rows(P.uc2ueF1, P.kUp, (int)uc), kUp4, (int)uc, tcAlloc));
+    FMMG_TRY(tc_prepare_operator(D.cUpF2, pad_cols(P.uc2ueF2, (int)ue, P.kUp), (int)ue, kUp4, tcAlloc));
+    FMMG_TRY(tc_prepare_operator(D.cDnF1, pad_rows(P.dc2deF1, P.kDn, (int)dc), kDn4, (int)dc, tcAlloc));
+    FMMG_TRY(tc_prepare_operator(D.cDnF2, pad_cols(P.dc2deF2, (int)de, P.kDn), (int)de, kDn4, tcAlloc));
+    FMMG_TRY(tc_prepare_operator(D.cM2MUp, fold, (int)ue, (int)(8 * ue), tcAlloc));
     std::vector<float2> t(P.m2lT32.size());
     for (size_t i = 0; i < t.size(); i++) t[i] = make_float2((float)P.m2lT32[i].real(), (float)P.m2lT32[i].imag());
     FMMG_CK(cudaMemcpy(D.m2lT32, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice));
@@ -999,13 +1007,17 @@ static void run_mixed_blocks(const Plan& P, DevState& D, int kc, int mask, bool 
   const int nl = (int)P.evtrLeaves.size();
   const int kb = (kc + KB - 1) / KB;
   const int64_t denStride = P.ns * P.sd, valStride = std::max<int64_t>(P.nt, 1) * P.td;
-  // tc: the product may run on the tensor cores (3xTF32) when that path is
-  // enabled.  The factored C2E products always stay on the CUDA cores: the 1/s
-  // factor of the pseudo-inverse amplifies the tensor core's accumulation
-  // rounding past the 1e-5 budget.
+  // tc: the operator split for the tensor cores (3xTF32), used when that
+  // path is on and the class is in the tuning mask (the wide CUDA-core tiles
+  // otherwise)
+  auto useTc = [&](const TcOp& tc) {
+    const int cls = &tc == &D.cUpF1 ? 0 : &tc == &D.cUpF2 ? 1 : &tc == &D.cM2MUp ? 2 : &tc == &D.cL2L ? 3
+                    : &tc == &D.cDnF1 ? 4 : 5;
+    return D.gemmPath == 1 && ((D.tune.tcMask >> cls) & 1);
+  };
   auto gemm = [&](int nrows, const int32_t* rows, int xChild, int yChild, const float* X, int64_t ldx, int64_t xR,
                   const float* W, const DevState::OpT& wt, float* Y, int64_t ldy, int64_t yR, int K, int N, Scale4 xs,
-                  Scale4 ys, float beta, bool tc) {
+                  Scale4 ys, float beta, const TcOp& tc) {
     if (nrows <= 0) return;
     GrScale<float> gx, gy;
     gx.mod = xs.mod;
@@ -1015,7 +1027,8 @@ static void run_mixed_blocks(const Plan& P, DevState& D, int kc, int mask, bool 
       gy.v[k] = (float)ys.v[k];
     }
     ls->launches += launch_gemm_rows_f32(st, D.numSMs * D.tune.gemmSplitMul, reinterpret_cast<float*>(D.gemmScratch),
-                                         D.gemmScratchBytes / sizeof(float), D.gemmPath == 1 && tc, D.devErr, nrows,
+                                         D.gemmScratchBytes / sizeof(float), useTc(tc) ? &tc : nullptr,
+                                         D.tune.tcProducts, D.devErr, nrows,
                                          kc, rows, D.chd, xChild, yChild, X, ldx, xR, W,
                                          D.gemmPath == 2 ? nullptr : wt.p, wt.ld, Y, ldy, yR, K, N, gx, gy, beta);
   };
@@ -1037,9 +1050,9 @@ static void run_mixed_blocks(const Plan& P, DevState& D, int kc, int mask, bool 
       // never multiplies in FP32
       int64_t a = D.offUpLeaf[d], b = D.offUpLeaf[d + 1];
       gemm((int)(b - a), D.levelRows + a, 0, 0, D.uchk32, uc, nn * uc, D.upF1, D.tUpF1, D.upT32, kUp4, nn * kUp4, uc,
-           kUp4, unit_scale(), unit_scale(), 0.f, false);
+           kUp4, unit_scale(), unit_scale(), 0.f, D.cUpF1);
       gemm((int)(b - a), D.levelRows + a, 0, 0, D.upT32, kUp4, nn * kUp4, D.upF2, D.tUpF2, D.uden32, ue, nn * ue, kUp4,
-           ue, unit_scale(), level_scale(P, d + rl, -1.0), 0.f, false);
+           ue, unit_scale(), level_scale(P, d + rl, -1.0), 0.f, D.cUpF2);
       // parents: C2E up x M2M folded on the host in FP64 (its norm is O(1)
       // where the pinv's is ~1e6), one product from the children's upward
       // densities (depth d + 1, done in the previous iteration) with no check
@@ -1047,7 +1060,7 @@ static void run_mixed_blocks(const Plan& P, DevState& D, int kc, int mask, bool 
       a = D.offUpM2M[d];
       b = D.offUpM2M[d + 1];
       gemm((int)(b - a), D.levelRows + a, 1, 0, D.uden32, ue, nn * ue, D.m2mUp32, D.tM2MUp, D.uden32, ue, nn * ue,
-           8 * ue, ue, level_scale(P, d + 1 + rl, +1.0), level_scale(P, d + rl, -1.0), 0.f, true);
+           8 * ue, ue, level_scale(P, d + 1 + rl, +1.0), level_scale(P, d + rl, -1.0), 0.f, D.cM2MUp);
     }
   }
   cudaEventRecord(D.ev[EV_UP_GEMM], st);
@@ -1235,13 +1248,13 @@ static void run_mixed_blocks(const Plan& P, DevState& D, int kc, int mask, bool 
       if (d >= 3) {
         int64_t a = D.offDnL2L[d - 1], b = D.offDnL2L[d];
         gemm((int)(b - a), D.levelRows + a, 0, 1, D.dden32, de, nn * de, D.l2l32, D.tL2L, D.dchk32, dc, nn * dc, de, 8 * dc,
-             level_scale(P, d - 1 + rl, +1.0), unit_scale(), 1.f, true);
+             level_scale(P, d - 1 + rl, +1.0), unit_scale(), 1.f, D.cL2L);
       }
       int64_t a = D.offDnC2E[d], b = D.offDnC2E[d + 1];
       gemm((int)(b - a), D.levelRows + a, 0, 0, D.dchk32, dc, nn * dc, D.dnF1, D.tDnF1, D.dnT32, kDn4, nn * kDn4, dc,
-           kDn4, unit_scale(), unit_scale(), 0.f, false);
+           kDn4, unit_scale(), unit_scale(), 0.f, D.cDnF1);
       gemm((int)(b - a), D.levelRows + a, 0, 0, D.dnT32, kDn4, nn * kDn4, D.dnF2, D.tDnF2, D.dden32, de, nn * de, kDn4,
-           de, unit_scale(), level_scale(P, d + rl, -1.0), 0.f, false);
+           de, unit_scale(), level_scale(P, d + rl, -1.0), 0.f, D.cDnF2);
     }
   }
   cudaEventRecord(D.ev[EV_DN_GEMM], st);

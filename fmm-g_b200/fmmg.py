@@ -347,7 +347,8 @@ class FMM3d:
 
     def tuning(self, values=None):
         """Current launch shapes, or install `values` (a dict as returned)."""
-        keys = ("had_rows_fp32", "had_rows_fp64", "gemm_split_ctas_per_sm", "had_fp32_rhs_per_thread")
+        keys = ("had_rows_fp32", "had_rows_fp64", "gemm_split_ctas_per_sm", "had_fp32_rhs_per_thread",
+                "tc_gemm_mask", "tc_products")
         v = (ctypes.c_int * len(keys))()
         if values is not None:
             self._chk(lib().fmmg_tuning(self.h, v, len(keys), 0))
