@@ -103,9 +103,9 @@ struct DevState {
   struct Tune {
     int hadRows = 64, pqParents = 128, gemmSplitMul = 2, hadRhsPerThread = 1, tcMask = 63, tcProducts = 3;
   } tune;
-  // FP32 row GEMMs: 0 wide-tile CUDA-core kernel (default), 1 on the tensor
-  // cores (3xTF32), 2 the 128 x 64 CUDA-core kernel
-  int gemmPath = 0;
+  // FP32 row GEMMs: 1 on the tensor cores (3xTF32, default), 0 the wide-tile
+  // CUDA-core kernel, 2 the 128 x 64 CUDA-core kernel
+  int gemmPath = 1;
   // the same operators split and laid out for the tensor-core kernel
   TcOp cL2L, cUpF1, cUpF2, cDnF1, cDnF2, cM2MUp;
   // FP32 operators transposed and zero padded for the wide-tile GEMM,

@@ -18,16 +18,18 @@
 // 1M-point workload it moved the evaluate from 1.7e-6 to 1.5e-5 against the
 // dense sum, per block it stays at 2.6e-6).
 //
-// Warp roles (256 threads, two warps per scheduler so that a thread may hold
-// the 160 sums): warps 0-3 stage the gathered X rows (128 rows x 32 K values
-// per block as 16-byte loads, three blocks in flight, split and stored K-major
-// with the 128-byte swizzle); warps 4-7 drain each block's accumulator (warp w
-// reads TMEM lanes 32 (w % 4) ..) into FP32 register sums and run the
-// epilogue; lane 0 of warp 4 also loads the pre-split operator tiles (BN rows
-// x 32 K, hi and lo) by TMA (cp.async.bulk.tensor, this GPU's own memory, no
-// multicast) and issues per K block 4 K steps x 3 products of tcgen05.mma
-// M = 128, N = BN, K = 8 into one of three TMEM accumulators: the tensor core
-// runs up to two blocks ahead of the drain.  Three smem stages.
+// Warp roles (416 threads): warps 0-3 stage the gathered X rows (128 rows x
+// 32 K values per block as 16-byte loads, two blocks in flight, split and
+// stored K-major with the 128-byte swizzle); warps 4-11 drain each block's
+// accumulator into FP32 register sums (warp w reads TMEM lanes 32 (w % 4) ..,
+// half the columns each) and run the epilogue; lane 0 of warp 12 loads the
+// pre-split operator tiles (BN rows x 32 K, hi and lo) by TMA
+// (cp.async.bulk.tensor, this GPU's own memory, no multicast) and issues per
+// K block 4 K steps x 3 products of tcgen05.mma M = 128, N = BN, K = 8 into
+// one of three TMEM accumulators, so the tensor core runs up to two blocks
+// ahead of the drain.  Issuing a block's MMAs occupies the lane for about the
+// tensor core's time on it, so that lane does nothing else.  Three smem
+// stages.
 //
 // Every mbarrier wait is bounded (TC_WAIT_NS): a wait that runs out sets the
 // CTA's abort flag and the kernel's error flag, nobody writes a stage the
@@ -55,8 +57,8 @@ constexpr int TC_THREADS = 128;                 // the wait self-test's CTA
 constexpr uint32_t TC_TMEM_COLS = 64;           // the wait self-test's TMEM
 constexpr long long TC_WAIT_NS = 1000000000ll;  // a bounded mbarrier wait gives up after 1 s
 
-constexpr int T3_BM = 128, T3_BK = 32, T3_STAGES = 3, T3_AWARPS = 4;
-constexpr int T3_DWARP0 = T3_AWARPS, T3_MWARP = T3_AWARPS, T3_THREADS = 32 * (2 * T3_AWARPS);
+constexpr int T3_BM = 128, T3_BK = 32, T3_STAGES = 3, T3_AWARPS = 4, T3_DWARPS = 8;
+constexpr int T3_DWARP0 = T3_AWARPS, T3_MWARP = T3_AWARPS + T3_DWARPS, T3_THREADS = 32 * (T3_MWARP + 1);
 constexpr int T3_NACC = 3;  // block accumulators in TMEM: the tensor core runs up to two blocks ahead of the drain
 constexpr int T3_A_BYTES = T3_BM * T3_BK * 4;  // 16 KB per A part (hi or lo)
 
@@ -115,10 +117,10 @@ __device__ __forceinline__ void tc_arrive(uint32_t bar) {
   asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(bar) : "memory");
 }
 
+// round to nearest TF32, ties away from zero (the rounding of
+// cvt.rna.tf32.f32), with two integer operations on the magnitude bits
 __device__ __forceinline__ float tc_rna(float x) {
-  uint32_t h;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
-  return __uint_as_float(h);
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xffffe000u);
 }
 
 // v = hi + lo with both parts TF32 numbers rounded to nearest
@@ -139,6 +141,7 @@ __global__ void __launch_bounds__(T3_THREADS, 1)
                int* __restrict__ errFlag) {
   using C = T3Cfg<BN>;
   static_assert(T3_NACC * BN <= 512 && BN % 32 == 0, "the block accumulators fit 512 TMEM columns");
+  static_assert(T3_DWARPS == 8, "two drain warps per TMEM lane group, half the columns each");
   extern __shared__ unsigned char t3_smem_raw[];
   __shared__ const float* xrow[T3_BM];
   __shared__ float* yrow[T3_BM];
@@ -174,7 +177,7 @@ __global__ void __launch_bounds__(T3_THREADS, 1)
     }
     for (int b = 0; b < T3_NACC; b++) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tc_smem_u32(&accFull[b])), "r"(1));
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tc_smem_u32(&accEmpty[b])), "r"(T3_AWARPS * 32));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tc_smem_u32(&accEmpty[b])), "r"(T3_DWARPS * 32));
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -191,11 +194,11 @@ __global__ void __launch_bounds__(T3_THREADS, 1)
   const uint32_t tmem = tmemSlot;
   const int kBeg = blockIdx.z * kChunk, kEnd = min(K, kBeg + kChunk);
   const int nKB = (kEnd - kBeg + T3_BK - 1) / T3_BK;
-  float R[BN];  // drain warps: the row's FP32 sums of the block accumulators
+  float R[BN / 2];  // drain warps: FP32 sums of half the row's columns
 
-  if (warp >= T3_DWARP0) {
-    // ------------------------------------------- drain (+ TMA and MMA, warp 4 lane 0)
-    const bool mma = warp == T3_MWARP && lane == 0;
+  if (warp == T3_MWARP) {
+    // ------------------------------------------------- TMA + MMA (one lane)
+    const bool mma = lane == 0;
     const uint64_t tmAddr = reinterpret_cast<uint64_t>(&tmW);
     auto loadB = [&](int kb) {  // operator block kb into stage kb % S (hi rows n0.., lo rows nPad + n0..)
       const int s = kb % T3_STAGES;
@@ -262,7 +265,15 @@ __global__ void __launch_bounds__(T3_THREADS, 1)
       }
       return true;
     };
-    // block kb's accumulator into R; false once the CTA aborts
+    if (mma) {
+      for (int kb = 0; kb < nKB && kb < T3_STAGES; kb++) loadB(kb);
+      for (int kb = 0; kb < nKB; kb++)
+        if (!issue(kb)) break;
+    }
+  } else if (warp >= T3_DWARP0) {
+    // ------------------------------------------------------------- drain
+    // block kb's accumulator columns [half * BN/2, +BN/2) into R; false once the CTA aborts
+    const int half = (warp - T3_DWARP0) / 4;
     const uint32_t lanes = (uint32_t)((warp % 4) * 32) << 16;
     auto ld16 = [&](uint32_t addr, uint32_t(&v)[16]) {
       asm volatile(
@@ -276,41 +287,27 @@ __global__ void __launch_bounds__(T3_THREADS, 1)
       if (!tc_wait(tc_smem_u32(&accFull[b]), (uint32_t)((kb / T3_NACC) & 1))) atomicExch(&abortFlag, 1);
       if (__any_sync(0xffffffffu, *(volatile int*)&abortFlag != 0)) return false;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      static_assert((BN / 16) % 2 == 0, "columns drained two loads of 16 at a time");
 #pragma unroll
-      for (int cb = 0; cb < BN / 16; cb += 2) {  // two loads in flight per wait
-        uint32_t v0[16], v1[16];
-        const uint32_t addr = tmem + lanes + (uint32_t)(b * BN + cb * 16);
-        ld16(addr, v0);
-        ld16(addr + 16, v1);
+      for (int cb = 0; cb < BN / 32; cb++) {
+        uint32_t v[16];
+        ld16(tmem + lanes + (uint32_t)(b * BN + half * (BN / 2) + cb * 16), v);
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int j = 0; j < 16; j++) {
-          R[cb * 16 + j] += __uint_as_float(v0[j]);
-          R[cb * 16 + 16 + j] += __uint_as_float(v1[j]);
-        }
+        for (int j = 0; j < 16; j++) R[cb * 16 + j] += __uint_as_float(v[j]);
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       tc_arrive(tc_smem_u32(&accEmpty[b]));
       return true;
     };
 #pragma unroll
-    for (int j = 0; j < BN; j++) R[j] = 0.f;
-    if (mma)
-      for (int kb = 0; kb < nKB && kb < T3_STAGES; kb++) loadB(kb);
-    bool going = true;
-    for (int kb = 0; kb < nKB + T3_NACC - 1 && going; kb++) {
-      if (mma && kb < nKB && !issue(kb)) going = false;  // block kb to the tensor core ...
-      __syncwarp();
-      going = __all_sync(0xffffffffu, going);
-      const int kd = kb - (T3_NACC - 1);
-      if (going && kd >= 0) going = drain(kd);  // ... while the warps drain block kb - 2
-    }
+    for (int j = 0; j < BN / 2; j++) R[j] = 0.f;
+    for (int kb = 0; kb < nKB; kb++)
+      if (!drain(kb)) break;
   } else {
     // ---------------------------------------------------------- X rows (A)
     const bool xsUni = xs.mod == 1;
     const float xs0 = xs.v[0];
-    float4 ra[3][8];  // three K blocks in flight
+    float4 ra[2][8];  // two K blocks in flight
     auto fetch = [&](float4(&dst)[8], int kb) {
       const int k0 = kBeg + kb * T3_BK;
 #pragma unroll
@@ -333,8 +330,10 @@ __global__ void __launch_bounds__(T3_THREADS, 1)
       for (int i = 0; i < 8; i++) {
         const int idx = tid + i * T3_AWARPS * 32, r = idx >> 3, c = idx & 7;
         float v[4] = {src[i].x, src[i].y, src[i].z, src[i].w};
+        if (!xsUni || xs0 != 1.f) {
 #pragma unroll
-        for (int j = 0; j < 4; j++) v[j] *= xsUni ? xs0 : gr_sel(xs, k0 + 4 * c + j);
+          for (int j = 0; j < 4; j++) v[j] *= xsUni ? xs0 : gr_sel(xs, k0 + 4 * c + j);
+        }
         float4 h, l;
         tc_split(v[0], h.x, l.x);
         tc_split(v[1], h.y, l.y);
@@ -349,16 +348,12 @@ __global__ void __launch_bounds__(T3_THREADS, 1)
     };
     if (nKB > 0) fetch(ra[0], 0);
     if (nKB > 1) fetch(ra[1], 1);
-    if (nKB > 2) fetch(ra[2], 2);
-    for (int kb = 0; kb < nKB; kb += 3) {
+    for (int kb = 0; kb < nKB; kb += 2) {
       if (!stage(ra[0], kb)) break;
-      if (kb + 3 < nKB) fetch(ra[0], kb + 3);
+      if (kb + 2 < nKB) fetch(ra[0], kb + 2);
       if (kb + 1 >= nKB) break;
       if (!stage(ra[1], kb + 1)) break;
-      if (kb + 4 < nKB) fetch(ra[1], kb + 4);
-      if (kb + 2 >= nKB) break;
-      if (!stage(ra[2], kb + 2)) break;
-      if (kb + 5 < nKB) fetch(ra[2], kb + 5);
+      if (kb + 3 < nKB) fetch(ra[1], kb + 3);
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -372,14 +367,16 @@ __global__ void __launch_bounds__(T3_THREADS, 1)
     const int lc = lastCommit;
     tc_wait(tc_smem_u32(&empty[lc % T3_STAGES]), (uint32_t)((lc / T3_STAGES) & 1));
   }
-  if (ok && warp >= T3_DWARP0) {
-    // epilogue: the drain warps hold the rows' sums (row m = 32 (w % 4) + lane)
+  if (ok && warp >= T3_DWARP0 && warp < T3_MWARP) {
+    // epilogue: the drain warps hold the rows' sums (row m = 32 (w % 4) + lane,
+    // columns half * BN/2 ..)
     const int m = (warp % 4) * 32 + lane;
+    const int half = (warp - T3_DWARP0) / 4;
     float* yr = yrow[m];
     const bool vecY = ((uintptr_t)yr % 16 == 0);
 #pragma unroll
-    for (int cb = 0; cb < BN / 16; cb++) {
-      const int nb = n0 + cb * 16;
+    for (int cb = 0; cb < BN / 32; cb++) {
+      const int nb = n0 + half * (BN / 2) + cb * 16;
       if (part) {
         if (r0 + m < M) {
           float* pr = part + ((int64_t)blockIdx.z * M + r0 + m) * N;

@@ -578,6 +578,7 @@ void dev_free(DevState& D) {
   D.upF1 = D.upF2 = D.dnF1 = D.dnF2 = D.upT32 = D.dnT32 = nullptr;
   D.m2mUp32 = nullptr;
   for (DevState::OpT* op : {&D.tL2L, &D.tUpF1, &D.tUpF2, &D.tDnF1, &D.tDnF2, &D.tM2MUp}) *op = DevState::OpT();
+  for (TcOp* op : {&D.cL2L, &D.cUpF1, &D.cUpF2, &D.cDnF1, &D.cDnF2, &D.cM2MUp}) *op = TcOp();  // memory freed above
   D.transIdDev = nullptr;
   D.m2lT32 = nullptr;
   D.m2lTw32 = nullptr;

@@ -320,10 +320,10 @@ class FMM3d:
 
     GEMM_PATHS = {"wide": 0, "tc": 1, "narrow": 2}
 
-    def set_gemm_path(self, path="wide"):
-        """Kernels of the FP32 row GEMMs: "wide" (CUDA cores, 128 x 160 tiles,
-        the default), "narrow" (CUDA cores, 128 x 64 tiles) or "tc" (M2M/L2L on
-        the tensor cores as 3xTF32, opt-in).  True/False mean "tc"/"wide"."""
+    def set_gemm_path(self, path="tc"):
+        """Kernels of the FP32 row GEMMs: "tc" (the tensor cores as 3xTF32,
+        the default), "wide" (CUDA cores, 128 x 160 tiles) or "narrow" (CUDA
+        cores, 128 x 64 tiles).  True/False mean "tc"/"wide"."""
         if path is True or path is False:
             path = "tc" if path else "wide"
         if path not in self.GEMM_PATHS:

@@ -210,15 +210,15 @@ fmmg_status fmmg_set_graph(fmmg_handle* h, int on);
 /* active: 1 while a captured graph is cached; note: why capture was refused ("" if not). */
 fmmg_status fmmg_graph_state(const fmmg_handle* h, int* active, const char** note);
 
-/* The kernels of the mixed form's FP32 row GEMMs.  path 0 (the default): all
- * on the CUDA cores with 128 x 160 tiles; 2: CUDA cores with 128 x 64 tiles;
- * 1: the M2M and L2L GEMMs on the tensor cores as 3xTF32 split products
- * (tcgen05) where the operand rows are 16-byte aligned, the rest as path 0.
- * The TF32 rounding of the low parts and the tensor-core accumulation,
- * amplified by the next check-to-equivalent pseudo-inverse, lift the error of
- * the 1M-point Laplace np=6 workload to 1.1e-5 on path 1, above its 1e-5
- * budget.  FMMG_INVALID_ARG for another path.  No counterpart in the
- * reference. */
+/* The kernels of the mixed form's FP32 row GEMMs (leaf and downward C2E
+ * factors, folded C2E x M2M, L2L).  path 1 (the default): the tensor cores
+ * (tcgen05, 3xTF32 split products with every 32-wide K block summed in FP32),
+ * for every GEMM whose X rows are 16-byte aligned with K % 4 == 0 (np = 3, 5
+ * and 7 Laplace surfaces are not, and take path 0); path 0: the CUDA cores
+ * with 128 x 160 tiles; 2: the CUDA cores with 128 x 64 tiles.  On the
+ * 1M-point Laplace np=6 workload, 8 right-hand sides, path 1 gives 3.0e-6
+ * against the dense sum where path 0 gives 2.5e-6.  FMMG_INVALID_ARG for
+ * another path.  No counterpart in the reference. */
 fmmg_status fmmg_set_gemm_path(fmmg_handle* h, int path);
 /* flag = 1 if a kernel gave up a bounded wait since the last call (its
  * results are then invalid), else 0; clears the flag.  Synchronises.  The
