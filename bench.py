@@ -343,10 +343,15 @@ def run_ours(args):
                                                      flush, barrier=tdist.barrier if dist else None)
         if dist:
             ms = FD.max_over_ranks(ms, device="cuda")
-        vals = out[0].cpu().numpy()
-        rel, mx, _ = f.check(dens[0], vals, idx)
+        # every right-hand side of the block against the dense sum; the form's
+        # error is the worst of them
+        vals = out[:k].cpu().numpy()
+        checks = [f.check(dens[r], vals[r], idx) for r in range(k)]
+        rel = max(c[0] for c in checks)
+        mx = max(c[1] for c in checks)
         results.append(dict(precision=name, k=k, ms_per_step=ms, points_per_s=n * k * ws / (ms * 1e-3),
-                            rel_err_vs_dense=rel, max_abs_err_vs_dense=mx, kernel_ms=kern,
+                            rel_err_vs_dense=rel, rel_err_per_rhs=[c[0] for c in checks],
+                            max_abs_err_vs_dense=mx, kernel_ms=kern,
                             stage_ms=stage, launches=launches, cuda_graph=graph, tuning=tuned))
     adj = {} if args.no_adjoint else time_adjoint(f, torch, stream, den, out, n, args.steps, args.warmup, flush)
     if dist and adj:
@@ -412,6 +417,7 @@ def run_ours(args):
                     "d2h_bytes_per_step": 8 * n * kh},
             "gpu_launches": head["launches"],
             "rel_err_vs_dense": head["rel_err_vs_dense"], "check_targets": CHECK_TARGETS,
+            "rel_err_checked": "worst of every right-hand side of the block, at the same sampled targets",
             "fp64_points_per_s": fp64["points_per_s"] if fp64 else None,
             "speedup_vs_fp64": head["points_per_s"] / fp64["points_per_s"] if fp64 else None,
             "speedups": speedups(results),

@@ -420,9 +420,9 @@ fmmg_status fmmg_autotune(fmmg_handle* h, int k, int precision, const double* dD
     float best = 1e30f, ms = 0.f;
     const bool mixed = precision == FMMG_PREC_MIXED;
     int* rowsKnob = mixed ? &T.hadRows : &T.pqParents;
-    if (mixed && k >= 2) {  // the 27-product Hadamard with 1 or 2 right-hand sides per thread
+    if (mixed && k >= 2) {  // the Hadamard's form: 27-product accumulators (1, 2) or output-child ones (3, 4)
       int bestForm = T.hadRhsPerThread;
-      for (int c : {2, 1}) {
+      for (int c : {4, 3, 2, 1}) {
         T.hadRhsPerThread = c;
         if ((s = timeIt(ms)) != FMMG_OK) break;
         if (ms < best) {
@@ -473,7 +473,7 @@ fmmg_status fmmg_tuning(fmmg_handle* h, int* vals, int n, int set) {
   if (!h || !vals || n < 3) return fail(h, FMMG_INVALID_ARG, "need 3 values");
   fmmg::DevState::Tune& T = h->dev.tune;
   if (set) {
-    if (vals[0] < 1 || vals[1] < 1 || vals[2] < 0 || (n >= 4 && vals[3] != 1 && vals[3] != 2) ||
+    if (vals[0] < 1 || vals[1] < 1 || vals[2] < 0 || (n >= 4 && (vals[3] < 1 || vals[3] > 4)) ||
         (n >= 5 && (vals[4] < 0 || vals[4] > 63)) || (n >= 6 && vals[5] != 3 && vals[5] != 4))
       return fail(h, FMMG_INVALID_ARG, "tuning values");
     T.hadRows = vals[0];

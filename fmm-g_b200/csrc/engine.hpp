@@ -95,13 +95,14 @@ struct DevState {
   // launch shapes chosen by fmmg_autotune (defaults otherwise): rows per CTA of
   // the FP32 and FP64 Hadamard kernels, and split-K when a GEMM's tiles fill
   // fewer than gemmSplitMul CTAs per SM (0: never split)
-  // fmmg_autotune (defaults otherwise), and the right-hand sides per thread
-  // of the FP32 27-product Hadamard (1 or 2)
+  // fmmg_autotune (defaults otherwise), and the form of the FP32 Hadamard
+  // (1, 2: 27-product accumulators, 1 or 2 right-hand sides a thread; 3, 4:
+  // output-child accumulators, 2 or 4 right-hand sides a thread)
   // tcMask: which FP32 GEMM classes the tensor-core path takes (bit 0 leaf
   // C2E F1, 1 leaf C2E F2, 2 folded C2E x M2M, 3 L2L, 4 downward C2E F1,
   // 5 downward C2E F2); tcProducts: 3 (hi*hi + hi*lo + lo*hi) or 4 (+ lo*lo)
   struct Tune {
-    int hadRows = 64, pqParents = 128, gemmSplitMul = 2, hadRhsPerThread = 1, tcMask = 63, tcProducts = 3;
+    int hadRows = 128, pqParents = 128, gemmSplitMul = 2, hadRhsPerThread = 4, tcMask = 63, tcProducts = 3;
   } tune;
   // FP32 row GEMMs: 1 on the tensor cores (3xTF32, default), 0 the wide-tile
   // CUDA-core kernel, 2 the 128 x 64 CUDA-core kernel

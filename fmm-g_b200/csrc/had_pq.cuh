@@ -621,4 +621,161 @@ static __global__ void __launch_bounds__(PQX_THREADS, 1)
   }
 }
 
+
+// k_m2l_had_o<R>: the 27-product Hadamard accumulated in the space of the 8
+// output children, R = 2 or 4 right-hand sides a lane.  The 27-product form
+// above keeps 27 accumulators per right-hand side, so a lane holds one
+// right-hand side and every combined translation read from shared memory
+// feeds one complex multiply-add: the kernel is bound by the L1 data path
+// (27 translation and 8 spectrum reads per neighbour).  Here each neighbour's
+// 27 products are folded into the 8 children at once, along one axis at a
+// time (m0 + m1 | m0 + m2 per axis, 28 adds for the three axes), so the state
+// per right-hand side is 8 accumulators and a lane can hold R of them: the 27
+// translations of a neighbour are read once into registers and used for all R
+// right-hand sides.  The input combinations go the same way (19 adds), the
+// products are 9 complex multiplies and 18 complex multiply-adds.  Per right-
+// hand side that is a few more FP32 operations than the 27-product kernel but
+// R times fewer translation reads.
+// Lanes: FB = 4 R frequencies x (8 / R) groups of R right-hand sides of a
+// block of 8; a warp owns one target parent; the CTA stages T'[27][27][FB].
+// Grid (rows / rows per CTA, nEff / FB, ceil(nrhs / 8)); dynamic shared
+// memory 27 * 27 * FB * 8 bytes.
+__device__ __forceinline__ unsigned long long ho_cmul(float2 t, unsigned long long u) {
+  unsigned long long r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pq_pk(t.x, t.x)), "l"(u));
+  float2 a = pq_unpk(r);
+  const float2 v = pq_unpk(u);
+  a.x = fmaf(-t.y, v.y, a.x);
+  a.y = fmaf(t.y, v.x, a.y);
+  return pq_pk(a.x, a.y);
+}
+__device__ __forceinline__ unsigned long long ho_cmac(unsigned long long acc, float2 t, unsigned long long u) {
+  pq_fma2(acc, pq_pk(t.x, t.x), u);
+  float2 a = pq_unpk(acc);
+  const float2 v = pq_unpk(u);
+  a.x = fmaf(-t.y, v.y, a.x);
+  a.y = fmaf(t.y, v.x, a.y);
+  return pq_pk(a.x, a.y);
+}
+
+// One neighbour's contribution for one right-hand side: children x[8]
+// (index 4 bx + 2 by + bz), translations t[27] (index 9 jx + 3 jy + jz),
+// added into acc[8] (index 4 cx + 2 cy + cz).  Codes per axis: inputs
+// 0: x0 + x1, 1: x1, 2: x0; outputs c = 0 take codes 0 and 1, c = 1 codes 0 and 2.
+__device__ __forceinline__ void ho_apply(unsigned long long (&acc)[8], const unsigned long long (&x)[8],
+                                         const float2 (&t)[27]) {
+#pragma unroll
+  for (int jz = 0; jz < 3; jz++) {
+    unsigned long long uz[4];  // [bx][by], z combined by code jz
+#pragma unroll
+    for (int q = 0; q < 4; q++) uz[q] = jz == 0 ? w8_add(x[2 * q], x[2 * q + 1]) : (jz == 1 ? x[2 * q + 1] : x[2 * q]);
+    unsigned long long uy[2][3];  // [bx][jy]
+#pragma unroll
+    for (int bx = 0; bx < 2; bx++) {
+      uy[bx][0] = w8_add(uz[2 * bx], uz[2 * bx + 1]);
+      uy[bx][1] = uz[2 * bx + 1];
+      uy[bx][2] = uz[2 * bx];
+    }
+    unsigned long long vx[2][3];  // [cx][jy]: the products folded along x
+#pragma unroll
+    for (int jy = 0; jy < 3; jy++) {
+      const int jyz = 3 * jy + jz;
+      const unsigned long long m0 = ho_cmul(t[jyz], w8_add(uy[0][jy], uy[1][jy]));
+      vx[0][jy] = ho_cmac(m0, t[9 + jyz], uy[1][jy]);
+      vx[1][jy] = ho_cmac(m0, t[18 + jyz], uy[0][jy]);
+    }
+#pragma unroll
+    for (int cx = 0; cx < 2; cx++) {
+      const unsigned long long w0 = w8_add(vx[cx][0], vx[cx][1]), w1 = w8_add(vx[cx][0], vx[cx][2]);  // cy = 0, 1
+      // fold along z into the children: cz = 0 takes jz 0, 1; cz = 1 takes jz 0, 2
+#pragma unroll
+      for (int cy = 0; cy < 2; cy++) {
+        const unsigned long long w = cy ? w1 : w0;
+        const int c = 4 * cx + 2 * cy;
+        if (jz == 0) {
+          acc[c] = w8_add(acc[c], w);
+          acc[c + 1] = w8_add(acc[c + 1], w);
+        } else if (jz == 1) {
+          acc[c] = w8_add(acc[c], w);
+        } else {
+          acc[c + 1] = w8_add(acc[c + 1], w);
+        }
+      }
+    }
+  }
+}
+
+template <int R>
+static __global__ void __launch_bounds__(PQX_THREADS, 1)
+    k_m2l_had_o(int nRows, const int32_t* __restrict__ rowOut, const int64_t* __restrict__ nPtr,
+                const int8_t* __restrict__ nOff, const int32_t* __restrict__ nIn, const float2* __restrict__ effIn,
+                PqLayout inL, const float2* __restrict__ Tw, float2* __restrict__ effOut, PqLayout outL, int nEff,
+                int nrhs, float nrmfc) {
+  static_assert(R == 2 || R == 4, "two or four right-hand sides a lane");
+  constexpr int G = 8 / R, FB = 32 / G;
+  extern __shared__ __align__(16) unsigned char ho_smem[];
+  float2* Ts = reinterpret_cast<float2*>(ho_smem);  // [27 offsets][27 combinations][FB frequencies]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int fl = lane % FB, rg = lane / FB;
+  const int f0 = blockIdx.y * FB;
+  const int f = f0 + fl;
+  const int rhs0 = blockIdx.z * 8 + rg * R;  // this lane's right-hand sides rhs0 .. rhs0 + R - 1
+  for (int i = threadIdx.x; i < W8_OFFS * 27 * FB; i += blockDim.x) {
+    const int oj = i / FB, ff = f0 + (i % FB);
+    Ts[i] = ff < nEff ? Tw[(int64_t)oj * nEff + ff] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  const bool act = f < nEff && rhs0 < nrhs;
+  // the block holds 8 right-hand-side slots, so rhs0 + R - 1 is in the buffer
+  const int64_t lanePos = act ? (int64_t)f * 8 + rg * R : 0;
+  const float4* inF = reinterpret_cast<const float4*>(effIn + (act ? blockIdx.z * inL.blk : 0) + lanePos);
+  float2* outF = effOut + blockIdx.z * outL.blk + lanePos;
+  const int64_t inSlot4 = inL.slot / 2;  // float4 units (slot strides are multiples of 8 float2)
+  const int per = (nRows + gridDim.x - 1) / gridDim.x;
+  const int bEnd = min(nRows, (int)(blockIdx.x + 1) * per);
+  for (int b = blockIdx.x * per + warp; b < bEnd; b += PQX_THREADS / 32) {
+    unsigned long long acc[R][8];
+#pragma unroll
+    for (int r = 0; r < R; r++)
+#pragma unroll
+      for (int c = 0; c < 8; c++) acc[r][c] = 0ull;
+    const int64_t e1 = nPtr[b + 1];
+    for (int64_t e = nPtr[b]; e < e1; e++) {
+      const int4 a0 = reinterpret_cast<const int4*>(nIn)[2 * e];
+      const int4 b0 = reinterpret_cast<const int4*>(nIn)[2 * e + 1];
+      const int sl[8] = {a0.x, a0.y, a0.z, a0.w, b0.x, b0.y, b0.z, b0.w};
+      const float2* Tn = Ts + (int)nOff[e] * 27 * FB + fl;
+      float2 t[27];
+#pragma unroll
+      for (int j = 0; j < 27; j++) t[j] = Tn[j * FB];
+#pragma unroll
+      for (int p = 0; p < R / 2; p++) {  // right-hand sides 2p, 2p + 1 of this lane
+        float4 raw[8];
+#pragma unroll
+        for (int c2 = 0; c2 < 8; c2++)
+          raw[c2] = (act && sl[c2] >= 0) ? inF[(int64_t)sl[c2] * inSlot4 + p] : make_float4(0.f, 0.f, 0.f, 0.f);
+        unsigned long long x[8];
+#pragma unroll
+        for (int c2 = 0; c2 < 8; c2++) x[c2] = pq_pk(raw[c2].x, raw[c2].y);
+        ho_apply(acc[2 * p], x, t);
+#pragma unroll
+        for (int c2 = 0; c2 < 8; c2++) x[c2] = pq_pk(raw[c2].z, raw[c2].w);
+        ho_apply(acc[2 * p + 1], x, t);
+      }
+    }
+    if (!act) continue;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      const int tt = rowOut[8 * b + c];
+      if (tt < 0) continue;
+      float4* o = reinterpret_cast<float4*>(outF + (int64_t)tt * outL.slot);
+#pragma unroll
+      for (int p = 0; p < R / 2; p++) {
+        const float2 a0 = pq_unpk(acc[2 * p][c]), a1 = pq_unpk(acc[2 * p + 1][c]);
+        o[p] = make_float4(a0.x * nrmfc, a0.y * nrmfc, a1.x * nrmfc, a1.y * nrmfc);
+      }
+    }
+  }
+}
+
 }  // namespace fmmg

@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(MX_THREADS)
   constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD, NRM = KTraits<KT>::NRM;
   constexpr int MX_TILE = mx_tile<SD * KB, NRM != 0>();
   __shared__ float4 sPos[MX_TILE];
-  __shared__ float4 sPosLo[NRM ? MX_TILE : 1];
+  __shared__ float4 sPosLo[MX_TILE];
   __shared__ float4 sNrm[NRM ? MX_TILE : 1];
   __shared__ __align__(16) float sDen[MX_TILE * SD * KB];
   __shared__ int64_t eBeg[MX_MAXE];
@@ -177,11 +177,9 @@ __global__ void __launch_bounds__(MX_THREADS)
       tx = (float)dx;
       ty = (float)dy;
       tz = (float)dz;
-      if (NRM) {
-        txl = (float)(dx - tx);
-        tyl = (float)(dy - ty);
-        tzl = (float)(dz - tz);
-      }
+      txl = (float)(dx - tx);
+      tyl = (float)(dy - ty);
+      tzl = (float)(dz - tz);
     }
     double acc[TD * KB];
 #pragma unroll
@@ -196,10 +194,8 @@ __global__ void __launch_bounds__(MX_THREADS)
           const int64_t s = entry_source(base + i, ne, eBeg, ePre);
           const double dx = src[3 * s] - cx, dy = src[3 * s + 1] - cy, dz = src[3 * s + 2] - cz;
           sPos[i] = make_float4((float)dx, (float)dy, (float)dz, 0.f);
-          if (NRM) {
-            sPosLo[i] = make_float4((float)(dx - (float)dx), (float)(dy - (float)dy), (float)(dz - (float)dz), 0.f);
-            sNrm[i] = make_float4((float)nrm[3 * s], (float)nrm[3 * s + 1], (float)nrm[3 * s + 2], 0.f);
-          }
+          sPosLo[i] = make_float4((float)(dx - (float)dx), (float)(dy - (float)dy), (float)(dz - (float)dz), 0.f);
+          if (NRM) sNrm[i] = make_float4((float)nrm[3 * s], (float)nrm[3 * s + 1], (float)nrm[3 * s + 2], 0.f);
 #pragma unroll
           for (int r = 0; r < KB; r++)
 #pragma unroll
@@ -213,14 +209,14 @@ __global__ void __launch_bounds__(MX_THREADS)
 #pragma unroll
           for (int c = 0; c < TD * KB; c++) part[c] = 0.f;
           for (int i = sp; i < cnt; i += S) {
-            const float4 q = sPos[i];
-            float ox = tx - q.x, oy = ty - q.y, oz = tz - q.z;
+            // offsets from hi/lo FP32 pairs of the box-centred coordinates:
+            // the hi difference of close points is exact, so a near-coincident
+            // pair keeps its separation to FP32 precision of the separation
+            const float4 q = sPos[i], ql = sPosLo[i];
+            const float ox = (tx - q.x) + (txl - ql.x), oy = (ty - q.y) + (tyl - ql.y), oz = (tz - q.z) + (tzl - ql.z);
             float nv[3] = {0.f, 0.f, 0.f};
             if (NRM) {
-              const float4 ql = sPosLo[i], qn = sNrm[i];
-              ox += txl - ql.x;
-              oy += tyl - ql.y;
-              oz += tzl - ql.z;
+              const float4 qn = sNrm[i];
               nv[0] = qn.x;
               nv[1] = qn.y;
               nv[2] = qn.z;
@@ -1146,6 +1142,21 @@ static void run_mixed_blocks(const Plan& P, DevState& D, int kc, int mask, bool 
         k_m2l_had_pqx2<32, false><<<g1, PQX_THREADS, smem, st>>>(
             npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen32, PqLayout{effDR, P.nEff32}, D.m2lT32, D.effVal32,
             PqLayout{effVR, P.nEff32}, 1, 0, P.nEff32, kc, nrmfc, D.transIdDev);
+      } else if (D.hadW && D.m2lTw32 && D.tune.hadRhsPerThread >= 3) {  // output-child accumulators
+#define FMMG_HADO(R_)                                                                                         \
+  do {                                                                                                        \
+    constexpr int FB = 4 * (R_);                                                                              \
+    const size_t smem = (size_t)W8_OFFS * 27 * FB * sizeof(float2);                                           \
+    cudaFuncSetAttribute(k_m2l_had_o<R_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);            \
+    dim3 go((npar + D.tune.hadRows - 1) / D.tune.hadRows, (P.nEff32 + FB - 1) / FB, nblk);                    \
+    k_m2l_had_o<R_><<<go, PQX_THREADS, smem, st>>>(npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen32,     \
+                                                   PqLayout{blkDen, (int64_t)P.nEff32 * 8}, D.m2lTw32,        \
+                                                   D.effVal32, PqLayout{blkVal, (int64_t)P.nEff32 * 8},       \
+                                                   P.nEff32, kc, nrmfc);                                      \
+  } while (0)
+        if (D.tune.hadRhsPerThread == 4) FMMG_HADO(4);
+        else FMMG_HADO(2);
+#undef FMMG_HADO
       } else if (D.hadW && D.m2lTw32 && D.tune.hadRhsPerThread == 2) {  // 27-product form, 2 RHS a thread
         const size_t smem = (size_t)W8_OFFS * 27 * W8X2_F * sizeof(float2);
         cudaFuncSetAttribute(k_m2l_had_w8x2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

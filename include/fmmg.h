@@ -236,16 +236,23 @@ fmmg_status fmmg_selftest_wait(int device, int arrive, int64_t limit_ns);
 
 /* Autotuner (no counterpart in the reference): times `reps` evaluates of
  * (k, precision) on the caller's device buffers for each candidate launch
- * shape -- rows per CTA of the Hadamard kernel (32, 64, 128, 256), then for
- * the mixed form the split-K threshold of the FP32 GEMMs (0, 1, 2, 4 CTAs per
- * SM) -- keeps the fastest in the handle and returns its time in best_ms.
- * d_trg_val is overwritten.  Synchronises. */
+ * shape -- for the mixed form with k >= 2 the form of the Hadamard kernel
+ * (1..4, see fmmg_tuning), then rows per CTA of the Hadamard kernel (32, 64,
+ * 128, 256), then for the mixed form the split-K threshold of the FP32 GEMMs
+ * (0, 1, 2, 4 CTAs per SM) -- keeps the fastest in the handle and returns its
+ * time in best_ms.  d_trg_val is overwritten.  Synchronises. */
 fmmg_status fmmg_autotune(fmmg_handle* h, int k, int precision, const double* d_src_den, double* d_trg_val,
                           int reps, double* best_ms);
 /* vals[0..2] = Hadamard rows per CTA (FP32 form), Hadamard rows per CTA (FP64
- * form), split-K threshold (CTAs per SM); with n >= 4, vals[3] = right-hand
- * sides per thread of the FP32 27-product Hadamard (1 or 2).  set != 0
- * installs them (FMMG_INVALID_ARG for values out of range), else reads. */
+ * form), split-K threshold (CTAs per SM); with n >= 4, vals[3] = the form of
+ * the FP32 Hadamard for k >= 2 (1, 2: 27 accumulators per right-hand side, 1
+ * or 2 right-hand sides a thread; 3, 4: 8 output-child accumulators, 2 or 4
+ * right-hand sides a thread; default 4); with n >= 5, vals[4] = the FP32 GEMM
+ * classes on the tensor cores when path 1 is on (bit 0 leaf C2E F1, 1 leaf
+ * C2E F2, 2 folded C2E x M2M, 3 L2L, 4 downward C2E F1, 5 downward C2E F2;
+ * default 63); with n >= 6, vals[5] = the products of the 3xTF32 split (3, or
+ * 4 with lo*lo).  set != 0 installs them (FMMG_INVALID_ARG for values out of
+ * range), else reads. */
 fmmg_status fmmg_tuning(fmmg_handle* h, int* vals, int n, int set);
 
 /* Host-plan introspection (valid after setup, also with device < 0).
