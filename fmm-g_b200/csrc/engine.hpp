@@ -75,6 +75,7 @@ struct DevState {
   float2* m2lTw32 = nullptr;  // combined translations of the 27-product Hadamard [27][27][nEff] (scalar kernels)
   bool hadW = true;           // FP32 k >= 2 Hadamard in the 27-product form
   double *denK = nullptr, *valK = nullptr;  // permuted densities / values of a RHS chunk
+  float* den32 = nullptr;  // the chunk's densities in FP32, [rhs / 8][n][8][sd] (what the pair kernels stage)
   bool mixedReady = false, mixedOpsStale = true;
   int mixedK = 0;                           // right-hand sides the mixed arrays hold
   double mixedBudgetBytes = 48e9;           // device bytes for per-density work arrays

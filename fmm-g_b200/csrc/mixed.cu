@@ -146,8 +146,8 @@ __global__ void __launch_bounds__(MX_THREADS)
     k_p2p_near32(const int32_t* __restrict__ rows, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
                  const int64_t* __restrict__ srcBeg, const int64_t* __restrict__ srcCnt,
                  const int64_t* __restrict__ trgBeg, const int64_t* __restrict__ trgCnt,
-                 const double* __restrict__ src, const double* __restrict__ nrm, const double* __restrict__ den,
-                 int64_t denStride, const double* __restrict__ trg, const double* __restrict__ ctr,
+                 const double* __restrict__ src, const double* __restrict__ nrm, const float* __restrict__ den32,
+                 int64_t den32Blk, const double* __restrict__ trg, const double* __restrict__ ctr,
                  double* __restrict__ val, int64_t valStride, int nrhs, float mu, float ve) {
   constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD, NRM = KTraits<KT>::NRM;
   constexpr int MX_TILE = mx_tile<SD * KB, NRM != 0>();
@@ -196,12 +196,11 @@ __global__ void __launch_bounds__(MX_THREADS)
           sPos[i] = make_float4((float)dx, (float)dy, (float)dz, 0.f);
           sPosLo[i] = make_float4((float)(dx - (float)dx), (float)(dy - (float)dy), (float)(dz - (float)dz), 0.f);
           if (NRM) sNrm[i] = make_float4((float)nrm[3 * s], (float)nrm[3 * s + 1], (float)nrm[3 * s + 2], 0.f);
+          // the block's KB x SD densities: contiguous in the FP32 copy (rows of
+          // 8 right-hand sides per source, zeros past the last one)
+          const float* ds = den32 + (rhs0 >> 3) * den32Blk + s * 8 * SD + (rhs0 & 7) * SD;
 #pragma unroll
-          for (int r = 0; r < KB; r++)
-#pragma unroll
-            for (int c = 0; c < SD; c++)
-              sDen[(i * KB + r) * SD + c] =
-                  rhs0 + r < nrhs ? (float)den[(int64_t)(rhs0 + r) * denStride + s * SD + c] : 0.f;
+          for (int r = 0; r < KB * SD; r++) sDen[i * KB * SD + r] = ds[r];
         }
         __syncthreads();
         if (act) {
@@ -231,6 +230,151 @@ __global__ void __launch_bounds__(MX_THREADS)
       }
     }
     reduce_store<TD, KB>(sRed, acc, tid, tl, sp, TG, S, act, val, tb + t, rhs0, nrhs, valStride);
+  }
+}
+
+// Laplace single layer (the headline kernel) with two targets a thread: the
+// offsets, r^2 and 1/(4 pi r) of a source against both targets and the
+// KB multiply-adds of its densities run as packed FP32x2 operations, so each
+// staged source costs about half the instructions of the one-target loop.
+// Same offsets (hi/lo pairs), the same coincidence rule (r^2 < 1e-16 adds
+// nothing) and the same per-tile FP64 partial sums as k_p2p_near32.
+__device__ __forceinline__ unsigned long long nl_pk(float a, float b) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ float2 nl_unpk(unsigned long long v) {
+  float2 r;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+  return r;
+}
+__device__ __forceinline__ unsigned long long nl_add(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long nl_sub(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long nl_mul(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long nl_fma(unsigned long long a, unsigned long long b,
+                                                     unsigned long long c) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+
+template <int KB>
+__global__ void __launch_bounds__(MX_THREADS, 6)
+    k_p2p_near32_lap2(const int32_t* __restrict__ rows, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                      const int64_t* __restrict__ srcBeg, const int64_t* __restrict__ srcCnt,
+                      const int64_t* __restrict__ trgBeg, const int64_t* __restrict__ trgCnt,
+                      const double* __restrict__ src, const float* __restrict__ den32, int64_t den32Blk,
+                      const double* __restrict__ trg, const double* __restrict__ ctr, double* __restrict__ val,
+                      int64_t valStride, int nrhs) {
+  constexpr int MX_TILE = mx_tile<KB, false>();
+  __shared__ float4 sPos[MX_TILE];
+  __shared__ float4 sPosLo[MX_TILE];
+  __shared__ __align__(16) float sDen[MX_TILE * KB];
+  __shared__ int64_t eBeg[MX_MAXE];
+  __shared__ int32_t ePre[MX_MAXE + 1];
+  __shared__ double sRed[MX_THREADS * KB];
+  const int row = blockIdx.x;
+  const int rhs0 = blockIdx.y * KB;
+  const int g = rows[row];
+  const int64_t tb = trgBeg[g], tn = trgCnt[g];
+  const int64_t e0 = ptr[row], e1 = ptr[row + 1];
+  const double cx = ctr[3 * g], cy = ctr[3 * g + 1], cz = ctr[3 * g + 2];
+  const int tid = threadIdx.x;
+  const int TG = mx_group<MX_THREADS>((tn + 1) / 2);  // lanes per group; each lane takes two targets
+  const int S = MX_THREADS / TG;
+  const int tl = tid % TG, sp = tid / TG;
+  const float c4pi = (float)(1.0 / (4.0 * 3.14159265358979323846));
+  for (int64_t t0 = 0; t0 < tn; t0 += 2 * TG) {
+    const int64_t ta = t0 + tl, tbb = t0 + tl + TG;
+    const bool actA = ta < tn, actB = tbb < tn;
+    // target coordinates as packed (A, B) hi and lo parts
+    unsigned long long txh = 0, tyh = 0, tzh = 0, txl = 0, tyl = 0, tzl = 0;
+    {
+      float h[2][3] = {{0, 0, 0}, {0, 0, 0}}, l[2][3] = {{0, 0, 0}, {0, 0, 0}};
+      for (int q = 0; q < 2; q++) {
+        const int64_t t = q ? tbb : ta;
+        if (!(q ? actB : actA)) continue;
+        const double d[3] = {trg[3 * (tb + t)] - cx, trg[3 * (tb + t) + 1] - cy, trg[3 * (tb + t) + 2] - cz};
+        for (int c = 0; c < 3; c++) {
+          h[q][c] = (float)d[c];
+          l[q][c] = (float)(d[c] - h[q][c]);
+        }
+      }
+      txh = nl_pk(h[0][0], h[1][0]);
+      tyh = nl_pk(h[0][1], h[1][1]);
+      tzh = nl_pk(h[0][2], h[1][2]);
+      txl = nl_pk(l[0][0], l[1][0]);
+      tyl = nl_pk(l[0][1], l[1][1]);
+      tzl = nl_pk(l[0][2], l[1][2]);
+    }
+    double acc[2][KB];
+#pragma unroll
+    for (int r = 0; r < KB; r++) acc[0][r] = acc[1][r] = 0.0;
+    for (int64_t ec = e0; ec < e1; ec += MX_MAXE) {
+      const int ne = (int)min((int64_t)MX_MAXE, e1 - ec);
+      const int total = load_entries(idx, ec, ne, 0, srcBeg, srcCnt, eBeg, ePre);
+      for (int base = 0; base < total; base += MX_TILE) {
+        const int cnt = min(MX_TILE, total - base);
+        __syncthreads();
+        for (int i = tid; i < cnt; i += MX_THREADS) {
+          const int64_t s = entry_source(base + i, ne, eBeg, ePre);
+          const double dx = src[3 * s] - cx, dy = src[3 * s + 1] - cy, dz = src[3 * s + 2] - cz;
+          sPos[i] = make_float4((float)dx, (float)dy, (float)dz, 0.f);
+          sPosLo[i] = make_float4((float)(dx - (float)dx), (float)(dy - (float)dy), (float)(dz - (float)dz), 0.f);
+          const float* ds = den32 + (rhs0 >> 3) * den32Blk + s * 8 + (rhs0 & 7);
+          if constexpr (KB % 4 == 0) {  // 16-byte aligned: rows of 8, rhs0 a multiple of KB
+#pragma unroll
+            for (int r = 0; r < KB; r += 4)
+              *reinterpret_cast<float4*>(&sDen[i * KB + r]) = *reinterpret_cast<const float4*>(ds + r);
+          } else {
+#pragma unroll
+            for (int r = 0; r < KB; r++) sDen[i * KB + r] = ds[r];
+          }
+        }
+        __syncthreads();
+        if (actA) {
+          unsigned long long part[KB];  // (target A, target B) for each right-hand side
+#pragma unroll
+          for (int r = 0; r < KB; r++) part[r] = 0ull;
+          for (int i = sp; i < cnt; i += S) {
+            const float4 q = sPos[i], ql = sPosLo[i];
+            // (t_hi - s_hi) + (t_lo - s_lo): exact hi difference for close points
+            const unsigned long long ox = nl_add(nl_sub(txh, nl_pk(q.x, q.x)), nl_sub(txl, nl_pk(ql.x, ql.x)));
+            const unsigned long long oy = nl_add(nl_sub(tyh, nl_pk(q.y, q.y)), nl_sub(tyl, nl_pk(ql.y, ql.y)));
+            const unsigned long long oz = nl_add(nl_sub(tzh, nl_pk(q.z, q.z)), nl_sub(tzl, nl_pk(ql.z, ql.z)));
+            const float2 r2 = nl_unpk(nl_fma(oz, oz, nl_fma(oy, oy, nl_mul(ox, ox))));
+            const float ka = r2.x < 1e-16f ? 0.f : c4pi * rsqrtf(r2.x);
+            const float kb = r2.y < 1e-16f ? 0.f : c4pi * rsqrtf(r2.y);
+            const unsigned long long k2 = nl_pk(ka, kb);
+            float d[KB];
+            mx_den<KB>(&sDen[i * KB], d);
+#pragma unroll
+            for (int r = 0; r < KB; r++) part[r] = nl_fma(k2, nl_pk(d[r], d[r]), part[r]);
+          }
+#pragma unroll
+          for (int r = 0; r < KB; r++) {
+            const float2 v = nl_unpk(part[r]);
+            acc[0][r] += (double)v.x;
+            acc[1][r] += (double)v.y;
+          }
+        }
+      }
+    }
+    reduce_store<1, KB>(sRed, acc[0], tid, tl, sp, TG, S, actA, val, tb + ta, rhs0, nrhs, valStride);
+    reduce_store<1, KB>(sRed, acc[1], tid, tl, sp, TG, S, actB, val, tb + tbb, rhs0, nrhs, valStride);
   }
 }
 
@@ -326,8 +470,8 @@ template <int KT, int KB>
 __global__ void __launch_bounds__(MX_SURF)
     k_src2surf32(const int32_t* __restrict__ rows, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
                  const int64_t* __restrict__ srcBeg, const int64_t* __restrict__ srcCnt,
-                 const double* __restrict__ src, const double* __restrict__ nrm, const double* __restrict__ den,
-                 int64_t denStride, const double* __restrict__ ctr, const double* __restrict__ rad,
+                 const double* __restrict__ src, const double* __restrict__ nrm, const float* __restrict__ den32,
+                 int64_t den32Blk, const double* __restrict__ ctr, const double* __restrict__ rad,
                  const double* __restrict__ sam, int nSurf, float* __restrict__ out, int64_t ldo,
                  int64_t outRhsStride, int nrhs, float mu, float ve, int assign) {
   constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD, NRM = KTraits<KT>::NRM;
@@ -372,12 +516,9 @@ __global__ void __launch_bounds__(MX_SURF)
         sPos[i] = make_float4((float)(src[3 * s] - cx), (float)(src[3 * s + 1] - cy), (float)(src[3 * s + 2] - cz),
                               0.f);
         if (NRM) sNrm[i] = make_float4((float)nrm[3 * s], (float)nrm[3 * s + 1], (float)nrm[3 * s + 2], 0.f);
+        const float* ds = den32 + (rhs0 >> 3) * den32Blk + s * 8 * SD + (rhs0 & 7) * SD;
 #pragma unroll
-        for (int q = 0; q < KB; q++)
-#pragma unroll
-          for (int c = 0; c < SD; c++)
-            sDen[(i * KB + q) * SD + c] =
-                rhs0 + q < nrhs ? (float)den[(int64_t)(rhs0 + q) * denStride + s * SD + c] : 0.f;
+        for (int q = 0; q < KB * SD; q++) sDen[i * KB * SD + q] = ds[q];
       }
       __syncthreads();
       if (act) {
@@ -889,6 +1030,7 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
     FMMG_TRY(dalloc(D, D.upT32, (size_t)kc * P.nn * kUpMax));
     FMMG_TRY(dalloc(D, D.dnT32, (size_t)kc * P.nn * kDnMax));
     FMMG_TRY(dalloc(D, D.denK, (size_t)kc * P.ns * P.sd));
+    FMMG_TRY(dalloc(D, D.den32, kc8 * P.ns * P.sd));
     FMMG_TRY(dalloc(D, D.valK, (size_t)kc * std::max<int64_t>(P.nt, 1) * P.td));
     if (!D.l2l32) {
       FMMG_TRY(dalloc(D, D.l2l32, P.l2l.size()));
@@ -1003,6 +1145,7 @@ static void run_mixed_blocks(const Plan& P, DevState& D, int kc, int mask, bool 
   const int nl = (int)P.evtrLeaves.size();
   const int kb = (kc + KB - 1) / KB;
   const int64_t denStride = P.ns * P.sd, valStride = std::max<int64_t>(P.nt, 1) * P.td;
+  const int64_t den32Blk = P.ns * 8 * P.sd;  // floats per block of 8 right-hand sides in D.den32
   // tc: the operator split for the tensor cores (3xTF32), used when that
   // path is on and the class is in the tuning mask (the wide CUDA-core tiles
   // otherwise)
@@ -1035,7 +1178,7 @@ static void run_mixed_blocks(const Plan& P, DevState& D, int kc, int mask, bool 
   }
   if ((mask & 1) && !P.s2mLeaves.empty()) {
     k_src2surf32<KT, KB><<<dim3((unsigned)P.s2mLeaves.size(), kb), mx_surf_threads(P.nUC), 0, st>>>(
-        D.s2mLeaves, nullptr, nullptr, D.srcBeg, D.srcCnt, D.src, D.nrm, D.denK, denStride, D.ctr, D.rad, D.sam[1],
+        D.s2mLeaves, nullptr, nullptr, D.srcBeg, D.srcCnt, D.src, D.nrm, D.den32, den32Blk, D.ctr, D.rad, D.sam[1],
         P.nUC, D.uchk32, uc, nn * uc, kc, mu, ve, 1);
     ls->launches++;
   }
@@ -1062,9 +1205,14 @@ static void run_mixed_blocks(const Plan& P, DevState& D, int kc, int mask, bool 
   cudaEventRecord(D.ev[EV_UP_GEMM], st);
   auto near = [&](const int64_t* ptr, const int32_t* idx, cudaStream_t sn) {
     if (nl == 0) return;
-    k_p2p_near32<KT, KB><<<dim3(nl, kb), MX_THREADS, 0, sn>>>(D.evtrLeaves, ptr, idx, D.srcBeg, D.srcCnt, D.trgBeg,
-                                                             D.trgCnt, D.src, D.nrm, D.denK, denStride, D.trg, D.ctr,
-                                                             D.valK, valStride, kc, mu, ve);
+    if constexpr (KT == LAP_S_U)  // two targets a thread, packed FP32x2
+      k_p2p_near32_lap2<KB><<<dim3(nl, kb), MX_THREADS, 0, sn>>>(D.evtrLeaves, ptr, idx, D.srcBeg, D.srcCnt,
+                                                                  D.trgBeg, D.trgCnt, D.src, D.den32, den32Blk, D.trg,
+                                                                  D.ctr, D.valK, valStride, kc);
+    else
+      k_p2p_near32<KT, KB><<<dim3(nl, kb), MX_THREADS, 0, sn>>>(D.evtrLeaves, ptr, idx, D.srcBeg, D.srcCnt, D.trgBeg,
+                                                               D.trgCnt, D.src, D.nrm, D.den32, den32Blk, D.trg, D.ctr,
+                                                               D.valK, valStride, kc, mu, ve);
     ls->launches++;
   };
   auto nearAll = [&](cudaStream_t sn) {
@@ -1249,7 +1397,7 @@ static void run_mixed_blocks(const Plan& P, DevState& D, int kc, int mask, bool 
   cudaEventRecord(D.ev[EV_M2T], st);
   if ((mask & 16) && !P.s2lNodes.empty()) {
     k_src2surf32<KT, KB><<<dim3((unsigned)P.s2lNodes.size(), kb), mx_surf_threads(P.nDC), 0, st>>>(
-        D.s2lNodes, D.s2lPtr, D.s2lIdx, D.srcBeg, D.srcCnt, D.src, D.nrm, D.denK, denStride, D.ctr, D.rad, D.sam[3],
+        D.s2lNodes, D.s2lPtr, D.s2lIdx, D.srcBeg, D.srcCnt, D.src, D.nrm, D.den32, den32Blk, D.ctr, D.rad, D.sam[3],
         P.nDC, D.dchk32, dc, nn * dc, kc, mu, ve, 0);
     ls->launches++;
   }
@@ -1284,13 +1432,21 @@ static void run_mixed(const Plan& P, DevState& D, int kc, int mask, bool overlap
     run_mixed_blocks<KT, KB>(P, D, kc, mask, overlap, ls);
 }
 
+// the densities of a pass in source (leaf) order: FP64 [rhs][n][sd] in out, and
+// the FP32 copy the pair kernels stage, den32[rhs / 8][n][8][sd], each source's
+// block of 8 right-hand sides contiguous (zeros past the last right-hand side)
 __global__ void k_gather_den_k(int64_t n, int sd, int kc, int64_t stride, const int64_t* __restrict__ perm,
-                               const double* __restrict__ in, double* __restrict__ out) {
+                               const double* __restrict__ in, double* __restrict__ out, float* __restrict__ den32) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   int64_t s = perm[i];
-  for (int q = 0; q < kc; q++)
-    for (int c = 0; c < sd; c++) out[q * stride + i * sd + c] = in[q * stride + s * sd + c];
+  const int kc8 = (kc + 7) & ~7;
+  for (int q = 0; q < kc8; q++)
+    for (int c = 0; c < sd; c++) {
+      const double v = q < kc ? in[q * stride + s * sd + c] : 0.0;
+      if (q < kc) out[q * stride + i * sd + c] = v;
+      den32[((int64_t)(q >> 3) * n + i) * 8 * sd + (q & 7) * sd + c] = (float)v;
+    }
 }
 __global__ void k_scatter_val_k(int64_t n, int td, int kc, int64_t stride, const int64_t* __restrict__ perm,
                                 const double* __restrict__ in, double* __restrict__ out) {
@@ -1350,7 +1506,7 @@ std::string dev_evaluate_mixed(const Plan& P, DevState& D, const double* dDen, d
     const int kk = std::min(kc, k - r0);
     cudaEventRecord(D.ev[EV_BEGIN], st);
     k_gather_den_k<<<(unsigned)((ns + 255) / 256), 256, 0, st>>>(ns, P.sd, kk, denStride, D.srcPerm,
-                                                                  dDen + r0 * denStride, D.denK);
+                                                                  dDen + r0 * denStride, D.denK, D.den32);
     ls->launches++;
     // Cleared per pass: the accumulated target values and downward check
     // potentials.  The upward C2E reads only the check rows of leaves with

@@ -583,6 +583,7 @@ void dev_free(DevState& D) {
   D.m2lT32 = nullptr;
   D.m2lTw32 = nullptr;
   D.denK = D.valK = nullptr;
+  D.den32 = nullptr;
   D.adjNearRows = D.adjNearIdx = D.adjFarRows = D.adjFarIdx = D.adjS2lRows = D.adjS2lIdx = nullptr;
   D.adjNearPtr = D.adjFarPtr = D.adjS2lPtr = nullptr;
   D.vParentsT = D.vNbrTIdx = nullptr;
