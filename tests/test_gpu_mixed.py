@@ -166,11 +166,14 @@ def test_mixed_rhs_blocks_at_other_np(np_):
 
 
 @pytest.mark.parametrize("k", [5, 8, 12])
-def test_hadamard_two_rhs_per_thread_identical(k):
-    """The 27-product Hadamard with two right-hand sides per thread does, per
-    right-hand side, the same operations in the same order as the kernel with
-    one per thread: the evaluates agree bit for bit (odd k leaves a lane with
-    one right-hand side, k = 12 spans two blocks of 8)."""
+def test_hadamard_forms(k):
+    """The four forms of the FP32 Hadamard on one evaluate.  Forms 1 and 2
+    (27 product accumulators, one or two right-hand sides per thread) do, per
+    right-hand side, the same operations in the same order, and so do forms 3
+    and 4 (8 output-child accumulators, two or four right-hand sides per
+    thread): each pair agrees bit for bit (odd k leaves lanes with unused
+    right-hand sides, k = 12 spans two blocks of 8).  Between the pairs only
+    the order of the sums differs."""
     import torch
     rng = np.random.default_rng(77 + k)
     n = 40000
@@ -178,18 +181,20 @@ def test_hadamard_two_rhs_per_thread_identical(k):
     lib = fmmg.FMM3d(111, np_=6, pts_max=64)
     lib.setup(src)
     D = torch.from_numpy(rng.normal(size=(k, n))).cuda()
-    outs = []
-    for per in (1, 2):
-        assert lib.tuning({"had_fp32_rhs_per_thread": per})["had_fp32_rhs_per_thread"] == per
+    outs = {}
+    for form in (1, 2, 3, 4):
+        assert lib.tuning({"had_fp32_rhs_per_thread": form})["had_fp32_rhs_per_thread"] == form
         out = torch.zeros(k, n, dtype=torch.float64, device="cuda")
         torch.cuda.synchronize()
         lib.evaluate_device(D, out, k, fmmg.PREC_MIXED)
         lib.sync()
         assert lib.device_error() == 0
-        outs.append(out.cpu().numpy())
-    assert np.array_equal(outs[0], outs[1])
+        outs[form] = out.cpu().numpy()
+    assert np.array_equal(outs[1], outs[2])
+    assert np.array_equal(outs[3], outs[4])
+    assert rel_l2(outs[4], outs[1]) <= 1e-6
     with pytest.raises(fmmg.FmmgError):
-        lib.tuning({"had_fp32_rhs_per_thread": 3})
+        lib.tuning({"had_fp32_rhs_per_thread": 5})
 
 
 def test_mixed_follows_replaced_pinv():
