@@ -213,3 +213,29 @@ def test_adjoint_k_right_hand_sides():
     for r in range(k):
         g1, gt1 = f.adjoint(w[r], den[r], target_grad=True)
         assert np.array_equal(g[r], g1) and np.array_equal(gt[r], gt1)
+
+
+@pytest.mark.parametrize("precision", [fmmg.PREC_FP64, fmmg.PREC_MIXED])
+def test_torch_autograd_k_right_hand_sides(precision):
+    """fmm_apply on a [k, n_src, 1] block: the forward equals the evaluate of
+    the block in the given precision, the density gradient is the transposed
+    FMM of each right-hand side, and the target gradient their sum."""
+    import torch
+    import fmmg_torch
+    n, k = 30000, 4
+    f, src, nrm, trg, rng = _setup(111, n, np_=6, pts=64, seed=14, n_trg=4000)
+    den = torch.tensor(rng.normal(size=(k, n, 1)), dtype=torch.float64, device="cuda", requires_grad=True)
+    x = torch.tensor(trg, dtype=torch.float64, device="cuda", requires_grad=True)
+    wt = torch.tensor(rng.normal(size=(k, f.nt, 1)), dtype=torch.float64, device="cuda")
+    phi = fmmg_torch.fmm_apply(f, den, x, precision)
+    assert phi.shape == (k, f.nt, 1)
+    (phi * wt).sum().backward()
+    ref = torch.zeros(k, f.nt, dtype=torch.float64, device="cuda")
+    f.evaluate_device(den.detach().view(k, n).contiguous(), ref, k, precision)
+    f.sync()
+    assert torch.equal(phi.detach().view(k, f.nt), ref)
+    g, gt = f.adjoint(wt.cpu().numpy().reshape(k, -1), den.detach().cpu().numpy().reshape(k, -1), target_grad=True,
+                      k=k)
+    assert den.grad.shape == den.shape and x.grad.shape == x.shape
+    assert rel_l2(den.grad.cpu().numpy().ravel(), g.ravel()) <= 1e-14
+    assert rel_l2(x.grad.cpu().numpy(), gt.sum(0)) <= 1e-13
