@@ -38,6 +38,7 @@ METRIC = json.load(open(os.path.join(ROOT, "BASELINE.json")))["metric"] if os.pa
 UNIT = "points/s"
 WORKLOAD = "laplace_s_1M_sphere_clusters_np6_ptsmax64"
 CHECK_TARGETS = 4096
+WORKLOADS = ("laplace_1m", "stokes_dl_ellipsoids_1m", "laplace_adjoint_4m", "navier_np8_2m")
 
 
 def parse():
@@ -54,6 +55,9 @@ def parse():
                     help="time one form only (profiling runs); the headline then comes from it")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint timing")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
+    ap.add_argument("--workload", default="laplace_1m", choices=list(WORKLOADS),
+                    help="laplace_1m: the headline line (the default); the others print one line for the other "
+                         "configurations at their stated sizes")
     return ap.parse_args()
 
 
@@ -499,10 +503,177 @@ def speedups(results):
     return out
 
 
+def time_calls(torch, stream, call, steps, warmup, flush):
+    """Mean device time (CUDA events on the launching stream) of call() over
+    steps calls, after warmup untimed calls, with L2 flushed before each."""
+    for _ in range(warmup):
+        call()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for i in range(steps):
+        flush.zero_()
+        ev[i][0].record(stream)
+        call()
+        ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    return float(np.mean([a.elapsed_time(b) for a, b in ev]))
+
+
+def dense_laplace_grads(src, den, w, chunk=1024):
+    """FP64 dense sums on the GPU for the Laplace single layer, sources = targets
+    = src ([n, 3]), right-hand sides den and weights w ([k, n]): per right-hand
+    side the density gradient of <w, phi> (K^T w) and the target-position
+    gradient w(t) grad_t phi(t) (r = 0 pairs add nothing, as the kernel)."""
+    import torch
+    x = torch.from_numpy(src).cuda()
+    sig = torch.from_numpy(den).cuda()
+    ww = torch.from_numpy(w).cuda()
+    k, n = sig.shape
+    gden = torch.zeros(k, n, dtype=torch.float64, device="cuda")
+    gpos = torch.zeros(k, n, 3, dtype=torch.float64, device="cuda")
+    c = 1.0 / (4.0 * np.pi)
+    for t0 in range(0, n, chunk):
+        d = x[t0:t0 + chunk, None, :] - x[None, :, :]  # [c, n, 3]
+        r2 = (d * d).sum(-1)
+        bad = r2 < 1e-16
+        ir = torch.where(bad, torch.zeros_like(r2), r2.clamp_min(1e-300).rsqrt())
+        K = c * ir                                 # K(t, s)
+        gden += ww[:, t0:t0 + chunk] @ K           # sum_t w(t) K(t, s)
+        G = -c * (ir ** 3)[..., None] * d          # grad_t K(t, s)
+        gpos[:, t0:t0 + chunk, :] = torch.einsum("tsd,ks->ktd", G, sig) * ww[:, t0:t0 + chunk, None]
+    return gden.cpu().numpy(), gpos.cpu().numpy()
+
+
+def run_workload(args):
+    """The other configurations at their stated sizes, one JSON line each:
+    stokes_dl_ellipsoids_1m -- Stokes double layer, 1,048,576 points on 64
+      ellipsoids, np=6, the mixed form on 8 right-hand sides;
+    navier_np8_2m -- Navier single layer, 2,097,152 points (uniform + shell),
+      np=8, the mixed form on 32 right-hand sides, autotuned, graph replays;
+    laplace_adjoint_4m -- Laplace single layer, 4,194,304 uniform points, np=6,
+      16 right-hand sides: forward and adjoint (density and target-position
+      gradients of <w, phi>) times at the same precision and k, central
+      differences (h = 1e-4) at 64 random target coordinates, and the dense FP64
+      gradients on a 32,768-point subset problem."""
+    import torch
+    import fmmg
+    import workloads as W
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    line = {"workload": args.workload, "unit": UNIT, "data": "synthetic", "steps": args.steps, "warmup": args.warmup,
+            "l2": "256 MB written between timed steps"}
+    clocks = ClockSampler(0)
+    if args.workload in ("stokes_dl_ellipsoids_1m", "navier_np8_2m"):
+        cfg = W.config3() if args.workload.startswith("stokes") else W.config5()
+        n, k = cfg["src"].shape[0], cfg["den"].shape[0]
+        t0 = time.perf_counter()
+        f = fmmg.FMM3d(cfg["kernel"], np_=cfg["np"], pts_max=cfg["pts_max"], coefs=cfg.get("coefs", (1.0, 0.25)),
+                       device=0, stream=stream.cuda_stream)
+        f.setup(cfg["src"], cfg["nrm"])
+        setup_s = time.perf_counter() - t0
+        den = torch.from_numpy(np.ascontiguousarray(cfg["den"])).cuda()
+        out = torch.zeros(k, n * f.td, dtype=torch.float64, device="cuda")
+        idx = np.random.default_rng(W.SEED + 99).choice(n, CHECK_TARGETS, replace=False)
+        clocks.start()
+        tuned = None
+        if not args.no_autotune:
+            _, tuned = f.autotune(den, out, k, fmmg.PREC_MIXED, reps=1)
+        ms, kern, stage, launches, graph = time_form(f, torch, stream, den, out, n, k, fmmg.PREC_MIXED, args.steps,
+                                                     args.warmup, flush)
+        vals = out.cpu().numpy()
+        errs = [f.check(cfg["den"][r], vals[r], idx)[0] for r in range(k)]
+        ms64, _, _, _, _ = time_form(f, torch, stream, den[:1].contiguous(), out[:1], n, 1, fmmg.PREC_FP64,
+                                     max(2, args.steps // 4), 3, flush)
+        err64 = f.check(cfg["den"][0], out[0].cpu().numpy(), idx)[0]
+        line.update({"metric": "points/s (targets x right-hand sides / device time)", "points": n, "k_rhs": k,
+                     "kernel": cfg["kernel"], "np": cfg["np"], "value": n * k / (ms * 1e-3), "ms_per_step": ms,
+                     "dtype": "f32+f64", "rel_err_vs_dense_max": max(errs), "rel_err_vs_dense_per_rhs": errs,
+                     "check_targets": CHECK_TARGETS, "fp64_k1": {"ms": ms64, "points_per_s": n / (ms64 * 1e-3),
+                                                                 "rel_err_vs_dense": err64},
+                     "kernel_ms": kern, "launches": launches, "cuda_graph": graph, "tuning": tuned,
+                     "setup_s": setup_s})
+    else:  # laplace_adjoint_4m
+        cfg = W.config4()
+        src, D = cfg["src"], cfg["den"]
+        n, k = src.shape[0], D.shape[0]
+        rng = np.random.default_rng(W.SEED + 40)
+        w = rng.normal(size=(k, n))
+        f = fmmg.FMM3d(111, np_=6, pts_max=64, device=0, stream=stream.cuda_stream)
+        f.setup(src)
+        den = torch.from_numpy(D).cuda()
+        wd = torch.from_numpy(w).cuda()
+        out = torch.zeros(k, n, dtype=torch.float64, device="cuda")
+        g = torch.empty(k, n, dtype=torch.float64, device="cuda")
+        gt = torch.empty(k, n, 3, dtype=torch.float64, device="cuda")
+        clocks.start()
+        ms_fwd, _, _, _, _ = time_form(f, torch, stream, den, out, n, k, fmmg.PREC_FP64, args.steps, args.warmup, flush)
+        ms_mix, _, _, _, _ = time_form(f, torch, stream, den, out, n, k, fmmg.PREC_MIXED, args.steps, args.warmup,
+                                       flush)
+        res = {}
+        for key, call in (("adjoint_ms", lambda: f.adjoint_device(None, wd, g, None, k=k)),
+                          ("target_grad_ms", lambda: f.adjoint_device(den, wd, None, gt, k=k))):
+            res[key] = time_calls(torch, stream, call, max(2, args.steps // 4), 3, flush)
+        # the same gradients through torch.autograd (fmm_apply forward + backward)
+        import fmmg_torch
+        den_t = den.clone().requires_grad_(True)
+        trg_t = torch.from_numpy(src).cuda().requires_grad_(True)
+
+        def autograd_step():
+            phi = fmmg_torch.fmm_apply(f, den_t, trg_t, fmmg.PREC_FP64)
+            (phi.view(k, n) * wd).sum().backward()
+
+        res["autograd_step_ms"] = time_calls(torch, stream, autograd_step, 2, 1, flush)
+        den_t.grad = trg_t.grad = None
+        autograd_step()
+        gsum = gt.sum(0).cpu().numpy()
+        autograd_vs_device = {
+            "target_grad_rel_l2": float(np.linalg.norm(trg_t.grad.cpu().numpy() - gsum) / np.linalg.norm(gsum)),
+            "density_grad_rel_l2": float(torch.linalg.norm(den_t.grad - g) / torch.linalg.norm(g))}
+        # central differences of <w_0, phi_0> in 64 random target coordinates: one
+        # handle whose targets are the 128 displaced positions (sources fixed)
+        h = 1e-4
+        pick = rng.choice(n, 64, replace=False)
+        dims = rng.integers(0, 3, 64)
+        moved = np.repeat(src[pick], 2, axis=0)
+        moved[0::2, :][np.arange(64), dims] += h
+        moved[1::2, :][np.arange(64), dims] -= h
+        fd_h = fmmg.FMM3d(111, np_=6, pts_max=64, device=0, stream=stream.cuda_stream)
+        fd_h.setup(src, None, moved)
+        phi = fd_h.evaluate(D[0]).ravel()
+        fd = w[0, pick] * (phi[0::2] - phi[1::2]) / (2 * h)
+        adj = gt[0].cpu().numpy()[pick, dims]
+        fd_err = float(np.linalg.norm(fd - adj) / np.linalg.norm(adj))
+        fd_h.close()
+        # the dense FP64 gradients on a 32,768-point subset problem
+        m = 32768
+        sub = fmmg.FMM3d(111, np_=6, pts_max=64, device=0, stream=stream.cuda_stream)
+        sub.setup(src[:m])
+        gs, gts = sub.adjoint(w[:, :m], D[:, :m], target_grad=True, k=k)
+        dg, dgt = dense_laplace_grads(src[:m], D[:, :m], w[:, :m])
+        sub.close()
+        line.update({"metric": "adjoint time / forward time (same precision and k)", "points": n, "k_rhs": k,
+                     "kernel": 111, "np": 6, "dtype": "f64",
+                     "forward_fp64_ms": ms_fwd, "forward_mixed_ms": ms_mix, "adjoint_fp64_ms": res["adjoint_ms"],
+                     "target_grad_fp64_ms": res["target_grad_ms"], "autograd_step_ms": res["autograd_step_ms"],
+                     "autograd_vs_device": autograd_vs_device,
+                     "value": res["adjoint_ms"] / ms_fwd, "target_grad_vs_forward": res["target_grad_ms"] / ms_fwd,
+                     "central_differences": {"h": h, "coordinates": 64, "rel_l2_vs_adjoint": fd_err},
+                     "dense_subset": {"points": m, "density_grad_rel_l2": float(np.linalg.norm(gs.reshape(k, m) - dg)
+                                                                                 / np.linalg.norm(dg)),
+                                      "target_grad_rel_l2": float(np.linalg.norm(gts - dgt) / np.linalg.norm(dgt))}})
+    line["clocks"] = clocks.stop()
+    print(json.dumps(line))
+    f.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload != "laplace_1m":
+        run_workload(args)
     else:
         run_ours(args)
 

@@ -78,7 +78,8 @@ struct DevState {
   float* den32 = nullptr;  // the chunk's densities in FP32, [rhs / 8][n][8][sd] (what the pair kernels stage)
   bool mixedReady = false, mixedOpsStale = true;
   int mixedK = 0;                           // right-hand sides the mixed arrays hold
-  double mixedBudgetBytes = 48e9;           // device bytes for per-density work arrays
+  int mixedPassFor = 0, mixedPassK = 0;     // the last k that needed several passes, and its pass size
+  double mixedBudgetBytes = 120e9;          // device bytes for per-density work arrays (at most)
   // transposed FMM: inverted work lists, transposed operator tables, target-gradient buffer
   int32_t *adjNearRows = nullptr, *adjNearIdx = nullptr; int64_t *adjNearPtr = nullptr;
   int32_t *adjFarRows = nullptr, *adjFarIdx = nullptr; int64_t *adjFarPtr = nullptr;

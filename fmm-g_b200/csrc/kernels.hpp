@@ -92,9 +92,12 @@ struct KCoef {
   double mu, ve;
 };
 
-// One block.  Returns false (block left unset) for a coincident pair.
+// One block.  Returns false (block left unset) for a coincident pair.  For
+// the double-layer kernels rnp, when given, holds (x, y, z) . n computed by
+// the caller (the FP32 near field forms it in FP64: for close points on a
+// smooth surface it is O(r^2) while its FP32 rounding error is O(eps r)).
 template <int KT, typename R>
-FMMG_HD bool kblock(R x, R y, R z, const R* n, R* K, R mu, R ve) {
+FMMG_HD bool kblock(R x, R y, R z, const R* n, R* K, R mu, R ve, const R* rnp = nullptr) {
   const R r2 = x * x + y * y + z * z;
   if (r2 < R(1e-16)) return false;
   const R ir = fmmg_rsqrt<R>(r2);
@@ -103,7 +106,7 @@ FMMG_HD bool kblock(R x, R y, R z, const R* n, R* K, R mu, R ve) {
   if constexpr (KT == LAP_S_U) {  // :152-167
     K[0] = R(1) / (R(4) * PI) * ir;
   } else if constexpr (KT == LAP_D_U) {  // :169-185
-    R rn = x * n[0] + y * n[1] + z * n[2];
+    R rn = rnp ? *rnp : x * n[0] + y * n[1] + z * n[2];
     K[0] = -(R(1) / (R(4) * PI)) * ir3 * rn;
   } else if constexpr (KT == STK_F_U) {  // :194-219
     R oomu = R(1) / mu;
@@ -129,20 +132,20 @@ FMMG_HD bool kblock(R x, R y, R z, const R* n, R* K, R mu, R ve) {
     R c = (R(1) / (R(4) * PI)) * ir3;
     K[0] = c * x; K[1] = c * y; K[2] = c * z;
   } else if constexpr (KT == STK_D_U) {  // :262-283
-    R rn = x * n[0] + y * n[1] + z * n[2];
+    R rn = rnp ? *rnp : x * n[0] + y * n[1] + z * n[2];
     R C = -(R(6) / (R(8) * PI)) * ir3 * ir * ir * rn;
     K[0] = C * x * x; K[1] = C * x * y; K[2] = C * x * z;
     K[3] = C * y * x; K[4] = C * y * y; K[5] = C * y * z;
     K[6] = C * z * x; K[7] = C * z * y; K[8] = C * z * z;
   } else if constexpr (KT == STK_D_P) {  // :285-308
-    R rn = x * n[0] + y * n[1] + z * n[2];
+    R rn = rnp ? *rnp : x * n[0] + y * n[1] + z * n[2];
     R c = mu * (R(1) / (R(2) * PI));
     R ir5 = ir3 * ir * ir;
     K[0] = c * (n[0] * ir3 - R(3) * rn * x * ir5);
     K[1] = c * (n[1] * ir3 - R(3) * rn * y * ir5);
     K[2] = c * (n[2] * ir3 - R(3) * rn * z * ir5);
   } else if constexpr (KT == NAV_D_U) {  // :387-419
-    R rn = x * n[0] + y * n[1] + z * n[2];
+    R rn = rnp ? *rnp : x * n[0] + y * n[1] + z * n[2];
     R A = -(R(1) - R(2) * ve) / (R(8) * PI * (R(1) - ve)) * ir3;
     R B = (R(1) - R(2) * ve) / (R(8) * PI * (R(1) - ve)) * ir3;
     R C = R(-3) / (R(8) * PI * (R(1) - ve)) * ir3 * ir * ir * rn;
@@ -172,10 +175,10 @@ FMMG_UNROLL
 // KB right-hand sides at once: acc[r*TD + t] += sum_s K[t][s] den[r*SD + s];
 // the kernel block is evaluated once and applied to every density.
 template <int KT, int KB, typename R, typename A>
-FMMG_HD void kaccum_multi(R x, R y, R z, const R* n, const R* den, A* acc, R mu, R ve) {
+FMMG_HD void kaccum_multi(R x, R y, R z, const R* n, const R* den, A* acc, R mu, R ve, const R* rnp = nullptr) {
   constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD;
   R K[SD * TD];
-  if (!kblock<KT, R>(x, y, z, n, K, mu, ve)) return;
+  if (!kblock<KT, R>(x, y, z, n, K, mu, ve, rnp)) return;
 FMMG_UNROLL
   for (int r = 0; r < KB; r++)
 FMMG_UNROLL

@@ -136,11 +136,14 @@ __device__ __forceinline__ void mx_den(const float* __restrict__ s, float (&d)[N
 }
 
 // near field: U-list, direct W and X entries; grid (evaluator leaves, RHS blocks).
-// For the double-layer kernels (source normal, NRM) the offsets are formed from
-// hi/lo FP32 pairs of the box-centred coordinates, (x_hi - y_hi) + (x_lo - y_lo):
-// on densely sampled surfaces near-coincident pairs dominate the sum and
-// n.(x - y) cancels to curvature size, so plain FP32 offsets (rounded at box
-// scale) lose digits there; the hi difference of close points is exact.
+// The offsets are formed from hi/lo FP32 pairs of the box-centred
+// coordinates, (x_hi - y_hi) + (x_lo - y_lo): the hi difference of close
+// points is exact, so near-coincident pairs keep their separation.  For the
+// double-layer kernels (source normal, NRM) n.(x - y) is formed in FP64 from
+// those pairs and the normal's hi/lo pair: on densely sampled surfaces
+// near-coincident pairs dominate the sum and n.(x - y) cancels to curvature
+// size, O(r^2), while any FP32 rounding of the offset or the normal leaves an
+// O(eps r) error in it (relative error eps / (kappa r), 1e-3 at r = 1e-6).
 template <int KT, int KB>
 __global__ void __launch_bounds__(MX_THREADS)
     k_p2p_near32(const int32_t* __restrict__ rows, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
@@ -154,6 +157,8 @@ __global__ void __launch_bounds__(MX_THREADS)
   __shared__ float4 sPos[MX_TILE];
   __shared__ float4 sPosLo[MX_TILE];
   __shared__ float4 sNrm[NRM ? MX_TILE : 1];
+  __shared__ double sPosD[NRM ? 3 * MX_TILE : 1];  // FP64 box-centred source positions and normals (NRM)
+  __shared__ double sNrmD[NRM ? 3 * MX_TILE : 1];
   __shared__ __align__(16) float sDen[MX_TILE * SD * KB];
   __shared__ int64_t eBeg[MX_MAXE];
   __shared__ int32_t ePre[MX_MAXE + 1];
@@ -172,8 +177,12 @@ __global__ void __launch_bounds__(MX_THREADS)
     const int64_t t = t0 + tl;
     const bool act = t < tn;
     float tx = 0, ty = 0, tz = 0, txl = 0, tyl = 0, tzl = 0;
+    double tdx = 0, tdy = 0, tdz = 0;  // FP64 box-centred target (NRM)
     if (act) {
       const double dx = trg[3 * (tb + t)] - cx, dy = trg[3 * (tb + t) + 1] - cy, dz = trg[3 * (tb + t) + 2] - cz;
+      tdx = dx;
+      tdy = dy;
+      tdz = dz;
       tx = (float)dx;
       ty = (float)dy;
       tz = (float)dz;
@@ -195,7 +204,16 @@ __global__ void __launch_bounds__(MX_THREADS)
           const double dx = src[3 * s] - cx, dy = src[3 * s + 1] - cy, dz = src[3 * s + 2] - cz;
           sPos[i] = make_float4((float)dx, (float)dy, (float)dz, 0.f);
           sPosLo[i] = make_float4((float)(dx - (float)dx), (float)(dy - (float)dy), (float)(dz - (float)dz), 0.f);
-          if (NRM) sNrm[i] = make_float4((float)nrm[3 * s], (float)nrm[3 * s + 1], (float)nrm[3 * s + 2], 0.f);
+          if (NRM) {
+            const double nx = nrm[3 * s], ny = nrm[3 * s + 1], nz = nrm[3 * s + 2];
+            sNrm[i] = make_float4((float)nx, (float)ny, (float)nz, 0.f);
+            sPosD[3 * i] = dx;
+            sPosD[3 * i + 1] = dy;
+            sPosD[3 * i + 2] = dz;
+            sNrmD[3 * i] = nx;
+            sNrmD[3 * i + 1] = ny;
+            sNrmD[3 * i + 2] = nz;
+          }
           // the block's KB x SD densities: contiguous in the FP32 copy (rows of
           // 8 right-hand sides per source, zeros past the last one)
           const float* ds = den32 + (rhs0 >> 3) * den32Blk + s * 8 * SD + (rhs0 & 7) * SD;
@@ -214,15 +232,18 @@ __global__ void __launch_bounds__(MX_THREADS)
             const float4 q = sPos[i], ql = sPosLo[i];
             const float ox = (tx - q.x) + (txl - ql.x), oy = (ty - q.y) + (tyl - ql.y), oz = (tz - q.z) + (tzl - ql.z);
             float nv[3] = {0.f, 0.f, 0.f};
+            float rn = 0.f;
             if (NRM) {
               const float4 qn = sNrm[i];
               nv[0] = qn.x;
               nv[1] = qn.y;
               nv[2] = qn.z;
+              rn = (float)((tdx - sPosD[3 * i]) * sNrmD[3 * i] + (tdy - sPosD[3 * i + 1]) * sNrmD[3 * i + 1] +
+                           (tdz - sPosD[3 * i + 2]) * sNrmD[3 * i + 2]);
             }
             float d[KB * SD];
             mx_den<KB * SD>(&sDen[i * KB * SD], d);
-            kaccum_multi<KT, KB, float, float>(ox, oy, oz, NRM ? nv : nullptr, d, part, mu, ve);
+            kaccum_multi<KT, KB, float, float>(ox, oy, oz, NRM ? nv : nullptr, d, part, mu, ve, NRM ? &rn : nullptr);
           }
 #pragma unroll
           for (int c = 0; c < TD * KB; c++) acc[c] += (double)part[c];
@@ -1278,10 +1299,20 @@ static void run_mixed_blocks(const Plan& P, DevState& D, int kc, int mask, bool 
   if ((mask & 4) && npar > 0 && ntrg > 0) {
     dim3 grid(npar, (P.nEff32 + 31) / 32, kb);
     const float nrmfc = 1.0f / float(P.nReg32);
+    // vector kernels: 8 right-hand sides a thread when there are more than 4
+    // (each translation value loaded serves twice the multiply-adds; the pair
+    // kernels keep their 4)
 #define FMMG_HAD32(SD_, TD_)                                                                                   \
-  k_m2l_had32<SD_, TD_, KB><<<grid, 256, 0, st>>>(D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot,      \
-                                                   D.vTrgSlot, D.effDen32, effDR, D.m2lT32, D.effVal32, effVR, \
-                                                   P.nEff32, kc, nrmfc)
+  do {                                                                                                         \
+    if (kc > 4)                                                                                                \
+      k_m2l_had32<SD_, TD_, 8><<<dim3(npar, (P.nEff32 + 31) / 32, (kc + 7) / 8), 256, 0, st>>>(                \
+          D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot, D.vTrgSlot, D.effDen32, effDR, D.m2lT32,      \
+          D.effVal32, effVR, P.nEff32, kc, nrmfc);                                                             \
+    else                                                                                                       \
+      k_m2l_had32<SD_, TD_, KB><<<grid, 256, 0, st>>>(D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot,  \
+                                                       D.vTrgSlot, D.effDen32, effDR, D.m2lT32, D.effVal32,    \
+                                                       effVR, P.nEff32, kc, nrmfc);                            \
+  } while (0)
     if (P.sdm == 1 && P.tdm == 1 && D.hadPQ) {
       if (!r8) {  // planes of one right-hand side
         const size_t smem = pqx_smem_bytes<32>();
@@ -1496,9 +1527,29 @@ std::string dev_evaluate_mixed(const Plan& P, DevState& D, const double* dDen, d
   const double perRhs = 4.0 * P.nn * (ue + uc + de + dc + pad4(P.kUp) + pad4(P.kDn)) +
                         8.0 * P.nEff32 * (P.vSrcNodes.size() * P.sdm + P.vTrgNodes.size() * P.tdm) +
                         8.0 * (ns * P.sd + nt * P.td);
-  const double budget = D.mixedBudgetBytes;
-  int kmax = (int)std::max(1.0, std::floor(budget / std::max(perRhs, 1.0)));
-  int kc = std::min(k, std::min(kmax, 32));
+  // the budget: at most mixedBudgetBytes and 70% of the free device memory;
+  // arrays already held for mixedK right-hand sides are reused as they are.
+  // The pass size of a k is fixed by its first call (a graph capture of a
+  // later call queries nothing).
+  int kc = 0;
+  if (D.mixedReady && k <= D.mixedK) {
+    kc = k;
+  } else if (D.mixedReady && k == D.mixedPassFor) {
+    kc = D.mixedPassK;
+  } else {
+    size_t freeB = 0, totalB = 0;
+    FMMG_CK(cudaMemGetInfo(&freeB, &totalB));
+    const double budget = std::min(D.mixedBudgetBytes, 0.7 * (double)freeB);
+    int kmax = std::max(D.mixedReady ? D.mixedK : 0, (int)std::floor(budget / std::max(perRhs, 1.0)));
+    kmax = std::max(1, std::min(kmax, 32));
+    // several passes: a whole number of launch blocks (8 right-hand sides for
+    // scalar targets, 4 otherwise) per pass, so no block runs part-empty
+    const int blk = P.td == 1 ? 8 : 4;
+    if (k > kmax && kmax > blk) kmax -= kmax % blk;
+    kc = std::min(k, kmax);
+    D.mixedPassFor = k;
+    D.mixedPassK = kc;
+  }
   FMMG_TRY(dev_prepare_mixed(P, D, kc));
   const int64_t denStride = ns * P.sd, valStride = std::max<int64_t>(nt, 1) * P.td;
   int passes = 0;

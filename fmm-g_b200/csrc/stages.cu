@@ -599,6 +599,7 @@ void dev_free(DevState& D) {
   D.mixedReady = false;
   D.mixedOpsStale = true;
   D.mixedK = 0;
+  D.mixedPassFor = D.mixedPassK = 0;
 }
 
 std::string dev_upload_operators(const Plan& P, DevState& D) {
