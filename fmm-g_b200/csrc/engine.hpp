@@ -49,6 +49,12 @@ struct DevState {
   int64_t *nearWPtr = nullptr; int32_t *nearWIdx = nullptr;
   int64_t *nearXPtr = nullptr; int32_t *nearXIdx = nullptr;
   int32_t *farLeaves = nullptr; int64_t *farPtr = nullptr; int32_t *farIdx = nullptr;
+  // FP32 M2T work items (rows with long W lists split in chunks of far
+  // entries), the split rows, and their partial sums
+  int4* m2tItems = nullptr; int nM2tItems = 0;
+  int32_t *m2tSplitLeaf = nullptr, *m2tSplitBase = nullptr, *m2tSplitCnt = nullptr; int nM2tSplit = 0;
+  int64_t m2tPartTargets = 0;  // partial-sum rows per right-hand side
+  double* m2tPart = nullptr;
   int32_t *l2tLeaves = nullptr;
   int32_t *s2lNodes = nullptr; int64_t *s2lPtr = nullptr; int32_t *s2lIdx = nullptr;
   int32_t *s2mLeaves = nullptr;

@@ -78,7 +78,7 @@ __device__ __forceinline__ int64_t entry_source(int j, int ne, const int64_t* eB
 template <int TD, int KB>
 __device__ __forceinline__ void reduce_store(double* sRed, const double* acc, int tid, int tl, int sp, int TG, int S,
                                              bool act, double* __restrict__ val, int64_t trgIdx, int rhs0, int nrhs,
-                                             int64_t valStride) {
+                                             int64_t valStride, bool assign = false) {
   __syncthreads();
 #pragma unroll
   for (int c = 0; c < TD * KB; c++) sRed[tid * TD * KB + c] = acc[c];
@@ -91,7 +91,8 @@ __device__ __forceinline__ void reduce_store(double* sRed, const double* acc, in
       for (int c = 0; c < TD; c++) {
         double s = 0;
         for (int k = 0; k < S; k++) s += sRed[(tl + k * TG) * TD * KB + r * TD + c];
-        val[(int64_t)(rhs0 + r) * valStride + trgIdx * TD + c] += s;
+        double& v = val[(int64_t)(rhs0 + r) * valStride + trgIdx * TD + c];
+        v = assign ? s : v + s;
       }
     }
   }
@@ -409,12 +410,18 @@ __global__ void __launch_bounds__(THREADS)
             const double* __restrict__ samDE, int nDE, const float* __restrict__ uden,
             const float* __restrict__ dden, int64_t rhsStrideU, int64_t rhsStrideD,
             const int64_t* __restrict__ trgBeg, const int64_t* __restrict__ trgCnt, const double* __restrict__ trg,
-            double* __restrict__ val, int64_t valStride, int nrhs, float mu, float ve, int gmin) {
+            double* __restrict__ val, int64_t valStride, int nrhs, float mu, float ve, int gmin,
+            const int4* __restrict__ items, double* __restrict__ partial, int64_t partStride) {
   constexpr int SD = KTraits<KM>::SD, TD = KTraits<KM>::TD;
   __shared__ float4 sPos[MX_TILE];
   __shared__ __align__(16) float sDen[MX_TILE * SD * KB];
   __shared__ double sRed[THREADS * TD * KB];
-  const int row = blockIdx.x;
+  // with work items (M2T): item = (row, first far entry, end far entry,
+  // partial-sum base); base >= 0 stores the sums in partial[rhs][base + t]
+  // (a row split in several items, combined by k_e2t_combine), else they
+  // are added to the targets' values
+  const int4 it = items ? items[blockIdx.x] : make_int4(blockIdx.x, 0, 0, -1);
+  const int row = it.x;
   const int rhs0 = blockIdx.y * KB;
   const int g = rows[row];
   const int64_t tb = trgBeg[g], tn = trgCnt[g];
@@ -424,7 +431,9 @@ __global__ void __launch_bounds__(THREADS)
   const int S = THREADS / TG;
   const int tl = tid % TG, sp = tid / TG;
   const int own = (useOwn && depth[g] >= 2) ? 1 : 0;
-  const int64_t f0 = useFar ? farPtr[row] : 0, nf = useFar ? farPtr[row + 1] - f0 : 0;
+  const int64_t f0 = !useFar ? 0 : items ? it.y : farPtr[row];
+  const int64_t nf = !useFar ? 0 : items ? it.z - it.y : farPtr[row + 1] - f0;
+  const bool toPart = it.w >= 0;
   for (int64_t t0 = 0; t0 < tn; t0 += TG) {
     const int64_t t = t0 + tl;
     const bool act = t < tn;
@@ -475,7 +484,109 @@ __global__ void __launch_bounds__(THREADS)
         }
       }
     }
-    reduce_store<TD, KB>(sRed, acc, tid, tl, sp, TG, S, act, val, tb + t, rhs0, nrhs, valStride);
+    if (toPart)
+      reduce_store<TD, KB>(sRed, acc, tid, tl, sp, TG, S, act, partial, it.w + t, rhs0, nrhs, partStride, true);
+    else
+      reduce_store<TD, KB>(sRed, acc, tid, tl, sp, TG, S, act, val, tb + t, rhs0, nrhs, valStride);
+  }
+}
+
+// L2T, one warp per leaf (four leaves a CTA): the leaf's downward
+// equivalent densities (KB right-hand sides) are staged in the warp's slice of
+// shared memory, the DE surface (scaled per leaf) is shared by the CTA, and
+// the lanes split as TG targets x (32 / TG) source strides whose partial sums
+// meet through warp shuffles -- no CTA-wide barriers after the staging of the
+// surface, so the four leaves run independently.  The leaves come from the
+// list of leaves at depth >= 2.  Dynamic shared memory
+// nDE * 16 + 4 * nDE * KB * SD * 4 bytes.
+constexpr int L2T_WARPS = 4;
+template <int KM, int KB>
+__global__ void __launch_bounds__(32 * L2T_WARPS)
+    k_l2t32w(int nLeaves, const int32_t* __restrict__ leaves, const double* __restrict__ ctr,
+             const double* __restrict__ rad, const double* __restrict__ samDE, int nDE, const float* __restrict__ dden,
+             int64_t rhsStride, const int64_t* __restrict__ trgBeg, const int64_t* __restrict__ trgCnt,
+             const double* __restrict__ trg, double* __restrict__ val, int64_t valStride, int nrhs, float mu,
+             float ve) {
+  constexpr int SD = KTraits<KM>::SD, TD = KTraits<KM>::TD;
+  extern __shared__ __align__(16) unsigned char l2t_smem[];
+  float4* sSam = reinterpret_cast<float4*>(l2t_smem);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* sDen = reinterpret_cast<float*>(sSam + nDE) + (size_t)warp * nDE * KB * SD;
+  for (int j = threadIdx.x; j < nDE; j += blockDim.x)
+    sSam[j] = make_float4((float)samDE[3 * j], (float)samDE[3 * j + 1], (float)samDE[3 * j + 2], 0.f);
+  __syncthreads();
+  const int li = blockIdx.x * L2T_WARPS + warp;
+  if (li >= nLeaves) return;
+  const int g = leaves[li];
+  const int rhs0 = blockIdx.y * KB;
+  const float* dsrc = dden + (int64_t)g * nDE * SD;
+  for (int i = lane; i < nDE * KB; i += 32) {
+    const int j = i % nDE, q = i / nDE;
+#pragma unroll
+    for (int c = 0; c < SD; c++)
+      sDen[(j * KB + q) * SD + c] = rhs0 + q < nrhs ? dsrc[(int64_t)(rhs0 + q) * rhsStride + (int64_t)j * SD + c] : 0.f;
+  }
+  __syncwarp();
+  const int64_t tb = trgBeg[g], tn = trgCnt[g];
+  const double gx = ctr[3 * g], gy = ctr[3 * g + 1], gz = ctr[3 * g + 2];
+  const float r = (float)rad[g];
+  const int TG = tn > 16 ? 32 : (tn > 8 ? 16 : 8), S = 32 / TG;
+  const int tl = lane % TG, sp = lane / TG;
+  for (int64_t t0 = 0; t0 < tn; t0 += TG) {
+    const int64_t t = t0 + tl;
+    const bool act = t < tn;
+    float tx = 0, ty = 0, tz = 0;
+    if (act) {
+      tx = (float)(trg[3 * (tb + t)] - gx);
+      ty = (float)(trg[3 * (tb + t) + 1] - gy);
+      tz = (float)(trg[3 * (tb + t) + 2] - gz);
+    }
+    float part[TD * KB];
+#pragma unroll
+    for (int c = 0; c < TD * KB; c++) part[c] = 0.f;
+    if (act) {
+      for (int j = sp; j < nDE; j += S) {
+        const float4 q = sSam[j];
+        float d[KB * SD];
+        mx_den<KB * SD>(&sDen[j * KB * SD], d);
+        kaccum_multi<KM, KB, float, float>(tx - r * q.x, ty - r * q.y, tz - r * q.z, nullptr, d, part, mu, ve);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < TD * KB; c++)
+      for (int o = TG; o < 32; o <<= 1) part[c] += __shfl_xor_sync(0xffffffffu, part[c], o);
+    if (act && sp == 0) {
+#pragma unroll
+      for (int q = 0; q < KB; q++) {
+        if (rhs0 + q >= nrhs) break;
+#pragma unroll
+        for (int c = 0; c < TD; c++) val[(int64_t)(rhs0 + q) * valStride + (tb + t) * TD + c] += (double)part[q * TD + c];
+      }
+    }
+  }
+}
+
+// The rows split into several M2T items: per split row (a run of items with
+// consecutive partial bases, the first base in splitBase[i], splitCnt[i]
+// items of tn targets each) the partial sums are added in item order, then
+// to the targets' values -- the same order on every run.  One thread per
+// (target component, right-hand side).
+__global__ void k_e2t_combine(int nSplit, const int32_t* __restrict__ splitLeaf,
+                              const int32_t* __restrict__ splitBase, const int32_t* __restrict__ splitCnt,
+                              const int64_t* __restrict__ trgBeg, const int64_t* __restrict__ trgCnt, int td,
+                              const double* __restrict__ partial, int64_t partStride, double* __restrict__ val,
+                              int64_t valStride, int nrhs) {
+  const int i = blockIdx.x;
+  if (i >= nSplit) return;
+  const int g = splitLeaf[i];
+  const int64_t tb = trgBeg[g], tn = trgCnt[g];
+  const int base = splitBase[i], cnt = splitCnt[i];
+  for (int64_t q = threadIdx.x; q < tn * td * nrhs; q += blockDim.x) {
+    const int r = (int)(q / (tn * td));
+    const int64_t tc = q % (tn * td);
+    double s = 0.0;
+    for (int c = 0; c < cnt; c++) s += partial[(int64_t)r * partStride + (base + c * tn) * td + tc];
+    val[(int64_t)r * valStride + tb * td + tc] += s;
   }
 }
 
@@ -569,6 +680,76 @@ __global__ void __launch_bounds__(MX_SURF)
         *o = assign ? acc[q * TD + c] : *o + acc[q * TD + c];
       }
     }
+}
+
+// S2M (a leaf's own sources onto its UC check surface), one warp per leaf
+// and S2M_WARPS leaves a CTA: the warp stages up to S2M_CH of the leaf's
+// sources (positions, normals, the KB x SD FP32 densities) in its slice of
+// shared memory, its lanes own the surface points j = lane + 32 m and sum the
+// staged sources in order into FP32 -- for leaves of up to S2M_CH sources the
+// same sums as k_src2surf32, without CTA-wide barriers.  Later chunks of a
+// larger leaf add to the stored sums.
+constexpr int S2M_WARPS = 4, S2M_CH = 64;
+template <int KT, int KB>
+__global__ void __launch_bounds__(32 * S2M_WARPS)
+    k_s2m32w(int nLeaves, const int32_t* __restrict__ leaves, const int64_t* __restrict__ srcBeg,
+             const int64_t* __restrict__ srcCnt, const double* __restrict__ src, const double* __restrict__ nrm,
+             const float* __restrict__ den32, int64_t den32Blk, const double* __restrict__ ctr,
+             const double* __restrict__ rad, const double* __restrict__ sam, int nSurf, float* __restrict__ out,
+             int64_t ldo, int64_t outRhsStride, int nrhs, float mu, float ve) {
+  constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD, NRM = KTraits<KT>::NRM;
+  __shared__ float4 sPos[S2M_WARPS][S2M_CH];
+  __shared__ float4 sNrm[S2M_WARPS][NRM ? S2M_CH : 1];
+  __shared__ __align__(16) float sDen[S2M_WARPS][S2M_CH * KB * SD];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int li = blockIdx.x * S2M_WARPS + warp;
+  if (li >= nLeaves) return;
+  const int g = leaves[li];
+  const int rhs0 = blockIdx.y * KB;
+  const int64_t sb = srcBeg[g], sn = srcCnt[g];
+  const double cx = ctr[3 * g], cy = ctr[3 * g + 1], cz = ctr[3 * g + 2], r = rad[g];
+  for (int64_t c0 = 0; c0 < sn; c0 += S2M_CH) {
+    const int cnt = (int)min((int64_t)S2M_CH, sn - c0);
+    __syncwarp();
+    for (int i = lane; i < cnt; i += 32) {
+      const int64_t s = sb + c0 + i;
+      sPos[warp][i] = make_float4((float)(src[3 * s] - cx), (float)(src[3 * s + 1] - cy),
+                                  (float)(src[3 * s + 2] - cz), 0.f);
+      if (NRM) sNrm[warp][i] = make_float4((float)nrm[3 * s], (float)nrm[3 * s + 1], (float)nrm[3 * s + 2], 0.f);
+      const float* ds = den32 + (rhs0 >> 3) * den32Blk + s * 8 * SD + (rhs0 & 7) * SD;
+#pragma unroll
+      for (int q = 0; q < KB * SD; q++) sDen[warp][i * KB * SD + q] = ds[q];
+    }
+    __syncwarp();
+    for (int j = lane; j < nSurf; j += 32) {
+      const float px = (float)(r * sam[3 * j]), py = (float)(r * sam[3 * j + 1]), pz = (float)(r * sam[3 * j + 2]);
+      float acc[TD * KB];
+#pragma unroll
+      for (int c = 0; c < TD * KB; c++) acc[c] = 0.f;
+      for (int i = 0; i < cnt; i++) {
+        const float4 q = sPos[warp][i];
+        float nv[3] = {0.f, 0.f, 0.f};
+        if (NRM) {
+          const float4 qn = sNrm[warp][i];
+          nv[0] = qn.x;
+          nv[1] = qn.y;
+          nv[2] = qn.z;
+        }
+        float d[KB * SD];
+        mx_den<KB * SD>(&sDen[warp][i * KB * SD], d);
+        kaccum_multi<KT, KB, float, float>(px - q.x, py - q.y, pz - q.z, NRM ? nv : nullptr, d, acc, mu, ve);
+      }
+#pragma unroll
+      for (int q = 0; q < KB; q++) {
+        if (rhs0 + q >= nrhs) break;
+#pragma unroll
+        for (int c = 0; c < TD; c++) {
+          float* o = &out[(rhs0 + q) * outRhsStride + (int64_t)g * ldo + (int64_t)j * TD + c];
+          *o = c0 == 0 ? acc[q * TD + c] : *o + acc[q * TD + c];
+        }
+      }
+    }
+  }
 }
 
 // s += a b and s += a conj(b) as four FMAs into the accumulator (a product
@@ -801,15 +982,15 @@ __global__ void __launch_bounds__(128)
 // the 32 shared-memory banks (2-way conflicts at most across right-hand sides)
 constexpr int r8_pad(int s) { return s + ((4 - s % 16) + 16) % 16; }
 template <int NP>
-constexpr size_t r8_fwd_smem() {  // cube + X1 + X2 (padded planes) + twiddles
+constexpr size_t r8_fwd_smem() {  // cube + X1 + X2 (padded planes) + twiddles + roots
   using F = FftDims32<NP>;
   return sizeof(float) * NP * NP * NP * 8 +
-         sizeof(float2) * (8 * r8_pad(NP * NP * F::NH) + 8 * r8_pad(NP * F::N * F::NH) + F::N * NP);
+         sizeof(float2) * (8 * r8_pad(NP * NP * F::NH) + 8 * r8_pad(NP * F::N * F::NH) + F::N * NP + F::N);
 }
 template <int NP>
-constexpr size_t r8_inv_smem() {  // Y1 + Y2 (padded planes) + twiddles
+constexpr size_t r8_inv_smem() {  // Y1 + Y2 (padded planes) + twiddles + roots
   using F = FftDims32<NP>;
-  return sizeof(float2) * (8 * r8_pad(NP * NP * F::NH) + 8 * r8_pad(NP * F::N * F::NH) + F::N * NP);
+  return sizeof(float2) * (8 * r8_pad(NP * NP * F::NH) + 8 * r8_pad(NP * F::N * F::NH) + F::N * NP + F::N);
 }
 
 __device__ __forceinline__ void r8_load(const float2* p, float2 (&v)[8]) {
@@ -827,14 +1008,35 @@ __device__ __forceinline__ void r8_store(float2* p, const float2 (&v)[8]) {
   for (int i = 0; i < 4; i++) q[i] = make_float4(v[2 * i].x, v[2 * i].y, v[2 * i + 1].x, v[2 * i + 1].y);
 }
 template <int NP>
-__device__ __forceinline__ void r8_twiddles(float2* twb) {
+__device__ __forceinline__ void r8_twiddles(float2* twb, float2* roots) {
   using F = FftDims32<NP>;
-  for (int i = threadIdx.x; i < F::N * NP; i += blockDim.x) {
-    const int k = i / NP, b = i % NP;
+  for (int i = threadIdx.x; i < F::N * NP + F::N; i += blockDim.x) {
+    const int m = i < F::N * NP ? ((i / NP) * (i % NP + F::H)) % F::N : i - F::N * NP;
     double sn, cs;
-    sincospi(2.0 * ((k * (b + F::H)) % F::N) / F::N, &sn, &cs);
-    twb[i] = make_float2((float)cs, (float)-sn);
+    sincospi(2.0 * m / F::N, &sn, &cs);
+    (i < F::N * NP ? twb[i] : roots[m]) = make_float2((float)cs, (float)-sn);
   }
+}
+// The line transforms with the twiddles in registers: twb[k][b] is the root
+// w^m, m = k (b + H) mod N, so with both loops unrolled each product names
+// its root at compile time and the N roots are held per thread as packed
+// pairs.  Forward products s += a w (r8_cmac) take (w.x, w.y) and (w.y, w.x);
+// inverse products s += a conj(w) (r8_cmacc) take (w.x, w.x) and (w.y, w.y).
+// Each is two packed FP32x2 FMAs with the same per-component order as the
+// scalar helpers, so the results are the same.
+template <int N, int H>
+struct R8Idx {
+  static constexpr int at(int k, int b) { return (k * (b + H)) % N; }
+};
+__device__ __forceinline__ void r8_cmac2(unsigned long long& s, unsigned long long axx, unsigned long long nayy,
+                                         unsigned long long wp, unsigned long long ws) {
+  pq_fma2(s, axx, wp);   // (s.x + a.x w.x, s.y + a.x w.y)
+  pq_fma2(s, nayy, ws);  // (s.x - a.y w.y, s.y + a.y w.x)
+}
+__device__ __forceinline__ void r8_cmacc2(unsigned long long& s, unsigned long long a, unsigned long long aswp,
+                                          unsigned long long wxx, unsigned long long wyy) {
+  pq_fma2(s, a, wxx);     // (s.x + a.x w.x, s.y + a.y w.x)
+  pq_fma2(s, aswp, wyy);  // (s.x + a.y w.y, s.y - a.x w.y)
 }
 
 template <int NP>
@@ -849,12 +1051,14 @@ __global__ void __launch_bounds__(256)
   float2* X1 = reinterpret_cast<float2*>(r8_smem);      // [8][NP][NP][NH]
   float2* X2 = X1 + S1 * 8;                              // [8][NP][N][NH]
   float2* twb = X2 + S2 * 8;                             // [N][NP]
-  float* cube = reinterpret_cast<float*>(twb + N * NP);  // [8][NP][NP][NP]
+  float2* roots = twb + N * NP;                          // [N]
+  float* cube = reinterpret_cast<float*>(roots + N);     // [8][NP][NP][NP]
   const int slot = blockIdx.x;
   const int v = nodes[slot];
   const int r0 = blockIdx.y * 8;
   const int tid = threadIdx.x;
-  r8_twiddles<NP>(twb);
+  using IX = R8Idx<N, F::H>;
+  r8_twiddles<NP>(twb, roots);
   const float scl = (float)exp2((double)(depth[v] + rootLevel) * deg);
   for (int i = tid; i < S3 * 8; i += blockDim.x) cube[i] = 0.f;
   __syncthreads();
@@ -866,22 +1070,28 @@ __global__ void __launch_bounds__(256)
         uden[(int64_t)(r0 + r) * udenRhs + (int64_t)v * nUE + j] * scl;
   }
   __syncthreads();
+  unsigned long long wp[N], ws[N];  // the roots as (w.x, w.y) and (w.y, w.x)
+#pragma unroll
+  for (int m = 0; m < N; m++) {
+    const float2 w = roots[m];
+    wp[m] = pq_pk(w.x, w.y);
+    ws[m] = pq_pk(w.y, w.x);
+  }
   // x pass (real -> half spectrum): a thread owns one x line of one right-hand side
   for (int i = tid; i < NP * NP * 8; i += blockDim.x) {
     const int row = i % (NP * NP), r = i / (NP * NP);  // row = zb * NP + yb
-    float c[NP];
+    unsigned long long cc[NP];
 #pragma unroll
-    for (int xb = 0; xb < NP; xb++) c[xb] = cube[r * S3 + row * NP + xb];
-#pragma unroll 1
-    for (int kx = 0; kx < NH; kx++) {  // rolled: twiddles stay in shared memory (warp-wide broadcast)
-      float2 s = make_float2(0.f, 0.f);
+    for (int xb = 0; xb < NP; xb++) {
+      const float c = cube[r * S3 + row * NP + xb];
+      cc[xb] = pq_pk(c, c);
+    }
 #pragma unroll
-      for (int xb = 0; xb < NP; xb++) {
-        const float2 w = twb[kx * NP + xb];
-        s.x += c[xb] * w.x;
-        s.y += c[xb] * w.y;
-      }
-      X1[r * S1 + row * NH + kx] = s;
+    for (int kx = 0; kx < NH; kx++) {
+      unsigned long long s = 0ull;
+#pragma unroll
+      for (int xb = 0; xb < NP; xb++) pq_fma2(s, cc[xb], wp[IX::at(kx, xb)]);
+      X1[r * S1 + row * NH + kx] = pq_unpk(s);
     }
   }
   __syncthreads();
@@ -889,15 +1099,19 @@ __global__ void __launch_bounds__(256)
   // ky outputs
   for (int i = tid; i < NH * NP * 8; i += blockDim.x) {
     const int kx = i % NH, zb = (i / NH) % NP, r = i / (NH * NP);
-    float2 c[NP];
+    unsigned long long axx[NP], nayy[NP];
 #pragma unroll
-    for (int yb = 0; yb < NP; yb++) c[yb] = X1[r * S1 + (zb * NP + yb) * NH + kx];
-#pragma unroll 1
+    for (int yb = 0; yb < NP; yb++) {
+      const float2 c = X1[r * S1 + (zb * NP + yb) * NH + kx];
+      axx[yb] = pq_pk(c.x, c.x);
+      nayy[yb] = pq_pk(-c.y, c.y);
+    }
+#pragma unroll
     for (int ky = 0; ky < N; ky++) {
-      float2 s = make_float2(0.f, 0.f);
+      unsigned long long s = 0ull;
 #pragma unroll
-      for (int yb = 0; yb < NP; yb++) r8_cmac(s, c[yb], twb[ky * NP + yb]);
-      X2[r * S2 + (zb * N + ky) * NH + kx] = s;
+      for (int yb = 0; yb < NP; yb++) r8_cmac2(s, axx[yb], nayy[yb], wp[IX::at(ky, yb)], ws[IX::at(ky, yb)]);
+      X2[r * S2 + (zb * N + ky) * NH + kx] = pq_unpk(s);
     }
   }
   __syncthreads();
@@ -906,15 +1120,19 @@ __global__ void __launch_bounds__(256)
   float2* out = effDen + blockIdx.y * blkStride + (int64_t)slot * nEff * 8;
   for (int i = tid; i < NH * N * 8; i += blockDim.x) {
     const int r = i & 7, kx = (i >> 3) % NH, ky = (i >> 3) / NH;
-    float2 c[NP];
+    unsigned long long axx[NP], nayy[NP];
 #pragma unroll
-    for (int zb = 0; zb < NP; zb++) c[zb] = X2[r * S2 + (zb * N + ky) * NH + kx];
-#pragma unroll 1
+    for (int zb = 0; zb < NP; zb++) {
+      const float2 c = X2[r * S2 + (zb * N + ky) * NH + kx];
+      axx[zb] = pq_pk(c.x, c.x);
+      nayy[zb] = pq_pk(-c.y, c.y);
+    }
+#pragma unroll
     for (int kz = 0; kz < N; kz++) {
-      float2 s = make_float2(0.f, 0.f);
+      unsigned long long s = 0ull;
 #pragma unroll
-      for (int zb = 0; zb < NP; zb++) r8_cmac(s, c[zb], twb[kz * NP + zb]);
-      out[((int64_t)(kz * N + ky) * NH + kx) * 8 + r] = s;
+      for (int zb = 0; zb < NP; zb++) r8_cmac2(s, axx[zb], nayy[zb], wp[IX::at(kz, zb)], ws[IX::at(kz, zb)]);
+      out[((int64_t)(kz * N + ky) * NH + kx) * 8 + r] = pq_unpk(s);
     }
   }
 }
@@ -934,13 +1152,22 @@ __global__ void __launch_bounds__(256)
   float2* Y1 = reinterpret_cast<float2*>(r8_smem);  // [8][NP][NP][NH]
   float2* Y2 = Y1 + S1 * 8;                          // [8][NP][N][NH]
   float2* twb = Y2 + S2 * 8;                         // [N][NP]
+  float2* roots = twb + N * NP;                      // [N]
   const int slot = blockIdx.x;
   const int node = nodes[slot];
   const int r0 = blockIdx.y * 8;
   const int tid = threadIdx.x;
+  using IX = R8Idx<N, F::H>;
   const float2* Xg = effVal + blockIdx.y * blkStride + (int64_t)slot * nEff * 8;
-  r8_twiddles<NP>(twb);
+  r8_twiddles<NP>(twb, roots);
   __syncthreads();
+  unsigned long long wxx[N], wyy[N];  // the roots as (w.x, w.x) and (w.y, w.y)
+#pragma unroll
+  for (int m = 0; m < N; m++) {
+    const float2 w = roots[m];
+    wxx[m] = pq_pk(w.x, w.x);
+    wyy[m] = pq_pk(w.y, w.y);
+  }
   // z pass, band outputs only: a thread owns one z line (kx, ky) of one
   // right-hand side, right-hand side fastest as in HBM
   for (int i = tid; i < NH * N * 8; i += blockDim.x) {
@@ -948,32 +1175,34 @@ __global__ void __launch_bounds__(256)
     float2 c[N];
 #pragma unroll
     for (int kz = 0; kz < N; kz++) c[kz] = Xg[((kz * N + ky) * NH + kx) * 8 + r];  // all loads of the line first
-    float2 s[NP];
+    unsigned long long s[NP];
 #pragma unroll
-    for (int zb = 0; zb < NP; zb++) s[zb] = make_float2(0.f, 0.f);
+    for (int zb = 0; zb < NP; zb++) s[zb] = 0ull;
 #pragma unroll
     for (int kz = 0; kz < N; kz++) {
+      const unsigned long long a = pq_pk(c[kz].x, c[kz].y), asw = pq_pk(c[kz].y, -c[kz].x);
 #pragma unroll
-      for (int zb = 0; zb < NP; zb++) r8_cmacc(s[zb], c[kz], twb[kz * NP + zb]);
+      for (int zb = 0; zb < NP; zb++) r8_cmacc2(s[zb], a, asw, wxx[IX::at(kz, zb)], wyy[IX::at(kz, zb)]);
     }
 #pragma unroll
-    for (int zb = 0; zb < NP; zb++) Y2[r * S2 + (zb * N + ky) * NH + kx] = s[zb];
+    for (int zb = 0; zb < NP; zb++) Y2[r * S2 + (zb * N + ky) * NH + kx] = pq_unpk(s[zb]);
   }
   __syncthreads();
   // y pass: a thread owns one y line (kx, zb) of one right-hand side
   for (int i = tid; i < NH * NP * 8; i += blockDim.x) {
     const int kx = i % NH, zb = (i / NH) % NP, r = i / (NH * NP);
-    float2 s[NP];
+    unsigned long long s[NP];
 #pragma unroll
-    for (int yb = 0; yb < NP; yb++) s[yb] = make_float2(0.f, 0.f);
-#pragma unroll 1
+    for (int yb = 0; yb < NP; yb++) s[yb] = 0ull;
+#pragma unroll
     for (int ky = 0; ky < N; ky++) {
       const float2 c = Y2[r * S2 + (zb * N + ky) * NH + kx];
+      const unsigned long long a = pq_pk(c.x, c.y), asw = pq_pk(c.y, -c.x);
 #pragma unroll
-      for (int yb = 0; yb < NP; yb++) r8_cmacc(s[yb], c, twb[ky * NP + yb]);
+      for (int yb = 0; yb < NP; yb++) r8_cmacc2(s[yb], a, asw, wxx[IX::at(ky, yb)], wyy[IX::at(ky, yb)]);
     }
 #pragma unroll
-    for (int yb = 0; yb < NP; yb++) Y1[r * S1 + (zb * NP + yb) * NH + kx] = s[yb];
+    for (int yb = 0; yb < NP; yb++) Y1[r * S1 + (zb * NP + yb) * NH + kx] = pq_unpk(s[yb]);
   }
   __syncthreads();
   for (int i = tid; i < nDC * 8; i += blockDim.x) {  // x pass (c2r) at the surface points
@@ -1030,9 +1259,73 @@ static std::vector<float> transpose_pad(const std::vector<double>& W, int n, int
 }
 
 // Work arrays for a chunk of kc right-hand sides, and the FP32 operator copies.
+// M2T work items.  A far row's cost is its targets x W entries x UE points;
+// rows above a cap (the total over 6 items per SM, at least 8,192 pairs) are
+// split into near-equal runs of entries, each item writing its own partial
+// sums; items run longest first.
+static void m2t_items(const Plan& P, int numSMs, std::vector<int4>& items, std::vector<int32_t>& splitLeaf,
+                      std::vector<int32_t>& splitBase, std::vector<int32_t>& splitCnt, int64_t& partTargets) {
+  items.clear();
+  splitLeaf.clear();
+  splitBase.clear();
+  splitCnt.clear();
+  partTargets = 0;
+  const int nr = (int)P.farLeaves.size();
+  std::vector<double> cost;
+  double total = 0;
+  for (int r = 0; r < nr; r++)
+    total += (double)P.trgCnt[P.farLeaves[r]] * P.nUE * (P.farUE.ptr[r + 1] - P.farUE.ptr[r]);
+  const double cap = std::max(8192.0, total / (6.0 * numSMs));
+  for (int r = 0; r < nr; r++) {
+    const int64_t e0 = P.farUE.ptr[r], ne = P.farUE.ptr[r + 1] - e0;
+    const int64_t tn = P.trgCnt[P.farLeaves[r]];
+    const double per = (double)std::max<int64_t>(tn, 1) * P.nUE;
+    const int64_t chunks = std::max<int64_t>(1, std::min<int64_t>(ne, (int64_t)std::ceil(per * ne / cap)));
+    if (chunks == 1) {
+      items.push_back(make_int4(r, (int)e0, (int)(e0 + ne), -1));
+      cost.push_back(per * ne);
+      continue;
+    }
+    splitLeaf.push_back(P.farLeaves[r]);
+    splitBase.push_back((int32_t)partTargets);
+    splitCnt.push_back((int32_t)chunks);
+    for (int64_t c = 0; c < chunks; c++) {
+      const int64_t a = e0 + ne * c / chunks, b = e0 + ne * (c + 1) / chunks;
+      items.push_back(make_int4(r, (int)a, (int)b, (int)(partTargets + c * tn)));
+      cost.push_back(per * (b - a));
+    }
+    partTargets += chunks * tn;
+  }
+  std::vector<int> order(items.size());
+  for (size_t i = 0; i < order.size(); i++) order[i] = (int)i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+  std::vector<int4> sorted(items.size());
+  for (size_t i = 0; i < order.size(); i++) sorted[i] = items[order[i]];
+  items.swap(sorted);
+}
+
 static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
   const size_t ue = (size_t)P.nUE * P.sdm, uc = (size_t)P.nUC * P.tdm;
   const size_t de = (size_t)P.nDE * P.sdm, dc = (size_t)P.nDC * P.tdm;
+  if (!D.m2tItems && !P.farLeaves.empty()) {
+    std::vector<int4> items;
+    std::vector<int32_t> sl, sb, sc;
+    m2t_items(P, D.numSMs, items, sl, sb, sc, D.m2tPartTargets);
+    FMMG_TRY(dalloc(D, D.m2tItems, items.size()));
+    FMMG_CK(cudaMemcpy(D.m2tItems, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    D.nM2tItems = (int)items.size();
+    D.nM2tSplit = (int)sl.size();
+    auto put = [&](int32_t*& dst, const std::vector<int32_t>& v) -> std::string {
+      FMMG_TRY(dalloc(D, dst, v.size()));
+      FMMG_CK(cudaMemcpy(dst, v.data(), v.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+      return std::string();
+    };
+    if (!sl.empty()) {
+      FMMG_TRY(put(D.m2tSplitLeaf, sl));
+      FMMG_TRY(put(D.m2tSplitBase, sb));
+      FMMG_TRY(put(D.m2tSplitCnt, sc));
+    }
+  }
   // rank-sized buffers take the largest rank a pinv can have, so factors
   // recomputed for a replaced table (Plan::refactor_c2e) always fit
   const int kUpMax = pad4((int)std::min(ue, uc)), kDnMax = pad4((int)std::min(de, dc));
@@ -1053,6 +1346,7 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
     FMMG_TRY(dalloc(D, D.denK, (size_t)kc * P.ns * P.sd));
     FMMG_TRY(dalloc(D, D.den32, kc8 * P.ns * P.sd));
     FMMG_TRY(dalloc(D, D.valK, (size_t)kc * std::max<int64_t>(P.nt, 1) * P.td));
+    FMMG_TRY(dalloc(D, D.m2tPart, (size_t)kc * std::max<int64_t>(D.m2tPartTargets, 1) * P.tdm));
     if (!D.l2l32) {
       FMMG_TRY(dalloc(D, D.l2l32, P.l2l.size()));
       FMMG_TRY(dalloc(D, D.m2lT32, P.m2lT32.size()));
@@ -1165,7 +1459,7 @@ static void run_mixed_blocks(const Plan& P, DevState& D, int kc, int mask, bool 
   const float mu = (float)P.o.coefs[0], ve = (float)P.o.coefs[1];
   const int nl = (int)P.evtrLeaves.size();
   const int kb = (kc + KB - 1) / KB;
-  const int64_t denStride = P.ns * P.sd, valStride = std::max<int64_t>(P.nt, 1) * P.td;
+  const int64_t valStride = std::max<int64_t>(P.nt, 1) * P.td;
   const int64_t den32Blk = P.ns * 8 * P.sd;  // floats per block of 8 right-hand sides in D.den32
   // tc: the operator split for the tensor cores (3xTF32), used when that
   // path is on and the class is in the tuning mask (the wide CUDA-core tiles
@@ -1198,9 +1492,10 @@ static void run_mixed_blocks(const Plan& P, DevState& D, int kc, int mask, bool 
     cudaStreamWaitEvent(D.side, D.evFork, 0);
   }
   if ((mask & 1) && !P.s2mLeaves.empty()) {
-    k_src2surf32<KT, KB><<<dim3((unsigned)P.s2mLeaves.size(), kb), mx_surf_threads(P.nUC), 0, st>>>(
-        D.s2mLeaves, nullptr, nullptr, D.srcBeg, D.srcCnt, D.src, D.nrm, D.den32, den32Blk, D.ctr, D.rad, D.sam[1],
-        P.nUC, D.uchk32, uc, nn * uc, kc, mu, ve, 1);
+    const int nlv = (int)P.s2mLeaves.size();
+    k_s2m32w<KT, KB><<<dim3((nlv + S2M_WARPS - 1) / S2M_WARPS, kb), 32 * S2M_WARPS, 0, st>>>(
+        nlv, D.s2mLeaves, D.srcBeg, D.srcCnt, D.src, D.nrm, D.den32, den32Blk, D.ctr, D.rad, D.sam[1], P.nUC,
+        D.uchk32, uc, nn * uc, kc, mu, ve);
     ls->launches++;
   }
   cudaEventRecord(D.ev[EV_S2M], st);
@@ -1413,15 +1708,27 @@ static void run_mixed_blocks(const Plan& P, DevState& D, int kc, int mask, bool 
     const int32_t* rows = far ? D.farLeaves : D.l2tLeaves;
     if (nr == 0) return;
     constexpr int KM = kernel_mm(KT) < 0 ? KT : kernel_mm(KT);  // the equivalent kernel of KT (301 is its own)
-    if (far)
-      k_e2t32<KM, KB, MX_THREADS_FAR><<<dim3(nr, kb), MX_THREADS_FAR, 0, se>>>(
+    const int64_t partStride = std::max<int64_t>(D.m2tPartTargets, 1) * P.tdm;
+    if (far) {
+      k_e2t32<KM, KB, MX_THREADS_FAR><<<dim3(D.nM2tItems, kb), MX_THREADS_FAR, 0, se>>>(
           rows, D.farPtr, D.farIdx, own, far, D.depth, D.ctr, D.rad, D.sam[0], P.nUE, D.sam[2], P.nDE, D.uden32,
-          D.dden32, nn * ue, nn * de, D.trgBeg, D.trgCnt, D.trg, D.valK, valStride, kc, mu, ve, 32);
-    else
-      k_e2t32<KM, KB, MX_THREADS><<<dim3(nr, kb), MX_THREADS, 0, se>>>(
-          rows, D.farPtr, D.farIdx, own, far, D.depth, D.ctr, D.rad, D.sam[0], P.nUE, D.sam[2], P.nDE, D.uden32,
-          D.dden32, nn * ue, nn * de, D.trgBeg, D.trgCnt, D.trg, D.valK, valStride, kc, mu, ve, 8);
-    ls->launches++;
+          D.dden32, nn * ue, nn * de, D.trgBeg, D.trgCnt, D.trg, D.valK, valStride, kc, mu, ve, 32, D.m2tItems,
+          D.m2tPart, partStride);
+      ls->launches++;
+      if (D.nM2tSplit > 0) {
+        k_e2t_combine<<<D.nM2tSplit, 256, 0, se>>>(D.nM2tSplit, D.m2tSplitLeaf, D.m2tSplitBase, D.m2tSplitCnt,
+                                                    D.trgBeg, D.trgCnt, P.tdm, D.m2tPart, partStride, D.valK,
+                                                    valStride, kc);
+        ls->launches++;
+      }
+    } else {
+      const size_t smem = (size_t)P.nDE * sizeof(float4) + (size_t)L2T_WARPS * P.nDE * KB * P.sdm * sizeof(float);
+      cudaFuncSetAttribute(k_l2t32w<KM, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_l2t32w<KM, KB><<<dim3((nr + L2T_WARPS - 1) / L2T_WARPS, kb), 32 * L2T_WARPS, smem, se>>>(
+          nr, rows, D.ctr, D.rad, D.sam[2], P.nDE, D.dden32, nn * de, D.trgBeg, D.trgCnt, D.trg, D.valK, valStride,
+          kc, mu, ve);
+      ls->launches++;
+    }
   };
   if (mask & 8) e2t(0, 1, ovl ? D.side : st);
   if (ovl) cudaEventRecord(D.evSide, D.side);

@@ -600,6 +600,11 @@ void dev_free(DevState& D) {
   D.mixedOpsStale = true;
   D.mixedK = 0;
   D.mixedPassFor = D.mixedPassK = 0;
+  D.m2tItems = nullptr;
+  D.nM2tItems = D.nM2tSplit = 0;
+  D.m2tSplitLeaf = D.m2tSplitBase = D.m2tSplitCnt = nullptr;
+  D.m2tPartTargets = 0;
+  D.m2tPart = nullptr;
 }
 
 std::string dev_upload_operators(const Plan& P, DevState& D) {
