@@ -1,6 +1,7 @@
 // capi.cpp -- the C ABI of include/fmmg.h over the host plan and the device
 // engine.  Every entry point validates its arguments, catches host
 // exceptions and reports CUDA failures as status codes.
+#include <chrono>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -46,6 +47,7 @@ struct fmmg_handle {
   int64_t graphLaunches = 0;
   std::string graphNote;
   std::vector<double> trgHost;  // caller-order targets for check()
+  double setupMs[3] = {0, 0, 0};  // last setup: input checks, plan build, device upload (ms)
   std::string err;
 };
 
@@ -126,11 +128,6 @@ fmmg_status fmmg_create(const fmmg_options* o, fmmg_handle** out) {
     h->device = o->device;
     h->hostOnly = o->device < 0;
     h->plan.o = h->opt;
-    std::string e = h->plan.build_operators();
-    if (!e.empty()) {
-      delete h;
-      return fail(nullptr, FMMG_NOT_SUPPORTED, e);
-    }
     if (!h->hostOnly) {
       int ndev = 0;
       cudaError_t ce = cudaGetDeviceCount(&ndev);
@@ -139,6 +136,19 @@ fmmg_status fmmg_create(const fmmg_options* o, fmmg_handle** out) {
         delete h;
         return fail(nullptr, FMMG_CUDA_ERROR, m);
       }
+    }
+    {
+      // a device handle builds the operator tables' SVDs on its GPU (the same
+      // tables as the host build)
+      fmmg::LinalgDeviceScope scope(h->hostOnly ? -1 : o->device);
+      std::string e = h->plan.build_operators();
+      if (!e.empty()) {
+        delete h;
+        return fail(nullptr, FMMG_NOT_SUPPORTED, e);
+      }
+    }
+    if (!h->hostOnly) {
+      cudaError_t ce = cudaSuccess;
       h->dev.device = o->device;
       ce = cudaSetDevice(o->device);
       if (ce == cudaSuccess) {
@@ -173,6 +183,13 @@ fmmg_status fmmg_setup(fmmg_handle* h, int64_t ns, const double* src, const doub
   if (ns < 1 || !src) return fail(h, FMMG_INVALID_ARG, "need n_src >= 1 and src_xyz");
   if (nt < 0 || (nt > 0 && !trg)) return fail(h, FMMG_INVALID_ARG, "need n_trg >= 0 and trg_xyz");
   if (ns > (int64_t)1 << 31 || nt > (int64_t)1 << 31) return fail(h, FMMG_INVALID_ARG, "too many points");
+  using Clock = std::chrono::steady_clock;
+  auto t0 = Clock::now();
+  auto lap = [&](int i) {
+    const auto t1 = Clock::now();
+    h->setupMs[i] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    t0 = t1;
+  };
   if (fmmg::kernel_has_normal(h->opt.kt) && !nrm)
     return fail(h, FMMG_INVALID_ARG, "double-layer kernel needs src_nrm");
   const double R = std::pow(2.0, -h->opt.rootLevel);
@@ -201,6 +218,7 @@ fmmg_status fmmg_setup(fmmg_handle* h, int64_t ns, const double* src, const doub
       fmmg::Plan fresh;
       fresh.o = h->opt;
       if (h->tablesReplaced) {  // back to the built tables
+        fmmg::LinalgDeviceScope scope(h->hostOnly ? -1 : h->device);
         std::string e = fresh.build_operators();
         if (!e.empty()) return fail(h, FMMG_NOT_SUPPORTED, e);
       } else {
@@ -210,8 +228,10 @@ fmmg_status fmmg_setup(fmmg_handle* h, int64_t ns, const double* src, const doub
       h->tablesReplaced = false;
       h->setupDone = false;
     }
+    lap(0);
     std::string e = h->plan.build(h->opt, ns, src, nrm, nt, nt > 0 ? trg : src);
     if (!e.empty()) return fail(h, FMMG_INVALID_ARG, e);
+    lap(1);
     h->trgHost.assign(trg ? trg : src, (trg ? trg : src) + 3 * nt);
     if (!h->hostOnly) {
       e = fmmg::dev_upload(h->plan, h->dev, src, nrm, nt > 0 ? trg : src);
@@ -229,10 +249,22 @@ fmmg_status fmmg_setup(fmmg_handle* h, int64_t ns, const double* src, const doub
       h->dev.allocs.push_back(p);
       h->dValIO = (double*)p;
     }
+    lap(2);
     h->opsDirty = false;
     h->setupDone = true;
   }
   FMMG_GUARD(h)
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_setup_times(const fmmg_handle* h, double* ms, int n) {
+  if (!h || !ms || n < 9) return FMMG_INVALID_ARG;
+  if (!h->setupDone) return FMMG_STATE;
+  ms[0] = h->setupMs[0];
+  for (int i = 0; i < 6; i++) ms[1 + i] = h->plan.buildMs[i];
+  ms[7] = h->setupMs[2];
+  ms[8] = h->setupMs[0] + h->setupMs[1] + h->setupMs[2];
+  for (int i = 0; i < 4 && 9 + i < n; i++) ms[9 + i] = h->plan.opsMs[i];
   return FMMG_OK;
 }
 

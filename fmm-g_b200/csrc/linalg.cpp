@@ -10,11 +10,27 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "plan.hpp"
 
 namespace fmmg {
+
+// The device that builds the operator tables on this thread (-1: the host).
+// linalg_gpu.cu repeats the host arithmetic exactly, so the tables do not
+// depend on the choice.
+static thread_local int tl_linalgDevice = -1;
+void set_linalg_device(int device) { tl_linalgDevice = device; }
+std::string svd_onesided_device(int device, int m, int n, std::vector<double>& Z);
+std::string gemm_rows_device(int device, int rows, int inner, int w, const double* A, const double* B, double* C);
+
+// sqrt(1 + z^2), the Jacobi rotation's hypot(1, z): 1 + z^2 rounds to z^2
+// long before z^2 overflows, where the root is |z|
+static inline double jacobi_hyp1(double z) {
+  const double az = std::fabs(z);
+  return az > 1e100 ? az : std::sqrt(1.0 + z * z);
+}
 
 // A is m x n column-major with m >= n after an optional transpose.  Columns
 // are orthogonalised pairwise in tournament order (n/2 disjoint pairs per
@@ -29,10 +45,16 @@ static void svd_onesided(int m, int n, std::vector<double>& W /* m x n, becomes 
     std::copy(W.begin() + (size_t)j * m, W.begin() + (size_t)(j + 1) * m, Z.begin() + j * ld);
     Z[j * ld + m + j] = 1.0;
   }
+  bool onDevice = false;
+  if (tl_linalgDevice >= 0 && n >= 64) {  // on a copy: a failed device run leaves Z for the host loop
+    std::vector<double> Zd(Z);
+    onDevice = svd_onesided_device(tl_linalgDevice, m, n, Zd).empty();
+    if (onDevice) Z.swap(Zd);
+  }
   const int nn = n + (n & 1);
   std::vector<int> top(nn / 2), bot(nn / 2);
   for (int i = 0; i < nn / 2; i++) { top[i] = 2 * i; bot[i] = 2 * i + 1; }
-  for (int sweep = 0; sweep < 80; sweep++) {
+  for (int sweep = 0; sweep < (onDevice ? 0 : 80); sweep++) {
     int rotated = 0;
     for (int round = 0; round < nn - 1; round++) {
       // two pairs per iteration: their dot products share one loop (six
@@ -78,8 +100,8 @@ static void svd_onesided(int m, int n, std::vector<double>& W /* m x n, becomes 
           if (std::fabs(g[h]) <= 1e-15 * std::sqrt(a[h] * b[h])) continue;
           rotated++;
           double zeta = (b[h] - a[h]) / (2.0 * g[h]);
-          double t = std::copysign(1.0, zeta) / (std::fabs(zeta) + std::hypot(1.0, zeta));
-          double c = 1.0 / std::hypot(1.0, t), s = c * t;
+          double t = std::copysign(1.0, zeta) / (std::fabs(zeta) + jacobi_hyp1(zeta));
+          double c = 1.0 / jacobi_hyp1(t), s = c * t;
           double *zph = zp[h], *zqh = zq[h];
 #pragma omp simd
           for (size_t i = 0; i < ld; i++) {  // element-wise: the same arithmetic vectorised
@@ -261,6 +283,12 @@ static void gemm_rows_blocked(int rows, int inner, int w, const double* A, const
 std::vector<double> fold_c2e_m2m(const Plan& P) {
   const int ue = P.nUE * P.sdm, uc = P.nUC * P.tdm, k = P.kUp, w = 8 * ue;
   std::vector<double> T((size_t)k * w, 0.0), R((size_t)ue * w, 0.0);
+  if (tl_linalgDevice >= 0 &&
+      gemm_rows_device(tl_linalgDevice, k, uc, w, P.uc2ueF1.data(), P.m2m.data(), T.data()).empty() &&
+      gemm_rows_device(tl_linalgDevice, ue, k, w, P.uc2ueF2.data(), T.data(), R.data()).empty())
+    return R;
+  std::fill(T.begin(), T.end(), 0.0);
+  std::fill(R.begin(), R.end(), 0.0);
   gemm_rows_blocked(k, uc, w, P.uc2ueF1.data(), P.m2m.data(), T.data());
   gemm_rows_blocked(ue, k, w, P.uc2ueF2.data(), T.data(), R.data());
   return R;

@@ -1392,7 +1392,10 @@ static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
     FMMG_TRY(putT(D.tDnF1, pad_rows(P.dc2deF1, P.kDn, (int)dc), kDn4, (int)dc));
     FMMG_TRY(putT(D.tDnF2, pad_cols(P.dc2deF2, (int)de, P.kDn), (int)de, kDn4));
     // a parent's upward density straight from its children's: C2E up x M2M
-    const std::vector<double>& fold = P.folded_upward();
+    const std::vector<double>& fold = [&]() -> const std::vector<double>& {
+      LinalgDeviceScope scope(D.device);  // formed on this GPU on first use (the host's sums, bit for bit)
+      return P.folded_upward();
+    }();
     FMMG_TRY(put(D.m2mUp32, fold));
     FMMG_TRY(putT(D.tM2MUp, fold, (int)ue, (int)(8 * ue)));
     // the same six operators split into TF32 hi / lo parts for the tensor cores

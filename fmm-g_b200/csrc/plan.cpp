@@ -2,6 +2,7 @@
 #include "plan.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <list>
@@ -525,8 +526,17 @@ std::string Plan::build(const Options& opt, int64_t ns_, const double* src, cons
                         const double* trg) {
   o = opt;
   ns = ns_; nt = nt_;
+  using Clock = std::chrono::steady_clock;
+  auto t0 = Clock::now();
+  auto lap = [&](int i) {
+    const auto t1 = Clock::now();
+    buildMs[i] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    t0 = t1;
+  };
   build_tree(src);
+  lap(0);
   bin_targets(trg);
+  lap(1);
   flags.assign(nn, 0);
   center.resize(3 * (size_t)nn);
   radius.resize(nn);
@@ -543,9 +553,13 @@ std::string Plan::build(const Options& opt, int64_t ns_, const double* src, cons
     node_center(depth[n], &path[3 * (size_t)n], &center[3 * (size_t)n]);
     radius[n] = R0 / double(1 << depth[n]);  // let3d_mpi.cpp:1824-1827
   }
+  lap(2);
   build_lists();
+  lap(3);
   build_worklists();
+  lap(4);
   build_adjoint_lists();
+  lap(5);
   (void)nrmIn;
   return std::string();
 }
@@ -649,6 +663,7 @@ template <class S> void Plan::assign_operators(S&& s) {
   dc2deF1 = std::forward<S>(s).dc2deF1; dc2deF2 = std::forward<S>(s).dc2deF2;
   std::memcpy(transId, s.transId, sizeof(transId));
   upFold = std::forward<S>(s).upFold;
+  std::memcpy(opsMs, s.opsMs, sizeof(opsMs));
 }
 
 const std::vector<double>& Plan::folded_upward() const {
@@ -687,6 +702,13 @@ std::string Plan::build_operators_uncached() {
   }
   const double eps = std::pow(0.1, np + 1);  // matmgnt3d_mpi.cpp:37-40
   const int ue = nUE * sdm, uc = nUC * tdm, de = nDE * sdm, dc = nDC * tdm;
+  using Clock = std::chrono::steady_clock;
+  auto t0 = Clock::now();
+  auto lap = [&](int i) {
+    const auto t1 = Clock::now();
+    opsMs[i] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    t0 = t1;
+  };
   std::vector<double> A, Rm;
   // C2E up: pinv of the UE -> UC matrix
   mm_matrix_rt(mm, o.coefs, nUE, sam[0].data(), nUC, sam[1].data(), A);
@@ -695,6 +717,7 @@ std::string Plan::build_operators_uncached() {
   uc2ue.resize((size_t)ue * uc);
   for (int r = 0; r < ue; r++)
     for (int c = 0; c < uc; c++) uc2ue[(size_t)r * uc + c] = Rm[(size_t)c * ue + r];
+  lap(0);
   // C2E down
   mm_matrix_rt(mm, o.coefs, nDE, sam[2].data(), nDC, sam[3].data(), A);
   Rm.assign((size_t)de * dc, 0.0);
@@ -702,6 +725,7 @@ std::string Plan::build_operators_uncached() {
   dc2de.resize((size_t)de * dc);
   for (int r = 0; r < de; r++)
     for (int c = 0; c < dc; c++) dc2de[(size_t)r * dc + c] = Rm[(size_t)c * de + r];
+  lap(1);
   // (refactor_c2e recovers these factors from the explicit tables)
   // M2M / L2L octant matrices
   m2m.assign((size_t)uc * 8 * ue, 0.0);
@@ -723,6 +747,7 @@ std::string Plan::build_operators_uncached() {
     for (int r = 0; r < dc; r++)
       for (int c = 0; c < de; c++) l2l[((size_t)oc * dc + r) * de + c] = A[(size_t)c * dc + r];
   }
+  lap(2);
   // M2L translation spectra: the kernel from a point at 2*idx sampled on the
   // (2np)^3 regular grid, r2c transformed (matmgnt3d_mpi.cpp:385-411)
   int cnt = 0;
@@ -765,6 +790,7 @@ std::string Plan::build_operators_uncached() {
   };
   spectra(n, nEff, m2lT);
   spectra(2 * np - 1, nEff32, m2lT32);
+  lap(3);
   return std::string();
 }
 

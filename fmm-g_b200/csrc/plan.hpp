@@ -56,6 +56,15 @@ struct Plan {
   int nReg32 = 0, nEff32 = 0;
   std::vector<double> sam[4];  // UE, UC, DE, DC templates at unit radius scale, [n][3]
 
+  // wall time of the phases of the last build(), ms: sources into the tree,
+  // targets binned, node flags and centres, U/V/W/X lists, work lists, the
+  // adjoint's lists
+  double buildMs[6] = {0, 0, 0, 0, 0, 0};
+  // wall time of the operator set's build, ms (0 when it came from the
+  // process cache): C2E up pseudo-inverse, C2E down, M2M / L2L tables, M2L
+  // translation spectra
+  double opsMs[4] = {0, 0, 0, 0};
+
   // ---- tree
   int64_t ns = 0, nt = 0;
   int nn = 0, maxDepth = 0;
@@ -165,7 +174,14 @@ struct Plan {
   void node_center(int depth, const int* path, double* c) const;
 };
 
-// linear algebra used by the operator builder (linalg.cpp)
+// linear algebra used by the operator builder (linalg.cpp); with a device
+// set (>= 0) on the calling thread the SVDs and the fold run there
+// (linalg_gpu.cu), with bit-identical results
+void set_linalg_device(int device);
+struct LinalgDeviceScope {
+  explicit LinalgDeviceScope(int device) { set_linalg_device(device); }
+  ~LinalgDeviceScope() { set_linalg_device(-1); }
+};
 // the truncated pseudo-inverse of A (m x n column-major) from one SVD, both as
 // the explicit table R (n x m column-major; skipped when R is NULL) and in
 // factored form R = F2 F1, F1 = diag(1/s) U^T (k x m, row-major), F2 = V

@@ -74,6 +74,7 @@ SIGNATURES = {
     "fmmg_check": ([ctypes.c_void_p, _dp, _dp, ctypes.c_int64, _i64p, _dp, _dp, _dp], ctypes.c_int),
     "fmmg_info": ([ctypes.c_void_p, _ip, _ip, _i64p, _i64p, _ip], ctypes.c_int),
     "fmmg_stage_times": ([ctypes.c_void_p, _dp, ctypes.c_int], ctypes.c_int),
+    "fmmg_setup_times": ([ctypes.c_void_p, _dp, ctypes.c_int], ctypes.c_int),
     "fmmg_kernel_times": ([ctypes.c_void_p, _dp, ctypes.c_int], ctypes.c_int),
     "fmmg_plan_stats": ([ctypes.c_void_p, _i64p, ctypes.c_int], ctypes.c_int),
     "fmmg_launch_count": ([ctypes.c_void_p, _i64p], ctypes.c_int),
@@ -243,6 +244,15 @@ class FMM3d:
         self._chk(lib().fmmg_info(self.h, ctypes.byref(sd), ctypes.byref(td), ctypes.byref(nn), ctypes.byref(nl),
                                   ctypes.byref(md)))
         return dict(src_dof=sd.value, trg_dof=td.value, nodes=nn.value, leaves=nl.value, max_depth=md.value)
+
+    SETUP_PHASES = ("checks", "tree", "targets", "flags", "lists", "worklists", "adjoint_lists", "upload", "total",
+                    "ops_c2e_up", "ops_c2e_down", "ops_m2m_l2l", "ops_m2l_spectra")
+
+    def setup_times(self):
+        """Wall time of the last setup by phase, ms."""
+        ms = np.zeros(len(self.SETUP_PHASES))
+        self._chk(lib().fmmg_setup_times(self.h, _d(ms), len(ms)))
+        return dict(zip(self.SETUP_PHASES, ms.tolist()))
 
     def stage_times(self):
         ms = np.zeros(7)

@@ -187,6 +187,15 @@ fmmg_status fmmg_kernel_times(const fmmg_handle* h, double* ms, int n);
  * C2E x M2M product) and downward GEMMs (factored pseudo-inverses). */
 fmmg_status fmmg_plan_stats(const fmmg_handle* h, int64_t* stats, int n);
 
+/* Wall time of the last fmmg_setup, ms (n >= 9): input checks; the plan's
+ * phases -- sources into the tree, targets binned, node flags and centres,
+ * U/V/W/X lists, work lists, the adjoint's lists; the upload to the device
+ * (and its work arrays); the total.  With n >= 13 also the build of the
+ * handle's operator set at fmmg_create (0 when the process had it cached):
+ * C2E up pseudo-inverse, C2E down pseudo-inverse, M2M / L2L tables, M2L
+ * translation spectra. */
+fmmg_status fmmg_setup_times(const fmmg_handle* h, double* ms, int n);
+
 /* Number of this library's kernels launched by the last evaluate call. */
 fmmg_status fmmg_launch_count(const fmmg_handle* h, int64_t* n);
 
