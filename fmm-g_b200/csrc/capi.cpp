@@ -48,6 +48,7 @@ struct fmmg_handle {
   std::string graphNote;
   std::vector<double> trgHost;  // caller-order targets for check()
   double setupMs[3] = {0, 0, 0};  // last setup: input checks, plan build, device upload (ms)
+  bool treeOnDevice = true;       // device handles build the tree and bin the targets on the GPU
   std::string err;
 };
 
@@ -229,7 +230,8 @@ fmmg_status fmmg_setup(fmmg_handle* h, int64_t ns, const double* src, const doub
       h->setupDone = false;
     }
     lap(0);
-    std::string e = h->plan.build(h->opt, ns, src, nrm, nt, nt > 0 ? trg : src);
+    std::string e = h->plan.build(h->opt, ns, src, nrm, nt, nt > 0 ? trg : src,
+                                  !h->hostOnly && h->treeOnDevice ? h->device : -1);
     if (!e.empty()) return fail(h, FMMG_INVALID_ARG, e);
     lap(1);
     h->trgHost.assign(trg ? trg : src, (trg ? trg : src) + 3 * nt);
@@ -254,6 +256,13 @@ fmmg_status fmmg_setup(fmmg_handle* h, int64_t ns, const double* src, const doub
     h->setupDone = true;
   }
   FMMG_GUARD(h)
+  return FMMG_OK;
+}
+
+fmmg_status fmmg_set_tree_device(fmmg_handle* h, int on) {
+  if (!h) return fail(nullptr, FMMG_INVALID_ARG, "handle is NULL");
+  if (h->hostOnly && on) return fail(h, FMMG_STATE, "host-only handle");
+  h->treeOnDevice = on != 0;
   return FMMG_OK;
 }
 

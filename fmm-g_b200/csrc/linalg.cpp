@@ -152,7 +152,32 @@ int pinv_truncated(int m, int n, const double* A, double eps, double* R, std::ve
   }
   double smax = *std::max_element(S.begin(), S.end());
   double cutoff = eps * smax;
-  if (R) {
+  bool rDone = false;
+  if (R && tl_linalgDevice >= 0) {
+    // the same sums on the device: R(i, j) = sum over kept c, in order, of
+    // a_c(i) * (b_c(j) / s_c^2), one rounding per product and per sum
+    std::vector<int> cs;
+    for (int c = 0; c < N; c++)
+      if (S[c] >= cutoff && S[c] != 0.0) cs.push_back(c);
+    const int K = (int)cs.size();
+    std::vector<double> Ad((size_t)n * K), Bd((size_t)K * m), Cd((size_t)n * m, 0.0);
+    for (int r = 0; r < K; r++) {
+      const int c = cs[r];
+      const double inv2 = 1.0 / (S[c] * S[c]);
+      const double* w = &W[(size_t)c * M];
+      const double* v = &V[(size_t)c * N];
+      const double* a = tr ? w : v;  // length n
+      const double* b = tr ? v : w;  // length m
+      for (int i = 0; i < n; i++) Ad[(size_t)i * K + r] = a[i];
+      for (int j = 0; j < m; j++) Bd[(size_t)r * m + j] = b[j] * inv2;
+    }
+    if (gemm_rows_device(tl_linalgDevice, n, K, m, Ad.data(), Bd.data(), Cd.data()).empty()) {
+      for (int j = 0; j < m; j++)
+        for (int i = 0; i < n; i++) R[(size_t)j * n + i] = Cd[(size_t)i * m + j];
+      rDone = true;
+    }
+  }
+  if (R && !rDone) {
     std::fill(R, R + (size_t)n * m, 0.0);
     // For A = W V^T with W = U S: pinv(A) = V S^-2 W^T restricted to kept columns.
     for (int c = 0; c < N; c++) {

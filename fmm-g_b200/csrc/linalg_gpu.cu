@@ -28,9 +28,11 @@ __device__ __forceinline__ double lg_hyp1(double z) {
 }
 
 // One tournament round: warp w takes pair w (columns p < q of Z, ld apart,
-// first m rows the working matrix, then the n rows of V).  Lane 0 forms the
-// three dot products in index order; when the pair is not yet orthogonal all
-// lanes apply the rotation to both full columns.
+// first m rows the working matrix, then the n rows of V).  The warp loads the
+// columns 32 rows at a time (coalesced) and every lane forms the three dot
+// products in index order from the shuffled values -- the same sums in every
+// lane; when the pair is not yet orthogonal all lanes apply the rotation to
+// both full columns.
 __global__ void __launch_bounds__(256) k_jacobi_round(double* __restrict__ Z, long long ld, int m, int n,
                                                       const int2* __restrict__ pairs, int npair,
                                                       int* __restrict__ rotated) {
@@ -41,29 +43,24 @@ __global__ void __launch_bounds__(256) k_jacobi_round(double* __restrict__ Z, lo
   if (pq.y >= n) return;
   double* zp = Z + (long long)pq.x * ld;
   double* zq = Z + (long long)pq.y * ld;
-  double c = 0.0, s = 0.0;
-  int go = 0;
-  if (lane == 0) {
-    double a = 0.0, b = 0.0, g = 0.0;
-    for (int i = 0; i < m; i++) {
-      const double x = zp[i], y = zq[i];
+  double a = 0.0, b = 0.0, g = 0.0;
+  for (int base = 0; base < m; base += 32) {
+    const int i = base + lane;
+    const double xl = i < m ? zp[i] : 0.0, yl = i < m ? zq[i] : 0.0;
+    const int cnt = min(32, m - base);
+    for (int j = 0; j < cnt; j++) {
+      const double x = __shfl_sync(0xffffffffu, xl, j), y = __shfl_sync(0xffffffffu, yl, j);
       a = __dadd_rn(a, __dmul_rn(x, x));
       b = __dadd_rn(b, __dmul_rn(y, y));
       g = __dadd_rn(g, __dmul_rn(x, y));
     }
-    if (a != 0.0 && b != 0.0 && !(fabs(g) <= __dmul_rn(1e-15, __dsqrt_rn(__dmul_rn(a, b))))) {
-      go = 1;
-      const double zeta = __ddiv_rn(__dsub_rn(b, a), __dmul_rn(2.0, g));
-      const double t = __ddiv_rn(copysign(1.0, zeta), __dadd_rn(fabs(zeta), lg_hyp1(zeta)));
-      c = __ddiv_rn(1.0, lg_hyp1(t));
-      s = __dmul_rn(c, t);
-      atomicAdd(rotated, 1);
-    }
   }
-  go = __shfl_sync(0xffffffffu, go, 0);
-  if (!go) return;
-  c = __shfl_sync(0xffffffffu, c, 0);
-  s = __shfl_sync(0xffffffffu, s, 0);
+  if (a == 0.0 || b == 0.0 || fabs(g) <= __dmul_rn(1e-15, __dsqrt_rn(__dmul_rn(a, b)))) return;
+  const double zeta = __ddiv_rn(__dsub_rn(b, a), __dmul_rn(2.0, g));
+  const double t = __ddiv_rn(copysign(1.0, zeta), __dadd_rn(fabs(zeta), lg_hyp1(zeta)));
+  const double c = __ddiv_rn(1.0, lg_hyp1(t));
+  const double s = __dmul_rn(c, t);
+  if (lane == 0) atomicAdd(rotated, 1);
   for (long long i = lane; i < ld; i += 32) {
     const double x = zp[i], y = zq[i];
     zp[i] = __dsub_rn(__dmul_rn(c, x), __dmul_rn(s, y));

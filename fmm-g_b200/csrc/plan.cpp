@@ -523,7 +523,7 @@ void Plan::build_adjoint_lists() {
 }
 
 std::string Plan::build(const Options& opt, int64_t ns_, const double* src, const double* nrmIn, int64_t nt_,
-                        const double* trg) {
+                        const double* trg, int treeDevice) {
   o = opt;
   ns = ns_; nt = nt_;
   using Clock = std::chrono::steady_clock;
@@ -533,9 +533,23 @@ std::string Plan::build(const Options& opt, int64_t ns_, const double* src, cons
     buildMs[i] = std::chrono::duration<double, std::milli>(t1 - t0).count();
     t0 = t1;
   };
-  build_tree(src);
-  lap(0);
-  bin_targets(trg);
+  // targets that are the sources repeat the sources' partition exactly
+  const bool trgIsSrc = trg == src && nt == ns;
+  if (treeDevice >= 0) {
+    std::string e = tree_build_device(treeDevice, *this, src, trg, trgIsSrc);
+    if (!e.empty()) return e;
+    lap(0);
+  } else {
+    build_tree(src);
+    lap(0);
+    if (trgIsSrc) {
+      trgBeg = srcBeg;
+      trgCnt = srcCnt;
+      trgPerm = srcPerm;
+    } else {
+      bin_targets(trg);
+    }
+  }
   lap(1);
   flags.assign(nn, 0);
   center.resize(3 * (size_t)nn);

@@ -75,6 +75,7 @@ SIGNATURES = {
     "fmmg_info": ([ctypes.c_void_p, _ip, _ip, _i64p, _i64p, _ip], ctypes.c_int),
     "fmmg_stage_times": ([ctypes.c_void_p, _dp, ctypes.c_int], ctypes.c_int),
     "fmmg_setup_times": ([ctypes.c_void_p, _dp, ctypes.c_int], ctypes.c_int),
+    "fmmg_set_tree_device": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "fmmg_kernel_times": ([ctypes.c_void_p, _dp, ctypes.c_int], ctypes.c_int),
     "fmmg_plan_stats": ([ctypes.c_void_p, _i64p, ctypes.c_int], ctypes.c_int),
     "fmmg_launch_count": ([ctypes.c_void_p, _i64p], ctypes.c_int),
@@ -244,6 +245,11 @@ class FMM3d:
         self._chk(lib().fmmg_info(self.h, ctypes.byref(sd), ctypes.byref(td), ctypes.byref(nn), ctypes.byref(nl),
                                   ctypes.byref(md)))
         return dict(src_dof=sd.value, trg_dof=td.value, nodes=nn.value, leaves=nl.value, max_depth=md.value)
+
+    def set_tree_device(self, on=True):
+        """Build the octree and bin the targets on the GPU (the default for
+        device handles) or on the host, from the next setup on."""
+        self._chk(lib().fmmg_set_tree_device(self.h, 1 if on else 0))
 
     SETUP_PHASES = ("checks", "tree", "targets", "flags", "lists", "worklists", "adjoint_lists", "upload", "total",
                     "ops_c2e_up", "ops_c2e_down", "ops_m2m_l2l", "ops_m2l_spectra")

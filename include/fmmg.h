@@ -187,6 +187,12 @@ fmmg_status fmmg_kernel_times(const fmmg_handle* h, double* ms, int n);
  * C2E x M2M product) and downward GEMMs (factored pseudo-inverses). */
 fmmg_status fmmg_plan_stats(const fmmg_handle* h, int64_t* stats, int n);
 
+/* on != 0 (the default for device handles): fmmg_setup builds the octree and
+ * bins the targets on the handle's GPU -- the same tree, permutations and
+ * ranges as the host build, which on == 0 selects.  Takes effect at the next
+ * fmmg_setup. */
+fmmg_status fmmg_set_tree_device(fmmg_handle* h, int on);
+
 /* Wall time of the last fmmg_setup, ms (n >= 9): input checks; the plan's
  * phases -- sources into the tree, targets binned, node flags and centres,
  * U/V/W/X lists, work lists, the adjoint's lists; the upload to the device

@@ -1,0 +1,75 @@
+"""The plan built on the GPU (tree_gpu.cu: octree and target binning) against
+the host build (plan.cpp, the restatement of let3d_mpi.cpp:611-726,
+1230-1285, 1470-1538): the same nodes, permutations, ranges, lists and work
+lists, bit for bit, on the workloads' point sets and the edge cases the tree
+has (coincident points that hit max_level, points on box faces, separate
+targets, a single point)."""
+import numpy as np
+import pytest
+
+import fmmg
+import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _plans(src, trg=None, **kw):
+    a = fmmg.FMM3d(111, np_=4, device=0, **kw)
+    b = fmmg.FMM3d(111, np_=4, device=0, **kw)
+    b.set_tree_device(False)
+    a.setup(src, None, trg)
+    b.setup(src, None, trg)
+    return a, b
+
+
+def _same(a, b):
+    ra, psa, pta = a.tree()
+    rb, psb, ptb = b.tree()
+    assert ra.shape == rb.shape
+    assert np.array_equal(ra, rb)
+    assert np.array_equal(psa, psb)
+    assert np.array_equal(pta, ptb)
+    for which in range(4):
+        pa, ia = a.lists(which)
+        pb, ib = b.lists(which)
+        assert np.array_equal(pa, pb) and np.array_equal(ia, ib)
+    for which in range(8):
+        for x, y in zip(a.worklist(which), b.worklist(which)):
+            assert (x is None and y is None) or np.array_equal(x, y)
+
+
+def _edge_sets():
+    rng = np.random.default_rng(11)
+    out = {}
+    out["sphere_clusters_200k"] = (W.sphere_clusters(200000, rng), None, dict(pts_max=64))
+    out["uniform_100k_targets_apart"] = (W.uniform(100000, rng), W.uniform(70000, rng), dict(pts_max=40))
+    pts = rng.random((3000, 3))
+    pts[:500] = 0.25  # coincident points: splits stop at max_level
+    out["coincident_max_level"] = (pts, None, dict(pts_max=30, max_level=9))
+    g = np.linspace(0.0, 1.0, 17)
+    grid = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)  # points on box faces
+    out["grid_on_faces"] = (grid, None, dict(pts_max=8))
+    out["single_point"] = (np.array([[0.3, 0.6, 0.9]]), None, dict(pts_max=1))
+    return out
+
+
+@pytest.mark.parametrize("name", list(_edge_sets().keys()))
+def test_device_tree_equals_host_tree(name):
+    src, trg, kw = _edge_sets()[name]
+    a, b = _plans(src, trg, **kw)
+    _same(a, b)
+
+
+def test_device_tree_at_1m_and_its_setup_time():
+    """The headline point set: bit-identical plan, and the tree + binning
+    phases on the GPU against the host's."""
+    src = W.config2()["src"]
+    a, b = _plans(src, pts_max=64)
+    _same(a, b)
+    ta, tb = a.setup_times(), b.setup_times()
+    for _ in range(2):  # again, warm
+        a.setup(src)
+        b.setup(src)
+        ta, tb = a.setup_times(), b.setup_times()
+    print("tree+targets device %.1f ms, host %.1f ms; setup total device %.1f ms, host %.1f ms" % (
+        ta["tree"] + ta["targets"], tb["tree"] + tb["targets"], ta["total"], tb["total"]))
