@@ -705,6 +705,13 @@ __device__ __forceinline__ void ho_apply(unsigned long long (&acc)[8], const uns
   }
 }
 
+// 32 bytes from global memory in one 256-bit load (sm_100); p is 32-byte aligned
+__device__ __forceinline__ void ho_ld256(const float* p, float4& a, float4& b) {
+  asm("ld.global.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+      : "l"(p));
+}
+
 template <int R>
 static __global__ void __launch_bounds__(PQX_THREADS, 1)
     k_m2l_had_o(int nRows, const int32_t* __restrict__ rowOut, const int64_t* __restrict__ nPtr,
@@ -748,19 +755,44 @@ static __global__ void __launch_bounds__(PQX_THREADS, 1)
       float2 t[27];
 #pragma unroll
       for (int j = 0; j < 27; j++) t[j] = Tn[j * FB];
+      if constexpr (R == 4) {
+        // the lane's 4 right-hand sides of a child are 32 contiguous bytes:
+        // one 256-bit load each, so a warp's load of a child covers whole
+        // 128-byte lines (two 16-byte loads each read half of 8 lines)
+        float4 lo[8], hi[8];
 #pragma unroll
-      for (int p = 0; p < R / 2; p++) {  // right-hand sides 2p, 2p + 1 of this lane
-        float4 raw[8];
+        for (int c2 = 0; c2 < 8; c2++) {
+          if (act && sl[c2] >= 0) {
+            ho_ld256(reinterpret_cast<const float*>(inF + (int64_t)sl[c2] * inSlot4), lo[c2], hi[c2]);
+          } else {
+            lo[c2] = hi[c2] = make_float4(0.f, 0.f, 0.f, 0.f);
+          }
+        }
 #pragma unroll
-        for (int c2 = 0; c2 < 8; c2++)
-          raw[c2] = (act && sl[c2] >= 0) ? inF[(int64_t)sl[c2] * inSlot4 + p] : make_float4(0.f, 0.f, 0.f, 0.f);
-        unsigned long long x[8];
+        for (int p = 0; p < 2; p++) {
+          unsigned long long x[8];
 #pragma unroll
-        for (int c2 = 0; c2 < 8; c2++) x[c2] = pq_pk(raw[c2].x, raw[c2].y);
-        ho_apply(acc[2 * p], x, t);
+          for (int c2 = 0; c2 < 8; c2++) x[c2] = p ? pq_pk(hi[c2].x, hi[c2].y) : pq_pk(lo[c2].x, lo[c2].y);
+          ho_apply(acc[2 * p], x, t);
 #pragma unroll
-        for (int c2 = 0; c2 < 8; c2++) x[c2] = pq_pk(raw[c2].z, raw[c2].w);
-        ho_apply(acc[2 * p + 1], x, t);
+          for (int c2 = 0; c2 < 8; c2++) x[c2] = p ? pq_pk(hi[c2].z, hi[c2].w) : pq_pk(lo[c2].z, lo[c2].w);
+          ho_apply(acc[2 * p + 1], x, t);
+        }
+      } else {
+#pragma unroll
+        for (int p = 0; p < R / 2; p++) {  // right-hand sides 2p, 2p + 1 of this lane
+          float4 raw[8];
+#pragma unroll
+          for (int c2 = 0; c2 < 8; c2++)
+            raw[c2] = (act && sl[c2] >= 0) ? inF[(int64_t)sl[c2] * inSlot4 + p] : make_float4(0.f, 0.f, 0.f, 0.f);
+          unsigned long long x[8];
+#pragma unroll
+          for (int c2 = 0; c2 < 8; c2++) x[c2] = pq_pk(raw[c2].x, raw[c2].y);
+          ho_apply(acc[2 * p], x, t);
+#pragma unroll
+          for (int c2 = 0; c2 < 8; c2++) x[c2] = pq_pk(raw[c2].z, raw[c2].w);
+          ho_apply(acc[2 * p + 1], x, t);
+        }
       }
     }
     if (!act) continue;

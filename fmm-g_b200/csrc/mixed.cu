@@ -302,21 +302,12 @@ __global__ void __launch_bounds__(MX_THREADS, 6)
                       const double* __restrict__ trg, const double* __restrict__ ctr, double* __restrict__ val,
                       int64_t valStride, int nrhs) {
   constexpr int MX_TILE = mx_tile<KB, false>();
-  // staged sources pre-packed as the FP32x2 operands the loop uses, so no
-  // register moves build them per pair: (hx, hx, hy, hy), (hz, hz, lx, lx),
-  // (ly, ly, lz, lz) and each density twice; the reduction space reuses the
-  // staging space once the sums are done
-  struct Stage {
-    ulonglong2 p[MX_TILE], q[MX_TILE], r[MX_TILE];
-    ulonglong2 d[MX_TILE * (KB + 1) / 2];
-  };
-  constexpr size_t SMEM = sizeof(Stage) > sizeof(double) * MX_THREADS * KB ? sizeof(Stage)
-                                                                           : sizeof(double) * MX_THREADS * KB;
-  __shared__ __align__(16) unsigned char sBuf[SMEM];
-  Stage& S_ = *reinterpret_cast<Stage*>(sBuf);
-  double* sRed = reinterpret_cast<double*>(sBuf);
+  __shared__ float4 sPos[MX_TILE];
+  __shared__ float4 sPosLo[MX_TILE];
+  __shared__ __align__(16) float sDen[MX_TILE * KB];
   __shared__ int64_t eBeg[MX_MAXE];
   __shared__ int32_t ePre[MX_MAXE + 1];
+  __shared__ double sRed[MX_THREADS * KB];
   const int row = blockIdx.x;
   const int rhs0 = blockIdx.y * KB;
   const int g = rows[row];
@@ -363,16 +354,16 @@ __global__ void __launch_bounds__(MX_THREADS, 6)
         for (int i = tid; i < cnt; i += MX_THREADS) {
           const int64_t s = entry_source(base + i, ne, eBeg, ePre);
           const double dx = src[3 * s] - cx, dy = src[3 * s + 1] - cy, dz = src[3 * s + 2] - cz;
-          const float hx = (float)dx, hy = (float)dy, hz = (float)dz;
-          const float lx = (float)(dx - hx), ly = (float)(dy - hy), lz = (float)(dz - hz);
-          S_.p[i] = make_ulonglong2(nl_pk(hx, hx), nl_pk(hy, hy));
-          S_.q[i] = make_ulonglong2(nl_pk(hz, hz), nl_pk(lx, lx));
-          S_.r[i] = make_ulonglong2(nl_pk(ly, ly), nl_pk(lz, lz));
+          sPos[i] = make_float4((float)dx, (float)dy, (float)dz, 0.f);
+          sPosLo[i] = make_float4((float)(dx - (float)dx), (float)(dy - (float)dy), (float)(dz - (float)dz), 0.f);
           const float* ds = den32 + (rhs0 >> 3) * den32Blk + s * 8 + (rhs0 & 7);
+          if constexpr (KB % 4 == 0) {  // 16-byte aligned: rows of 8, rhs0 a multiple of KB
 #pragma unroll
-          for (int r = 0; r < KB; r += 2) {
-            const float d0 = ds[r], d1 = r + 1 < KB ? ds[r + 1] : 0.f;
-            S_.d[i * ((KB + 1) / 2) + r / 2] = make_ulonglong2(nl_pk(d0, d0), nl_pk(d1, d1));
+            for (int r = 0; r < KB; r += 4)
+              *reinterpret_cast<float4*>(&sDen[i * KB + r]) = *reinterpret_cast<const float4*>(ds + r);
+          } else {
+#pragma unroll
+            for (int r = 0; r < KB; r++) sDen[i * KB + r] = ds[r];
           }
         }
         __syncthreads();
@@ -381,21 +372,19 @@ __global__ void __launch_bounds__(MX_THREADS, 6)
 #pragma unroll
           for (int r = 0; r < KB; r++) part[r] = 0ull;
           for (int i = sp; i < cnt; i += S) {
-            const ulonglong2 P = S_.p[i], Q = S_.q[i], Rl = S_.r[i];
+            const float4 q = sPos[i], ql = sPosLo[i];
             // (t_hi - s_hi) + (t_lo - s_lo): exact hi difference for close points
-            const unsigned long long ox = nl_add(nl_sub(txh, P.x), nl_sub(txl, Q.y));
-            const unsigned long long oy = nl_add(nl_sub(tyh, P.y), nl_sub(tyl, Rl.x));
-            const unsigned long long oz = nl_add(nl_sub(tzh, Q.x), nl_sub(tzl, Rl.y));
+            const unsigned long long ox = nl_add(nl_sub(txh, nl_pk(q.x, q.x)), nl_sub(txl, nl_pk(ql.x, ql.x)));
+            const unsigned long long oy = nl_add(nl_sub(tyh, nl_pk(q.y, q.y)), nl_sub(tyl, nl_pk(ql.y, ql.y)));
+            const unsigned long long oz = nl_add(nl_sub(tzh, nl_pk(q.z, q.z)), nl_sub(tzl, nl_pk(ql.z, ql.z)));
             const float2 r2 = nl_unpk(nl_fma(oz, oz, nl_fma(oy, oy, nl_mul(ox, ox))));
             const float ka = r2.x < 1e-16f ? 0.f : c4pi * rsqrtf(r2.x);
             const float kb = r2.y < 1e-16f ? 0.f : c4pi * rsqrtf(r2.y);
             const unsigned long long k2 = nl_pk(ka, kb);
+            float d[KB];
+            mx_den<KB>(&sDen[i * KB], d);
 #pragma unroll
-            for (int r = 0; r < KB; r += 2) {
-              const ulonglong2 D = S_.d[i * ((KB + 1) / 2) + r / 2];
-              part[r] = nl_fma(k2, D.x, part[r]);
-              if (r + 1 < KB) part[r + 1] = nl_fma(k2, D.y, part[r + 1]);
-            }
+            for (int r = 0; r < KB; r++) part[r] = nl_fma(k2, nl_pk(d[r], d[r]), part[r]);
           }
 #pragma unroll
           for (int r = 0; r < KB; r++) {
