@@ -32,6 +32,37 @@ static inline double jacobi_hyp1(double z) {
   return az > 1e100 ? az : std::sqrt(1.0 + z * z);
 }
 
+// The three dot products of a column pair in the order the GPU forms them:
+// 32 partial sums over the rows i = l (mod 32), each in increasing i, then
+// combined pairwise as a butterfly over offsets 16, 8, 4, 2, 1 (every lane of
+// a warp ends with the same value; IEEE addition is commutative).
+static void jacobi_dots32(const double* p, const double* q, int m, double& a, double& b, double& g) {
+  double pa[32], pb[32], pg[32];
+  for (int l = 0; l < 32; l++) pa[l] = pb[l] = pg[l] = 0.0;
+  for (int i = 0; i < m; i++) {
+    const int l = i & 31;
+    pa[l] += p[i] * p[i];
+    pb[l] += q[i] * q[i];
+    pg[l] += p[i] * q[i];
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    double ta[32], tb[32], tg[32];
+    for (int l = 0; l < 32; l++) {
+      ta[l] = pa[l] + pa[l ^ off];
+      tb[l] = pb[l] + pb[l ^ off];
+      tg[l] = pg[l] + pg[l ^ off];
+    }
+    for (int l = 0; l < 32; l++) {
+      pa[l] = ta[l];
+      pb[l] = tb[l];
+      pg[l] = tg[l];
+    }
+  }
+  a = pa[0];
+  b = pb[0];
+  g = pg[0];
+}
+
 // A is m x n column-major with m >= n after an optional transpose.  Columns
 // are orthogonalised pairwise in tournament order (n/2 disjoint pairs per
 // round, so rounds parallelise and the result is thread-count independent).
@@ -73,27 +104,8 @@ static void svd_onesided(int m, int n, std::vector<double>& W /* m x n, becomes 
           zq[h] = &Z[q * ld];
         }
         double a[2] = {0, 0}, b[2] = {0, 0}, g[2] = {0, 0};
-        if (zp[0] && zp[1]) {
-          const double *p0 = zp[0], *q0 = zq[0], *p1 = zp[1], *q1 = zq[1];
-          for (int i = 0; i < m; i++) {
-            a[0] += p0[i] * p0[i];
-            b[0] += q0[i] * q0[i];
-            g[0] += p0[i] * q0[i];
-            a[1] += p1[i] * p1[i];
-            b[1] += q1[i] * q1[i];
-            g[1] += p1[i] * q1[i];
-          }
-        } else {
-          for (int h = 0; h < 2; h++) {
-            if (!zp[h]) continue;
-            const double *ph = zp[h], *qh = zq[h];
-            for (int i = 0; i < m; i++) {
-              a[h] += ph[i] * ph[i];
-              b[h] += qh[i] * qh[i];
-              g[h] += ph[i] * qh[i];
-            }
-          }
-        }
+        for (int h = 0; h < 2; h++)
+          if (zp[h]) jacobi_dots32(zp[h], zq[h], m, a[h], b[h], g[h]);
         for (int h = 0; h < 2; h++) {
           if (!zp[h]) continue;
           if (a[h] == 0.0 || b[h] == 0.0) continue;

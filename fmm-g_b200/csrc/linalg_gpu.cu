@@ -2,10 +2,10 @@
 // (setup only): the one-sided Jacobi SVD behind the truncated pseudo-inverses
 // (common/vecmatop.cpp:129-164, common/svdrep.cpp:38-80) and the C2E x M2M
 // fold.  Both reproduce linalg.cpp's host arithmetic operation for operation
-// -- every dot product summed in index order, products and sums rounded
-// separately (no FMA contraction, as the host build), the same tournament
-// pairing and the same rotation formulas -- so the tables are bit-identical
-// to the host's whichever side builds them.
+// -- every sum in the host's order, products and sums rounded separately (no
+// FMA contraction, as the host build), the same tournament pairing and the
+// same rotation formulas -- so the tables are bit-identical to the host's
+// whichever side builds them.
 #include <cuda_runtime.h>
 
 #include <string>
@@ -28,11 +28,11 @@ __device__ __forceinline__ double lg_hyp1(double z) {
 }
 
 // One tournament round: warp w takes pair w (columns p < q of Z, ld apart,
-// first m rows the working matrix, then the n rows of V).  The warp loads the
-// columns 32 rows at a time (coalesced) and every lane forms the three dot
-// products in index order from the shuffled values -- the same sums in every
-// lane; when the pair is not yet orthogonal all lanes apply the rotation to
-// both full columns.
+// first m rows the working matrix, then the n rows of V).  Lane l sums the
+// rows i = l (mod 32) in increasing i and a butterfly over offsets 16 .. 1
+// combines the 32 partial sums (the host's jacobi_dots32 order; every lane
+// ends with the same value); when the pair is not yet orthogonal all lanes
+// apply the rotation to both full columns.
 __global__ void __launch_bounds__(256) k_jacobi_round(double* __restrict__ Z, long long ld, int m, int n,
                                                       const int2* __restrict__ pairs, int npair,
                                                       int* __restrict__ rotated) {
@@ -44,16 +44,17 @@ __global__ void __launch_bounds__(256) k_jacobi_round(double* __restrict__ Z, lo
   double* zp = Z + (long long)pq.x * ld;
   double* zq = Z + (long long)pq.y * ld;
   double a = 0.0, b = 0.0, g = 0.0;
-  for (int base = 0; base < m; base += 32) {
-    const int i = base + lane;
-    const double xl = i < m ? zp[i] : 0.0, yl = i < m ? zq[i] : 0.0;
-    const int cnt = min(32, m - base);
-    for (int j = 0; j < cnt; j++) {
-      const double x = __shfl_sync(0xffffffffu, xl, j), y = __shfl_sync(0xffffffffu, yl, j);
-      a = __dadd_rn(a, __dmul_rn(x, x));
-      b = __dadd_rn(b, __dmul_rn(y, y));
-      g = __dadd_rn(g, __dmul_rn(x, y));
-    }
+  for (int i = lane; i < m; i += 32) {
+    const double x = zp[i], y = zq[i];
+    a = __dadd_rn(a, __dmul_rn(x, x));
+    b = __dadd_rn(b, __dmul_rn(y, y));
+    g = __dadd_rn(g, __dmul_rn(x, y));
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    a = __dadd_rn(a, __shfl_xor_sync(0xffffffffu, a, off));
+    b = __dadd_rn(b, __shfl_xor_sync(0xffffffffu, b, off));
+    g = __dadd_rn(g, __shfl_xor_sync(0xffffffffu, g, off));
   }
   if (a == 0.0 || b == 0.0 || fabs(g) <= __dmul_rn(1e-15, __dsqrt_rn(__dmul_rn(a, b)))) return;
   const double zeta = __ddiv_rn(__dsub_rn(b, a), __dmul_rn(2.0, g));
