@@ -568,7 +568,12 @@ std::string Plan::build(const Options& opt, int64_t ns_, const double* src, cons
     radius[n] = R0 / double(1 << depth[n]);  // let3d_mpi.cpp:1824-1827
   }
   lap(2);
-  build_lists();
+  if (treeDevice >= 0) {
+    std::string e = lists_build_device(treeDevice, *this);
+    if (!e.empty()) return e;
+  } else {
+    build_lists();
+  }
   lap(3);
   build_worklists();
   lap(4);

@@ -145,8 +145,8 @@ struct Plan {
   const std::vector<double>& folded_upward() const;
   void drop_folded_upward() { upFold.clear(); }
 
-  // treeDevice >= 0: the tree and the target binning on that GPU
-  // (tree_gpu.cu, the same result as the host's)
+  // treeDevice >= 0: the tree, the target binning and the U/V/W/X lists on
+  // that GPU (tree_gpu.cu, lists_gpu.cu; the same result as the host's)
   std::string build(const Options& opt, int64_t ns, const double* src, const double* nrm, int64_t nt,
                     const double* trg, int treeDevice = -1);
   // the operator tables of (kt, coefs, np), copied from the process's most
@@ -183,6 +183,8 @@ void set_linalg_device(int device);
 // Plan::build_tree + bin_targets on a GPU (tree_gpu.cu); trgIsSrc: the
 // targets are the sources
 std::string tree_build_device(int device, Plan& P, const double* src, const double* trg, bool trgIsSrc);
+// Plan::build_lists on a GPU (lists_gpu.cu): the same U/V/W/X lists
+std::string lists_build_device(int device, Plan& P);
 struct LinalgDeviceScope {
   explicit LinalgDeviceScope(int device) { set_linalg_device(device); }
   ~LinalgDeviceScope() { set_linalg_device(-1); }

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "plan.hpp"
+#include "plan_pool.cuh"
 
 namespace fmmg {
 
@@ -246,50 +247,6 @@ __global__ void k_tg_iota(int64_t n, int64_t* __restrict__ perm, int32_t* __rest
   posNode[i] = 0;
 }
 
-namespace {
-// Device buffers of one build.  Released blocks stay with the process, per
-// device, for the next build (a setup per time step for moving points), so
-// repeated setups allocate nothing; the best-fitting free block is taken.
-struct TgBlock {
-  int device;
-  size_t bytes;
-  void* p;
-};
-std::mutex gTgMu;
-std::vector<TgBlock> gTgFree;
-
-struct TgBufs {
-  int device = 0;
-  std::vector<TgBlock> held;
-  template <typename T>
-  cudaError_t get(T*& p, size_t n) {
-    const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
-    {
-      std::lock_guard<std::mutex> g(gTgMu);
-      int best = -1;
-      for (int i = 0; i < (int)gTgFree.size(); i++)
-        if (gTgFree[i].device == device && gTgFree[i].bytes >= bytes &&
-            (best < 0 || gTgFree[i].bytes < gTgFree[best].bytes))
-          best = i;
-      if (best >= 0) {
-        held.push_back(gTgFree[best]);
-        gTgFree.erase(gTgFree.begin() + best);
-        p = (T*)held.back().p;
-        return cudaSuccess;
-      }
-    }
-    void* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, bytes);
-    if (e == cudaSuccess) held.push_back(TgBlock{device, bytes, q});
-    p = (T*)q;
-    return e;
-  }
-  ~TgBufs() {
-    std::lock_guard<std::mutex> g(gTgMu);
-    for (const TgBlock& b : held) gTgFree.push_back(b);
-  }
-};
-}  // namespace
 
 // One level's stable partition of the positions whose node in [lvS, lvE) has
 // children: octant codes and the children's counts, the children's ranges,
@@ -318,7 +275,7 @@ static void tg_level(cudaStream_t st, TgLevelBufs& L, int64_t np, int lvS, int l
   std::swap(L.posNode, L.posNode2);
 }
 
-static std::string tg_level_bufs(TgBufs& B, int64_t np, int maxLevelNodes, TgLevelBufs& L) {
+static std::string tg_level_bufs(PlanBufs& B, int64_t np, int maxLevelNodes, TgLevelBufs& L) {
   const int64_t nchunks = (np + TG_CHUNK - 1) / TG_CHUNK;
   TG_CK(B.get(L.perm, np));
   TG_CK(B.get(L.perm2, np));
@@ -339,7 +296,7 @@ std::string tree_build_device(int device, Plan& P, const double* src, const doub
   TG_CK(cudaSetDevice(device));
   cudaStream_t st = nullptr;
   TG_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-  TgBufs B;  // released after the stream has drained (sg is destroyed first)
+  PlanBufs B;  // released after the stream has drained (sg is destroyed first)
   B.device = device;
   struct StreamGuard {
     cudaStream_t s;

@@ -247,8 +247,9 @@ class FMM3d:
         return dict(src_dof=sd.value, trg_dof=td.value, nodes=nn.value, leaves=nl.value, max_depth=md.value)
 
     def set_tree_device(self, on=True):
-        """Build the octree and bin the targets on the GPU (the default for
-        device handles) or on the host, from the next setup on."""
+        """Build the octree, bin the targets and build the U/V/W/X lists on
+        the GPU (the default for device handles) or on the host, from the next
+        setup on."""
         self._chk(lib().fmmg_set_tree_device(self.h, 1 if on else 0))
 
     SETUP_PHASES = ("checks", "tree", "targets", "flags", "lists", "worklists", "adjoint_lists", "upload", "total",

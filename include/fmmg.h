@@ -187,10 +187,10 @@ fmmg_status fmmg_kernel_times(const fmmg_handle* h, double* ms, int n);
  * C2E x M2M product) and downward GEMMs (factored pseudo-inverses). */
 fmmg_status fmmg_plan_stats(const fmmg_handle* h, int64_t* stats, int n);
 
-/* on != 0 (the default for device handles): fmmg_setup builds the octree and
- * bins the targets on the handle's GPU -- the same tree, permutations and
- * ranges as the host build, which on == 0 selects.  Takes effect at the next
- * fmmg_setup. */
+/* on != 0 (the default for device handles): fmmg_setup builds the octree,
+ * bins the targets and builds the U/V/W/X lists on the handle's GPU -- the
+ * same tree, permutations, ranges and lists as the host build, which on == 0
+ * selects.  Takes effect at the next fmmg_setup. */
 fmmg_status fmmg_set_tree_device(fmmg_handle* h, int on);
 
 /* Wall time of the last fmmg_setup, ms (n >= 9): input checks; the plan's

@@ -1,9 +1,9 @@
-"""The plan built on the GPU (tree_gpu.cu: octree and target binning) against
-the host build (plan.cpp, the restatement of let3d_mpi.cpp:611-726,
-1230-1285, 1470-1538): the same nodes, permutations, ranges, lists and work
-lists, bit for bit, on the workloads' point sets and the edge cases the tree
-has (coincident points that hit max_level, points on box faces, separate
-targets, a single point)."""
+"""The plan built on the GPU (tree_gpu.cu: octree and target binning;
+lists_gpu.cu: U/V/W/X lists) against the host build (plan.cpp, the
+restatement of let3d_mpi.cpp:611-726, 1230-1285, 1470-1538, 1637-1768): the
+same nodes, permutations, ranges, lists and work lists, bit for bit, on the
+workloads' point sets and the edge cases the tree has (coincident points that
+hit max_level, points on box faces, separate targets, a single point)."""
 import numpy as np
 import pytest
 
@@ -71,5 +71,9 @@ def test_device_tree_at_1m_and_its_setup_time():
         a.setup(src)
         b.setup(src)
         ta, tb = a.setup_times(), b.setup_times()
-    print("tree+targets device %.1f ms, host %.1f ms; setup total device %.1f ms, host %.1f ms" % (
-        ta["tree"] + ta["targets"], tb["tree"] + tb["targets"], ta["total"], tb["total"]))
+    print("tree+targets device %.1f ms, host %.1f ms; lists device %.1f ms, host %.1f ms; "
+          "setup total device %.1f ms, host %.1f ms" % (
+              ta["tree"] + ta["targets"], tb["tree"] + tb["targets"], ta["lists"], tb["lists"], ta["total"],
+              tb["total"]))
+    print("phases device", {k: round(v, 1) for k, v in ta.items() if not k.startswith("ops")})
+    print("phases host  ", {k: round(v, 1) for k, v in tb.items() if not k.startswith("ops")})
