@@ -1,7 +1,7 @@
 """Mixed precision (FP32 bulk, FP64 final accumulation): accuracy against the FP64
 dense sum (the reference check()) and against the plain FP64 GPU form.
 
-relative L2 <= 1e-5 against the FP64 dense sum for Laplace
+Accuracy bound: relative L2 <= 1e-5 against the FP64 dense sum for Laplace
 at np = 6.
 """
 import numpy as np

@@ -1,6 +1,6 @@
 """GPU parity: the plain FP64 CUDA evaluate vs the CPU oracle, through the C ABI.
 
-Gate (north star): relative L2 <= 1e-10 on the same tree, operators and inputs.
+Gate: relative L2 <= 1e-10 on the same tree, operators and inputs.
 The oracle is handed the library's operator tables for that gate; with each
 side's own tables the two pseudo-inverses come from different SVD codes and the
 bound is looser (tested separately).  Accuracy against the FP64 dense sum (the
