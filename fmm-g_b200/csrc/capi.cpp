@@ -274,6 +274,7 @@ fmmg_status fmmg_setup_times(const fmmg_handle* h, double* ms, int n) {
   ms[7] = h->setupMs[2];
   ms[8] = h->setupMs[0] + h->setupMs[1] + h->setupMs[2];
   for (int i = 0; i < 4 && 9 + i < n; i++) ms[9 + i] = h->plan.opsMs[i];
+  for (int i = 0; i < 4 && 13 + i < n; i++) ms[13 + i] = h->dev.uploadMs[i];
   return FMMG_OK;
 }
 

@@ -138,6 +138,9 @@ struct DevState {
   bool evReady = false;
   float stageMs[7] = {0, 0, 0, 0, 0, 0, 0};
   float kernMs[EV_COUNT - 1] = {};
+  // wall time of the last dev_upload, ms: geometry and tree arrays, work
+  // lists, operator tables, work arrays and the rest
+  double uploadMs[4] = {0, 0, 0, 0};
   int lastLaunches = 0;  // kernels launched by the last single-RHS evaluate  // interval k = ev[k] .. ev[k+1]
   std::vector<void*> allocs;
 };

@@ -15,6 +15,8 @@
 // stages are plain stream-ordered launches.
 #include <cuda_runtime.h>
 
+#include <chrono>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -643,26 +645,55 @@ static void csr_rows(const CSR& L, const std::vector<int32_t>& rows, std::vector
   }
 }
 
+// out[i] = in[perm[i]] for xyz triples
+__global__ void k_gather3(int64_t n, const int64_t* __restrict__ perm, const double* __restrict__ in,
+                          double* __restrict__ out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t s = perm[i];
+  out[3 * i] = in[3 * s];
+  out[3 * i + 1] = in[3 * s + 1];
+  out[3 * i + 2] = in[3 * s + 2];
+}
+
 std::string dev_upload(const Plan& P, DevState& D, const double* src, const double* nrm, const double* trg) {
+  using Clock = std::chrono::steady_clock;
+  auto t0 = Clock::now();
+  auto lap = [&](int i) {
+    const auto t1 = Clock::now();
+    D.uploadMs[i] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    t0 = t1;
+  };
   FMMG_CK(cudaSetDevice(D.device));
   const int64_t ns = P.ns, nt = P.nt;
-  {  // permuted geometry
-    std::vector<double> a(3 * (size_t)ns);
-    for (int64_t i = 0; i < ns; i++)
-      for (int d = 0; d < 3; d++) a[3 * i + d] = src[3 * P.srcPerm[i] + d];
-    FMMG_TRY(dput(D, D.src, a));
-    if (P.nrm) {
-      for (int64_t i = 0; i < ns; i++)
-        for (int d = 0; d < 3; d++) a[3 * i + d] = nrm[3 * P.srcPerm[i] + d];
-      FMMG_TRY(dput(D, D.nrm, a));
-    }
-    std::vector<double> b(3 * (size_t)nt);
-    for (int64_t i = 0; i < nt; i++)
-      for (int d = 0; d < 3; d++) b[3 * i + d] = trg[3 * P.trgPerm[i] + d];
-    FMMG_TRY(dput(D, D.trg, b));
-  }
   FMMG_TRY(dput(D, D.srcPerm, P.srcPerm));
   FMMG_TRY(dput(D, D.trgPerm, P.trgPerm));
+  {  // permuted geometry: the caller's arrays go up as they are and are
+     // gathered into tree order on the device
+    double* raw = nullptr;
+    FMMG_CK(cudaMalloc(&raw, sizeof(double) * 3 * (size_t)std::max<int64_t>(std::max(ns, nt), 1)));
+    struct RawFree {
+      double* p;
+      ~RawFree() { cudaFree(p); }
+    } rawFree{raw};
+    auto gather = [&](const double* host, int64_t n, const int64_t* dPerm, double*& dst) -> std::string {
+      FMMG_TRY(dput<double>(D, dst, nullptr, 3 * (size_t)n));
+      if (n == 0) return std::string();
+      FMMG_CK(cudaMemcpy(raw, host, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
+      k_gather3<<<(unsigned)((n + 255) / 256), 256>>>(n, dPerm, raw, dst);
+      FMMG_CK(cudaGetLastError());
+      return std::string();
+    };
+    FMMG_TRY(gather(src, ns, D.srcPerm, D.src));
+    if (P.nrm) FMMG_TRY(gather(nrm, ns, D.srcPerm, D.nrm));
+    if (trg == src && nt == ns && P.trgPerm == P.srcPerm) {  // targets are the sources
+      FMMG_TRY(dput<double>(D, D.trg, nullptr, 3 * (size_t)nt));
+      if (nt > 0) FMMG_CK(cudaMemcpy(D.trg, D.src, sizeof(double) * 3 * nt, cudaMemcpyDeviceToDevice));
+    } else {
+      FMMG_TRY(gather(trg, nt, D.trgPerm, D.trg));
+    }
+    FMMG_CK(cudaDeviceSynchronize());
+  }
   FMMG_TRY(dput(D, D.ctr, P.center));
   FMMG_TRY(dput(D, D.rad, P.radius));
   FMMG_TRY(dput(D, D.srcBeg, P.srcBeg));
@@ -682,6 +713,7 @@ std::string dev_upload(const Plan& P, DevState& D, const double* src, const doub
             ijk.push_back(i | (j << 8) | (k << 16));
     FMMG_TRY(dput(D, D.surfIJK, ijk));
   }
+  lap(0);
   // work lists
   FMMG_TRY(dput(D, D.evtrLeaves, P.evtrLeaves));
   FMMG_TRY(dput(D, D.nearPtr, P.nearSrc.ptr));
@@ -740,7 +772,9 @@ std::string dev_upload(const Plan& P, DevState& D, const double* src, const doub
   FMMG_TRY(dput(D, D.vSrcEnt, P.vSrcEnt));
   FMMG_TRY(dput(D, D.vRowOut, P.vRowOut));
   FMMG_TRY(dput(D, D.vNbrIn, P.vNbrIn));
+  lap(1);
   FMMG_TRY(dev_upload_operators(P, D));
+  lap(2);
   // work arrays
   const int64_t ue = (int64_t)P.nUE * P.sdm, uc = (int64_t)P.nUC * P.tdm;
   const int64_t de = (int64_t)P.nDE * P.sdm, dc = (int64_t)P.nDC * P.tdm;
@@ -771,6 +805,7 @@ std::string dev_upload(const Plan& P, DevState& D, const double* src, const doub
     for (cudaEvent_t* e : {&D.evFork, &D.evUp, &D.evSide}) FMMG_CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     D.evReady = true;
   }
+  lap(3);
   return std::string();
 }
 

@@ -253,7 +253,8 @@ class FMM3d:
         self._chk(lib().fmmg_set_tree_device(self.h, 1 if on else 0))
 
     SETUP_PHASES = ("checks", "tree", "targets", "flags", "lists", "worklists", "adjoint_lists", "upload", "total",
-                    "ops_c2e_up", "ops_c2e_down", "ops_m2m_l2l", "ops_m2l_spectra")
+                    "ops_c2e_up", "ops_c2e_down", "ops_m2m_l2l", "ops_m2l_spectra",
+                    "upload_geometry", "upload_lists", "upload_operators", "upload_work")
 
     def setup_times(self):
         """Wall time of the last setup by phase, ms."""

@@ -199,7 +199,8 @@ fmmg_status fmmg_set_tree_device(fmmg_handle* h, int on);
  * (and its work arrays); the total.  With n >= 13 also the build of the
  * handle's operator set at fmmg_create (0 when the process had it cached):
  * C2E up pseudo-inverse, C2E down pseudo-inverse, M2M / L2L tables, M2L
- * translation spectra. */
+ * translation spectra.  With n >= 17 also the upload's parts: geometry and
+ * tree arrays, work lists, operator tables, work arrays and the rest. */
 fmmg_status fmmg_setup_times(const fmmg_handle* h, double* ms, int n);
 
 /* Number of this library's kernels launched by the last evaluate call. */

@@ -77,3 +77,5 @@ def test_device_tree_at_1m_and_its_setup_time():
               tb["total"]))
     print("phases device", {k: round(v, 1) for k, v in ta.items() if not k.startswith("ops")})
     print("phases host  ", {k: round(v, 1) for k, v in tb.items() if not k.startswith("ops")})
+    # the upload's parts lie inside it (the phase also allocates the handle's I/O buffers)
+    assert sum(ta[k] for k in ("upload_geometry", "upload_lists", "upload_operators", "upload_work")) <= ta["upload"] + 1.0
