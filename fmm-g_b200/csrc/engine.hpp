@@ -52,6 +52,7 @@ struct DevState {
   // FP32 M2T work items (rows with long W lists split in chunks of far
   // entries), the split rows, and their partial sums
   int4* m2tItems = nullptr; int nM2tItems = 0;
+  int32_t* nearOrder = nullptr;  // FP32 near-field rows by decreasing pair count
   int32_t *m2tSplitLeaf = nullptr, *m2tSplitBase = nullptr, *m2tSplitCnt = nullptr; int nM2tSplit = 0;
   int64_t m2tPartTargets = 0;  // partial-sum rows per right-hand side
   double* m2tPart = nullptr;

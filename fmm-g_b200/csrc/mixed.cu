@@ -298,12 +298,15 @@ __device__ __forceinline__ unsigned long long nl_fma(unsigned long long a, unsig
 // packed FP32x2 operations (half the instructions of a one-target loop), with
 // the offsets from hi/lo pairs and the coincidence rule (r^2 < 1e-16 adds
 // nothing) of k_p2p_near32; per-chunk FP32 partial sums go into FP64
-// accumulators, which meet through warp shuffles at the end.  Six CTAs an SM
+// accumulators, which meet through warp shuffles at the end.  The leaves come
+// in order[] (rows by decreasing targets x near sources), so the four warps of
+// a CTA carry similar work and the longest leaves start first.  Six CTAs an SM
 // (80 registers) measured faster than four without spills (1.73 vs 2.00 ms).
 constexpr int NW_WARPS = 4, NW_CH = 64, NW_MAXE = 128;
 template <int KB>
 __global__ void __launch_bounds__(32 * NW_WARPS, 6)
-    k_p2p_near32_lap2w(int nLeaves, const int32_t* __restrict__ rows, const int64_t* __restrict__ ptr,
+    k_p2p_near32_lap2w(int nLeaves, const int32_t* __restrict__ order, const int32_t* __restrict__ rows,
+                       const int64_t* __restrict__ ptr,
                        const int32_t* __restrict__ idx, const int64_t* __restrict__ srcBeg,
                        const int64_t* __restrict__ srcCnt, const int64_t* __restrict__ trgBeg,
                        const int64_t* __restrict__ trgCnt, const double* __restrict__ src,
@@ -315,8 +318,8 @@ __global__ void __launch_bounds__(32 * NW_WARPS, 6)
   __shared__ int64_t eBeg[NW_WARPS][NW_MAXE];
   __shared__ int32_t ePre[NW_WARPS][NW_MAXE + 1];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int row = blockIdx.x * NW_WARPS + warp;
-  if (row >= nLeaves) return;
+  if (blockIdx.x * NW_WARPS + warp >= nLeaves) return;
+  const int row = order[blockIdx.x * NW_WARPS + warp];
   const int rhs0 = blockIdx.y * KB;
   const int g = rows[row];
   const int64_t tb = trgBeg[g], tn = trgCnt[g];
@@ -1347,6 +1350,20 @@ static void m2t_items(const Plan& P, int numSMs, std::vector<int4>& items, std::
 static std::string dev_prepare_mixed(const Plan& P, DevState& D, int kc) {
   const size_t ue = (size_t)P.nUE * P.sdm, uc = (size_t)P.nUC * P.tdm;
   const size_t de = (size_t)P.nDE * P.sdm, dc = (size_t)P.nDC * P.tdm;
+  if (!D.nearOrder && !P.evtrLeaves.empty()) {  // near-field rows by decreasing pair count
+    const size_t nl = P.evtrLeaves.size();
+    std::vector<int64_t> cost(nl);
+    for (size_t r = 0; r < nl; r++) {
+      int64_t sc = 0;
+      for (int64_t e = P.nearSrc.ptr[r]; e < P.nearSrc.ptr[r + 1]; e++) sc += P.srcCnt[P.nearSrc.idx[e]];
+      cost[r] = sc * P.trgCnt[P.evtrLeaves[r]];
+    }
+    std::vector<int32_t> order(nl);
+    for (size_t r = 0; r < nl; r++) order[r] = (int32_t)r;
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return cost[a] > cost[b]; });
+    FMMG_TRY(dalloc(D, D.nearOrder, nl));
+    FMMG_CK(cudaMemcpy(D.nearOrder, order.data(), nl * sizeof(int32_t), cudaMemcpyHostToDevice));
+  }
   if (!D.m2tItems && !P.farLeaves.empty()) {
     std::vector<int4> items;
     std::vector<int32_t> sl, sb, sc;
@@ -1566,8 +1583,8 @@ static void run_mixed_blocks(const Plan& P, DevState& D, int kc, int mask, bool 
     if (nl == 0) return;
     if constexpr (KT == LAP_S_U)  // two targets a thread, packed FP32x2, a warp per leaf
       k_p2p_near32_lap2w<KB><<<dim3((nl + NW_WARPS - 1) / NW_WARPS, kb), 32 * NW_WARPS, 0, sn>>>(
-          nl, D.evtrLeaves, ptr, idx, D.srcBeg, D.srcCnt, D.trgBeg, D.trgCnt, D.src, D.den32, den32Blk, D.trg, D.ctr,
-          D.valK, valStride, kc);
+          nl, D.nearOrder, D.evtrLeaves, ptr, idx, D.srcBeg, D.srcCnt, D.trgBeg, D.trgCnt, D.src, D.den32, den32Blk,
+          D.trg, D.ctr, D.valK, valStride, kc);
     else
       k_p2p_near32<KT, KB><<<dim3(nl, kb), MX_THREADS, 0, sn>>>(D.evtrLeaves, ptr, idx, D.srcBeg, D.srcCnt, D.trgBeg,
                                                                D.trgCnt, D.src, D.nrm, D.den32, den32Blk, D.trg, D.ctr,

@@ -603,6 +603,7 @@ void dev_free(DevState& D) {
   D.mixedK = 0;
   D.mixedPassFor = D.mixedPassK = 0;
   D.m2tItems = nullptr;
+  D.nearOrder = nullptr;
   D.nM2tItems = D.nM2tSplit = 0;
   D.m2tSplitLeaf = D.m2tSplitBase = D.m2tSplitCnt = nullptr;
   D.m2tPartTargets = 0;
