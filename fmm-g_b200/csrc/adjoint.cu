@@ -519,6 +519,8 @@ static std::vector<double> transposed(const std::vector<double>& W, int N, int K
 }
 
 static std::string adj_prepare(const Plan& P, DevState& D) {
+  P.build_adjoint_lists();
+  if (!(P.sdm == 1 && P.tdm == 1 && D.hadPQ)) FMMG_TRY(dev_upload_vlists(P, D));  // the list-form M2L^T
   if (!D.adjListsReady) {
     FMMG_TRY(aj_put(D, D.adjNearRows, P.adjNearRows.data(), P.adjNearRows.size()));
     FMMG_TRY(aj_put(D, D.adjNearPtr, P.adjNear.ptr.data(), P.adjNear.ptr.size()));

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -194,19 +195,34 @@ fmmg_status fmmg_setup(fmmg_handle* h, int64_t ns, const double* src, const doub
   if (fmmg::kernel_has_normal(h->opt.kt) && !nrm)
     return fail(h, FMMG_INVALID_ARG, "double-layer kernel needs src_nrm");
   const double R = std::pow(2.0, -h->opt.rootLevel);
+  // branch-free over blocks of points so the compiler vectorises the scan: a
+  // NaN fails both comparisons and an infinity the range, so one test per
+  // coordinate covers "finite and inside the root box"
+  const double lo[3] = {h->opt.ctr[0] - R, h->opt.ctr[1] - R, h->opt.ctr[2] - R};
+  const double hi[3] = {h->opt.ctr[0] + R, h->opt.ctr[1] + R, h->opt.ctr[2] + R};
   auto inside = [&](const double* p, int64_t n) {
-    for (int64_t i = 0; i < n; i++)
-      for (int d = 0; d < 3; d++) {
-        double v = p[3 * i + d];
-        if (!std::isfinite(v) || v < h->opt.ctr[d] - R || v > h->opt.ctr[d] + R) return false;
-      }
+    constexpr int64_t B = 4096;
+    for (int64_t i0 = 0; i0 < n; i0 += B) {
+      const int64_t i1 = std::min(n, i0 + B);
+      int bad = 0;
+      for (int64_t i = i0; i < i1; i++)
+        for (int d = 0; d < 3; d++) {
+          const double v = p[3 * i + d];
+          bad |= !(v >= lo[d] && v <= hi[d]);
+        }
+      if (bad) return false;
+    }
     return true;
   };
+  auto finite = [](const double* p, int64_t n) {
+    int bad = 0;
+    for (int64_t i = 0; i < n; i++) bad |= !(std::fabs(p[i]) <= DBL_MAX);
+    return !bad;
+  };
   if (!inside(src, ns)) return fail(h, FMMG_INVALID_ARG, "a source lies outside the root box or is not finite");
-  if (nt > 0 && !inside(trg, nt)) return fail(h, FMMG_INVALID_ARG, "a target lies outside the root box or is not finite");
-  if (nrm)
-    for (int64_t i = 0; i < 3 * ns; i++)
-      if (!std::isfinite(nrm[i])) return fail(h, FMMG_INVALID_ARG, "a normal is not finite");
+  if (nt > 0 && trg != src && !inside(trg, nt))
+    return fail(h, FMMG_INVALID_ARG, "a target lies outside the root box or is not finite");
+  if (nrm && !finite(nrm, 3 * ns)) return fail(h, FMMG_INVALID_ARG, "a normal is not finite");
   try {
     if (h->setupDone) {
       drop_graph(h);
@@ -286,6 +302,10 @@ static fmmg_status ready(fmmg_handle* h) {
     std::string e = fmmg::dev_upload_operators(h->plan, h->dev);
     if (!e.empty()) return fail(h, FMMG_CUDA_ERROR, e);
     h->opsDirty = false;
+  }
+  if (!h->dev.hadPQ) {  // FMMG_HADAMARD=list: the expanded-list M2L reads them
+    std::string e = fmmg::dev_upload_vlists(h->plan, h->dev);
+    if (!e.empty()) return fail(h, e.find("cudaMalloc") != std::string::npos ? FMMG_OOM : FMMG_CUDA_ERROR, e);
   }
   return FMMG_OK;
 }
@@ -829,6 +849,7 @@ fmmg_status fmmg_worklist(const fmmg_handle* h, int which, int32_t* rows, int64_
   if (!h->setupDone) return FMMG_STATE;
   const fmmg::Plan& P = h->plan;
   if (which >= 6) {  // expanded V lists: (slot, translation id) pairs per slot
+    P.expand_v_lists();
     const std::vector<int32_t>& R = which == 6 ? P.vTrgNodes : P.vSrcNodes;
     const std::vector<int64_t>& Lp = which == 6 ? P.vTrgPtr : P.vSrcPtr;
     const std::vector<int32_t>& Le = which == 6 ? P.vTrgEnt : P.vSrcEnt;

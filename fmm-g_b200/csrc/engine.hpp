@@ -96,6 +96,7 @@ struct DevState {
   int32_t *vParentsT = nullptr, *vNbrTIdx = nullptr; int64_t *vNbrTPtr = nullptr; int8_t *vNbrOffT = nullptr;
   int32_t *vRowOut = nullptr, *vNbrIn = nullptr, *vRowOutT = nullptr, *vNbrInT = nullptr;  // [rows|entries][8]
   bool adjListsReady = false, adjOpsStale = true;
+  bool vListsReady = false;  // the expanded V lists (vTrgPtr .. vSrcEnt) are on the device
   bool hadPQ = true;
   // split-K partial tiles of the FP32 row GEMMs, and the SM count
   double* gemmScratch = nullptr;
@@ -153,6 +154,9 @@ struct LaunchStats {
 
 std::string dev_upload(const Plan& P, DevState& D, const double* src, const double* nrm, const double* trg);
 std::string dev_upload_operators(const Plan& P, DevState& D);
+// the expanded V lists on the device (formed on the host first if need be);
+// a no-op once done.  Call before any capture of a path that reads them
+std::string dev_upload_vlists(const Plan& P, DevState& D);
 void dev_free(DevState& D);
 // run one right-hand side; den/val are device arrays in caller order
 std::string dev_evaluate(const Plan& P, DevState& D, const double* dDenCaller, double* dValCaller,

@@ -13,6 +13,7 @@
 //    values are accumulated in FP64;
 //  * the equivalent-density GEMMs and the spectral M2L (FFTs and Hadamard
 //    products) run in FP32 with FP32 operator tables.
+#include <stdexcept>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -1713,6 +1714,7 @@ static void run_mixed_blocks(const Plan& P, DevState& D, int kc, int mask, bool 
             D.effVal32, PqLayout{blkVal, (int64_t)P.nEff32 * 8}, 8, 1, P.nEff32, kc, nrmfc, D.transIdDev);
       }
     } else if (P.sdm == 1 && P.tdm == 1) {
+      if (!D.vListsReady) throw std::logic_error("the expanded V lists are not on the device (dev_upload_vlists)");
       const size_t smem = had_smem_bytes<float2>();
       cudaFuncSetAttribute(k_m2l_had_list<float2, KB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);

@@ -344,33 +344,48 @@ void Plan::build_worklists() {
   vParents.clear(); vNbr.clear(); vNbrOff.clear();
   vSrcSlot.assign(nn, -1); vTrgSlot.assign(nn, -1);
   vSrcNodes.clear(); vTrgNodes.clear();
+  std::vector<int32_t> nbrQ;  // per node of the level: its 27 same-depth non-leaf neighbours or -1
   for (int d = 1; d < maxDepth; d++) {
-    for (int P = levelBeg[d]; P < levelBeg[d + 1]; P++) {
+    // the neighbour searches are independent: in parallel, then the slots
+    // are numbered in node order below
+    const int l0 = levelBeg[d], l1 = levelBeg[d + 1];
+    nbrQ.assign(27 * (size_t)(l1 - l0), -1);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int P = l0; P < l1; P++) {
       if (leaf(P)) continue;
       bool anyE = false;
       for (int c = 0; c < 8; c++) anyE = anyE || (flags[chd[P] + c] & NF_EVTR);
       if (!anyE) continue;
       const int* pp = &path[3 * (size_t)P];
       const int lim = 1 << d;
+      for (int j = 0; j < 27; j++) {
+        const int dx = j / 9 - 1, dy = (j / 3) % 3 - 1, dz = j % 3 - 1;
+        if (!dx && !dy && !dz) continue;
+        int q[3] = {pp[0] + dx, pp[1] + dy, pp[2] + dz};
+        if (q[0] < 0 || q[1] < 0 || q[2] < 0 || q[0] >= lim || q[1] >= lim || q[2] >= lim) continue;
+        const int Q = find_node(d, q);
+        if (depth[Q] == d && !leaf(Q)) nbrQ[27 * (size_t)(P - l0) + j] = Q;
+      }
+    }
+    for (int P = l0; P < l1; P++) {
+      if (leaf(P)) continue;
+      bool anyE = false;
+      for (int c = 0; c < 8; c++) anyE = anyE || (flags[chd[P] + c] & NF_EVTR);
+      if (!anyE) continue;
       size_t before = vNbr.idx.size();
-      for (int dx = -1; dx <= 1; dx++)
-        for (int dy = -1; dy <= 1; dy++)
-          for (int dz = -1; dz <= 1; dz++) {
-            if (!dx && !dy && !dz) continue;
-            int q[3] = {pp[0] + dx, pp[1] + dy, pp[2] + dz};
-            if (q[0] < 0 || q[1] < 0 || q[2] < 0 || q[0] >= lim || q[1] >= lim || q[2] >= lim) continue;
-            int Q = find_node(d, q);
-            if (depth[Q] != d || leaf(Q)) continue;
-            vNbr.idx.push_back(Q);
-            vNbrOff.push_back((int8_t)((dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)));
-            for (int c = 0; c < 8; c++) {
-              int v = chd[Q] + c;
-              if ((flags[v] & NF_CBTR) && vSrcSlot[v] < 0) {
-                vSrcSlot[v] = (int32_t)vSrcNodes.size();
-                vSrcNodes.push_back(v);
-              }
-            }
+      for (int j = 0; j < 27; j++) {  // offset code (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)
+        const int Q = nbrQ[27 * (size_t)(P - l0) + j];
+        if (Q < 0) continue;
+        vNbr.idx.push_back(Q);
+        vNbrOff.push_back((int8_t)j);
+        for (int c = 0; c < 8; c++) {
+          int v = chd[Q] + c;
+          if ((flags[v] & NF_CBTR) && vSrcSlot[v] < 0) {
+            vSrcSlot[v] = (int32_t)vSrcNodes.size();
+            vSrcNodes.push_back(v);
           }
+        }
+      }
       if (vNbr.idx.size() == before) continue;
       vParents.push_back(P);
       vNbr.ptr.push_back((int64_t)vNbr.idx.size());
@@ -383,10 +398,21 @@ void Plan::build_worklists() {
       }
     }
   }
-  // expanded per-target lists: v = child c2 of Q, c = child of P, idx = v - c.
-  // A target slot is one child c of one row P, so the slots are counted, then
-  // filled, row by row in parallel; each keeps its entries neighbour by
-  // neighbour, child by child.
+  auto slots8 = [&](const std::vector<int32_t>& nodes, const std::vector<int32_t>& slot, std::vector<int32_t>& out) {
+    out.resize(8 * nodes.size());
+    for (size_t i = 0; i < nodes.size(); i++)
+      for (int c = 0; c < 8; c++) out[8 * i + c] = slot[chd[nodes[i]] + c];
+  };
+  slots8(vParents, vTrgSlot, vRowOut);
+  slots8(vNbr.idx, vSrcSlot, vNbrIn);
+}
+
+// Expanded per-target lists: v = child c2 of Q, c = child of P, idx = v - c.
+// A target slot is one child c of one row P, so the slots are counted, then
+// filled, row by row in parallel; each keeps its entries neighbour by
+// neighbour, child by child.
+void Plan::expand_v_lists() const {
+  if (vExpanded) return;
   const size_t nTrgSlots = vTrgNodes.size(), nSrcSlots = vSrcNodes.size();
   auto expand = [&](size_t r, int c, auto&& emit) {
     for (int64_t e = vNbr.ptr[r]; e < vNbr.ptr[r + 1]; e++) {
@@ -461,6 +487,7 @@ void Plan::build_worklists() {
         vSrcEnt[2 * o + 1] = vTrgEnt[2 * i + 1];
       }
   }
+  vExpanded = true;
 }
 
 // Inverse of a CSR (rows -> column ids): for every id that occurs, the rows
@@ -487,7 +514,8 @@ static void invert_csr(const std::vector<int32_t>& rows, const CSR& L, int nn, s
 // The transposed FMM runs every forward stage backwards: its direct sums go
 // from the forward targets to the forward sources, so each forward work list
 // is needed grouped by its other end.
-void Plan::build_adjoint_lists() {
+void Plan::build_adjoint_lists() const {
+  if (adjBuilt) return;
   invert_csr(evtrLeaves, nearSrc, nn, adjNearRows, adjNear);
   invert_csr(farLeaves, farUE, nn, adjFarRows, adjFar);
   invert_csr(s2lNodes, s2lSrc, nn, adjS2lRows, adjS2l);
@@ -516,10 +544,9 @@ void Plan::build_adjoint_lists() {
     for (size_t i = 0; i < nodes.size(); i++)
       for (int c = 0; c < 8; c++) out[8 * i + c] = slot[chd[nodes[i]] + c];
   };
-  slots8(vParents, vTrgSlot, vRowOut);
-  slots8(vNbr.idx, vSrcSlot, vNbrIn);
   slots8(vParentsT, vSrcSlot, vRowOutT);
   slots8(vNbrT.idx, vTrgSlot, vNbrInT);
+  adjBuilt = true;
 }
 
 std::string Plan::build(const Options& opt, int64_t ns_, const double* src, const double* nrmIn, int64_t nt_,
@@ -577,7 +604,9 @@ std::string Plan::build(const Options& opt, int64_t ns_, const double* src, cons
   lap(3);
   build_worklists();
   lap(4);
-  build_adjoint_lists();
+  // the expanded V lists and the adjoint's lists wait for their first use
+  vExpanded = adjBuilt = false;
+  vTrgPtr.clear(); vTrgEnt.clear(); vSrcPtr.clear(); vSrcEnt.clear();
   lap(5);
   (void)nrmIn;
   return std::string();

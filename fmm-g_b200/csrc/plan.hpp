@@ -57,8 +57,8 @@ struct Plan {
   std::vector<double> sam[4];  // UE, UC, DE, DC templates at unit radius scale, [n][3]
 
   // wall time of the phases of the last build(), ms: sources into the tree,
-  // targets binned, node flags and centres, U/V/W/X lists, work lists, the
-  // adjoint's lists
+  // targets binned, node flags and centres, U/V/W/X lists, work lists, and a
+  // last phase that is now empty (the adjoint's lists are formed on first use)
   double buildMs[6] = {0, 0, 0, 0, 0, 0};
   // wall time of the operator set's build, ms (0 when it came from the
   // process cache): C2E up pseudo-inverse, C2E down, M2M / L2L tables, M2L
@@ -105,27 +105,33 @@ struct Plan {
   std::vector<int32_t> vTrgSlot;  // per node: row in the target-spectrum array or -1
   std::vector<int32_t> vTrgNodes; // slot -> node
   // the same V-lists expanded per target slot: (source slot, translation id),
-  // and inverted per source slot for the transposed operator
-  std::vector<int64_t> vTrgPtr;   // [nTrgSlots + 1]
-  std::vector<int32_t> vTrgEnt;   // pairs (source slot, translation id)
-  std::vector<int64_t> vSrcPtr;   // [nSrcSlots + 1]
-  std::vector<int32_t> vSrcEnt;   // pairs (target slot, translation id)
+  // and inverted per source slot for the transposed operator.  Only the
+  // expanded-list Hadamards read them (the vector kernels' transposed M2L and
+  // the list form chosen by FMMG_HADAMARD=list), so they are formed on first
+  // use by expand_v_lists(), not by build()
+  mutable std::vector<int64_t> vTrgPtr;   // [nTrgSlots + 1]
+  mutable std::vector<int32_t> vTrgEnt;   // pairs (source slot, translation id)
+  mutable std::vector<int64_t> vSrcPtr;   // [nSrcSlots + 1]
+  mutable std::vector<int32_t> vSrcEnt;   // pairs (target slot, translation id)
+  void expand_v_lists() const;            // idempotent until the next build()
 
-  // ---- adjoint (transposed FMM) work lists: every forward list inverted
-  std::vector<int32_t> adjNearRows;  // source leaves in some near list
-  CSR adjNear;                       // per row: the evaluator leaves that list it
-  std::vector<int32_t> adjFarRows;   // nodes used through their UE surface (M2T)
-  CSR adjFar;                        // per row: the evaluator leaves that list it
-  std::vector<int32_t> adjS2lRows;   // source leaves used by S2L
-  CSR adjS2l;                        // per row: the nodes whose DC surface they feed
-  std::vector<int32_t> vParentsT;    // source parents Q of the grouped M2L
-  CSR vNbrT;                         // per row: target parents P
-  std::vector<int8_t> vNbrOffT;      // offset code of P - Q
   // the parent-pair lists with child slots resolved: per row its 8 output
   // child slots, per neighbour entry its 8 input child slots (-1: no spectrum)
   std::vector<int32_t> vRowOut, vNbrIn;     // forward: target slots of P, source slots of Q
-  std::vector<int32_t> vRowOutT, vNbrInT;   // transposed: source slots of Q, target slots of P
-  void build_adjoint_lists();
+
+  // ---- adjoint (transposed FMM) work lists: every forward list inverted.
+  // Formed on the first adjoint call by build_adjoint_lists(), not by build()
+  mutable std::vector<int32_t> adjNearRows;  // source leaves in some near list
+  mutable CSR adjNear;                       // per row: the evaluator leaves that list it
+  mutable std::vector<int32_t> adjFarRows;   // nodes used through their UE surface (M2T)
+  mutable CSR adjFar;                        // per row: the evaluator leaves that list it
+  mutable std::vector<int32_t> adjS2lRows;   // source leaves used by S2L
+  mutable CSR adjS2l;                        // per row: the nodes whose DC surface they feed
+  mutable std::vector<int32_t> vParentsT;    // source parents Q of the grouped M2L
+  mutable CSR vNbrT;                         // per row: target parents P
+  mutable std::vector<int8_t> vNbrOffT;      // offset code of P - Q
+  mutable std::vector<int32_t> vRowOutT, vNbrInT;  // transposed: source slots of Q, target slots of P
+  void build_adjoint_lists() const;                // idempotent until the next build()
 
   // ---- operators (homogeneous equivalent kernels: unit-radius tables)
   // row-major for the GPU GEMMs:
@@ -165,6 +171,7 @@ struct Plan {
 
  private:
   mutable std::vector<double> upFold;  // [nUE*sdm][8*nUE*sdm], empty until formed
+  mutable bool vExpanded = false, adjBuilt = false;  // the lazily formed lists are current
   std::string build_operators_uncached();
   template <class S> void assign_operators(S&& s);  // copies or moves, as S is
   void build_tree(const double* src);

@@ -13,6 +13,7 @@
 // Every output row (a leaf's targets, a box's check surface, a node's
 // spectrum) is owned by exactly one CTA, so no atomics are needed and the
 // stages are plain stream-ordered launches.
+#include <stdexcept>
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -597,6 +598,9 @@ void dev_free(DevState& D) {
   D.vNbrOffT = nullptr;
   D.uc2ueT = D.m2mT = D.dc2deT = D.l2lT = D.gradT = nullptr;
   D.adjListsReady = false;
+  D.vListsReady = false;
+  D.vTrgPtr = D.vSrcPtr = nullptr;
+  D.vTrgEnt = D.vSrcEnt = nullptr;
   D.adjOpsStale = true;
   D.mixedReady = false;
   D.mixedOpsStale = true;
@@ -632,6 +636,18 @@ std::string dev_upload_operators(const Plan& P, DevState& D) {
   if (!D.transIdDev) FMMG_TRY(dput(D, D.transIdDev, tid, 343));
   D.mixedOpsStale = true;
   D.adjOpsStale = true;
+  return std::string();
+}
+
+std::string dev_upload_vlists(const Plan& P, DevState& D) {
+  if (D.vListsReady) return std::string();
+  FMMG_CK(cudaSetDevice(D.device));
+  P.expand_v_lists();
+  FMMG_TRY(dput(D, D.vTrgPtr, P.vTrgPtr));
+  FMMG_TRY(dput(D, D.vTrgEnt, P.vTrgEnt));
+  FMMG_TRY(dput(D, D.vSrcPtr, P.vSrcPtr));
+  FMMG_TRY(dput(D, D.vSrcEnt, P.vSrcEnt));
+  D.vListsReady = true;
   return std::string();
 }
 
@@ -767,10 +783,6 @@ std::string dev_upload(const Plan& P, DevState& D, const double* src, const doub
   FMMG_TRY(dput(D, D.vTrgSlot, P.vTrgSlot));
   FMMG_TRY(dput(D, D.vSrcNodes, P.vSrcNodes));
   FMMG_TRY(dput(D, D.vTrgNodes, P.vTrgNodes));
-  FMMG_TRY(dput(D, D.vTrgPtr, P.vTrgPtr));
-  FMMG_TRY(dput(D, D.vTrgEnt, P.vTrgEnt));
-  FMMG_TRY(dput(D, D.vSrcPtr, P.vSrcPtr));
-  FMMG_TRY(dput(D, D.vSrcEnt, P.vSrcEnt));
   FMMG_TRY(dput(D, D.vRowOut, P.vRowOut));
   FMMG_TRY(dput(D, D.vNbrIn, P.vNbrIn));
   lap(1);
@@ -893,6 +905,7 @@ static void launch_m2l_np(const Plan& P, DevState& D, LaunchStats* ls) {
           npar, D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen, 0, D.m2lT, D.effVal, 0, P.nEff, 1, nrmfc,
           D.transIdDev);
     } else if (P.sdm == 1 && P.tdm == 1) {
+      if (!D.vListsReady) throw std::logic_error("the expanded V lists are not on the device (dev_upload_vlists)");
       const size_t smem = had_smem_bytes<double2>();
       cudaFuncSetAttribute(k_m2l_had_list<double2, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);

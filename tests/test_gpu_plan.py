@@ -79,3 +79,52 @@ def test_device_tree_at_1m_and_its_setup_time():
     print("phases host  ", {k: round(v, 1) for k, v in tb.items() if not k.startswith("ops")})
     # the upload's parts lie inside it (the phase also allocates the handle's I/O buffers)
     assert sum(ta[k] for k in ("upload_geometry", "upload_lists", "upload_operators", "upload_work")) <= ta["upload"] + 1.0
+
+
+def test_lists_formed_on_first_use():
+    """The expanded V lists and the adjoint's inverted lists are formed on
+    first use, not by setup: the list-form M2L (FMMG_HADAMARD=list, which
+    reads the expanded lists) agrees with the parent-pair form, forward and
+    transposed, and the expanded lists read through fmmg_worklist are the same
+    whether or not an evaluate formed them first."""
+    import os
+    import torch
+    rng = np.random.default_rng(5)
+    src = W.sphere_clusters(120000, rng)
+    n = src.shape[0]
+    den = torch.from_numpy(rng.normal(size=n)).cuda()
+    w = torch.from_numpy(rng.normal(size=n)).cuda()
+    a = fmmg.FMM3d(111, np_=6, pts_max=64, device=0)
+    a.setup(src)
+    old = os.environ.get("FMMG_HADAMARD")
+    os.environ["FMMG_HADAMARD"] = "list"
+    try:
+        b = fmmg.FMM3d(111, np_=6, pts_max=64, device=0)
+        b.setup(src)
+    finally:
+        if old is None:
+            del os.environ["FMMG_HADAMARD"]
+        else:
+            os.environ["FMMG_HADAMARD"] = old
+    # the two forms add the same products in different orders: the FP64 gate
+    # is the oracle-parity gate
+    for prec, tol in ((fmmg.PREC_FP64, 1e-10), (fmmg.PREC_MIXED, 1e-5)):
+        va = torch.zeros(n, dtype=torch.float64, device="cuda")
+        vb = torch.zeros_like(va)
+        a.evaluate_device(den, va, precision=prec)
+        b.evaluate_device(den, vb, precision=prec)
+        a.sync()
+        b.sync()
+        rel = float((va - vb).norm() / va.norm())
+        assert rel <= tol, (prec, rel)
+    ga = torch.zeros(n, dtype=torch.float64, device="cuda")
+    gb = torch.zeros_like(ga)
+    a.adjoint_device(None, w, ga)
+    b.adjoint_device(None, w, gb)
+    a.sync()
+    b.sync()
+    rel = float((ga - gb).norm() / ga.norm())
+    assert rel <= 1e-10, rel
+    for which in (6, 7):  # a never formed them for an evaluate; b did
+        for x, y in zip(a.worklist(which), b.worklist(which)):
+            assert (x is None and y is None) or np.array_equal(x, y)
