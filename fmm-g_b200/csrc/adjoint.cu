@@ -501,9 +501,8 @@ static std::string aj_put(DevState& D, T*& dst, const T* src, size_t n) {
   }
   if (!dst) {
     void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+    cudaError_t e = dev_alloc(D, &p, n * sizeof(T));
     if (e != cudaSuccess) return std::string("cudaMalloc: ") + cudaGetErrorString(e);
-    D.allocs.push_back(p);
     dst = (T*)p;
   }
   if (src) FMMG_CK(cudaMemcpy(dst, src, n * sizeof(T), cudaMemcpyHostToDevice));

@@ -47,7 +47,7 @@ struct fmmg_handle {
   cudaGraphExec_t graphExec = nullptr;
   int64_t graphLaunches = 0;
   std::string graphNote;
-  std::vector<double> trgHost;  // caller-order targets for check()
+  std::vector<double> trgHost;  // caller-order targets for check(), read back on its first call
   double setupMs[3] = {0, 0, 0};  // last setup: input checks, plan build, device upload (ms)
   bool treeOnDevice = true;       // device handles build the tree and bin the targets on the GPU
   std::string err;
@@ -226,7 +226,9 @@ fmmg_status fmmg_setup(fmmg_handle* h, int64_t ns, const double* src, const doub
   try {
     if (h->setupDone) {
       drop_graph(h);
-      fmmg::dev_free(h->dev);
+      // the blocks of this setup serve the next one (dev_alloc), and what is
+      // left over is freed at its end
+      fmmg::dev_release_for_reuse(h->dev);
       h->dDenIO = h->dValIO = nullptr;
       h->dDenK = h->dValK = nullptr;
       h->dAdjW = h->dAdjG = h->dAdjGrad = h->dAdjDen = nullptr;
@@ -250,7 +252,7 @@ fmmg_status fmmg_setup(fmmg_handle* h, int64_t ns, const double* src, const doub
                                   !h->hostOnly && h->treeOnDevice ? h->device : -1);
     if (!e.empty()) return fail(h, FMMG_INVALID_ARG, e);
     lap(1);
-    h->trgHost.assign(trg ? trg : src, (trg ? trg : src) + 3 * nt);
+    h->trgHost.clear();  // check() reads the targets back from the device when it needs them
     if (!h->hostOnly) {
       e = fmmg::dev_upload(h->plan, h->dev, src, nrm, nt > 0 ? trg : src);
       if (!e.empty()) {
@@ -258,14 +260,13 @@ fmmg_status fmmg_setup(fmmg_handle* h, int64_t ns, const double* src, const doub
         return fail(h, e.find("cudaMalloc") != std::string::npos ? FMMG_OOM : FMMG_CUDA_ERROR, e);
       }
       void* p = nullptr;
-      if (cudaMalloc(&p, sizeof(double) * (size_t)ns * h->plan.sd) != cudaSuccess)
+      if (fmmg::dev_alloc(h->dev, &p, sizeof(double) * (size_t)ns * h->plan.sd) != cudaSuccess)
         return fail(h, FMMG_OOM, "cudaMalloc density buffer");
-      h->dev.allocs.push_back(p);
       h->dDenIO = (double*)p;
-      if (cudaMalloc(&p, sizeof(double) * (size_t)std::max<int64_t>(nt, 1) * h->plan.td) != cudaSuccess)
+      if (fmmg::dev_alloc(h->dev, &p, sizeof(double) * (size_t)std::max<int64_t>(nt, 1) * h->plan.td) != cudaSuccess)
         return fail(h, FMMG_OOM, "cudaMalloc value buffer");
-      h->dev.allocs.push_back(p);
       h->dValIO = (double*)p;
+      fmmg::dev_trim(h->dev);  // the previous setup's blocks that nothing reused
     }
     lap(2);
     h->opsDirty = false;
@@ -597,8 +598,7 @@ fmmg_status fmmg_adjoint_host(fmmg_handle* h, int k, const double* den, const do
     if (k > h->adjK) {
       auto get = [&](double*& p, size_t n) {
         void* q = nullptr;
-        if (cudaMalloc(&q, std::max<size_t>(n, 8)) != cudaSuccess) return false;
-        h->dev.allocs.push_back(q);
+        if (fmmg::dev_alloc(h->dev, &q, std::max<size_t>(n, 8)) != cudaSuccess) return false;
         p = (double*)q;
         return true;
       };
@@ -664,11 +664,10 @@ fmmg_status fmmg_evaluate_host(fmmg_handle* h, int k, const double* den, double*
     const size_t bo = sizeof(double) * (size_t)h->plan.nt * h->plan.td;
     if (k > h->ioK) {
       void* p = nullptr;
-      if (cudaMalloc(&p, bi * k) != cudaSuccess) return fail(h, FMMG_OOM, "cudaMalloc density buffers");
-      h->dev.allocs.push_back(p);
+      if (fmmg::dev_alloc(h->dev, &p, bi * k) != cudaSuccess) return fail(h, FMMG_OOM, "cudaMalloc density buffers");
       h->dDenK = (double*)p;
-      if (cudaMalloc(&p, std::max<size_t>(bo, 8) * k) != cudaSuccess) return fail(h, FMMG_OOM, "cudaMalloc values");
-      h->dev.allocs.push_back(p);
+      if (fmmg::dev_alloc(h->dev, &p, std::max<size_t>(bo, 8) * k) != cudaSuccess)
+        return fail(h, FMMG_OOM, "cudaMalloc values");
       h->dValK = (double*)p;
       h->ioK = k;
     }
@@ -695,6 +694,16 @@ fmmg_status fmmg_check(fmmg_handle* h, const double* den, const double* val, int
   if (!den || !val || !idx || nchk < 1) return fail(h, FMMG_INVALID_ARG, "bad check arguments");
   try {
     const int td = h->plan.td;
+    const int64_t nt = h->plan.nt;
+    if ((int64_t)h->trgHost.size() != 3 * nt) {  // the caller-order targets, once per setup
+      std::vector<double> tree(3 * (size_t)nt);
+      cudaError_t ce = cudaMemcpy(tree.data(), h->dev.trg, sizeof(double) * 3 * nt, cudaMemcpyDeviceToHost);
+      if (ce != cudaSuccess) return fail(h, FMMG_CUDA_ERROR, cudaGetErrorString(ce));
+      h->trgHost.resize(3 * (size_t)nt);
+      const std::vector<int64_t>& perm = h->plan.trgPerm;
+      for (int64_t q = 0; q < nt; q++)
+        for (int d = 0; d < 3; d++) h->trgHost[3 * perm[q] + d] = tree[3 * q + d];
+    }
     std::vector<double> pos(3 * (size_t)nchk), dense((size_t)nchk * td);
     for (int64_t i = 0; i < nchk; i++) {
       if (idx[i] < 0 || idx[i] >= h->plan.nt) return fail(h, FMMG_INVALID_ARG, "check index out of range");

@@ -144,7 +144,15 @@ struct DevState {
   // lists, operator tables, work arrays and the rest
   double uploadMs[4] = {0, 0, 0, 0};
   int lastLaunches = 0;  // kernels launched by the last single-RHS evaluate  // interval k = ev[k] .. ev[k+1]
+  // every device block of the handle (sizes in allocBytes); after a re-setup
+  // the previous setup's blocks wait in spare for dev_alloc to reuse them
   std::vector<void*> allocs;
+  std::vector<size_t> allocBytes;
+  struct Block {
+    void* p;
+    size_t bytes;
+  };
+  std::vector<Block> spare;
 };
 
 // counts of the last stage launch list (for reporting)
@@ -157,7 +165,15 @@ std::string dev_upload_operators(const Plan& P, DevState& D);
 // the expanded V lists on the device (formed on the host first if need be);
 // a no-op once done.  Call before any capture of a path that reads them
 std::string dev_upload_vlists(const Plan& P, DevState& D);
+// a device block owned by D: a spare block of the previous setup when one
+// fits (bytes .. 1.5 bytes), else cudaMalloc
+cudaError_t dev_alloc(DevState& D, void** p, size_t bytes);
 void dev_free(DevState& D);
+// re-setup: after the handle's streams drain, every block moves to D.spare
+// for the next setup's dev_alloc calls and the pointers are cleared as by
+// dev_free; dev_trim then frees the blocks nothing reused
+void dev_release_for_reuse(DevState& D);
+void dev_trim(DevState& D);
 // run one right-hand side; den/val are device arrays in caller order
 std::string dev_evaluate(const Plan& P, DevState& D, const double* dDenCaller, double* dValCaller,
                          int precision, int stageMask, bool timed, LaunchStats* st);

@@ -203,6 +203,13 @@ __global__ void k_ls_compact(int nn, const int64_t* __restrict__ rawOff, const i
   for (int64_t x = threadIdx.x; x < e - d; x += blockDim.x) idx[d + x] = rawIdx[s + x];
 }
 
+// NF_USER: every node that some list names (one byte per node; several
+// threads may store the same 1)
+__global__ void k_ls_user(int64_t n, const int32_t* __restrict__ idx, uint8_t* __restrict__ user) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    user[idx[i]] = 1;
+}
+
 // Plan::build_lists on a GPU: P's tree and flags in, P.U/V/W/X out.
 std::string lists_build_device(int device, Plan& P) {
   const int nn = P.nn;
@@ -263,17 +270,30 @@ std::string lists_build_device(int device, Plan& P) {
     LS_CK(cudaMemcpyAsync(keep, keepOff.data(), sizeof(int64_t) * keepOff.size(), cudaMemcpyHostToDevice, st));
     k_ls_compact<<<dim3(nn, 4), 32, 0, st>>>(nn, raw, rawIdx, keep, idx);
     LS_CK(cudaGetLastError());
-    std::vector<int32_t> all((size_t)kbase[4]);
-    LS_CK(cudaMemcpyAsync(all.data(), idx, sizeof(int32_t) * all.size(), cudaMemcpyDeviceToHost, st));
-    LS_CK(cudaStreamSynchronize(st));
+    uint8_t* user = nullptr;
+    LS_CK(get(user, nn));
+    LS_CK(cudaMemsetAsync(user, 0, nn, st));
+    if (kbase[4] > 0) k_ls_user<<<1184, 256, 0, st>>>(kbase[4], idx, user);
+    LS_CK(cudaGetLastError());
+    // each list straight into its host CSR, while the host fills the offsets
     CSR* outs[4] = {&P.U, &P.V, &P.W, &P.X};
+    for (int l = 0; l < 4; l++) {
+      CSR& o = *outs[l];
+      o.idx.resize((size_t)(kbase[l + 1] - kbase[l]));
+      if (!o.idx.empty())
+        LS_CK(cudaMemcpyAsync(o.idx.data(), idx + kbase[l], sizeof(int32_t) * o.idx.size(), cudaMemcpyDeviceToHost,
+                              st));
+    }
+    std::vector<uint8_t> userH((size_t)nn);
+    LS_CK(cudaMemcpyAsync(userH.data(), user, nn, cudaMemcpyDeviceToHost, st));
     for (int l = 0; l < 4; l++) {
       CSR& o = *outs[l];
       o.ptr.resize((size_t)nn + 1);
       for (int g = 0; g <= nn; g++) o.ptr[g] = keepOff[(size_t)l * (nn + 1) + g] - kbase[l];
-      o.idx.assign(all.begin() + kbase[l], all.begin() + kbase[l + 1]);
-      for (int32_t s2 : o.idx) P.flags[s2] |= NF_USER;
     }
+    LS_CK(cudaStreamSynchronize(st));
+    for (int g = 0; g < nn; g++)
+      if (userH[g]) P.flags[g] |= NF_USER;
     return std::string();
   };
   std::string err = run();

@@ -1269,9 +1269,8 @@ __global__ void __launch_bounds__(256)
 template <typename T>
 static std::string dalloc(DevState& D, T*& p, size_t n) {
   void* q = nullptr;
-  cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
+  cudaError_t e = dev_alloc(D, &q, std::max<size_t>(n, 1) * sizeof(T));
   if (e != cudaSuccess) return std::string("cudaMalloc: ") + cudaGetErrorString(e);
-  D.allocs.push_back(q);
   p = (T*)q;
   return std::string();
 }

@@ -1,5 +1,5 @@
 // plan_pool.cuh -- device work buffers of the GPU plan build (tree_gpu.cu,
-// lists_gpu.cu).  Released blocks stay with the process, per device, for the
+// lists_gpu.cu) and of the coordinate staging of the upload.  Released blocks stay with the process, per device, for the
 // next build (a setup per time step for moving points), so repeated setups
 // allocate nothing; the best-fitting free block is taken.  The blocks are
 // freed at process exit.

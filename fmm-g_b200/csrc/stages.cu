@@ -28,6 +28,7 @@
 
 #include "cuda_common.cuh"
 #include "engine.hpp"
+#include "plan_pool.cuh"
 #include "dense_kernel.cuh"
 #include "gemm_rows.cuh"
 #include "had_pq.cuh"
@@ -544,9 +545,8 @@ static std::string dput(DevState& D, T*& dst, const T* src, size_t n) {
   dst = nullptr;
   if (n == 0) return std::string();
   void* p = nullptr;
-  cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+  cudaError_t e = dev_alloc(D, &p, n * sizeof(T));
   if (e != cudaSuccess) return std::string("cudaMalloc: ") + cudaGetErrorString(e);
-  D.allocs.push_back(p);
   dst = (T*)p;
   if (src) {
     e = cudaMemcpy(p, src, n * sizeof(T), cudaMemcpyHostToDevice);
@@ -560,9 +560,65 @@ static std::string dput(DevState& D, T*& dst, const std::vector<T>& v) {
 }
 
 
+cudaError_t dev_alloc(DevState& D, void** p, size_t bytes) {
+  bytes = std::max<size_t>(bytes, 1);
+  int best = -1;
+  for (int i = 0; i < (int)D.spare.size(); i++) {
+    const size_t b = D.spare[i].bytes;
+    if (b >= bytes && b <= bytes + bytes / 2 && (best < 0 || b < D.spare[best].bytes)) best = i;
+  }
+  void* q = nullptr;
+  if (best >= 0) {
+    q = D.spare[best].p;
+    bytes = D.spare[best].bytes;
+    D.spare[best] = D.spare.back();
+    D.spare.pop_back();
+  } else {
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e == cudaErrorMemoryAllocation && !D.spare.empty()) {  // the kept blocks give way
+      cudaGetLastError();
+      dev_trim(D);
+      e = cudaMalloc(&q, bytes);
+    }
+    if (e != cudaSuccess) {
+      *p = nullptr;
+      return e;
+    }
+  }
+  D.allocs.push_back(q);
+  D.allocBytes.push_back(bytes);
+  *p = q;
+  return cudaSuccess;
+}
+
+void dev_trim(DevState& D) {
+  for (const DevState::Block& b : D.spare) cudaFree(b.p);
+  D.spare.clear();
+}
+
+static void dev_clear(DevState& D);
+
+void dev_release_for_reuse(DevState& D) {
+  // the blocks may still be read by queued work of the handle
+  if (D.stream) cudaStreamSynchronize(D.stream);
+  if (D.side) cudaStreamSynchronize(D.side);
+  for (size_t i = 0; i < D.allocs.size(); i++) D.spare.push_back(DevState::Block{D.allocs[i], D.allocBytes[i]});
+  D.allocs.clear();
+  D.allocBytes.clear();
+  dev_clear(D);
+}
+
 void dev_free(DevState& D) {
   for (void* p : D.allocs) cudaFree(p);
   D.allocs.clear();
+  D.allocBytes.clear();
+  dev_trim(D);
+  dev_clear(D);
+}
+
+// every pointer and flag of D back to "nothing uploaded" (the memory itself
+// is freed or kept by the callers)
+static void dev_clear(DevState& D) {
   if (D.evReady) {
     for (auto& e : D.ev) cudaEventDestroy(e);
     for (cudaEvent_t e : {D.evFork, D.evUp, D.evSide}) cudaEventDestroy(e);
@@ -683,16 +739,23 @@ std::string dev_upload(const Plan& P, DevState& D, const double* src, const doub
   };
   FMMG_CK(cudaSetDevice(D.device));
   const int64_t ns = P.ns, nt = P.nt;
+  // targets that are the sources share their partition: a device copy
+  const bool trgIsSrc = trg == src && nt == ns && P.trgPerm == P.srcPerm;
   FMMG_TRY(dput(D, D.srcPerm, P.srcPerm));
-  FMMG_TRY(dput(D, D.trgPerm, P.trgPerm));
+  if (trgIsSrc) {
+    FMMG_TRY(dput<int64_t>(D, D.trgPerm, nullptr, (size_t)nt));
+    if (nt > 0) FMMG_CK(cudaMemcpy(D.trgPerm, D.srcPerm, sizeof(int64_t) * nt, cudaMemcpyDeviceToDevice));
+  } else {
+    FMMG_TRY(dput(D, D.trgPerm, P.trgPerm));
+  }
   {  // permuted geometry: the caller's arrays go up as they are and are
-     // gathered into tree order on the device
+     // gathered into tree order on the device, through a staging block of
+     // the plan builder's pool (the tree build's own copy of the sources
+     // left one of this size there)
     double* raw = nullptr;
-    FMMG_CK(cudaMalloc(&raw, sizeof(double) * 3 * (size_t)std::max<int64_t>(std::max(ns, nt), 1)));
-    struct RawFree {
-      double* p;
-      ~RawFree() { cudaFree(p); }
-    } rawFree{raw};
+    PlanBufs stage;
+    stage.device = D.device;
+    FMMG_CK(stage.get(raw, 3 * (size_t)std::max<int64_t>(std::max(ns, nt), 1)));
     auto gather = [&](const double* host, int64_t n, const int64_t* dPerm, double*& dst) -> std::string {
       FMMG_TRY(dput<double>(D, dst, nullptr, 3 * (size_t)n));
       if (n == 0) return std::string();
@@ -703,7 +766,7 @@ std::string dev_upload(const Plan& P, DevState& D, const double* src, const doub
     };
     FMMG_TRY(gather(src, ns, D.srcPerm, D.src));
     if (P.nrm) FMMG_TRY(gather(nrm, ns, D.srcPerm, D.nrm));
-    if (trg == src && nt == ns && P.trgPerm == P.srcPerm) {  // targets are the sources
+    if (trgIsSrc) {
       FMMG_TRY(dput<double>(D, D.trg, nullptr, 3 * (size_t)nt));
       if (nt > 0) FMMG_CK(cudaMemcpy(D.trg, D.src, sizeof(double) * 3 * nt, cudaMemcpyDeviceToDevice));
     } else {

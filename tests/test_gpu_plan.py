@@ -128,3 +128,38 @@ def test_lists_formed_on_first_use():
     for which in (6, 7):  # a never formed them for an evaluate; b did
         for x, y in zip(a.worklist(which), b.worklist(which)):
             assert (x is None and y is None) or np.array_equal(x, y)
+
+
+def test_resetup_reuses_device_blocks():
+    """A handle set up again keeps its device blocks for the next setup and
+    frees the ones nothing reused: growing, shrinking and separate-target
+    setups on one handle give what a fresh handle gives, forward, mixed and
+    through check() (whose targets are read back from the device)."""
+    import torch
+    rng = np.random.default_rng(9)
+    cases = [(W.uniform(50000, rng), None), (W.sphere_clusters(90000, rng), None),
+             (W.uniform(30000, rng), W.uniform(20000, rng)), (W.uniform(50000, rng), None)]
+    h = fmmg.FMM3d(111, np_=5, pts_max=48, device=0)
+    for src, trg in cases:
+        h.setup(src, None, trg)
+        g = fmmg.FMM3d(111, np_=5, pts_max=48, device=0)
+        g.setup(src, None, trg)
+        ns, nt = src.shape[0], (src if trg is None else trg).shape[0]
+        den = torch.from_numpy(rng.normal(size=ns)).cuda()
+        for prec, tol in ((fmmg.PREC_FP64, 1e-13), (fmmg.PREC_MIXED, 1e-6)):
+            vh = torch.zeros(nt, dtype=torch.float64, device="cuda")
+            vg = torch.zeros_like(vh)
+            h.evaluate_device(den, vh, precision=prec)
+            g.evaluate_device(den, vg, precision=prec)
+            h.sync()
+            g.sync()
+            assert float((vh - vg).norm() / vg.norm()) <= tol, prec
+        idx = rng.choice(nt, 200, replace=False)
+        dh = den.cpu().numpy()
+        val = h.evaluate(dh).ravel()
+        rh, mh, densh = h.check(dh, val, idx)
+        rg, mg, densg = g.check(dh, val, idx)
+        # the same targets (a wrong read-back moves them: errors of O(1)); the
+        # dense sums add in block order, so they agree to rounding
+        assert np.abs(densh - densg).max() <= 1e-12 * np.abs(densg).max()
+        assert rh < 1e-4 and abs(rh - rg) <= 1e-9 * max(rg, 1e-12) + 1e-15  # np=5 truncation
