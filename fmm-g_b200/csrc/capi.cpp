@@ -50,6 +50,7 @@ struct fmmg_handle {
   std::vector<double> trgHost;  // caller-order targets for check(), read back on its first call
   double setupMs[3] = {0, 0, 0};  // last setup: input checks, plan build, device upload (ms)
   bool treeOnDevice = true;       // device handles build the tree and bin the targets on the GPU
+  int callsSinceSetup = 0;        // device calls since the last setup (ready())
   std::string err;
 };
 
@@ -266,7 +267,10 @@ fmmg_status fmmg_setup(fmmg_handle* h, int64_t ns, const double* src, const doub
       if (fmmg::dev_alloc(h->dev, &p, sizeof(double) * (size_t)std::max<int64_t>(nt, 1) * h->plan.td) != cudaSuccess)
         return fail(h, FMMG_OOM, "cudaMalloc value buffer");
       h->dValIO = (double*)p;
-      fmmg::dev_trim(h->dev);  // the previous setup's blocks that nothing reused
+      // the previous setup's blocks that nothing reused wait for the first
+      // call's lazily allocated work arrays (the mixed pass, the adjoint) and
+      // are freed at the start of the second (ready())
+      h->callsSinceSetup = 0;
     }
     lap(2);
     h->opsDirty = false;
@@ -299,6 +303,7 @@ static fmmg_status ready(fmmg_handle* h) {
   if (!h) return fail(nullptr, FMMG_INVALID_ARG, "handle is NULL");
   if (!h->setupDone) return fail(h, FMMG_STATE, "evaluate before setup");
   if (h->hostOnly) return fail(h, FMMG_STATE, "handle was created host-only (device < 0)");
+  if (++h->callsSinceSetup == 2) fmmg::dev_trim(h->dev);
   if (h->opsDirty) {
     std::string e = fmmg::dev_upload_operators(h->plan, h->dev);
     if (!e.empty()) return fail(h, FMMG_CUDA_ERROR, e);

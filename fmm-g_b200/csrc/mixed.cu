@@ -1907,6 +1907,7 @@ std::string dev_evaluate_mixed(const Plan& P, DevState& D, const double* dDen, d
   } else {
     size_t freeB = 0, totalB = 0;
     FMMG_CK(cudaMemGetInfo(&freeB, &totalB));
+    for (const DevState::Block& b : D.spare) freeB += b.bytes;  // the previous setup's blocks are this handle's
     const double budget = std::min(D.mixedBudgetBytes, 0.7 * (double)freeB);
     int kmax = std::max(D.mixedReady ? D.mixedK : 0, (int)std::floor(budget / std::max(perRhs, 1.0)));
     kmax = std::max(1, std::min(kmax, 32));
