@@ -738,6 +738,10 @@ static __global__ void __launch_bounds__(PQX_THREADS, 1)
   const float4* inF = reinterpret_cast<const float4*>(effIn + (act ? blockIdx.z * inL.blk : 0) + lanePos);
   float2* outF = effOut + blockIdx.z * outL.blk + lanePos;
   const int64_t inSlot4 = inL.slot / 2;  // float4 units (slot strides are multiples of 8 float2)
+  // the warp's parent's neighbour entries (input child slots, offset code),
+  // up to 32 at a time, so each neighbour starts on shared-memory reads
+  __shared__ int4 sIn[PQX_THREADS / 32][32][2];
+  __shared__ int sOff[PQX_THREADS / 32][32];
   const int per = (nRows + gridDim.x - 1) / gridDim.x;
   const int bEnd = min(nRows, (int)(blockIdx.x + 1) * per);
   for (int b = blockIdx.x * per + warp; b < bEnd; b += PQX_THREADS / 32) {
@@ -747,11 +751,20 @@ static __global__ void __launch_bounds__(PQX_THREADS, 1)
 #pragma unroll
       for (int c = 0; c < 8; c++) acc[r][c] = 0ull;
     const int64_t e1 = nPtr[b + 1];
-    for (int64_t e = nPtr[b]; e < e1; e++) {
-      const int4 a0 = reinterpret_cast<const int4*>(nIn)[2 * e];
-      const int4 b0 = reinterpret_cast<const int4*>(nIn)[2 * e + 1];
+    for (int64_t c0 = nPtr[b]; c0 < e1; c0 += 32) {
+    const int ne = (int)min((int64_t)32, e1 - c0);
+    __syncwarp();
+    if (lane < ne) {
+      sIn[warp][lane][0] = reinterpret_cast<const int4*>(nIn)[2 * (c0 + lane)];
+      sIn[warp][lane][1] = reinterpret_cast<const int4*>(nIn)[2 * (c0 + lane) + 1];
+      sOff[warp][lane] = nOff[c0 + lane];
+    }
+    __syncwarp();
+    for (int j = 0; j < ne; j++) {
+      const int4 a0 = sIn[warp][j][0];
+      const int4 b0 = sIn[warp][j][1];
       const int sl[8] = {a0.x, a0.y, a0.z, a0.w, b0.x, b0.y, b0.z, b0.w};
-      const float2* Tn = Ts + (int)nOff[e] * 27 * FB + fl;
+      const float2* Tn = Ts + sOff[warp][j] * 27 * FB + fl;
       float2 t[27];
 #pragma unroll
       for (int j = 0; j < 27; j++) t[j] = Tn[j * FB];
@@ -794,6 +807,7 @@ static __global__ void __launch_bounds__(PQX_THREADS, 1)
           ho_apply(acc[2 * p + 1], x, t);
         }
       }
+    }
     }
     if (!act) continue;
 #pragma unroll
