@@ -882,64 +882,72 @@ __global__ void __launch_bounds__(128)
 }
 
 // grid (target parents, 32-frequency chunks, RHS blocks); warp c owns child c;
-// each translation spectrum value is loaded once and applied to KB densities
+// each translation spectrum value is loaded once and applied to KB densities.
+// The parent's neighbour entries (the 8 input child slots resolved at setup,
+// the offset code) are staged in shared memory once for the CTA, 32 at a
+// time, so each (neighbour, child) pair starts on shared-memory reads instead
+// of a chain of dependent global loads (neighbour -> its children -> slot).
 template <int SDM, int TDM, int KB>
 __global__ void __launch_bounds__(256)
-    k_m2l_had32(const int32_t* __restrict__ parents, const int64_t* __restrict__ vPtr,
-                const int32_t* __restrict__ vIdx, const int8_t* __restrict__ vOff, const int32_t* __restrict__ chd,
-                const int32_t* __restrict__ srcSlot, const int32_t* __restrict__ trgSlot,
+    k_m2l_had32(const int32_t* __restrict__ rowOut, const int64_t* __restrict__ vPtr,
+                const int8_t* __restrict__ vOff, const int32_t* __restrict__ nIn,
                 const float2* __restrict__ effDen, int64_t denRhs, const float2* __restrict__ T,
                 float2* __restrict__ effVal, int64_t valRhs, int nEff, int nrhs, float nrmfc) {
+  __shared__ int sSl[32 * 8];
+  __shared__ int sOf[32];
   const int b = blockIdx.x;
-  const int P = parents[b];
   const int c = threadIdx.x >> 5;
   const int f = blockIdx.y * 32 + (threadIdx.x & 31);
   const int rhs0 = blockIdx.z * KB;
-  const int t = chd[P] + c;
-  const int ts = trgSlot[t];
-  if (ts < 0) return;
+  const int ts = rowOut[8 * b + c];
   const int cx = c >> 2, cy = (c >> 1) & 1, cz = c & 1;
   float2 acc[KB][TDM];
 #pragma unroll
   for (int q = 0; q < KB; q++)
 #pragma unroll
     for (int i = 0; i < TDM; i++) acc[q][i] = make_float2(0.f, 0.f);
-  const bool fin = f < nEff;
-  for (int64_t e = vPtr[b]; e < vPtr[b + 1]; e++) {
-    const int Q = vIdx[e];
-    const int off = vOff[e];
-    const int dx = off / 9 - 1, dy = (off / 3) % 3 - 1, dz = off % 3 - 1;
-    const int q0 = chd[Q];
+  const bool live = ts >= 0 && f < nEff;  // every thread stays for the CTA's barriers
+  const int64_t e1 = vPtr[b + 1];
+  for (int64_t e0 = vPtr[b]; e0 < e1; e0 += 32) {
+    const int ne = (int)min((int64_t)32, e1 - e0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < ne * 8; i += blockDim.x) sSl[i] = nIn[8 * e0 + i];
+    if (threadIdx.x < ne) sOf[threadIdx.x] = vOff[e0 + threadIdx.x];
+    __syncthreads();
+    if (!live) continue;
+    for (int j = 0; j < ne; j++) {
+      const int off = sOf[j];
+      const int dx = off / 9 - 1, dy = (off / 3) % 3 - 1, dz = off % 3 - 1;
 #pragma unroll 1
-    for (int c2 = 0; c2 < 8; c2++) {
-      const int s = srcSlot[q0 + c2];
-      if (s < 0) continue;
-      const int rx = 2 * dx + (c2 >> 2) - cx, ry = 2 * dy + ((c2 >> 1) & 1) - cy, rz = 2 * dz + (c2 & 1) - cz;
-      if (max(abs(rx), max(abs(ry), abs(rz))) <= 1) continue;
-      const int id = c_transId32[(rx + 3) * 49 + (ry + 3) * 7 + (rz + 3)];
-      if (!fin) continue;
-      const float2* Tf = T + ((int64_t)id * nEff + f) * (SDM * TDM);
-      float2 tv[SDM * TDM];
+      for (int c2 = 0; c2 < 8; c2++) {
+        const int s = sSl[j * 8 + c2];
+        if (s < 0) continue;
+        const int rx = 2 * dx + (c2 >> 2) - cx, ry = 2 * dy + ((c2 >> 1) & 1) - cy, rz = 2 * dz + (c2 & 1) - cz;
+        if (max(abs(rx), max(abs(ry), abs(rz))) <= 1) continue;
+        const int id = c_transId32[(rx + 3) * 49 + (ry + 3) * 7 + (rz + 3)];
+        const float2* Tf = T + ((int64_t)id * nEff + f) * (SDM * TDM);
+        float2 tv[SDM * TDM];
 #pragma unroll
-      for (int j = 0; j < SDM * TDM; j++) tv[j] = Tf[j];
+        for (int jj = 0; jj < SDM * TDM; jj++) tv[jj] = Tf[jj];
 #pragma unroll
-      for (int q = 0; q < KB; q++) {
-        if (rhs0 + q >= nrhs) break;
-        const float2* dp = effDen + (rhs0 + q) * denRhs + ((int64_t)s * nEff + f) * SDM;
+        for (int q = 0; q < KB; q++) {
+          if (rhs0 + q >= nrhs) break;
+          const float2* dp = effDen + (rhs0 + q) * denRhs + ((int64_t)s * nEff + f) * SDM;
 #pragma unroll
-        for (int j = 0; j < SDM; j++) {
-          const float2 d = dp[j];
+          for (int jj = 0; jj < SDM; jj++) {
+            const float2 d = dp[jj];
 #pragma unroll
-          for (int i = 0; i < TDM; i++) {
-            const float2 w = tv[j * TDM + i];
-            acc[q][i].x += w.x * d.x - w.y * d.y;
-            acc[q][i].y += w.x * d.y + w.y * d.x;
+            for (int i = 0; i < TDM; i++) {
+              const float2 w = tv[jj * TDM + i];
+              acc[q][i].x += w.x * d.x - w.y * d.y;
+              acc[q][i].y += w.x * d.y + w.y * d.x;
+            }
           }
         }
       }
     }
   }
-  if (fin) {
+  if (live) {
 #pragma unroll
     for (int q = 0; q < KB; q++) {
       if (rhs0 + q >= nrhs) break;
@@ -1661,12 +1669,11 @@ static void run_mixed_blocks(const Plan& P, DevState& D, int kc, int mask, bool 
   do {                                                                                                         \
     if (kc > 4)                                                                                                \
       k_m2l_had32<SD_, TD_, 8><<<dim3(npar, (P.nEff32 + 31) / 32, (kc + 7) / 8), 256, 0, st>>>(                \
-          D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot, D.vTrgSlot, D.effDen32, effDR, D.m2lT32,      \
-          D.effVal32, effVR, P.nEff32, kc, nrmfc);                                                             \
+          D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen32, effDR, D.m2lT32, D.effVal32, effVR, P.nEff32, kc,   \
+          nrmfc);                                                                                              \
     else                                                                                                       \
-      k_m2l_had32<SD_, TD_, KB><<<grid, 256, 0, st>>>(D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot,  \
-                                                       D.vTrgSlot, D.effDen32, effDR, D.m2lT32, D.effVal32,    \
-                                                       effVR, P.nEff32, kc, nrmfc);                            \
+      k_m2l_had32<SD_, TD_, KB><<<grid, 256, 0, st>>>(D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen32, effDR, \
+                                                       D.m2lT32, D.effVal32, effVR, P.nEff32, kc, nrmfc);      \
   } while (0)
     if (P.sdm == 1 && P.tdm == 1 && D.hadPQ) {
       if (!r8) {  // planes of one right-hand side

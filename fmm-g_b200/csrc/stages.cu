@@ -422,50 +422,56 @@ __global__ void __launch_bounds__(128)
 // c; idx = v - c in child widths.
 template <int SDM, int TDM>
 __global__ void __launch_bounds__(256)
-    k_m2l_had(const int32_t* __restrict__ parents, const int64_t* __restrict__ vPtr, const int32_t* __restrict__ vIdx,
-              const int8_t* __restrict__ vOff, const int32_t* __restrict__ chd, const int32_t* __restrict__ srcSlot,
-              const int32_t* __restrict__ trgSlot, const double2* __restrict__ effDen,
-              const double2* __restrict__ T, double2* __restrict__ effVal, int nEff, double nrmfc) {
+    k_m2l_had(const int32_t* __restrict__ rowOut, const int64_t* __restrict__ vPtr, const int8_t* __restrict__ vOff,
+              const int32_t* __restrict__ nIn, const double2* __restrict__ effDen, const double2* __restrict__ T,
+              double2* __restrict__ effVal, int nEff, double nrmfc) {
+  // the parent's neighbour entries (input child slots resolved at setup,
+  // offset code), 32 at a time in shared memory for the CTA
+  __shared__ int sSl[32 * 8];
+  __shared__ int sOf[32];
   const int b = blockIdx.x;
-  const int P = parents[b];
   const int c = threadIdx.x >> 5;
   const int f = blockIdx.y * 32 + (threadIdx.x & 31);
-  const int t = chd[P] + c;
-  const int ts = trgSlot[t];
-  if (ts < 0) return;
+  const int ts = rowOut[8 * b + c];
   const int cx = c >> 2, cy = (c >> 1) & 1, cz = c & 1;
   double2 acc[TDM];
 #pragma unroll
   for (int i = 0; i < TDM; i++) acc[i] = make_double2(0, 0);
-  const bool fin = f < nEff;
-  for (int64_t e = vPtr[b]; e < vPtr[b + 1]; e++) {
-    const int Q = vIdx[e];
-    const int off = vOff[e];
-    const int dx = off / 9 - 1, dy = (off / 3) % 3 - 1, dz = off % 3 - 1;
-    const int q0 = chd[Q];
+  const bool live = ts >= 0 && f < nEff;  // every thread stays for the CTA's barriers
+  const int64_t e1 = vPtr[b + 1];
+  for (int64_t e0 = vPtr[b]; e0 < e1; e0 += 32) {
+    const int ne = (int)min((int64_t)32, e1 - e0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < ne * 8; i += blockDim.x) sSl[i] = nIn[8 * e0 + i];
+    if (threadIdx.x < ne) sOf[threadIdx.x] = vOff[e0 + threadIdx.x];
+    __syncthreads();
+    if (!live) continue;
+    for (int j = 0; j < ne; j++) {
+      const int off = sOf[j];
+      const int dx = off / 9 - 1, dy = (off / 3) % 3 - 1, dz = off % 3 - 1;
 #pragma unroll 1
-    for (int c2 = 0; c2 < 8; c2++) {
-      const int s = srcSlot[q0 + c2];
-      if (s < 0) continue;
-      const int rx = 2 * dx + (c2 >> 2) - cx, ry = 2 * dy + ((c2 >> 1) & 1) - cy, rz = 2 * dz + (c2 & 1) - cz;
-      if (max(abs(rx), max(abs(ry), abs(rz))) <= 1) continue;
-      const int id = c_transId[(rx + 3) * 49 + (ry + 3) * 7 + (rz + 3)];
-      if (!fin) continue;
-      double2 d[SDM];
+      for (int c2 = 0; c2 < 8; c2++) {
+        const int s = sSl[j * 8 + c2];
+        if (s < 0) continue;
+        const int rx = 2 * dx + (c2 >> 2) - cx, ry = 2 * dy + ((c2 >> 1) & 1) - cy, rz = 2 * dz + (c2 & 1) - cz;
+        if (max(abs(rx), max(abs(ry), abs(rz))) <= 1) continue;
+        const int id = c_transId[(rx + 3) * 49 + (ry + 3) * 7 + (rz + 3)];
+        double2 d[SDM];
 #pragma unroll
-      for (int j = 0; j < SDM; j++) d[j] = effDen[((int64_t)s * nEff + f) * SDM + j];
-      const double2* Tf = T + ((int64_t)id * nEff + f) * (SDM * TDM);
+        for (int jj = 0; jj < SDM; jj++) d[jj] = effDen[((int64_t)s * nEff + f) * SDM + jj];
+        const double2* Tf = T + ((int64_t)id * nEff + f) * (SDM * TDM);
 #pragma unroll
-      for (int j = 0; j < SDM; j++)
+        for (int jj = 0; jj < SDM; jj++)
 #pragma unroll
-        for (int i = 0; i < TDM; i++) {
-          double2 tv = Tf[j * TDM + i];
-          acc[i].x += tv.x * d[j].x - tv.y * d[j].y;
-          acc[i].y += tv.x * d[j].y + tv.y * d[j].x;
-        }
+          for (int i = 0; i < TDM; i++) {
+            double2 tv = Tf[jj * TDM + i];
+            acc[i].x += tv.x * d[jj].x - tv.y * d[jj].y;
+            acc[i].y += tv.x * d[jj].y + tv.y * d[jj].x;
+          }
+      }
     }
   }
-  if (fin) {
+  if (live) {
 #pragma unroll
     for (int i = 0; i < TDM; i++)
       effVal[((int64_t)ts * nEff + f) * TDM + i] = make_double2(acc[i].x * nrmfc, acc[i].y * nrmfc);
@@ -977,11 +983,11 @@ static void launch_m2l_np(const Plan& P, DevState& D, LaunchStats* ls) {
           ntrg, D.vTrgPtr, (const int2*)D.vTrgEnt, D.effDen, 0, D.m2lT, D.effVal, 0, P.nEff, 1, nrmfc);
     }
     else if (P.sdm == 4 && P.tdm == 3)
-      k_m2l_had<4, 3><<<grid, 256, 0, D.stream>>>(D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot, D.vTrgSlot,
-                                                  D.effDen, D.m2lT, D.effVal, P.nEff, nrmfc);
+      k_m2l_had<4, 3><<<grid, 256, 0, D.stream>>>(D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen, D.m2lT, D.effVal,
+                                                  P.nEff, nrmfc);
     else
-      k_m2l_had<3, 3><<<grid, 256, 0, D.stream>>>(D.vParents, D.vPtr, D.vIdx, D.vOff, D.chd, D.vSrcSlot, D.vTrgSlot,
-                                                  D.effDen, D.m2lT, D.effVal, P.nEff, nrmfc);
+      k_m2l_had<3, 3><<<grid, 256, 0, D.stream>>>(D.vRowOut, D.vPtr, D.vOff, D.vNbrIn, D.effDen, D.m2lT, D.effVal,
+                                                  P.nEff, nrmfc);
     cudaEventRecord(D.ev[EV_M2L_HAD], D.stream);
     Scale4 none;
     none.mod = 0;
