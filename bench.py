@@ -441,7 +441,7 @@ def run_ours(args):
 # algorithmic bytes of that launch; a full launch's traffic is scaled by the
 # algorithmic bytes (the units processed).  Summaries under profiles/.
 TRAFFIC = {
-    ("m2l_had", "mixed", 8): {"dram_bytes": 861.581568e6 + 570.941696e6, "algorithmic_bytes": 1209899328,
+    ("m2l_had", "mixed", 8): {"dram_bytes": 859.948800e6 + 571.790592e6, "algorithmic_bytes": 1209899328,
                                "profile": "profiles/k_m2l_had_o4_laplace_sphere_clusters_262k_np6_k8.md"},
     ("m2l_had", "fp64", 1): {"dram_bytes": 253.321472e6 + 175.060480e6, "algorithmic_bytes": 424424448,
                               "profile": "profiles/k_m2l_had_pq_fp64_laplace_sphere_clusters_262k_np6.md"},
