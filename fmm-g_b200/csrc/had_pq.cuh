@@ -751,7 +751,7 @@ static __global__ void __launch_bounds__(PQX_THREADS, 1)
 #pragma unroll
       for (int c = 0; c < 8; c++) acc[r][c] = 0ull;
     const int64_t e1 = nPtr[b + 1];
-    for (int64_t c0 = nPtr[b]; c0 < e1; c0 += 32) {
+    for (int64_t c0 = nPtr[b]; c0 < e1; c0 += 32) {  // one pass: a parent has at most 26 neighbours
     const int ne = (int)min((int64_t)32, e1 - c0);
     __syncwarp();
     if (lane < ne) {
@@ -767,7 +767,7 @@ static __global__ void __launch_bounds__(PQX_THREADS, 1)
       const float2* Tn = Ts + sOff[warp][j] * 27 * FB + fl;
       float2 t[27];
 #pragma unroll
-      for (int j = 0; j < 27; j++) t[j] = Tn[j * FB];
+      for (int jj = 0; jj < 27; jj++) t[jj] = Tn[jj * FB];
       if constexpr (R == 4) {
         // the lane's 4 right-hand sides of a child are 32 contiguous bytes:
         // one 256-bit load each, so a warp's load of a child covers whole
