@@ -457,8 +457,11 @@ __global__ void __launch_bounds__(THREADS)
             double* __restrict__ val, int64_t valStride, int nrhs, float mu, float ve, int gmin,
             const int4* __restrict__ items, double* __restrict__ partial, int64_t partStride) {
   constexpr int SD = KTraits<KM>::SD, TD = KTraits<KM>::TD;
-  __shared__ float4 sPos[MX_TILE];
-  __shared__ __align__(16) float sDen[MX_TILE * SD * KB];
+  // scalar kernels: a whole equivalent surface (up to 256 points: np <= 7)
+  // a tile, so each node takes one staging round and two barriers
+  constexpr int TILE = SD * KB <= 8 ? 256 : MX_TILE;
+  __shared__ float4 sPos[TILE];
+  __shared__ __align__(16) float sDen[TILE * SD * KB];
   __shared__ double sRed[THREADS * TD * KB];
   // with work items (M2T): item = (row, first far entry, end far entry,
   // partial-sum base); base >= 0 stores the sums in partial[rhs][base + t]
@@ -499,8 +502,8 @@ __global__ void __launch_bounds__(THREADS)
       const int64_t rstr = isOwn ? rhsStrideD : rhsStrideU;
       const double ox = ctr[3 * node] - gx, oy = ctr[3 * node + 1] - gy, oz = ctr[3 * node + 2] - gz;
       const double r = rad[node];
-      for (int base = 0; base < ns; base += MX_TILE) {
-        const int cnt = min(MX_TILE, ns - base);
+      for (int base = 0; base < ns; base += TILE) {
+        const int cnt = min(TILE, ns - base);
         __syncthreads();
         for (int i = tid; i < cnt; i += THREADS) {
           const int j = base + i;
