@@ -7,6 +7,7 @@
 #pragma once
 
 #include <cmath>
+#include <type_traits>
 
 #if defined(__CUDACC__)
 #define FMMG_HD __host__ __device__ __forceinline__
@@ -179,18 +180,37 @@ FMMG_HD void kaccum_multi(R x, R y, R z, const R* n, const R* den, A* acc, R mu,
   constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD;
   R K[SD * TD];
   if (!kblock<KT, R>(x, y, z, n, K, mu, ve, rnp)) return;
+#if defined(__CUDA_ARCH__)
+  if constexpr (SD == 1 && TD == 1 && KB % 2 == 0 && std::is_same<R, float>::value &&
+                std::is_same<A, float>::value) {
+    // scalar FP32 kernels: two right-hand sides per packed FP32x2 FMA (one
+    // rounding per component, as fmaf(K, den, acc))
+    unsigned long long kk;
+    asm("mov.b64 %0, {%1, %1};" : "=l"(kk) : "f"(K[0]));
 FMMG_UNROLL
-  for (int r = 0; r < KB; r++)
-FMMG_UNROLL
-    for (int t = 0; t < TD; t++) {
-      // the first product starts the sum: an explicit 0 + x cannot be dropped
-      // under IEEE rules and would cost an add per term (with SD = 1 the
-      // product and the accumulate fuse into one FMA)
-      R s = K[t * SD] * den[r * SD];
-FMMG_UNROLL
-      for (int c = 1; c < SD; c++) s += K[t * SD + c] * den[r * SD + c];
-      acc[r * TD + t] += s;
+    for (int r = 0; r < KB; r += 2) {
+      unsigned long long a, d;
+      asm("mov.b64 %0, {%1, %2};" : "=l"(a) : "f"(acc[r]), "f"(acc[r + 1]));
+      asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(den[r]), "f"(den[r + 1]));
+      asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(a) : "l"(kk), "l"(d));
+      asm("mov.b64 {%0, %1}, %2;" : "=f"(acc[r]), "=f"(acc[r + 1]) : "l"(a));
     }
+  } else
+#endif
+  {
+FMMG_UNROLL
+    for (int r = 0; r < KB; r++)
+FMMG_UNROLL
+      for (int t = 0; t < TD; t++) {
+        // the first product starts the sum: an explicit 0 + x cannot be
+        // dropped under IEEE rules and would cost an add per term (with SD = 1
+        // the product and the accumulate fuse into one FMA)
+        R s = K[t * SD] * den[r * SD];
+FMMG_UNROLL
+        for (int c = 1; c < SD; c++) s += K[t * SD + c] * den[r * SD + c];
+        acc[r * TD + t] += s;
+      }
+  }
 }
 
 // Run-time dispatch to a functor templated on the kernel id.
