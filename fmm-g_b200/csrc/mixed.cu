@@ -567,11 +567,28 @@ __global__ void __launch_bounds__(32 * L2T_WARPS)
   const int g = leaves[li];
   const int rhs0 = blockIdx.y * KB;
   const float* dsrc = dden + (int64_t)g * nDE * SD;
-  for (int i = lane; i < nDE * KB; i += 32) {
-    const int j = i % nDE, q = i / nDE;
+  if (SD == 1 && KB == 8 && nDE % 4 == 0 && rhsStride % 4 == 0 && (reinterpret_cast<uintptr_t>(dsrc) & 15) == 0) {
+    // lane = (right-hand side q, run of 4 points v): a warp load reads 64
+    // contiguous bytes of each of the 8 right-hand sides (whole sectors),
+    // and the stores of one point meet 4-way at most in a bank
+    const int q = lane & 7;
+    for (int v = lane >> 3; v < nDE / 4; v += 4) {
+      const float4 x = rhs0 + q < nrhs
+                           ? *reinterpret_cast<const float4*>(dsrc + (int64_t)(rhs0 + q) * rhsStride + 4 * v)
+                           : make_float4(0.f, 0.f, 0.f, 0.f);
+      sDen[(4 * v) * KB + q] = x.x;
+      sDen[(4 * v + 1) * KB + q] = x.y;
+      sDen[(4 * v + 2) * KB + q] = x.z;
+      sDen[(4 * v + 3) * KB + q] = x.w;
+    }
+  } else {
+    for (int i = lane; i < nDE * KB; i += 32) {
+      const int j = i % nDE, q = i / nDE;
 #pragma unroll
-    for (int c = 0; c < SD; c++)
-      sDen[(j * KB + q) * SD + c] = rhs0 + q < nrhs ? dsrc[(int64_t)(rhs0 + q) * rhsStride + (int64_t)j * SD + c] : 0.f;
+      for (int c = 0; c < SD; c++)
+        sDen[(j * KB + q) * SD + c] =
+            rhs0 + q < nrhs ? dsrc[(int64_t)(rhs0 + q) * rhsStride + (int64_t)j * SD + c] : 0.f;
+    }
   }
   __syncwarp();
   const int64_t tb = trgBeg[g], tn = trgCnt[g];
