@@ -170,3 +170,23 @@ def test_expanded_v_lists(kt, np_, pts, kind, n, n_trg):
     assert [tuple(e) for e in sent.tolist()] == inv
     assert sptr.tolist() == np.concatenate([[0], np.cumsum(np.bincount([p[0] for p in pairs],
                                                                         minlength=len(snodes)))]).tolist()
+
+
+def test_lazy_lists_follow_each_setup():
+    """The expanded V lists are formed on first use after each setup: a
+    handle that formed them for one point set and is set up again on another
+    returns the new set's lists, the same as a fresh handle's, and the
+    setup's last phase (the adjoint's lists, formed on first use too) is empty."""
+    rng = np.random.default_rng(41)
+    a_pts, b_pts = _points("clustered", 5000, rng), _points("uniform", 7000, rng)
+    f = fmmg.FMM3d(111, np_=4, pts_max=30, device=-1)
+    f.setup(a_pts)
+    first = [x.copy() for x in f.worklist(6)]
+    f.setup(b_pts)
+    assert f.setup_times()["adjoint_lists"] < 1.0  # ms: only the lazily formed lists are reset
+    g = fmmg.FMM3d(111, np_=4, pts_max=30, device=-1)
+    g.setup(b_pts)
+    for which in (6, 7):
+        for x, y in zip(f.worklist(which), g.worklist(which)):
+            assert np.array_equal(x, y)
+    assert not all(np.array_equal(x, y) for x, y in zip(first, f.worklist(6)))
