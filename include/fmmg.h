@@ -102,7 +102,13 @@ fmmg_status fmmg_create(const fmmg_options* opt, fmmg_handle** out);
  * kernels.  All points must lie in the closed root box; n_src >= 1, n_trg >= 0.
  * May be called again on the same handle with new points (points that moved):
  * the tree, lists and device data are rebuilt and the operator tables reset to
- * the built ones (tables replaced through fmmg_operator are dropped). */
+ * the built ones (tables replaced through fmmg_operator are dropped).  A setup
+ * again first waits for the handle's queued work; the previous setup's device
+ * blocks serve the new one, and those it does not reuse stay with the handle
+ * until the start of its second device call after the setup (so the first
+ * call's own work arrays can reuse them too), or until an allocation needs
+ * the memory.  The V lists expanded per spectrum slot (fmmg_worklist 6 and 7)
+ * and the adjoint's lists are formed when first needed, not by setup. */
 fmmg_status fmmg_setup(fmmg_handle* h, int64_t n_src, const double* src_xyz, const double* src_nrm,
                        int64_t n_trg, const double* trg_xyz);
 
