@@ -3,12 +3,12 @@
 // Stage map (reference fmm3d_mpi/fmm3d_eval_mpi.cpp):
 //   upward  :557-595  S2M (k_src2surf on each leaf's UC surface), then per level
 //                     M2M + C2E as batched row GEMMs (k_gemm_rows)
-//   U-list  :773-785  k_p2p_near   (true kernel, sources of adjacent leaves)
+//   U-list  :773-785  k_p2p_near_w (true kernel, sources of adjacent leaves)
 //   V-list  :1015-1051 k_m2l_fwd (r2c of each upward density on the (2np)^3
 //                     grid), k_m2l_had (per-frequency products grouped by
 //                     parent pairs), k_m2l_inv (c2r + gather onto DC)
-//   W-list  :1139-1175 S2T entries folded into k_p2p_near, M2T in k_e2t
-//   X-list  :1241-1257 S2T entries folded into k_p2p_near, S2L in k_src2surf
+//   W-list  :1139-1175 S2T entries folded into k_p2p_near_w, M2T in k_e2t
+//   X-list  :1241-1257 S2T entries folded into k_p2p_near_w, S2L in k_src2surf
 //   downward:1368-1438 per level L2L + C2E row GEMMs, L2T in k_e2t
 // Every output row (a leaf's targets, a box's check surface, a node's
 // spectrum) is owned by exactly one CTA, so no atomics are needed and the
@@ -58,38 +58,47 @@ __global__ void k_scatter_val(int64_t n, int td, const int64_t* __restrict__ per
 }
 
 // ------------------------------------------------------------------ near field
-// k_p2p_near: for one evaluator leaf, val[targets] += K(trg, src) den(src)
-// over the source leaves of its near list (U-list, direct W and X entries).
-// The source ranges are concatenated into tiles of P2P_TILE in shared memory;
-// when the leaf has few targets the CTA splits the tile between thread groups
-// and reduces the partial sums at the end.
+// The CTA-per-box FP64 kernels below (k_e2t, k_src2surf) stage their sources
+// in tiles of P2P_TILE in shared memory; when a box has few targets the CTA
+// splits the tile between thread groups and reduces the partial sums at the
+// end.  The near field itself, for one evaluator leaf val[targets] +=
+// K(trg, src) den(src) over the source leaves of its near list (U-list,
+// direct W and X entries), is k_p2p_near_w: one warp per leaf.
 constexpr int P2P_THREADS = 128;
 constexpr int P2P_TILE = 128;
 constexpr int P2P_MAXE = 256;
 
-template <int KT>
-__global__ void __launch_bounds__(P2P_THREADS)
-    k_p2p_near(const int32_t* __restrict__ rows, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-               const int64_t* __restrict__ srcBeg, const int64_t* __restrict__ srcCnt,
-               const int64_t* __restrict__ trgBeg, const int64_t* __restrict__ trgCnt,
-               const double* __restrict__ src, const double* __restrict__ nrm, const double* __restrict__ den,
-               const double* __restrict__ trg, double* __restrict__ val, double mu, double ve) {
-  constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD, NRM = KTraits<KT>::NRM;
-  __shared__ double sPos[P2P_TILE * 3];
-  __shared__ double sNrm[NRM ? P2P_TILE * 3 : 1];
-  __shared__ double sDen[P2P_TILE * SD];
-  __shared__ int64_t eBeg[P2P_MAXE];
-  __shared__ int32_t ePre[P2P_MAXE + 1];
-  __shared__ double sRed[P2P_THREADS * TD];
 
-  const int row = blockIdx.x;
+// k_p2p_near_w: the same sums, one warp per evaluator leaf (P2PW_WARPS
+// leaves a CTA) and no CTA-wide barrier: the warp builds its entry table
+// (source ranges and their prefix counts, a shuffle scan per 32 entries),
+// stages P2PW_CH sources at a time in its own slice of shared memory, and
+// splits them over S = 32 / TG lane groups of TG = 8, 16 or 32 targets; the
+// groups' FP64 partial sums meet through warp shuffles.  A leaf with few
+// targets no longer leaves most of a CTA idle behind block barriers.
+constexpr int P2PW_WARPS = 4, P2PW_CH = 64, P2PW_MAXE = 128;
+template <int KT>
+__global__ void __launch_bounds__(32 * P2PW_WARPS)
+    k_p2p_near_w(int nLeaves, const int32_t* __restrict__ rows, const int64_t* __restrict__ ptr,
+                 const int32_t* __restrict__ idx, const int64_t* __restrict__ srcBeg,
+                 const int64_t* __restrict__ srcCnt, const int64_t* __restrict__ trgBeg,
+                 const int64_t* __restrict__ trgCnt, const double* __restrict__ src, const double* __restrict__ nrm,
+                 const double* __restrict__ den, const double* __restrict__ trg, double* __restrict__ val, double mu,
+                 double ve) {
+  constexpr int SD = KTraits<KT>::SD, TD = KTraits<KT>::TD, NRM = KTraits<KT>::NRM;
+  __shared__ double sPos[P2PW_WARPS][P2PW_CH * 3];
+  __shared__ double sNrm[P2PW_WARPS][NRM ? P2PW_CH * 3 : 1];
+  __shared__ double sDen[P2PW_WARPS][P2PW_CH * SD];
+  __shared__ int64_t eBeg[P2PW_WARPS][P2PW_MAXE];
+  __shared__ int32_t ePre[P2PW_WARPS][P2PW_MAXE + 1];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = blockIdx.x * P2PW_WARPS + warp;
+  if (row >= nLeaves) return;  // no CTA-wide barrier below
   const int g = rows[row];
   const int64_t tb = trgBeg[g], tn = trgCnt[g];
   const int64_t e0 = ptr[row], e1 = ptr[row + 1];
-  const int tid = threadIdx.x;
-  const int TG = tn <= 32 ? 32 : (tn <= 64 ? 64 : 128);
-  const int S = P2P_THREADS / TG;
-  const int tl = tid % TG, sp = tid / TG;
+  const int TG = tn > 16 ? 32 : (tn > 8 ? 16 : 8), S = 32 / TG;
+  const int tl = lane % TG, sp = lane / TG;
   for (int64_t t0 = 0; t0 < tn; t0 += TG) {
     const int64_t t = t0 + tl;
     const bool act = t < tn;
@@ -102,62 +111,66 @@ __global__ void __launch_bounds__(P2P_THREADS)
     double acc[TD];
 #pragma unroll
     for (int c = 0; c < TD; c++) acc[c] = 0.0;
-    for (int64_t ec = e0; ec < e1; ec += P2P_MAXE) {
-      const int ne = (int)min((int64_t)P2P_MAXE, e1 - ec);
-      __syncthreads();
-      for (int e = tid; e < ne; e += P2P_THREADS) {
-        int s = idx[ec + e];
-        eBeg[e] = srcBeg[s];
-        ePre[e + 1] = (int32_t)srcCnt[s];
+    for (int64_t ec = e0; ec < e1; ec += P2PW_MAXE) {
+      const int ne = (int)min((int64_t)P2PW_MAXE, e1 - ec);
+      __syncwarp();
+      int running = 0;
+      for (int eb = 0; eb < ne; eb += 32) {
+        const int e = eb + lane;
+        int c = 0;
+        if (e < ne) {
+          const int s2 = idx[ec + e];
+          eBeg[warp][e] = srcBeg[s2];
+          c = (int)srcCnt[s2];
+        }
+        int incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += v;
+        }
+        if (e < ne) ePre[warp][e + 1] = running + incl;
+        running += __shfl_sync(0xffffffffu, incl, 31);
       }
-      __syncthreads();
-      if (tid == 0) {
-        ePre[0] = 0;
-        for (int e = 0; e < ne; e++) ePre[e + 1] += ePre[e];
-      }
-      __syncthreads();
-      const int total = ePre[ne];
-      for (int base = 0; base < total; base += P2P_TILE) {
-        const int cnt = min(P2P_TILE, total - base);
-        __syncthreads();
-        for (int i = tid; i < cnt; i += P2P_THREADS) {
+      if (lane == 0) ePre[warp][0] = 0;
+      __syncwarp();
+      const int total = running;
+      for (int base = 0; base < total; base += P2PW_CH) {
+        const int cnt = min(P2PW_CH, total - base);
+        __syncwarp();
+        for (int i = lane; i < cnt; i += 32) {
           const int j = base + i;
           int lo = 0, hi = ne;
           while (hi - lo > 1) {
-            int mid = (lo + hi) >> 1;
-            if (ePre[mid] <= j) lo = mid; else hi = mid;
+            const int mid = (lo + hi) >> 1;
+            if (ePre[warp][mid] <= j) lo = mid; else hi = mid;
           }
-          const int64_t s = eBeg[lo] + (j - ePre[lo]);
-          sPos[3 * i] = src[3 * s];
-          sPos[3 * i + 1] = src[3 * s + 1];
-          sPos[3 * i + 2] = src[3 * s + 2];
+          const int64_t s2 = eBeg[warp][lo] + (j - ePre[warp][lo]);
+          sPos[warp][3 * i] = src[3 * s2];
+          sPos[warp][3 * i + 1] = src[3 * s2 + 1];
+          sPos[warp][3 * i + 2] = src[3 * s2 + 2];
           if (NRM) {
-            sNrm[3 * i] = nrm[3 * s];
-            sNrm[3 * i + 1] = nrm[3 * s + 1];
-            sNrm[3 * i + 2] = nrm[3 * s + 2];
+            sNrm[warp][3 * i] = nrm[3 * s2];
+            sNrm[warp][3 * i + 1] = nrm[3 * s2 + 1];
+            sNrm[warp][3 * i + 2] = nrm[3 * s2 + 2];
           }
 #pragma unroll
-          for (int c = 0; c < SD; c++) sDen[SD * i + c] = den[s * SD + c];
+          for (int c = 0; c < SD; c++) sDen[warp][SD * i + c] = den[s2 * SD + c];
         }
-        __syncthreads();
+        __syncwarp();
         if (act) {
           for (int i = sp; i < cnt; i += S)
-            kaccum<KT, double, double>(tx - sPos[3 * i], ty - sPos[3 * i + 1], tz - sPos[3 * i + 2],
-                                       NRM ? &sNrm[3 * i] : nullptr, &sDen[SD * i], acc, mu, ve);
+            kaccum<KT, double, double>(tx - sPos[warp][3 * i], ty - sPos[warp][3 * i + 1], tz - sPos[warp][3 * i + 2],
+                                       NRM ? &sNrm[warp][3 * i] : nullptr, &sDen[warp][SD * i], acc, mu, ve);
         }
       }
     }
-    __syncthreads();
 #pragma unroll
-    for (int c = 0; c < TD; c++) sRed[tid * TD + c] = acc[c];
-    __syncthreads();
-    if (sp == 0 && act) {
+    for (int c = 0; c < TD; c++)
+      for (int o = TG; o < 32; o <<= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+    if (act && sp == 0) {
 #pragma unroll
-      for (int c = 0; c < TD; c++) {
-        double s = 0;
-        for (int k = 0; k < S; k++) s += sRed[(tl + k * TG) * TD + c];
-        val[(tb + t) * TD + c] += s;
-      }
+      for (int c = 0; c < TD; c++) val[(tb + t) * TD + c] += acc[c];
     }
   }
 }
@@ -915,8 +928,9 @@ static void launch_near(const Plan& P, DevState& D, const int64_t* ptr, const in
                         cudaStream_t sn) {
   int n = (int)P.evtrLeaves.size();
   if (n == 0) return;
-  k_p2p_near<KT><<<n, P2P_THREADS, 0, sn>>>(D.evtrLeaves, ptr, idx, D.srcBeg, D.srcCnt, D.trgBeg, D.trgCnt,
-                                                  D.src, D.nrm, D.den, D.trg, D.val, P.o.coefs[0], P.o.coefs[1]);
+  k_p2p_near_w<KT><<<(n + P2PW_WARPS - 1) / P2PW_WARPS, 32 * P2PW_WARPS, 0, sn>>>(
+      n, D.evtrLeaves, ptr, idx, D.srcBeg, D.srcCnt, D.trgBeg, D.trgCnt, D.src, D.nrm, D.den, D.trg, D.val,
+      P.o.coefs[0], P.o.coefs[1]);
   if (ls) ls->launches++;
 }
 
