@@ -294,32 +294,64 @@ void Plan::build_worklists() {
   const int64_t ueSize = (int64_t)nUE * sdm, dcSize = (int64_t)nDC * tdm;
   evtrLeaves.clear(); nearSrc.clear(); farUE.clear(); farLeaves.clear(); l2tLeaves.clear();
   s2lNodes.clear(); s2lSrc.clear(); s2mLeaves.clear();
+  // A W node is summed directly (near list) when it is a source leaf with
+  // fewer source values than its UE surface, else through that surface (far
+  // list); a leaf's X list is summed directly when the leaf has fewer target
+  // values than its DC surface, else onto the DC surface (S2L).  Per node the
+  // entry counts are found in parallel, the row lists and offsets follow in
+  // node order, and the entries are written in parallel at those offsets, in
+  // the order U, direct W, direct X (near) and W order (far).
+  auto wDirect = [&](int w) { return (flags[w] & NF_LSRC) && srcCnt[w] * sd < ueSize; };
+  auto xDirect = [&](int g) { return leaf(g) && trgCnt[g] * td < dcSize; };
+  std::vector<int32_t> cNear(nn, 0), cFar(nn, 0);
+#pragma omp parallel for schedule(static, 1024)
+  for (int g = 0; g < nn; g++) {
+    if (!(flags[g] & NF_EVTR) || !leaf(g)) continue;
+    int nd = 0;
+    for (int64_t e = W.ptr[g]; e < W.ptr[g + 1]; e++) nd += wDirect(W.idx[e]) ? 1 : 0;
+    cNear[g] = (int32_t)(U.ptr[g + 1] - U.ptr[g]) + nd + (xDirect(g) ? (int32_t)(X.ptr[g + 1] - X.ptr[g]) : 0);
+    cFar[g] = (int32_t)(W.ptr[g + 1] - W.ptr[g]) - nd;
+  }
+  std::vector<int64_t> oNear(nn, -1), oFar(nn, -1), oS2l(nn, -1);
   for (int g = 0; g < nn; g++) {
     if ((flags[g] & NF_LSRC)) s2mLeaves.push_back(g);
     if (!(flags[g] & NF_EVTR)) continue;
-    bool xDirect = leaf(g) && trgCnt[g] * td < dcSize;
     if (leaf(g)) {
       evtrLeaves.push_back(g);
       if (depth[g] >= 2) l2tLeaves.push_back(g);
-      size_t farBefore = farUE.idx.size();
-      for (int64_t e = U.ptr[g]; e < U.ptr[g + 1]; e++) nearSrc.idx.push_back(U.idx[e]);
-      for (int64_t e = W.ptr[g]; e < W.ptr[g + 1]; e++) {
-        int w = W.idx[e];
-        if ((flags[w] & NF_LSRC) && srcCnt[w] * sd < ueSize) nearSrc.idx.push_back(w);
-        else farUE.idx.push_back(w);
-      }
-      if (xDirect)
-        for (int64_t e = X.ptr[g]; e < X.ptr[g + 1]; e++) nearSrc.idx.push_back(X.idx[e]);
-      nearSrc.ptr.push_back((int64_t)nearSrc.idx.size());
-      if (farUE.idx.size() > farBefore) {
+      oNear[g] = nearSrc.ptr.back();
+      nearSrc.ptr.push_back(oNear[g] + cNear[g]);
+      if (cFar[g] > 0) {
         farLeaves.push_back(g);
-        farUE.ptr.push_back((int64_t)farUE.idx.size());
+        oFar[g] = farUE.ptr.back();
+        farUE.ptr.push_back(oFar[g] + cFar[g]);
       }
     }
-    if (!xDirect && X.ptr[g + 1] > X.ptr[g]) {
+    if (!xDirect(g) && X.ptr[g + 1] > X.ptr[g]) {
       s2lNodes.push_back(g);
-      for (int64_t e = X.ptr[g]; e < X.ptr[g + 1]; e++) s2lSrc.idx.push_back(X.idx[e]);
-      s2lSrc.ptr.push_back((int64_t)s2lSrc.idx.size());
+      oS2l[g] = s2lSrc.ptr.back();
+      s2lSrc.ptr.push_back(oS2l[g] + (X.ptr[g + 1] - X.ptr[g]));
+    }
+  }
+  nearSrc.idx.resize((size_t)nearSrc.ptr.back());
+  farUE.idx.resize((size_t)farUE.ptr.back());
+  s2lSrc.idx.resize((size_t)s2lSrc.ptr.back());
+#pragma omp parallel for schedule(static, 1024)
+  for (int g = 0; g < nn; g++) {
+    if (oNear[g] >= 0) {
+      int64_t o = oNear[g], of = oFar[g];
+      for (int64_t e = U.ptr[g]; e < U.ptr[g + 1]; e++) nearSrc.idx[o++] = U.idx[e];
+      for (int64_t e = W.ptr[g]; e < W.ptr[g + 1]; e++) {
+        const int w = W.idx[e];
+        if (wDirect(w)) nearSrc.idx[o++] = w;
+        else farUE.idx[of++] = w;
+      }
+      if (xDirect(g))
+        for (int64_t e = X.ptr[g]; e < X.ptr[g + 1]; e++) nearSrc.idx[o++] = X.idx[e];
+    }
+    if (oS2l[g] >= 0) {
+      int64_t o = oS2l[g];
+      for (int64_t e = X.ptr[g]; e < X.ptr[g + 1]; e++) s2lSrc.idx[o++] = X.idx[e];
     }
   }
   // level lists for the batched equivalent-density GEMMs
@@ -400,6 +432,7 @@ void Plan::build_worklists() {
   }
   auto slots8 = [&](const std::vector<int32_t>& nodes, const std::vector<int32_t>& slot, std::vector<int32_t>& out) {
     out.resize(8 * nodes.size());
+#pragma omp parallel for schedule(static, 4096)
     for (size_t i = 0; i < nodes.size(); i++)
       for (int c = 0; c < 8; c++) out[8 * i + c] = slot[chd[nodes[i]] + c];
   };
