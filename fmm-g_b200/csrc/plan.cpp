@@ -376,21 +376,24 @@ void Plan::build_worklists() {
   vParents.clear(); vNbr.clear(); vNbrOff.clear();
   vSrcSlot.assign(nn, -1); vTrgSlot.assign(nn, -1);
   vSrcNodes.clear(); vTrgNodes.clear();
-  std::vector<int32_t> nbrQ;  // per node of the level: its 27 same-depth non-leaf neighbours or -1
+  // Per level: the 26 same-depth non-leaf neighbours of every non-leaf node
+  // (in parallel; the relation is symmetric), the rows (non-leaf parents with
+  // an evaluator child and a neighbour) numbered in node order with their
+  // target slots, the entries written in parallel, and the source slots in
+  // first-seen order: a source parent Q is first seen in the earliest row
+  // that lists it -- its earliest row neighbour P, at P's offset code for Q --
+  // and its children with sources take the next slots there, child by child.
+  std::vector<int32_t> nbrQ, rowOf, keyQ;
+  std::vector<int64_t> base;
   for (int d = 1; d < maxDepth; d++) {
-    // the neighbour searches are independent: in parallel, then the slots
-    // are numbered in node order below
-    const int l0 = levelBeg[d], l1 = levelBeg[d + 1];
-    nbrQ.assign(27 * (size_t)(l1 - l0), -1);
+    const int l0 = levelBeg[d], l1 = levelBeg[d + 1], nL = l1 - l0;
+    nbrQ.assign(27 * (size_t)nL, -1);
 #pragma omp parallel for schedule(dynamic, 256)
     for (int P = l0; P < l1; P++) {
       if (leaf(P)) continue;
-      bool anyE = false;
-      for (int c = 0; c < 8; c++) anyE = anyE || (flags[chd[P] + c] & NF_EVTR);
-      if (!anyE) continue;
       const int* pp = &path[3 * (size_t)P];
       const int lim = 1 << d;
-      for (int j = 0; j < 27; j++) {
+      for (int j = 0; j < 27; j++) {  // offset code (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)
         const int dx = j / 9 - 1, dy = (j / 3) % 3 - 1, dz = j % 3 - 1;
         if (!dx && !dy && !dz) continue;
         int q[3] = {pp[0] + dx, pp[1] + dy, pp[2] + dz};
@@ -399,33 +402,64 @@ void Plan::build_worklists() {
         if (depth[Q] == d && !leaf(Q)) nbrQ[27 * (size_t)(P - l0) + j] = Q;
       }
     }
+    // rows in node order
+    rowOf.assign(nL, -1);
+    base.assign(nL, 0);
+    const size_t row0 = vParents.size();
     for (int P = l0; P < l1; P++) {
       if (leaf(P)) continue;
       bool anyE = false;
       for (int c = 0; c < 8; c++) anyE = anyE || (flags[chd[P] + c] & NF_EVTR);
       if (!anyE) continue;
-      size_t before = vNbr.idx.size();
-      for (int j = 0; j < 27; j++) {  // offset code (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)
-        const int Q = nbrQ[27 * (size_t)(P - l0) + j];
-        if (Q < 0) continue;
-        vNbr.idx.push_back(Q);
-        vNbrOff.push_back((int8_t)j);
-        for (int c = 0; c < 8; c++) {
-          int v = chd[Q] + c;
-          if ((flags[v] & NF_CBTR) && vSrcSlot[v] < 0) {
-            vSrcSlot[v] = (int32_t)vSrcNodes.size();
-            vSrcNodes.push_back(v);
-          }
-        }
-      }
-      if (vNbr.idx.size() == before) continue;
+      int n = 0;
+      for (int j = 0; j < 27; j++) n += nbrQ[27 * (size_t)(P - l0) + j] >= 0 ? 1 : 0;
+      if (n == 0) continue;
+      rowOf[P - l0] = (int32_t)(vParents.size() - row0);
+      base[P - l0] = (int64_t)vNbr.idx.size();
       vParents.push_back(P);
+      vNbr.idx.resize(vNbr.idx.size() + n);
       vNbr.ptr.push_back((int64_t)vNbr.idx.size());
       for (int c = 0; c < 8; c++) {
-        int t = chd[P] + c;
+        const int t = chd[P] + c;
         if ((flags[t] & NF_EVTR) && vTrgSlot[t] < 0) {
           vTrgSlot[t] = (int32_t)vTrgNodes.size();
           vTrgNodes.push_back(t);
+        }
+      }
+    }
+    const int nRows = (int)(vParents.size() - row0);
+    vNbrOff.resize(vNbr.idx.size());
+    keyQ.assign(27 * (size_t)nRows, -1);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int X = l0; X < l1; X++) {
+      const int32_t* nb = &nbrQ[27 * (size_t)(X - l0)];
+      if (rowOf[X - l0] >= 0) {  // X as a row: its entries
+        int64_t o = base[X - l0];
+        for (int j = 0; j < 27; j++)
+          if (nb[j] >= 0) {
+            vNbr.idx[o] = nb[j];
+            vNbrOff[o++] = (int8_t)j;
+          }
+      }
+      // X as a source parent: its earliest row neighbour P, which lists X at
+      // the opposite offset
+      int best = -1;
+      for (int j = 0; j < 27; j++) {
+        const int P = nb[j];
+        if (P < 0 || rowOf[P - l0] < 0) continue;
+        const int k = rowOf[P - l0] * 27 + (26 - j);
+        if (best < 0 || k < best) best = k;
+      }
+      if (best >= 0) keyQ[best] = X;
+    }
+    for (size_t k = 0; k < keyQ.size(); k++) {
+      const int Q = keyQ[k];
+      if (Q < 0) continue;
+      for (int c = 0; c < 8; c++) {
+        const int v = chd[Q] + c;
+        if ((flags[v] & NF_CBTR) && vSrcSlot[v] < 0) {
+          vSrcSlot[v] = (int32_t)vSrcNodes.size();
+          vSrcNodes.push_back(v);
         }
       }
     }
