@@ -649,6 +649,7 @@ std::string Plan::build(const Options& opt, int64_t ns_, const double* src, cons
   center.resize(3 * (size_t)nn);
   radius.resize(nn);
   const double R0 = std::pow(2.0, -o.rootLevel);
+#pragma omp parallel for schedule(static, 2048)
   for (int n = 0; n < nn; n++) {
     uint8_t f = 0;
     bool lf = chd[n] < 0;
